@@ -1,0 +1,133 @@
+// ref_driver.cpp -- C entry points into the REFERENCE's own CPU NewtonSolver
+// (TEST INFRASTRUCTURE ONLY).
+//
+// Built by oracle/Makefile together with the reference's CPU core sources
+// (cuPF/CMakeLists.txt:243-262 CUPF_CORE_SOURCES, compiled where they lie) and
+// the KLU shim, into oracle/_ref/libcupf_ref.so.  Each function runs the
+// reference's public C++ API (NewtonSolver, cuPF/cpp/inc/newton_solver/core/
+// newton_solver.hpp:26-102) on the CPU backend and copies the results out, so
+// the oracle restatement and the GPU engine can be checked against the
+// reference itself.
+#include <complex>
+#include <cstdint>
+#include <cstring>
+#include <exception>
+#include <string>
+#include <vector>
+
+#include "newton_solver/core/newton_solver.hpp"
+#include "newton_solver/ops/jacobian/jacobian_analysis.hpp"
+
+namespace {
+thread_local std::string g_error;
+
+YbusView make_view(int n, const int32_t* indptr, const int32_t* indices, const double* ydata) {
+  return YbusView{indptr, indices, reinterpret_cast<const std::complex<double>*>(ydata), n, n, indptr[n]};
+}
+}  // namespace
+
+extern "C" {
+
+const char* ref_last_error() { return g_error.c_str(); }
+
+// NewtonSolver::solve_batch on the CPU backend (batch 1 per call; the CPU
+// pipeline rejects batch > 1, newton_solver.cpp:268-276).
+int ref_nr_solve(int n_bus, const int32_t* indptr, const int32_t* indices, const double* ydata,
+                 const double* sbus, const double* v0, const int32_t* pv, int n_pv, const int32_t* pq,
+                 int n_pq, double tol, int max_iter, double* v_out, int32_t* iterations,
+                 double* final_mismatch, int32_t* converged) {
+  try {
+    NewtonOptions opts;
+    opts.backend = BackendKind::CPU;
+    opts.cpu_linear_solver = CpuLinearSolverKind::KLU;
+    NewtonSolver solver(opts);
+    const YbusView y = make_view(n_bus, indptr, indices, ydata);
+    solver.initialize(y, pv, n_pv, pq, n_pq);
+    NRConfig cfg;
+    cfg.tolerance = tol;
+    cfg.max_iter = max_iter;
+    NRResult res;
+    solver.solve(y, reinterpret_cast<const std::complex<double>*>(sbus),
+                 reinterpret_cast<const std::complex<double>*>(v0), pv, n_pv, pq, n_pq, cfg, SolveOptions{}, res);
+    std::memcpy(v_out, res.V.data(), sizeof(double) * 2 * n_bus);
+    *iterations = res.iterations;
+    *final_mismatch = res.final_mismatch;
+    *converged = res.converged ? 1 : 0;
+    return 0;
+  } catch (const std::exception& e) {
+    g_error = e.what();
+    return 1;
+  }
+}
+
+// Forward solve with the adjoint cache, then NewtonSolver::solve_adjoint
+// (newton_solver_adjoint.cpp:33-153).
+int ref_nr_adjoint(int n_bus, const int32_t* indptr, const int32_t* indices, const double* ydata,
+                   const double* sbus, const double* v0, const int32_t* pv, int n_pv, const int32_t* pq,
+                   int n_pq, double tol, int max_iter, const double* grad_va, const double* grad_vm,
+                   double* v_out, double* lambda, double* grad_p, double* grad_q, double* residual) {
+  try {
+    NewtonOptions opts;
+    opts.backend = BackendKind::CPU;
+    NewtonSolver solver(opts);
+    const YbusView y = make_view(n_bus, indptr, indices, ydata);
+    solver.initialize(y, pv, n_pv, pq, n_pq);
+    NRConfig cfg;
+    cfg.tolerance = tol;
+    cfg.max_iter = max_iter;
+    SolveOptions so;
+    so.prepare_adjoint_cache = true;
+    NRResult res;
+    solver.solve(y, reinterpret_cast<const std::complex<double>*>(sbus),
+                 reinterpret_cast<const std::complex<double>*>(v0), pv, n_pv, pq, n_pq, cfg, so, res);
+    std::memcpy(v_out, res.V.data(), sizeof(double) * 2 * n_bus);
+    AdjointOptions ao;
+    AdjointResult ar;
+    solver.solve_adjoint(grad_va, n_bus, grad_vm, n_bus, 1, pv, n_pv, pq, n_pq, ao, ar);
+    std::memcpy(lambda, ar.lambda.data(), sizeof(double) * ar.lambda.size());
+    std::memcpy(grad_p, ar.grad_load_p.data(), sizeof(double) * n_bus);
+    std::memcpy(grad_q, ar.grad_load_q.data(), sizeof(double) * n_bus);
+    *residual = ar.jt_residual_norm;
+    return 0;
+  } catch (const std::exception& e) {
+    g_error = e.what();
+    return 1;
+  }
+}
+
+// make_jacobian_indexing + JacobianPatternGenerator + JacobianMapBuilder
+// (jacobian_analysis.cpp:257-445).  Call with row_ptr == nullptr first to get
+// dim and nnz.
+int ref_jacobian_analysis(int n_bus, const int32_t* indptr, const int32_t* indices, const double* ydata,
+                          const int32_t* pv, int n_pv, const int32_t* pq, int n_pq, int32_t* dim_out,
+                          int32_t* nnz_out, int32_t* row_ptr, int32_t* col_idx, int32_t* maps_out) {
+  try {
+    const YbusView y = make_view(n_bus, indptr, indices, ydata);
+    const JacobianIndexing ix = make_jacobian_indexing(n_bus, pv, n_pv, pq, n_pq);
+    const JacobianPattern pat = JacobianPatternGenerator().generate(y, ix);
+    *dim_out = pat.dim;
+    *nnz_out = pat.nnz;
+    if (!row_ptr) return 0;
+    const JacobianScatterMap m = JacobianMapBuilder().build(y, ix, pat);
+    std::memcpy(row_ptr, pat.row_ptr.data(), sizeof(int32_t) * (pat.dim + 1));
+    std::memcpy(col_idx, pat.col_idx.data(), sizeof(int32_t) * pat.nnz);
+    const int nnz_y = indptr[n_bus];
+    const std::vector<int32_t>* per_entry[4] = {&m.mapJ11, &m.mapJ21, &m.mapJ12, &m.mapJ22};
+    const std::vector<int32_t>* per_bus[4] = {&m.diagJ11, &m.diagJ21, &m.diagJ12, &m.diagJ22};
+    int32_t* w = maps_out;
+    for (auto* v : per_entry) {
+      std::memcpy(w, v->data(), sizeof(int32_t) * nnz_y);
+      w += nnz_y;
+    }
+    for (auto* v : per_bus) {
+      std::memcpy(w, v->data(), sizeof(int32_t) * n_bus);
+      w += n_bus;
+    }
+    return 0;
+  } catch (const std::exception& e) {
+    g_error = e.what();
+    return 1;
+  }
+}
+
+}  // extern "C"
