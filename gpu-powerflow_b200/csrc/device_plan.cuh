@@ -1,0 +1,79 @@
+// device_plan.cuh -- device views shared by the kernels.
+//
+// Per-scenario arrays are stored element-major with the scenario index
+// innermost: value (element e, scenario b) lives at e * Bp + b, where Bp is the
+// batch rounded up to a multiple of 32.  A warp therefore always reads the same
+// element for 32 consecutive scenarios: one coalesced 128 B (fp32) or 256 B
+// (fp64) transaction, with every plan index warp-uniform.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace cupf_b200 {
+
+constexpr int kWarp = 32;
+
+// The factor program of one grid (see analysis.hpp FactorProgram).
+struct DevPlan {
+  int P = 0, dim = 0, nnz = 0;
+  const int* fsz = nullptr;
+  const int* nc = nullptr;
+  const int* first = nullptr;
+  const int* front_ptr = nullptr;
+  const int* front_rows = nullptr;
+  const long long* u_off = nullptr;
+  const long long* l_off = nullptr;
+  const long long* cb_off = nullptr;
+  const long long* tv_off = nullptr;  // adjoint update vectors: prefix sum of uc
+  const int* arow_ptr = nullptr;
+  const int* arow_q = nullptr;
+  const int* arow_col = nullptr;
+  const int* crow_ptr = nullptr;
+  const int* crow_child = nullptr;
+  const int* crow_r = nullptr;
+  const int* asm_ptr = nullptr;
+  const int* asm_local = nullptr;
+  const int* perm = nullptr;   // permuted index -> Jacobian row
+  const int* iperm = nullptr;  // Jacobian row -> permuted index
+  const int* level_fronts = nullptr;
+};
+
+// Ybus and the Jacobian maps of one grid.
+struct DevGrid {
+  int n_bus = 0, nnz_y = 0, dim = 0, nnz_j = 0, n_pv = 0, n_pq = 0;
+  const int* y_ptr = nullptr;
+  const int* y_col = nullptr;
+  const int* y_row = nullptr;
+  const double* y_re = nullptr;
+  const double* y_im = nullptr;
+  const int* map11 = nullptr;
+  const int* map21 = nullptr;
+  const int* map12 = nullptr;
+  const int* map22 = nullptr;
+  const int* bus_fa = nullptr;  // bus -> angle row (P equation), -1 for slack
+  const int* bus_fm = nullptr;  // bus -> magnitude row (Q equation), -1 for slack/PV
+  const int* pv = nullptr;
+  const int* pq = nullptr;
+  const int* jt_ptr = nullptr;  // J^T as CSR over J's CSR positions: column j of J
+  const int* jt_row = nullptr;  //   rows i and positions q of column j
+  const int* jt_q = nullptr;
+};
+
+// Per-batch state (all [rows][Bp]).
+struct DevState {
+  int B = 0, Bp = 0;
+  double* v_re = nullptr;
+  double* v_im = nullptr;
+  double* va = nullptr;
+  double* vm = nullptr;
+  double* s_re = nullptr;
+  double* s_im = nullptr;
+  double* i_re = nullptr;
+  double* i_im = nullptr;
+  double* F = nullptr;
+  unsigned long long* norm_bits = nullptr;  // [Bp] max |F| per scenario as IEEE bits
+  int* sing = nullptr;                      // [Bp] static-pivot shift applied
+};
+
+}  // namespace cupf_b200

@@ -1,0 +1,799 @@
+// engine.cpp -- host orchestration of the batched Newton-Raphson engine.
+//
+// The NR loop follows NewtonSolver::run_iteration_stages
+// (cuPF/cpp/src/newton_solver/core/newton_solver.cpp:497-558): evaluate the
+// mismatch and its norm, stop when the batch maximum is within tolerance
+// (checked before the Jacobian, so the converged state is not perturbed),
+// otherwise Jacobian -> factorize -> solve -> voltage update.  The iteration
+// count is shared by the batch and reported per scenario; per-scenario
+// convergence is final_mismatch <= tol (newton_solver.cpp:321-341).
+#include "engine.hpp"
+
+#include <algorithm>
+#include <type_traits>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+
+#include "kernels.hpp"
+
+namespace cupf_b200 {
+
+#define CUPF_CUDA(expr)                                                                                   \
+  do {                                                                                                    \
+    cudaError_t _e = (expr);                                                                              \
+    if (_e != cudaSuccess)                                                                                \
+      throw std::runtime_error(std::string("CUDA error: ") + cudaGetErrorString(_e) + " at " #expr);      \
+  } while (0)
+
+namespace {
+
+// CUPF_DEBUG_SYNC=1: synchronize and check for an error after every launch
+// (diagnostics; off by default, never inside a graph capture).
+bool debug_sync() {
+  static const bool on = [] {
+    const char* v = std::getenv("CUPF_DEBUG_SYNC");
+    return v && v[0] == '1';
+  }();
+  return on;
+}
+
+void debug_check(cudaStream_t s, const char* what) {
+  if (!debug_sync()) return;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  cudaStreamIsCapturing(s, &cs);
+  if (cs != cudaStreamCaptureStatusNone) return;
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e != cudaSuccess) throw std::runtime_error(std::string("CUDA error after ") + what + ": " + cudaGetErrorString(e));
+}
+
+struct DBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DBuf() = default;
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  ~DBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  void reserve(size_t nbytes) {
+    if (nbytes <= bytes && p) return;
+    release();
+    if (nbytes == 0) nbytes = 16;
+    CUPF_CUDA(cudaMalloc(&p, nbytes));
+    bytes = nbytes;
+  }
+  template <typename T>
+  T* as() const {
+    return static_cast<T*>(p);
+  }
+  template <typename T>
+  void upload(const std::vector<T>& v) {
+    reserve(std::max<size_t>(v.size(), 1) * sizeof(T));
+    if (!v.empty()) CUPF_CUDA(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  }
+};
+
+template <typename T>
+std::vector<long long> to_ll(const std::vector<T>& v) {
+  return std::vector<long long>(v.begin(), v.end());
+}
+
+}  // namespace
+
+struct Engine::Impl {
+  // grid
+  DBuf y_ptr, y_col, y_row, y_re, y_im, map11, map21, map12, map22, bus_fa, bus_fm, pv, pq, jt_ptr, jt_row, jt_q;
+  // factor program
+  DBuf fsz, nc, first, front_ptr, front_rows, u_off, l_off, cb_off, tv_off, arow_ptr, arow_q, arow_col, crow_ptr,
+      crow_child, crow_r, asm_ptr, asm_local, perm, iperm, level_fronts;
+  std::vector<LevelLaunch> levels;
+  int64_t tv_total = 0;
+  DevGrid g;
+  DevPlan pl;
+  // workspace
+  int Bp_cap = 0, B = 0, Bp = 0;
+  DBuf v_re, v_im, va, vm, s_re, s_im, i_re, i_im, F, norm, sing;
+  DBuf J, U, L, CB, Y, X;
+  DBuf stage_in, stage_out, fin;
+  DBuf G, R, lam, dlam, TV, W, Z, Jd;
+  unsigned long long* h_norm = nullptr;
+  double* h_final = nullptr;
+  int h_cap = 0;
+  cudaStream_t own = nullptr;
+  // graph of one iteration tail (+ the next mismatch), per batch
+  cudaGraphExec_t exec = nullptr;
+  int graph_Bp = -1;
+  bool graph_double = false;
+
+  ~Impl() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (h_norm) cudaFreeHost(h_norm);
+    if (h_final) cudaFreeHost(h_final);
+    if (own) cudaStreamDestroy(own);
+  }
+
+  DevState state() const {
+    DevState st;
+    st.B = B;
+    st.Bp = Bp;
+    st.v_re = v_re.as<double>();
+    st.v_im = v_im.as<double>();
+    st.va = va.as<double>();
+    st.vm = vm.as<double>();
+    st.s_re = s_re.as<double>();
+    st.s_im = s_im.as<double>();
+    st.i_re = i_re.as<double>();
+    st.i_im = i_im.as<double>();
+    st.F = F.as<double>();
+    st.norm_bits = norm.as<unsigned long long>();
+    st.sing = sing.as<int>();
+    return st;
+  }
+};
+
+Engine::Engine(const EngineConfig& cfg) : d_(new Impl()), cfg_(cfg) {
+  if (cfg_.max_panel_width < 1 || cfg_.max_panel_width > 8)
+    throw std::invalid_argument("max_panel_width must be in [1, 8] for this engine");
+}
+
+Engine::~Engine() = default;
+
+bool Engine::factor_is_double() const {
+  return cfg_.compute == kComputeFP64 || cfg_.factor_precision == kFactorFP64;
+}
+
+void Engine::initialize(int32_t n_bus, const int32_t* indptr, const int32_t* indices, const double* ydata,
+                        const int32_t* pv, int32_t n_pv, const int32_t* pq, int32_t n_pq) {
+  if (!indptr || !indices || !ydata) throw std::invalid_argument("initialize: Ybus arrays must not be null");
+  analyze_host(n_bus, indptr, indices, pv, n_pv, pq, n_pq);
+
+  auto& d = *d_;
+  const int32_t nnz_y = indptr[n_bus];
+  std::vector<int32_t> yptr(indptr, indptr + n_bus + 1), ycol(indices, indices + nnz_y), yrow(nnz_y);
+  std::vector<double> yre(nnz_y), yim(nnz_y);
+  for (int32_t r = 0; r < n_bus; ++r)
+    for (int32_t k = indptr[r]; k < indptr[r + 1]; ++k) yrow[k] = r;
+  for (int32_t k = 0; k < nnz_y; ++k) {
+    yre[k] = ydata[2 * k];
+    yim[k] = ydata[2 * k + 1];
+  }
+  d.y_ptr.upload(yptr);
+  d.y_col.upload(ycol);
+  d.y_row.upload(yrow);
+  d.y_re.upload(yre);
+  d.y_im.upload(yim);
+  d.map11.upload(ja_.map11);
+  d.map21.upload(ja_.map21);
+  d.map12.upload(ja_.map12);
+  d.map22.upload(ja_.map22);
+  d.bus_fa.upload(ja_.row_pvpq);
+  d.bus_fm.upload(ja_.row_pq);
+  d.pv.upload(std::vector<int32_t>(pv, pv + n_pv));
+  d.pq.upload(std::vector<int32_t>(pq, pq + n_pq));
+  // J^T as CSR over J's positions (csr_transpose.cpp:257-289, own layout)
+  {
+    std::vector<int32_t> tp(ja_.dim + 1, 0), trow(ja_.nnz), tq(ja_.nnz);
+    for (int32_t q = 0; q < ja_.nnz; ++q) tp[ja_.col_idx[q] + 1]++;
+    for (int32_t c = 0; c < ja_.dim; ++c) tp[c + 1] += tp[c];
+    std::vector<int32_t> cur(tp.begin(), tp.end() - 1);
+    for (int32_t r = 0; r < ja_.dim; ++r)
+      for (int32_t q = ja_.row_ptr[r]; q < ja_.row_ptr[r + 1]; ++q) {
+        const int32_t dst = cur[ja_.col_idx[q]]++;
+        trow[dst] = r;
+        tq[dst] = q;
+      }
+    d.jt_ptr.upload(tp);
+    d.jt_row.upload(trow);
+    d.jt_q.upload(tq);
+  }
+  upload_plan();
+
+  DevGrid& g = d.g;
+  g.n_bus = n_bus;
+  g.nnz_y = nnz_y;
+  g.dim = ja_.dim;
+  g.nnz_j = ja_.nnz;
+  g.n_pv = n_pv;
+  g.n_pq = n_pq;
+  g.y_ptr = d.y_ptr.as<int>();
+  g.y_col = d.y_col.as<int>();
+  g.y_row = d.y_row.as<int>();
+  g.y_re = d.y_re.as<double>();
+  g.y_im = d.y_im.as<double>();
+  g.map11 = d.map11.as<int>();
+  g.map21 = d.map21.as<int>();
+  g.map12 = d.map12.as<int>();
+  g.map22 = d.map22.as<int>();
+  g.bus_fa = d.bus_fa.as<int>();
+  g.bus_fm = d.bus_fm.as<int>();
+  g.pv = d.pv.as<int>();
+  g.pq = d.pq.as<int>();
+  g.jt_ptr = d.jt_ptr.as<int>();
+  g.jt_row = d.jt_row.as<int>();
+  g.jt_q = d.jt_q.as<int>();
+  if (!d.own) CUPF_CUDA(cudaStreamCreateWithFlags(&d.own, cudaStreamNonBlocking));
+  if (d.exec) {
+    cudaGraphExecDestroy(d.exec);
+    d.exec = nullptr;
+    d.graph_Bp = -1;
+  }
+  initialized_ = true;
+  adjoint_ready_ = false;
+}
+
+void Engine::update_ybus_values(const double* ydata) {
+  auto& d = *d_;
+  const size_t nnz = ja_.map11.size();
+  std::vector<double> yre(nnz), yim(nnz);
+  for (size_t k = 0; k < nnz; ++k) {
+    yre[k] = ydata[2 * k];
+    yim[k] = ydata[2 * k + 1];
+  }
+  d.y_re.upload(yre);
+  d.y_im.upload(yim);
+  adjoint_ready_ = false;
+}
+
+void Engine::upload_plan() {
+  auto& d = *d_;
+  d.fsz.upload(fp_.fsz);
+  d.nc.upload(fp_.nc);
+  d.first.upload(fp_.first);
+  d.front_ptr.upload(fp_.front_ptr);
+  d.front_rows.upload(fp_.front_rows);
+  d.u_off.upload(to_ll(fp_.u_off));
+  d.l_off.upload(to_ll(fp_.l_off));
+  d.cb_off.upload(to_ll(fp_.cb_off));
+  {
+    std::vector<long long> tv(fp_.P + 1, 0);
+    for (int32_t p = 0; p < fp_.P; ++p) tv[p + 1] = tv[p] + (fp_.fsz[p] - fp_.nc[p]);
+    d.tv_total = tv[fp_.P];
+    d.tv_off.upload(tv);
+  }
+  d.arow_ptr.upload(fp_.arow_ptr);
+  d.arow_q.upload(fp_.arow_q);
+  d.arow_col.upload(fp_.arow_col);
+  d.crow_ptr.upload(fp_.crow_ptr);
+  d.crow_child.upload(fp_.crow_child);
+  d.crow_r.upload(fp_.crow_r);
+  d.asm_ptr.upload(fp_.asm_ptr);
+  d.asm_local.upload(fp_.asm_local);
+  d.perm.upload(fp_.perm);
+  d.iperm.upload(fp_.iperm);
+  d.level_fronts.upload(fp_.level_fronts);
+  d.levels.clear();
+  for (int32_t L = 0; L < fp_.num_levels; ++L) {
+    LevelLaunch lv;
+    lv.begin = fp_.level_ptr[L];
+    lv.count = fp_.level_ptr[L + 1] - fp_.level_ptr[L];
+    lv.max_fsz = 0;
+    lv.max_nc = 0;
+    for (int32_t q = lv.begin; q < lv.begin + lv.count; ++q) {
+      lv.max_fsz = std::max(lv.max_fsz, fp_.fsz[fp_.level_fronts[q]]);
+      lv.max_nc = std::max(lv.max_nc, fp_.nc[fp_.level_fronts[q]]);
+    }
+    d.levels.push_back(lv);
+  }
+
+  DevPlan& pl = d.pl;
+  pl.P = fp_.P;
+  pl.dim = fp_.dim;
+  pl.nnz = fp_.nnz;
+  pl.fsz = d.fsz.as<int>();
+  pl.nc = d.nc.as<int>();
+  pl.first = d.first.as<int>();
+  pl.front_ptr = d.front_ptr.as<int>();
+  pl.front_rows = d.front_rows.as<int>();
+  pl.u_off = d.u_off.as<long long>();
+  pl.l_off = d.l_off.as<long long>();
+  pl.cb_off = d.cb_off.as<long long>();
+  pl.tv_off = d.tv_off.as<long long>();
+  pl.arow_ptr = d.arow_ptr.as<int>();
+  pl.arow_q = d.arow_q.as<int>();
+  pl.arow_col = d.arow_col.as<int>();
+  pl.crow_ptr = d.crow_ptr.as<int>();
+  pl.crow_child = d.crow_child.as<int>();
+  pl.crow_r = d.crow_r.as<int>();
+  pl.asm_ptr = d.asm_ptr.as<int>();
+  pl.asm_local = d.asm_local.as<int>();
+  pl.perm = d.perm.as<int>();
+  pl.iperm = d.iperm.as<int>();
+  pl.level_fronts = d.level_fronts.as<int>();
+  if (!d.own) CUPF_CUDA(cudaStreamCreateWithFlags(&d.own, cudaStreamNonBlocking));
+  if (d.exec) {
+    cudaGraphExecDestroy(d.exec);
+    d.exec = nullptr;
+    d.graph_Bp = -1;
+  }
+  d.Bp_cap = 0;
+}
+
+void Engine::analyze_host(int32_t n_bus, const int32_t* indptr, const int32_t* indices, const int32_t* pv,
+                          int32_t n_pv, const int32_t* pq, int32_t n_pq) {
+  initialized_ = false;
+  adjoint_ready_ = false;
+  ja_ = analyze_jacobian(n_bus, indptr, indices, pv, n_pv, pq, n_pq);
+  SymbolicOptions so;
+  so.max_panel_width = cfg_.max_panel_width;
+  so.serial_nd = cfg_.serial_nd != 0;
+  sp_ = analyze_symbolic(ja_.dim, ja_.row_ptr.data(), ja_.col_idx.data(), so);
+  fp_ = build_factor_program(sp_);
+  if (fp_.max_fsz > 128) throw std::runtime_error("initialize: a front exceeds 128 rows (unsupported)");
+}
+
+void Engine::analyze_matrix_host(int32_t n, int32_t nnz, const int32_t* row_ptr, const int32_t* col_idx) {
+  if (n <= 0 || nnz < 0 || !row_ptr || !col_idx) throw std::invalid_argument("SetData: invalid CSR pattern");
+  if (row_ptr[n] != nnz) throw std::invalid_argument("SetData: row_ptr[n] != nnz");
+  initialized_ = false;
+  adjoint_ready_ = false;
+  ja_ = JacobianAnalysis();
+  ja_.dim = n;
+  ja_.nnz = nnz;
+  ja_.row_ptr.assign(row_ptr, row_ptr + n + 1);
+  ja_.col_idx.assign(col_idx, col_idx + nnz);
+  SymbolicOptions so;
+  so.max_panel_width = cfg_.max_panel_width;
+  so.serial_nd = cfg_.serial_nd != 0;
+  sp_ = analyze_symbolic(n, row_ptr, col_idx, so);
+  fp_ = build_factor_program(sp_);
+}
+
+void Engine::initialize_matrix(int32_t n, int32_t nnz, const int32_t* row_ptr, const int32_t* col_idx) {
+  if (n <= 0 || nnz < 0 || !row_ptr || !col_idx) throw std::invalid_argument("SetData: invalid CSR pattern");
+  if (row_ptr[n] != nnz) throw std::invalid_argument("SetData: row_ptr[n] != nnz");
+  ja_ = JacobianAnalysis();
+  ja_.dim = n;
+  ja_.nnz = nnz;
+  ja_.row_ptr.assign(row_ptr, row_ptr + n + 1);
+  ja_.col_idx.assign(col_idx, col_idx + nnz);
+  SymbolicOptions so;
+  so.max_panel_width = cfg_.max_panel_width;
+  so.serial_nd = cfg_.serial_nd != 0;
+  sp_ = analyze_symbolic(n, row_ptr, col_idx, so);
+  fp_ = build_factor_program(sp_);
+  if (fp_.max_fsz > 128) throw std::runtime_error("Analyze: a front exceeds 128 rows (unsupported)");
+  upload_plan();
+  initialized_ = true;
+  adjoint_ready_ = false;
+}
+
+void Engine::ensure_workspace(int32_t B) {
+  if (!initialized_) throw std::runtime_error("NewtonSolver::solve_batch(): initialize() must be called first");
+  if (B <= 0) throw std::invalid_argument("NewtonSolver::solve_batch(): batch_size must be positive");
+  auto& d = *d_;
+  const int Bp = (B + kWarp - 1) / kWarp * kWarp;
+  d.B = B;
+  d.Bp = Bp;
+  if (Bp > d.Bp_cap) {
+    const size_t n = ja_.n_bus, dim = ja_.dim;
+    const size_t es = factor_is_double() ? sizeof(double) : sizeof(float);
+    for (DBuf* b : {&d.v_re, &d.v_im, &d.va, &d.vm, &d.s_re, &d.s_im, &d.i_re, &d.i_im}) b->reserve(n * Bp * 8);
+    d.F.reserve(dim * Bp * 8);
+    d.norm.reserve(Bp * 8);
+    d.sing.reserve(Bp * 4);
+    d.J.reserve((size_t)ja_.nnz * Bp * es);
+    d.U.reserve((size_t)fp_.u_total * Bp * es);
+    d.L.reserve((size_t)std::max<int64_t>(fp_.l_total, 1) * Bp * es);
+    d.CB.reserve((size_t)std::max<int64_t>(fp_.cb_total, 1) * Bp * es);
+    d.Y.reserve(dim * Bp * es);
+    d.X.reserve(dim * Bp * es);
+    d.Bp_cap = Bp;
+    if (d.exec) {
+      cudaGraphExecDestroy(d.exec);
+      d.exec = nullptr;
+      d.graph_Bp = -1;
+    }
+    adjoint_ready_ = false;
+  }
+  if (Bp > d.h_cap) {
+    if (d.h_norm) cudaFreeHost(d.h_norm);
+    if (d.h_final) cudaFreeHost(d.h_final);
+    CUPF_CUDA(cudaMallocHost(&d.h_norm, Bp * sizeof(unsigned long long)));
+    CUPF_CUDA(cudaMallocHost(&d.h_final, Bp * sizeof(double)));
+    d.h_cap = Bp;
+  }
+  if (d.graph_Bp != Bp && d.exec) {
+    cudaGraphExecDestroy(d.exec);
+    d.exec = nullptr;
+    d.graph_Bp = -1;
+  }
+}
+
+template <typename T>
+void Engine::factor_all(cudaStream_t s, int store_l, const void* J) {
+  auto& d = *d_;
+  FactorArgs<T, T> a;
+  a.plan = d.pl;
+  a.groups = d.Bp / kWarp;
+  a.Bp = d.Bp;
+  a.J = static_cast<const T*>(J);
+  a.F = d.F.as<double>();
+  a.U = d.U.as<T>();
+  a.L = d.L.as<T>();
+  a.CB = d.CB.as<T>();
+  a.Y = d.Y.as<T>();
+  a.store_l = store_l;
+  a.eps = cfg_.shift_epsilon;
+  a.static_pivot = (cfg_.static_pivot && cfg_.shift_epsilon > 0.0) ? 1 : 0;
+  a.sing = d.sing.as<int>();
+  for (const auto& lv : d.levels) {
+    launch_factor_level<T, T>(lv, a, s);
+    debug_check(s, "factor level");
+    ++launches_;
+  }
+}
+
+template <typename T>
+void Engine::backward_all(cudaStream_t s) {
+  auto& d = *d_;
+  SweepArgs<T> a;
+  a.plan = d.pl;
+  a.groups = d.Bp / kWarp;
+  a.Bp = d.Bp;
+  a.U = d.U.as<T>();
+  a.Y = d.Y.as<T>();
+  a.X = d.X.as<T>();
+  for (int L = (int)d.levels.size() - 1; L >= 0; --L) {
+    launch_backward_level<T>(d.levels[L], a, s);
+    debug_check(s, "backward level");
+    ++launches_;
+  }
+}
+
+template <typename T>
+void Engine::iteration_tail(cudaStream_t s, int store_l) {
+  auto& d = *d_;
+  const DevState st = d.state();
+  launch_jacobian<T>(d.g, st, d.J.as<T>(), s);
+  debug_check(s, "jacobian");
+  ++launches_;
+  factor_all<T>(s, store_l, d.J.p);
+  backward_all<T>(s);
+  launch_voltage_update<T>(d.g, d.pl, st, d.X.as<T>(), s);
+  debug_check(s, "voltage update");
+  ++launches_;
+}
+
+template <typename T>
+SolveStats Engine::run_loop(double tol, int32_t max_iter, int32_t prepare_adjoint, cudaStream_t s, double* d_final) {
+  auto& d = *d_;
+  const DevState st = d.state();
+  SolveStats stats;
+  launches_ = 0;
+  adjoint_ready_ = false;
+  CUPF_CUDA(cudaMemsetAsync(d.norm.p, 0, d.Bp * sizeof(unsigned long long), s));
+  CUPF_CUDA(cudaMemsetAsync(d.sing.p, 0, d.Bp * sizeof(int), s));
+  for (int b = 0; b < d.B; ++b) d.h_final[b] = 0.0;
+  int completed = 0;
+  double gmax = 0.0;
+  if (max_iter > 0) {
+    launch_ibus_mismatch(d.g, st, s);
+    ++launches_;
+  }
+  const bool use_graph = cfg_.use_cuda_graph != 0;
+  for (int it = 0; it < max_iter; ++it) {
+    completed = it + 1;
+    CUPF_CUDA(cudaMemcpyAsync(d.h_norm, d.norm.p, d.Bp * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    CUPF_CUDA(cudaStreamSynchronize(s));
+    gmax = 0.0;
+    bool finite = true;
+    for (int b = 0; b < d.B; ++b) {
+      double v;
+      std::memcpy(&v, &d.h_norm[b], sizeof(double));
+      d.h_final[b] = v;
+      if (!std::isfinite(v)) finite = false;
+      gmax = std::max(gmax, v);
+    }
+    if (debug_sync()) std::fprintf(stderr, "[cupf] iteration %d max ||F||inf = %.3e\n", it, gmax);
+    if (!finite) throw std::runtime_error("NewtonSolver: mismatch norm is not finite");
+    if (gmax <= tol) break;
+    if (use_graph) {
+      if (!d.exec || d.graph_Bp != d.Bp || d.graph_double != std::is_same<T, double>::value) {
+        if (d.exec) cudaGraphExecDestroy(d.exec);
+        d.exec = nullptr;
+        cudaStream_t cs = d.own;
+        cudaGraph_t graph;
+        const int64_t before = launches_;
+        CUPF_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+        iteration_tail<T>(cs, 0);
+        launch_ibus_mismatch(d.g, st, cs);
+        CUPF_CUDA(cudaStreamEndCapture(cs, &graph));
+        CUPF_CUDA(cudaGraphInstantiate(&d.exec, graph, 0));
+        cudaGraphDestroy(graph);
+        d.graph_Bp = d.Bp;
+        d.graph_double = std::is_same<T, double>::value;
+        launches_ = before;
+      }
+      CUPF_CUDA(cudaGraphLaunch(d.exec, s));
+      launches_ += 3 + 2 * (int64_t)d.levels.size();
+    } else {
+      iteration_tail<T>(s, 0);
+      if (it + 1 < max_iter) {
+        launch_ibus_mismatch(d.g, st, s);
+        ++launches_;
+      }
+    }
+  }
+  CUPF_CUDA(cudaGetLastError());
+  stats.iterations = completed;
+  stats.max_final_mismatch = gmax;
+  stats.all_converged = (gmax <= tol) ? 1 : 0;
+  if (prepare_adjoint) {
+    // final-state factorization with L kept (newton_solver.cpp:388-491)
+    CUPF_CUDA(cudaMemsetAsync(d.norm.p, 0, d.Bp * sizeof(unsigned long long), s));
+    launch_ibus_mismatch(d.g, st, s);
+    launch_jacobian<T>(d.g, st, d.J.as<T>(), s);
+    factor_all<T>(s, 1, d.J.p);
+    launches_ += 2;
+    B_ = d.B;
+    adjoint_ready_ = true;
+  }
+  if (d_final) CUPF_CUDA(cudaMemcpyAsync(d_final, d.h_final, d.B * sizeof(double), cudaMemcpyHostToDevice, s));
+  CUPF_CUDA(cudaStreamSynchronize(s));
+  CUPF_CUDA(cudaGetLastError());
+  return stats;
+}
+
+SolveStats Engine::solve_batch_host(const double* sbus, int64_t sbus_stride, const double* v0, int64_t v0_stride,
+                                    int32_t B, double tol, int32_t max_iter, int32_t prepare_adjoint, double* v_out,
+                                    int32_t* iterations, double* final_mismatch, uint8_t* converged) {
+  if (!sbus || !v0) throw std::invalid_argument("NewtonSolver::solve_batch(): sbus/V0 must not be null");
+  if (sbus_stride < ja_.n_bus) throw std::invalid_argument("NewtonSolver::solve_batch(): sbus stride must be at least n_bus");
+  if (v0_stride < ja_.n_bus) throw std::invalid_argument("NewtonSolver::solve_batch(): V0 stride must be at least n_bus");
+  ensure_workspace(B);
+  auto& d = *d_;
+  const size_t n = ja_.n_bus;
+  const size_t in_elems = 2 * ((size_t)B * sbus_stride + (size_t)B * v0_stride);
+  d.stage_in.reserve(in_elems * sizeof(double));
+  d.stage_out.reserve(2 * (size_t)B * n * sizeof(double));
+  d.fin.reserve(std::max<size_t>(B, 1) * sizeof(double));
+  double* din = d.stage_in.as<double>();
+  double* dv0 = din + 2 * (size_t)B * sbus_stride;
+  cudaStream_t s = d.own;
+  CUPF_CUDA(cudaMemcpyAsync(din, sbus, 2 * (size_t)B * sbus_stride * sizeof(double), cudaMemcpyHostToDevice, s));
+  CUPF_CUDA(cudaMemcpyAsync(dv0, v0, 2 * (size_t)B * v0_stride * sizeof(double), cudaMemcpyHostToDevice, s));
+  SolveStats st = solve_batch_device(din, sbus_stride, dv0, v0_stride, B, tol, max_iter, prepare_adjoint,
+                                     d.stage_out.as<double>(), nullptr, s);
+  if (v_out)
+    CUPF_CUDA(cudaMemcpyAsync(v_out, d.stage_out.p, 2 * (size_t)B * n * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CUPF_CUDA(cudaStreamSynchronize(s));
+  for (int b = 0; b < B; ++b) {
+    if (iterations) iterations[b] = st.iterations;
+    if (final_mismatch) final_mismatch[b] = max_iter > 0 ? d.h_final[b] : 0.0;
+    if (converged) converged[b] = (max_iter > 0 ? d.h_final[b] : 0.0) <= tol ? 1 : 0;
+  }
+  return st;
+}
+
+SolveStats Engine::solve_batch_device(const double* d_sbus, int64_t sbus_stride, const double* d_v0, int64_t v0_stride,
+                                      int32_t B, double tol, int32_t max_iter, int32_t prepare_adjoint,
+                                      double* d_v_out, double* d_final_mismatch, cudaStream_t stream) {
+  ensure_workspace(B);
+  auto& d = *d_;
+  cudaStream_t s = stream ? stream : d.own;
+  const DevState st = d.state();
+  launch_seed_state(d.g, st, d_sbus, sbus_stride, d_v0, v0_stride, s);
+  SolveStats out = factor_is_double() ? run_loop<double>(tol, max_iter, prepare_adjoint, s, d_final_mismatch)
+                                      : run_loop<float>(tol, max_iter, prepare_adjoint, s, d_final_mismatch);
+  if (d_v_out) launch_pack_voltage(d.g, st, d_v_out, s);
+  launches_ += 2;
+  CUPF_CUDA(cudaStreamSynchronize(s));
+  return out;
+}
+
+SolveStats Engine::solve_from_load(const void* base_re, const void* base_im, const void* load_p, const void* load_q,
+                                   const void* va0, const void* vm0, int32_t batched_v0, void* va_out, void* vm_out,
+                                   int32_t B, int32_t is_double, double tol, int32_t max_iter,
+                                   int32_t prepare_adjoint, cudaStream_t stream, double* d_final_mismatch) {
+  if (!base_re || !base_im || !load_p || !load_q || !va0 || !vm0 || !va_out || !vm_out)
+    throw std::invalid_argument("cupf::torch_api::solve_forward(): null device pointer");
+  ensure_workspace(B);
+  auto& d = *d_;
+  cudaStream_t s = stream ? stream : d.own;
+  const DevState st = d.state();
+  if (batched_v0)
+    launch_set_inputs_batched(d.g, st, base_re, base_im, load_p, load_q, va0, vm0, is_double, s);
+  else
+    launch_set_inputs_from_load(d.g, st, base_re, base_im, load_p, load_q, va0, vm0, is_double, s);
+  SolveStats out = factor_is_double() ? run_loop<double>(tol, max_iter, prepare_adjoint, s, d_final_mismatch)
+                                      : run_loop<float>(tol, max_iter, prepare_adjoint, s, d_final_mismatch);
+  launch_copy_voltage_outputs(d.g, st, va_out, vm_out, is_double, s);
+  launches_ += 2;
+  CUPF_CUDA(cudaStreamSynchronize(s));
+  return out;
+}
+
+template <typename T>
+void Engine::transpose_solve(const double* d_G, double* d_lam, cudaStream_t s) {
+  auto& d = *d_;
+  AdjointSweepArgs<T> a;
+  a.plan = d.pl;
+  a.groups = d.Bp / kWarp;
+  a.Bp = d.Bp;
+  a.U = d.U.as<T>();
+  a.L = d.L.as<T>();
+  a.G = d_G;
+  a.TV = d.TV.as<T>();
+  a.W = d.W.as<T>();
+  a.Z = d.Z.as<T>();
+  for (const auto& lv : d.levels) launch_ut_forward_level<T>(lv, a, s);
+  for (int L = (int)d.levels.size() - 1; L >= 0; --L) launch_lt_backward_level<T>(d.levels[L], a, s);
+  launch_permuted_to_rows<T>(d.pl, ja_.dim, d.Bp, d.Z.as<T>(), d_lam, s);
+}
+
+double Engine::solve_adjoint_device(const void* grad_va, const void* grad_vm, void* grad_p, void* grad_q,
+                                    double* d_lambda, int32_t B, int32_t is_double, cudaStream_t stream) {
+  if (!adjoint_ready_)
+    throw std::runtime_error("NewtonSolver::solve_adjoint(): missing exact final-state adjoint cache");
+  if (B != B_) throw std::invalid_argument("NewtonSolver::solve_adjoint(): batch_size does not match the last forward solve");
+  if (!grad_va || !grad_vm) throw std::invalid_argument("NewtonSolver::solve_adjoint(): grad_va/grad_vm must not be null");
+  auto& d = *d_;
+  cudaStream_t s = stream ? stream : d.own;
+  const size_t dim = ja_.dim, Bp = d.Bp;
+  const size_t es = factor_is_double() ? sizeof(double) : sizeof(float);
+  for (DBuf* b : {&d.G, &d.R, &d.lam, &d.dlam}) b->reserve(dim * Bp * 8);
+  d.TV.reserve((size_t)std::max<int64_t>(d.tv_total, 1) * Bp * es);
+  d.W.reserve(dim * Bp * es);
+  d.Z.reserve(dim * Bp * es);
+  const DevState st = d.state();
+  launch_gather_adjoint_rhs(d.g, st, grad_va, grad_vm, is_double, d.G.as<double>(), s);
+  const bool dbl = factor_is_double();
+  if (dbl) transpose_solve<double>(d.G.as<double>(), d.lam.as<double>(), s);
+  else transpose_solve<float>(d.G.as<double>(), d.lam.as<double>(), s);
+  // FP64 residual refinement: r = g - J^T lambda with the FP64 Jacobian at the
+  // final state, lambda += (J^T)^-1 r on the cached factors.
+  d.Jd.reserve((size_t)ja_.nnz * Bp * 8);
+  launch_jacobian<double>(d.g, st, d.Jd.as<double>(), s);
+  const int steps = std::max(0, cfg_.adjoint_refine_steps);
+  for (int k = 0; k < steps; ++k) {
+    launch_jt_residual(d.g, d.Bp, d.Jd.as<double>(), d.lam.as<double>(), d.G.as<double>(), d.R.as<double>(), s);
+    if (dbl) transpose_solve<double>(d.R.as<double>(), d.dlam.as<double>(), s);
+    else transpose_solve<float>(d.R.as<double>(), d.dlam.as<double>(), s);
+    launch_axpy(d.lam.as<double>(), d.dlam.as<double>(), (long long)(dim * Bp), s);
+  }
+  launch_jt_residual(d.g, d.Bp, d.Jd.as<double>(), d.lam.as<double>(), d.G.as<double>(), d.R.as<double>(), s);
+  launch_project_load_gradients(d.g, st, d.lam.as<double>(), grad_p, grad_q, is_double, s);
+  if (d_lambda) launch_rows_to_batch<double, double>(d.lam.as<double>(), d_lambda, (int)dim, B, d.Bp, s);
+  // relative residual ||J^T lambda - g|| / ||g|| over the real scenarios
+  std::vector<double> hr(dim * Bp), hg(dim * Bp);
+  CUPF_CUDA(cudaMemcpyAsync(hr.data(), d.R.p, dim * Bp * 8, cudaMemcpyDeviceToHost, s));
+  CUPF_CUDA(cudaMemcpyAsync(hg.data(), d.G.p, dim * Bp * 8, cudaMemcpyDeviceToHost, s));
+  CUPF_CUDA(cudaStreamSynchronize(s));
+  CUPF_CUDA(cudaGetLastError());
+  long double rr = 0.0L, gg = 0.0L;
+  for (size_t f = 0; f < dim; ++f)
+    for (int b = 0; b < B; ++b) {
+      rr += (long double)hr[f * Bp + b] * hr[f * Bp + b];
+      gg += (long double)hg[f * Bp + b] * hg[f * Bp + b];
+    }
+  const long double den = std::max(std::sqrt(std::max(gg, 1e-60L)), 1e-30L);
+  return (double)(std::sqrt(rr) / den);
+}
+
+void Engine::factorize_values(const void* d_values, int32_t values_is_double, int32_t B, cudaStream_t stream) {
+  ensure_workspace(B);
+  auto& d = *d_;
+  cudaStream_t s = stream ? stream : d.own;
+  const bool dbl = factor_is_double();
+  // [B][nnz] (batch-strided, solver.hpp:76-79) -> [nnz][Bp]
+  if (dbl) {
+    if (values_is_double)
+      launch_batch_to_rows<double, double>(static_cast<const double*>(d_values), d.J.as<double>(), ja_.nnz, B, d.Bp, s);
+    else
+      launch_batch_to_rows<float, double>(static_cast<const float*>(d_values), d.J.as<double>(), ja_.nnz, B, d.Bp, s);
+  } else {
+    if (values_is_double)
+      launch_batch_to_rows<double, float>(static_cast<const double*>(d_values), d.J.as<float>(), ja_.nnz, B, d.Bp, s);
+    else
+      launch_batch_to_rows<float, float>(static_cast<const float*>(d_values), d.J.as<float>(), ja_.nnz, B, d.Bp, s);
+  }
+  CUPF_CUDA(cudaMemsetAsync(d.F.p, 0, (size_t)ja_.dim * d.Bp * 8, s));
+  CUPF_CUDA(cudaMemsetAsync(d.sing.p, 0, d.Bp * sizeof(int), s));
+  if (dbl) factor_all<double>(s, 1, d.J.p);
+  else factor_all<float>(s, 1, d.J.p);
+  B_ = B;
+  adjoint_ready_ = false;
+  CUPF_CUDA(cudaStreamSynchronize(s));
+  CUPF_CUDA(cudaGetLastError());
+}
+
+void Engine::solve_values(const void* d_rhs, int32_t rhs_is_double, void* d_x, int32_t x_is_double, int32_t B,
+                          bool transpose, cudaStream_t stream) {
+  if (B != B_) throw std::invalid_argument("Solve: batch size differs from the factorization");
+  auto& d = *d_;
+  cudaStream_t s = stream ? stream : d.own;
+  const size_t dim = ja_.dim, Bp = d.Bp;
+  const bool dbl = factor_is_double();
+  const size_t es = dbl ? sizeof(double) : sizeof(float);
+  d.G.reserve(dim * Bp * 8);
+  d.lam.reserve(dim * Bp * 8);
+  d.TV.reserve((size_t)std::max<int64_t>(d.tv_total, 1) * Bp * es);
+  d.W.reserve(dim * Bp * es);
+  d.Z.reserve(dim * Bp * es);
+  if (rhs_is_double)
+    launch_batch_to_rows<double, double>(static_cast<const double*>(d_rhs), d.G.as<double>(), (int)dim, B, (int)Bp, s);
+  else
+    launch_batch_to_rows<float, double>(static_cast<const float*>(d_rhs), d.G.as<double>(), (int)dim, B, (int)Bp, s);
+  auto run = [&](auto tag) {
+    using T = decltype(tag);
+    if (transpose) {
+      transpose_solve<T>(d.G.as<double>(), d.lam.as<double>(), s);
+      return;
+    }
+    AdjointSweepArgs<T> a;
+    a.plan = d.pl;
+    a.groups = (int)Bp / kWarp;
+    a.Bp = (int)Bp;
+    a.U = d.U.as<T>();
+    a.L = d.L.as<T>();
+    a.G = d.G.as<double>();
+    a.TV = d.TV.as<T>();
+    a.W = d.W.as<T>();
+    for (const auto& lv : d.levels) launch_l_forward_level<T>(lv, a, s);
+    SweepArgs<T> bk;
+    bk.plan = d.pl;
+    bk.groups = (int)Bp / kWarp;
+    bk.Bp = (int)Bp;
+    bk.U = d.U.as<T>();
+    bk.Y = d.W.as<T>();
+    bk.X = d.X.as<T>();
+    for (int L = (int)d.levels.size() - 1; L >= 0; --L) launch_backward_level<T>(d.levels[L], bk, s);
+    launch_permuted_to_rows<T>(d.pl, (int)dim, (int)Bp, d.X.as<T>(), d.lam.as<double>(), s);
+  };
+  if (dbl) run(double{});
+  else run(float{});
+  if (x_is_double)
+    launch_rows_to_batch<double, double>(d.lam.as<double>(), static_cast<double*>(d_x), (int)dim, B, (int)Bp, s);
+  else
+    launch_rows_to_batch<double, float>(d.lam.as<double>(), static_cast<float*>(d_x), (int)dim, B, (int)Bp, s);
+  CUPF_CUDA(cudaStreamSynchronize(s));
+  CUPF_CUDA(cudaGetLastError());
+}
+
+void Engine::evaluate_host(const double* V, const double* sbus, int32_t B, double* F_out, double* J_out) {
+  ensure_workspace(B);
+  auto& d = *d_;
+  cudaStream_t s = d.own;
+  const size_t n = ja_.n_bus, dim = ja_.dim;
+  d.stage_in.reserve(4 * (size_t)B * n * sizeof(double));
+  double* ds = d.stage_in.as<double>();
+  double* dv = ds + 2 * (size_t)B * n;
+  CUPF_CUDA(cudaMemcpyAsync(ds, sbus, 2 * (size_t)B * n * sizeof(double), cudaMemcpyHostToDevice, s));
+  CUPF_CUDA(cudaMemcpyAsync(dv, V, 2 * (size_t)B * n * sizeof(double), cudaMemcpyHostToDevice, s));
+  const DevState st = d.state();
+  launch_seed_state(d.g, st, ds, (long long)n, dv, (long long)n, s);
+  CUPF_CUDA(cudaMemsetAsync(d.norm.p, 0, d.Bp * sizeof(unsigned long long), s));
+  launch_ibus_mismatch(d.g, st, s);
+  d.Jd.reserve((size_t)ja_.nnz * d.Bp * 8);
+  launch_jacobian<double>(d.g, st, d.Jd.as<double>(), s);
+  d.G.reserve(std::max<size_t>(dim, (size_t)ja_.nnz) * B * 8);
+  launch_rows_to_batch<double, double>(d.F.as<double>(), d.G.as<double>(), (int)dim, B, d.Bp, s);
+  CUPF_CUDA(cudaMemcpyAsync(F_out, d.G.p, dim * B * 8, cudaMemcpyDeviceToHost, s));
+  CUPF_CUDA(cudaStreamSynchronize(s));
+  launch_rows_to_batch<double, double>(d.Jd.as<double>(), d.G.as<double>(), ja_.nnz, B, d.Bp, s);
+  CUPF_CUDA(cudaMemcpyAsync(J_out, d.G.p, (size_t)ja_.nnz * B * 8, cudaMemcpyDeviceToHost, s));
+  CUPF_CUDA(cudaStreamSynchronize(s));
+  CUPF_CUDA(cudaGetLastError());
+}
+
+std::vector<int32_t> Engine::singular_flags() const {
+  std::vector<int32_t> out;
+  if (!d_->sing.p || d_->B == 0) return out;
+  std::vector<int32_t> tmp(d_->Bp);
+  cudaMemcpy(tmp.data(), d_->sing.p, d_->Bp * sizeof(int32_t), cudaMemcpyDeviceToHost);
+  out.assign(tmp.begin(), tmp.begin() + d_->B);
+  return out;
+}
+
+template SolveStats Engine::run_loop<float>(double, int32_t, int32_t, cudaStream_t, double*);
+template SolveStats Engine::run_loop<double>(double, int32_t, int32_t, cudaStream_t, double*);
+
+}  // namespace cupf_b200

@@ -1,0 +1,131 @@
+// engine.hpp -- batched Newton-Raphson power-flow engine (host orchestration).
+//
+// One Engine = one grid (Ybus pattern + PV/PQ sets) analysed once, solved for
+// any number of scenarios.  It is the engine behind the C ABI in
+// include/cupf_b200.h and the role the reference's NewtonSolver + cuda-custom
+// pipeline play (cuPF/cpp/inc/newton_solver/core/newton_solver.hpp:26-102,
+// cuPF/cpp/src/newton_solver/core/pipeline.hpp:350-388).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "analysis.hpp"
+#include "device_plan.cuh"
+
+namespace cupf_b200 {
+
+enum ComputeMode : int32_t { kComputeFP64 = 0, kComputeFP32 = 1, kComputeMixed = 2 };
+enum FactorPrecision : int32_t { kFactorFP64 = 0, kFactorFP32 = 1, kFactorTF32 = 2 };
+
+struct EngineConfig {
+  int32_t compute = kComputeMixed;
+  int32_t factor_precision = kFactorFP32;
+  int32_t max_panel_width = 8;
+  int32_t serial_nd = 1;
+  int32_t static_pivot = 1;       // StaticDiagonalShift
+  double shift_epsilon = 1e-8;    // threshold and replacement magnitude
+  int32_t use_cuda_graph = 0;     // capture one iteration and replay it
+  int32_t adjoint_refine_steps = 2;
+};
+
+struct SolveStats {
+  int32_t iterations = 0;
+  double max_final_mismatch = 0.0;
+  int32_t all_converged = 0;
+  int32_t any_shifted_pivot = 0;
+};
+
+class Engine {
+ public:
+  explicit Engine(const EngineConfig& cfg);
+  ~Engine();
+  Engine(const Engine&) = delete;
+  Engine& operator=(const Engine&) = delete;
+
+  // Host CSR Ybus (complex as interleaved doubles), PV/PQ bus lists.
+  void initialize(int32_t n_bus, const int32_t* indptr, const int32_t* indices, const double* ydata,
+                  const int32_t* pv, int32_t n_pv, const int32_t* pq, int32_t n_pq);
+  // Linear-solver use: analyse an n x n CSR pattern (no Ybus / NR state).
+  void initialize_matrix(int32_t n, int32_t nnz, const int32_t* row_ptr, const int32_t* col_idx);
+  // Host-only analysis (no device memory): for plan introspection on machines
+  // without a GPU.  The engine cannot solve after this call alone.
+  void analyze_host(int32_t n_bus, const int32_t* indptr, const int32_t* indices, const int32_t* pv, int32_t n_pv,
+                    const int32_t* pq, int32_t n_pq);
+  void analyze_matrix_host(int32_t n, int32_t nnz, const int32_t* row_ptr, const int32_t* col_idx);
+  bool initialized() const { return initialized_; }
+  // New Ybus values on the analysed pattern (complex interleaved, CSR order).
+  void update_ybus_values(const double* ydata);
+
+  // NewtonSolver::solve_batch semantics with host buffers: sbus / v0 are
+  // complex [B][stride]; outputs V [B][n] complex, per-scenario stats.
+  SolveStats solve_batch_host(const double* sbus, int64_t sbus_stride, const double* v0, int64_t v0_stride,
+                              int32_t B, double tol, int32_t max_iter, int32_t prepare_adjoint, double* v_out,
+                              int32_t* iterations, double* final_mismatch, uint8_t* converged);
+  // Same with device-resident inputs/outputs in the same host layout.
+  SolveStats solve_batch_device(const double* d_sbus, int64_t sbus_stride, const double* d_v0, int64_t v0_stride,
+                                int32_t B, double tol, int32_t max_iter, int32_t prepare_adjoint, double* d_v_out,
+                                double* d_final_mismatch, cudaStream_t stream);
+  // torch-style: Sbus = base - load, V0 = (va0, vm0); base/v0 shared [n] or
+  // v0 batched [B][n]; outputs Va/Vm [B][n]; float or double per is_double.
+  SolveStats solve_from_load(const void* base_re, const void* base_im, const void* load_p, const void* load_q,
+                             const void* va0, const void* vm0, int32_t batched_v0, void* va_out, void* vm_out,
+                             int32_t B, int32_t is_double, double tol, int32_t max_iter, int32_t prepare_adjoint,
+                             cudaStream_t stream, double* d_final_mismatch);
+  // Adjoint on the cached final-state factors: grads [B][n] device, outputs
+  // grad_p / grad_q [B][n]; optional lambda [B][dimF] (double, device).
+  double solve_adjoint_device(const void* grad_va, const void* grad_vm, void* grad_p, void* grad_q,
+                              double* d_lambda, int32_t B, int32_t is_double, cudaStream_t stream);
+
+  // Linear-solver boundary: factor caller-supplied Jacobian values and solve.
+  void factorize_values(const void* d_values, int32_t values_is_double, int32_t B, cudaStream_t stream);
+  void solve_values(const void* d_rhs, int32_t rhs_is_double, void* d_x, int32_t x_is_double, int32_t B,
+                    bool transpose, cudaStream_t stream);
+
+  // Evaluate F and J (fp64) at host states V / Sbus ([B][n] complex).
+  void evaluate_host(const double* V, const double* sbus, int32_t B, double* F_out, double* J_out);
+
+  const JacobianAnalysis& jacobian() const { return ja_; }
+  const SymbolicPlan& symbolic() const { return sp_; }
+  const FactorProgram& program() const { return fp_; }
+  const EngineConfig& config() const { return cfg_; }
+  int32_t n_bus() const { return ja_.n_bus; }
+  int32_t dim() const { return ja_.dim; }
+  bool factor_is_double() const;
+  bool adjoint_cache_valid() const { return adjoint_ready_; }
+  int32_t cached_batch() const { return B_; }
+  std::vector<int32_t> singular_flags() const;  // per scenario of the last factorization
+  // kernel launches issued by the last solve (for reporting)
+  int64_t last_launches() const { return launches_; }
+
+ private:
+  struct Impl;
+  std::unique_ptr<Impl> d_;
+  EngineConfig cfg_;
+  JacobianAnalysis ja_;
+  SymbolicPlan sp_;
+  FactorProgram fp_;
+  bool initialized_ = false;
+  bool adjoint_ready_ = false;
+  int32_t B_ = 0;
+  int64_t launches_ = 0;
+
+  void ensure_workspace(int32_t B);
+  void upload_plan();
+  template <typename T>
+  SolveStats run_loop(double tol, int32_t max_iter, int32_t prepare_adjoint, cudaStream_t s, double* d_final);
+  template <typename T>
+  void iteration_tail(cudaStream_t s, int store_l);
+  template <typename T>
+  void factor_all(cudaStream_t s, int store_l, const void* J);
+  template <typename T>
+  void backward_all(cudaStream_t s);
+  template <typename T>
+  void transpose_solve(const double* d_G, double* d_lam, cudaStream_t s);
+};
+
+}  // namespace cupf_b200

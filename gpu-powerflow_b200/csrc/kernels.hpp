@@ -1,0 +1,105 @@
+// kernels.hpp -- host-side launchers of the engine's CUDA kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "device_plan.cuh"
+
+namespace cupf_b200 {
+
+// One level of the front tree as the launchers see it.
+struct LevelLaunch {
+  int begin = 0;   // offset into DevPlan::level_fronts
+  int count = 0;   // fronts in the level
+  int max_fsz = 0; // largest front of the level (selects the register bucket)
+  int max_nc = 0;  // widest panel of the level
+};
+
+template <typename T, typename TJ>
+struct FactorArgs {
+  DevPlan plan;
+  int groups = 0, Bp = 0;
+  const TJ* J = nullptr;
+  const double* F = nullptr;
+  T* U = nullptr;
+  T* L = nullptr;
+  T* CB = nullptr;
+  T* Y = nullptr;
+  int store_l = 0;
+  double eps = 1e-8;
+  int static_pivot = 1;
+  int* sing = nullptr;
+};
+
+template <typename T>
+struct SweepArgs {
+  DevPlan plan;
+  int groups = 0, Bp = 0;
+  const T* U = nullptr;
+  const T* Y = nullptr;
+  T* X = nullptr;
+};
+
+template <typename T>
+struct AdjointSweepArgs {
+  DevPlan plan;
+  int groups = 0, Bp = 0;
+  const T* U = nullptr;
+  const T* L = nullptr;
+  const double* G = nullptr;  // rhs in Jacobian-row order
+  T* TV = nullptr;            // update vectors [tv_total][Bp]
+  T* W = nullptr;             // U^T solution (permuted order)
+  T* Z = nullptr;             // L^T solution (permuted order)
+};
+
+template <typename T, typename TJ>
+void launch_factor_level(const LevelLaunch& lv, const FactorArgs<T, TJ>& a, cudaStream_t s);
+template <typename T>
+void launch_backward_level(const LevelLaunch& lv, const SweepArgs<T>& a, cudaStream_t s);
+template <typename T>
+void launch_ut_forward_level(const LevelLaunch& lv, const AdjointSweepArgs<T>& a, cudaStream_t s);
+// L y = P g for a rhs given after factorization (y written to a.W)
+template <typename T>
+void launch_l_forward_level(const LevelLaunch& lv, const AdjointSweepArgs<T>& a, cudaStream_t s);
+template <typename T>
+void launch_lt_backward_level(const LevelLaunch& lv, const AdjointSweepArgs<T>& a, cudaStream_t s);
+
+// ---- element-wise NR stages (kernels_nr.cu) ----
+void launch_ibus_mismatch(const DevGrid& g, const DevState& st, cudaStream_t s);
+template <typename TJ>
+void launch_jacobian(const DevGrid& g, const DevState& st, TJ* J, cudaStream_t s);
+template <typename T>
+void launch_voltage_update(const DevGrid& g, const DevPlan& pl, const DevState& st, const T* X, cudaStream_t s);
+// seed from host-layout complex arrays [B][stride] (interleaved re/im) staged on device
+void launch_seed_state(const DevGrid& g, const DevState& st, const double* sbus_c, long long sbus_stride,
+                       const double* v0_c, long long v0_stride, cudaStream_t s);
+void launch_pack_voltage(const DevGrid& g, const DevState& st, double* v_c, cudaStream_t s);
+// torch-style inputs: base injection [n], loads [B][n], flat start [n]; dtype float or double
+void launch_set_inputs_from_load(const DevGrid& g, const DevState& st, const void* base_re, const void* base_im,
+                                 const void* load_p, const void* load_q, const void* va0, const void* vm0,
+                                 int is_double, cudaStream_t s);
+void launch_set_inputs_batched(const DevGrid& g, const DevState& st, const void* base_re, const void* base_im,
+                               const void* load_p, const void* load_q, const void* va0, const void* vm0,
+                               int is_double, cudaStream_t s);
+void launch_copy_voltage_outputs(const DevGrid& g, const DevState& st, void* va_out, void* vm_out, int is_double,
+                                 cudaStream_t s);
+// adjoint helpers
+void launch_gather_adjoint_rhs(const DevGrid& g, const DevState& st, const void* grad_va, const void* grad_vm,
+                               int is_double, double* G, cudaStream_t s);
+template <typename T>
+void launch_permuted_to_rows(const DevPlan& pl, int dim, int Bp, const T* Z, double* lam, cudaStream_t s);
+void launch_project_load_gradients(const DevGrid& g, const DevState& st, const double* lam, void* grad_p,
+                                   void* grad_q, int is_double, cudaStream_t s);
+// r = g - J^T lambda, J given by its CSR values [nnz_j][Bp] (fp64)
+void launch_jt_residual(const DevGrid& g, int Bp, const double* Jd, const double* lam, const double* G, double* R,
+                        cudaStream_t s);
+void launch_axpy(double* y, const double* x, long long n, cudaStream_t s);
+// [B][rows] (TS) -> [rows][Bp] (TD) and back; pad scenarios copy scenario B - 1
+template <typename TS, typename TD>
+void launch_batch_to_rows(const TS* src, TD* dst, int rows, int B, int Bp, cudaStream_t s);
+template <typename TS, typename TD>
+void launch_rows_to_batch(const TS* src, TD* dst, int rows, int B, int Bp, cudaStream_t s);
+
+}  // namespace cupf_b200

@@ -1,0 +1,495 @@
+// kernels_nr.cu -- element-wise stages of one Newton-Raphson iteration and
+// the host<->engine layout conversions.
+//
+// All per-scenario state is [element][Bp] with the scenario innermost: a warp
+// covers 32 scenarios of one bus or one Ybus entry, so Ybus values and map
+// indices are warp-uniform broadcasts and the state accesses are coalesced.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+
+#include "device_plan.cuh"
+#include "kernels.hpp"
+
+namespace cupf_b200 {
+namespace {
+
+constexpr int kRows = 8;  // warps per block in the (lane, row) kernels
+
+__device__ __forceinline__ double dmax_nan(double m, double a, bool& bad) {
+  if (!(a == a) || a > 1.7976931348623157e308) bad = true;
+  return a > m ? a : m;
+}
+
+// ---------------------------------------------------------------------------
+// Ibus = Ybus V, F = [Re mis@pv, Re mis@pq, Im mis@pq] with mis = V conj(I) - S,
+// and per-scenario ||F||_inf (cuPF compute_ibus.cu:58-95,
+// compute_mismatch_from_ibus.cu:32-85, reduce_mismatch_norm.cu:49-119 fused).
+// The norm is an atomicMax on the IEEE bits of |F| (order preserving for
+// non-negative doubles); a non-finite entry forces NaN bits.
+// ---------------------------------------------------------------------------
+__global__ void k_ibus_mismatch(DevGrid g, DevState st) {
+  const int lane = threadIdx.x, wy = threadIdx.y;
+  const int Bp = st.Bp;
+  const size_t b = (size_t)blockIdx.y * kWarp + lane;
+  double nmax = 0.0;
+  bool bad = false;
+  for (int i = blockIdx.x * kRows + wy; i < g.n_bus; i += gridDim.x * kRows) {
+    double ir = 0.0, ii = 0.0;
+    for (int k = g.y_ptr[i]; k < g.y_ptr[i + 1]; ++k) {
+      const size_t c = (size_t)g.y_col[k] * Bp + b;
+      const double yr = g.y_re[k], yi = g.y_im[k];
+      const double vr = st.v_re[c], vi = st.v_im[c];
+      ir += yr * vr - yi * vi;
+      ii += yr * vi + yi * vr;
+    }
+    const size_t o = (size_t)i * Bp + b;
+    st.i_re[o] = ir;
+    st.i_im[o] = ii;
+    const double vr = st.v_re[o], vi = st.v_im[o];
+    const double mr = (vr * ir + vi * ii) - st.s_re[o];
+    const double mi = (vi * ir - vr * ii) - st.s_im[o];
+    const int fa = g.bus_fa[i], fm = g.bus_fm[i];
+    if (fa >= 0) {
+      st.F[(size_t)fa * Bp + b] = mr;
+      nmax = dmax_nan(nmax, fabs(mr), bad);
+    }
+    if (fm >= 0) {
+      st.F[(size_t)fm * Bp + b] = mi;
+      nmax = dmax_nan(nmax, fabs(mi), bad);
+    }
+  }
+  __shared__ double red[kRows][kWarp];
+  __shared__ int redbad[kRows][kWarp];
+  red[wy][lane] = nmax;
+  redbad[wy][lane] = bad ? 1 : 0;
+  __syncthreads();
+  if (wy == 0) {
+    double m = red[0][lane];
+    int anybad = redbad[0][lane];
+    for (int r = 1; r < kRows; ++r) {
+      m = red[r][lane] > m ? red[r][lane] : m;
+      anybad |= redbad[r][lane];
+    }
+    const unsigned long long bits =
+        anybad ? 0x7FF8000000000000ull : (unsigned long long)__double_as_longlong(m);
+    atomicMax(&st.norm_bits[b], bits);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Jacobian values into the fixed CSR pattern through the scatter maps
+// (cuPF fill_jacobian_edge_kernel.hpp:30-197, jacobian_gpu_common.hpp:96-127):
+//   off-diagonal  dS/dVa = -j V_i conj(y V_j),  dS/dVm = V_i conj(y V_j / |V_j|)
+//   diagonal adds          j V_i conj(I_i)   and         conj(I_i) V_i / |V_i|
+// J11/J21 take the real/imaginary parts of dS/dVa, J12/J22 of dS/dVm.  The
+// diagonal terms are added by the thread of the Ybus diagonal entry, so every
+// slot is written exactly once (no memset, no atomics).
+// ---------------------------------------------------------------------------
+template <typename TJ>
+__global__ void k_jacobian(DevGrid g, DevState st, TJ* __restrict__ J) {
+  const int lane = threadIdx.x, wy = threadIdx.y;
+  const int Bp = st.Bp;
+  const size_t b = (size_t)blockIdx.y * kWarp + lane;
+  for (int k = blockIdx.x * kRows + wy; k < g.nnz_y; k += gridDim.x * kRows) {
+    const int i = g.y_row[k], c = g.y_col[k];
+    const double yr = g.y_re[k], yi = g.y_im[k];
+    const size_t oi = (size_t)i * Bp + b, oc = (size_t)c * Bp + b;
+    const double vir = st.v_re[oi], vii = st.v_im[oi];
+    const double vcr = st.v_re[oc], vci = st.v_im[oc];
+    const double yvr = yr * vcr - yi * vci, yvi = yr * vci + yi * vcr;  // y V_c
+    // -j V_i conj(y V_c)
+    double var = vii * yvr - vir * yvi;
+    double vai = -(vii * yvi + vir * yvr);
+    // V_i conj(y V_c / |V_c|)
+    double mc = hypot(vcr, vci);
+    mc = mc < 1e-8 ? 1e-8 : mc;
+    const double ynr = yvr / mc, yni = yvi / mc;
+    double vmr = vir * ynr + vii * yni;
+    double vmi = vii * ynr - vir * yni;
+    if (i == c) {
+      const double ir = st.i_re[oi], ii = st.i_im[oi];
+      // j V conj(I)
+      var += -(vii * ir - vir * ii);
+      vai += vir * ir + vii * ii;
+      // conj(I) V / |V|
+      const double nr = vir / mc, ni = vii / mc;
+      vmr += ir * nr + ii * ni;
+      vmi += ir * ni - ii * nr;
+    }
+    const int p11 = g.map11[k], p21 = g.map21[k], p12 = g.map12[k], p22 = g.map22[k];
+    if (p11 >= 0) J[(size_t)p11 * Bp + b] = static_cast<TJ>(var);
+    if (p21 >= 0) J[(size_t)p21 * Bp + b] = static_cast<TJ>(vai);
+    if (p12 >= 0) J[(size_t)p12 * Bp + b] = static_cast<TJ>(vmr);
+    if (p22 >= 0) J[(size_t)p22 * Bp + b] = static_cast<TJ>(vmi);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Va/Vm -= dx at the pv/pq rows, V = Vm (cos Va + j sin Va)
+// (cuPF voltage_update_kernels.hpp:44-104).  dx is read from the permuted
+// solution X (x_perm[iperm[row]]).  The bus-0 thread clears the scenario's
+// norm for the next mismatch evaluation.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_voltage_update(DevGrid g, DevPlan pl, DevState st, const T* __restrict__ X) {
+  const int lane = threadIdx.x, wy = threadIdx.y;
+  const int Bp = st.Bp;
+  const size_t b = (size_t)blockIdx.y * kWarp + lane;
+  for (int i = blockIdx.x * kRows + wy; i < g.n_bus; i += gridDim.x * kRows) {
+    const size_t o = (size_t)i * Bp + b;
+    double va = st.va[o], vm = st.vm[o];
+    const int fa = g.bus_fa[i], fm = g.bus_fm[i];
+    if (fa >= 0) va -= static_cast<double>(X[(size_t)pl.iperm[fa] * Bp + b]);
+    if (fm >= 0) vm -= static_cast<double>(X[(size_t)pl.iperm[fm] * Bp + b]);
+    double s, c;
+    sincos(va, &s, &c);
+    st.va[o] = va;
+    st.vm[o] = vm;
+    st.v_re[o] = vm * c;
+    st.v_im[o] = vm * s;
+    if (i == 0) st.norm_bits[b] = 0ull;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Layout conversions through a 32 x 32 shared tile: host arrays are
+// scenario-major [B][stride], the engine is bus-major [n][Bp].
+// Pad scenarios (B <= b < Bp) replicate scenario B - 1.
+// ---------------------------------------------------------------------------
+__global__ void k_seed_state(DevGrid g, DevState st, const double* __restrict__ sbus_c, long long sbus_stride,
+                             const double* __restrict__ v0_c, long long v0_stride) {
+  __shared__ double t[4][kWarp][kWarp + 1];
+  const int tx = threadIdx.x, ty = threadIdx.y;  // (32, 8)
+  const int bus0 = blockIdx.x * kWarp, b0 = blockIdx.y * kWarp;
+  for (int r = ty; r < kWarp; r += kRows) {
+    const int bb = min(b0 + r, st.B - 1);
+    const int bus = bus0 + tx;
+    if (bus < g.n_bus) {
+      const size_t so = ((size_t)bb * sbus_stride + bus) * 2, vo = ((size_t)bb * v0_stride + bus) * 2;
+      t[0][r][tx] = sbus_c[so];
+      t[1][r][tx] = sbus_c[so + 1];
+      t[2][r][tx] = v0_c[vo];
+      t[3][r][tx] = v0_c[vo + 1];
+    }
+  }
+  __syncthreads();
+  for (int r = ty; r < kWarp; r += kRows) {
+    const int bus = bus0 + r;
+    if (bus >= g.n_bus) continue;
+    const size_t o = (size_t)bus * st.Bp + b0 + tx;
+    const double vr = t[2][tx][r], vi = t[3][tx][r];
+    st.s_re[o] = t[0][tx][r];
+    st.s_im[o] = t[1][tx][r];
+    st.v_re[o] = vr;
+    st.v_im[o] = vi;
+    st.va[o] = atan2(vi, vr);
+    st.vm[o] = hypot(vr, vi);
+  }
+}
+
+__global__ void k_pack_voltage(DevGrid g, DevState st, double* __restrict__ v_c) {
+  __shared__ double t[2][kWarp][kWarp + 1];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int bus0 = blockIdx.x * kWarp, b0 = blockIdx.y * kWarp;
+  for (int r = ty; r < kWarp; r += kRows) {
+    const int bus = bus0 + r;
+    if (bus < g.n_bus) {
+      const size_t o = (size_t)bus * st.Bp + b0 + tx;
+      t[0][r][tx] = st.v_re[o];
+      t[1][r][tx] = st.v_im[o];
+    }
+  }
+  __syncthreads();
+  for (int r = ty; r < kWarp; r += kRows) {
+    const int bb = b0 + r, bus = bus0 + tx;
+    if (bb < st.B && bus < g.n_bus) {
+      const size_t o = ((size_t)bb * g.n_bus + bus) * 2;
+      v_c[o] = t[0][tx][r];
+      v_c[o + 1] = t[1][tx][r];
+    }
+  }
+}
+
+template <typename TI>
+__device__ __forceinline__ double ld_in(const void* p, size_t i) {
+  return static_cast<double>(static_cast<const TI*>(p)[i]);
+}
+
+// Sbus = base - load, V0 from (va0, vm0); torch_bridge_kernels.cu:116-152.
+// batched_v0 = 1: va0/vm0 are [B][n] (warm starts), else [n] shared.
+template <typename TI>
+__global__ void k_set_inputs(DevGrid g, DevState st, const void* base_re, const void* base_im, const void* load_p,
+                             const void* load_q, const void* va0, const void* vm0, int batched_v0) {
+  __shared__ double t[4][kWarp][kWarp + 1];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int bus0 = blockIdx.x * kWarp, b0 = blockIdx.y * kWarp;
+  const int bus = bus0 + tx;
+  for (int r = ty; r < kWarp; r += kRows) {
+    const int bb = min(b0 + r, st.B - 1);
+    if (bus < g.n_bus) {
+      const size_t o = (size_t)bb * g.n_bus + bus;
+      t[0][r][tx] = ld_in<TI>(load_p, o);
+      t[1][r][tx] = ld_in<TI>(load_q, o);
+      t[2][r][tx] = batched_v0 ? ld_in<TI>(va0, o) : 0.0;
+      t[3][r][tx] = batched_v0 ? ld_in<TI>(vm0, o) : 0.0;
+    }
+  }
+  __syncthreads();
+  for (int r = ty; r < kWarp; r += kRows) {
+    const int bs = bus0 + r;
+    if (bs >= g.n_bus) continue;
+    const size_t o = (size_t)bs * st.Bp + b0 + tx;
+    const double a = batched_v0 ? t[2][tx][r] : ld_in<TI>(va0, bs);
+    const double m = batched_v0 ? t[3][tx][r] : ld_in<TI>(vm0, bs);
+    st.s_re[o] = ld_in<TI>(base_re, bs) - t[0][tx][r];
+    st.s_im[o] = ld_in<TI>(base_im, bs) - t[1][tx][r];
+    double s, c;
+    sincos(a, &s, &c);
+    st.va[o] = a;
+    st.vm[o] = m;
+    st.v_re[o] = m * c;
+    st.v_im[o] = m * s;
+  }
+}
+
+template <typename TO>
+__global__ void k_copy_voltage_outputs(DevGrid g, DevState st, TO* __restrict__ va_out, TO* __restrict__ vm_out) {
+  __shared__ double t[2][kWarp][kWarp + 1];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int bus0 = blockIdx.x * kWarp, b0 = blockIdx.y * kWarp;
+  for (int r = ty; r < kWarp; r += kRows) {
+    const int bus = bus0 + r;
+    if (bus < g.n_bus) {
+      const size_t o = (size_t)bus * st.Bp + b0 + tx;
+      t[0][r][tx] = st.va[o];
+      t[1][r][tx] = st.vm[o];
+    }
+  }
+  __syncthreads();
+  for (int r = ty; r < kWarp; r += kRows) {
+    const int bb = b0 + r, bus = bus0 + tx;
+    if (bb < st.B && bus < g.n_bus) {
+      const size_t o = (size_t)bb * g.n_bus + bus;
+      va_out[o] = static_cast<TO>(t[0][tx][r]);
+      vm_out[o] = static_cast<TO>(t[1][tx][r]);
+    }
+  }
+}
+
+// dL/dx = [grad_va@pv, grad_va@pq, grad_vm@pq] (torch_bridge_kernels.cu:32-54)
+template <typename TI>
+__global__ void k_gather_adjoint_rhs(DevGrid g, DevState st, const void* grad_va, const void* grad_vm,
+                                     double* __restrict__ G) {
+  const int lane = threadIdx.x, wy = threadIdx.y;
+  const size_t b = (size_t)blockIdx.y * kWarp + lane;
+  const int bb = min((int)b, st.B - 1);
+  const int npvpq = g.n_pv + g.n_pq;
+  for (int f = blockIdx.x * kRows + wy; f < g.dim; f += gridDim.x * kRows) {
+    double v;
+    if (f < g.n_pv) v = ld_in<TI>(grad_va, (size_t)bb * g.n_bus + g.pv[f]);
+    else if (f < npvpq) v = ld_in<TI>(grad_va, (size_t)bb * g.n_bus + g.pq[f - g.n_pv]);
+    else v = ld_in<TI>(grad_vm, (size_t)bb * g.n_bus + g.pq[f - npvpq]);
+    G[(size_t)f * st.Bp + b] = v;
+  }
+}
+
+template <typename T>
+__global__ void k_permuted_to_rows(DevPlan pl, int dim, int Bp, const T* __restrict__ Z, double* __restrict__ lam) {
+  const int lane = threadIdx.x, wy = threadIdx.y;
+  const size_t b = (size_t)blockIdx.y * kWarp + lane;
+  for (int f = blockIdx.x * kRows + wy; f < dim; f += gridDim.x * kRows)
+    lam[(size_t)f * Bp + b] = static_cast<double>(Z[(size_t)pl.iperm[f] * Bp + b]);
+}
+
+// grad_load = -lambda at the bus's rows (adjoint_math.cpp:189-216)
+template <typename TO>
+__global__ void k_project_load_gradients(DevGrid g, DevState st, const double* __restrict__ lam, TO* grad_p,
+                                         TO* grad_q) {
+  const int lane = threadIdx.x, wy = threadIdx.y;
+  const size_t b = (size_t)blockIdx.y * kWarp + lane;
+  if ((int)b >= st.B) return;
+  for (int i = blockIdx.x * kRows + wy; i < g.n_bus; i += gridDim.x * kRows) {
+    const int fa = g.bus_fa[i], fm = g.bus_fm[i];
+    const size_t o = b * g.n_bus + i;
+    grad_p[o] = static_cast<TO>(fa >= 0 ? -lam[(size_t)fa * st.Bp + b] : 0.0);
+    grad_q[o] = static_cast<TO>(fm >= 0 ? -lam[(size_t)fm * st.Bp + b] : 0.0);
+  }
+}
+
+// R = G - J^T lambda: row j of J^T is column j of J
+__global__ void k_jt_residual(DevGrid g, int Bp, const double* __restrict__ Jd, const double* __restrict__ lam,
+                              const double* __restrict__ G, double* __restrict__ R) {
+  const int lane = threadIdx.x, wy = threadIdx.y;
+  const size_t b = (size_t)blockIdx.y * kWarp + lane;
+  for (int j = blockIdx.x * kRows + wy; j < g.dim; j += gridDim.x * kRows) {
+    double acc = 0.0;
+    for (int e = g.jt_ptr[j]; e < g.jt_ptr[j + 1]; ++e)
+      acc += Jd[(size_t)g.jt_q[e] * Bp + b] * lam[(size_t)g.jt_row[e] * Bp + b];
+    R[(size_t)j * Bp + b] = G[(size_t)j * Bp + b] - acc;
+  }
+}
+
+__global__ void k_axpy(double* y, const double* x, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    y[i] += x[i];
+}
+
+template <typename TS, typename TD>
+__global__ void k_batch_to_rows(const TS* __restrict__ src, TD* __restrict__ dst, int rows, int B, int Bp) {
+  __shared__ double t[kWarp][kWarp + 1];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int r0 = blockIdx.x * kWarp, b0 = blockIdx.y * kWarp;
+  for (int r = ty; r < kWarp; r += kRows) {
+    const int bb = min(b0 + r, B - 1), row = r0 + tx;
+    if (row < rows) t[r][tx] = static_cast<double>(src[(size_t)bb * rows + row]);
+  }
+  __syncthreads();
+  for (int r = ty; r < kWarp; r += kRows) {
+    const int row = r0 + r;
+    if (row < rows) dst[(size_t)row * Bp + b0 + tx] = static_cast<TD>(t[tx][r]);
+  }
+}
+
+template <typename TS, typename TD>
+__global__ void k_rows_to_batch(const TS* __restrict__ src, TD* __restrict__ dst, int rows, int B, int Bp) {
+  __shared__ double t[kWarp][kWarp + 1];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int r0 = blockIdx.x * kWarp, b0 = blockIdx.y * kWarp;
+  for (int r = ty; r < kWarp; r += kRows) {
+    const int row = r0 + r;
+    if (row < rows) t[r][tx] = static_cast<double>(src[(size_t)row * Bp + b0 + tx]);
+  }
+  __syncthreads();
+  for (int r = ty; r < kWarp; r += kRows) {
+    const int bb = b0 + r, row = r0 + tx;
+    if (bb < B && row < rows) dst[(size_t)bb * rows + row] = static_cast<TD>(t[tx][r]);
+  }
+}
+
+dim3 rows_grid(int rows, int Bp) {
+  int bx = (rows + kRows * 4 - 1) / (kRows * 4);
+  if (bx < 1) bx = 1;
+  return dim3(bx, Bp / kWarp);
+}
+
+}  // namespace
+
+void launch_ibus_mismatch(const DevGrid& g, const DevState& st, cudaStream_t s) {
+  k_ibus_mismatch<<<rows_grid(g.n_bus, st.Bp), dim3(kWarp, kRows), 0, s>>>(g, st);
+}
+
+template <typename TJ>
+void launch_jacobian(const DevGrid& g, const DevState& st, TJ* J, cudaStream_t s) {
+  k_jacobian<TJ><<<rows_grid(g.nnz_y, st.Bp), dim3(kWarp, kRows), 0, s>>>(g, st, J);
+}
+template void launch_jacobian<float>(const DevGrid&, const DevState&, float*, cudaStream_t);
+template void launch_jacobian<double>(const DevGrid&, const DevState&, double*, cudaStream_t);
+
+template <typename T>
+void launch_voltage_update(const DevGrid& g, const DevPlan& pl, const DevState& st, const T* X, cudaStream_t s) {
+  k_voltage_update<T><<<rows_grid(g.n_bus, st.Bp), dim3(kWarp, kRows), 0, s>>>(g, pl, st, X);
+}
+template void launch_voltage_update<float>(const DevGrid&, const DevPlan&, const DevState&, const float*,
+                                           cudaStream_t);
+template void launch_voltage_update<double>(const DevGrid&, const DevPlan&, const DevState&, const double*,
+                                            cudaStream_t);
+
+void launch_seed_state(const DevGrid& g, const DevState& st, const double* sbus_c, long long sbus_stride,
+                       const double* v0_c, long long v0_stride, cudaStream_t s) {
+  dim3 grid((g.n_bus + kWarp - 1) / kWarp, st.Bp / kWarp);
+  k_seed_state<<<grid, dim3(kWarp, kRows), 0, s>>>(g, st, sbus_c, sbus_stride, v0_c, v0_stride);
+}
+
+void launch_pack_voltage(const DevGrid& g, const DevState& st, double* v_c, cudaStream_t s) {
+  dim3 grid((g.n_bus + kWarp - 1) / kWarp, st.Bp / kWarp);
+  k_pack_voltage<<<grid, dim3(kWarp, kRows), 0, s>>>(g, st, v_c);
+}
+
+void launch_set_inputs_from_load(const DevGrid& g, const DevState& st, const void* base_re, const void* base_im,
+                                 const void* load_p, const void* load_q, const void* va0, const void* vm0,
+                                 int is_double, cudaStream_t s) {
+  dim3 grid((g.n_bus + kWarp - 1) / kWarp, st.Bp / kWarp);
+  if (is_double)
+    k_set_inputs<double><<<grid, dim3(kWarp, kRows), 0, s>>>(g, st, base_re, base_im, load_p, load_q, va0, vm0, 0);
+  else
+    k_set_inputs<float><<<grid, dim3(kWarp, kRows), 0, s>>>(g, st, base_re, base_im, load_p, load_q, va0, vm0, 0);
+}
+
+void launch_set_inputs_batched(const DevGrid& g, const DevState& st, const void* base_re, const void* base_im,
+                               const void* load_p, const void* load_q, const void* va0, const void* vm0,
+                               int is_double, cudaStream_t s) {
+  dim3 grid((g.n_bus + kWarp - 1) / kWarp, st.Bp / kWarp);
+  if (is_double)
+    k_set_inputs<double><<<grid, dim3(kWarp, kRows), 0, s>>>(g, st, base_re, base_im, load_p, load_q, va0, vm0, 1);
+  else
+    k_set_inputs<float><<<grid, dim3(kWarp, kRows), 0, s>>>(g, st, base_re, base_im, load_p, load_q, va0, vm0, 1);
+}
+
+void launch_copy_voltage_outputs(const DevGrid& g, const DevState& st, void* va_out, void* vm_out, int is_double,
+                                 cudaStream_t s) {
+  dim3 grid((g.n_bus + kWarp - 1) / kWarp, st.Bp / kWarp);
+  if (is_double)
+    k_copy_voltage_outputs<double><<<grid, dim3(kWarp, kRows), 0, s>>>(g, st, static_cast<double*>(va_out),
+                                                                       static_cast<double*>(vm_out));
+  else
+    k_copy_voltage_outputs<float><<<grid, dim3(kWarp, kRows), 0, s>>>(g, st, static_cast<float*>(va_out),
+                                                                      static_cast<float*>(vm_out));
+}
+
+void launch_gather_adjoint_rhs(const DevGrid& g, const DevState& st, const void* grad_va, const void* grad_vm,
+                               int is_double, double* G, cudaStream_t s) {
+  if (is_double)
+    k_gather_adjoint_rhs<double><<<rows_grid(g.dim, st.Bp), dim3(kWarp, kRows), 0, s>>>(g, st, grad_va, grad_vm, G);
+  else
+    k_gather_adjoint_rhs<float><<<rows_grid(g.dim, st.Bp), dim3(kWarp, kRows), 0, s>>>(g, st, grad_va, grad_vm, G);
+}
+
+template <typename T>
+void launch_permuted_to_rows(const DevPlan& pl, int dim, int Bp, const T* Z, double* lam, cudaStream_t s) {
+  k_permuted_to_rows<T><<<rows_grid(dim, Bp), dim3(kWarp, kRows), 0, s>>>(pl, dim, Bp, Z, lam);
+}
+template void launch_permuted_to_rows<float>(const DevPlan&, int, int, const float*, double*, cudaStream_t);
+template void launch_permuted_to_rows<double>(const DevPlan&, int, int, const double*, double*, cudaStream_t);
+
+void launch_project_load_gradients(const DevGrid& g, const DevState& st, const double* lam, void* grad_p,
+                                   void* grad_q, int is_double, cudaStream_t s) {
+  if (is_double)
+    k_project_load_gradients<double><<<rows_grid(g.n_bus, st.Bp), dim3(kWarp, kRows), 0, s>>>(
+        g, st, lam, static_cast<double*>(grad_p), static_cast<double*>(grad_q));
+  else
+    k_project_load_gradients<float><<<rows_grid(g.n_bus, st.Bp), dim3(kWarp, kRows), 0, s>>>(
+        g, st, lam, static_cast<float*>(grad_p), static_cast<float*>(grad_q));
+}
+
+void launch_jt_residual(const DevGrid& g, int Bp, const double* Jd, const double* lam, const double* G, double* R,
+                        cudaStream_t s) {
+  k_jt_residual<<<rows_grid(g.dim, Bp), dim3(kWarp, kRows), 0, s>>>(g, Bp, Jd, lam, G, R);
+}
+
+template <typename TS, typename TD>
+void launch_batch_to_rows(const TS* src, TD* dst, int rows, int B, int Bp, cudaStream_t s) {
+  dim3 grid((rows + kWarp - 1) / kWarp, Bp / kWarp);
+  k_batch_to_rows<TS, TD><<<grid, dim3(kWarp, kRows), 0, s>>>(src, dst, rows, B, Bp);
+}
+template <typename TS, typename TD>
+void launch_rows_to_batch(const TS* src, TD* dst, int rows, int B, int Bp, cudaStream_t s) {
+  dim3 grid((rows + kWarp - 1) / kWarp, Bp / kWarp);
+  k_rows_to_batch<TS, TD><<<grid, dim3(kWarp, kRows), 0, s>>>(src, dst, rows, B, Bp);
+}
+template void launch_batch_to_rows<double, double>(const double*, double*, int, int, int, cudaStream_t);
+template void launch_batch_to_rows<double, float>(const double*, float*, int, int, int, cudaStream_t);
+template void launch_batch_to_rows<float, float>(const float*, float*, int, int, int, cudaStream_t);
+template void launch_batch_to_rows<float, double>(const float*, double*, int, int, int, cudaStream_t);
+template void launch_rows_to_batch<double, double>(const double*, double*, int, int, int, cudaStream_t);
+template void launch_rows_to_batch<float, double>(const float*, double*, int, int, int, cudaStream_t);
+template void launch_rows_to_batch<double, float>(const double*, float*, int, int, int, cudaStream_t);
+
+void launch_axpy(double* y, const double* x, long long n, cudaStream_t s) {
+  long long blocks = (n + 255) / 256;
+  if (blocks > 4096) blocks = 4096;
+  k_axpy<<<(unsigned)blocks, 256, 0, s>>>(y, x, n);
+}
+
+}  // namespace cupf_b200

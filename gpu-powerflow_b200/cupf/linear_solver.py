@@ -1,0 +1,130 @@
+"""Batched sparse direct solver: the phase API of custom_linear_solver::Solver
+(custom_linear_solver/src/solver.hpp:67-114) over the cls_* C ABI.
+
+    s = LinearSolver(SolverConfig(precision=CustomPrecision.FP64))
+    s.set_data(row_ptr, col_idx)          # CSR pattern (host numpy or device tensor)
+    s.analyze(); s.setup(batch)
+    s.factorize(values)                   # CUDA tensor [batch, nnz] float64/float32
+    x = s.solve(rhs)                      # CUDA tensor [batch, n]
+    y = s.solve_transpose(rhs)            # A^T y = rhs on the same factors
+
+Status codes become exceptions carrying StatusString (solver.cpp:214-232).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _capi
+
+
+class SolverConfig:
+    """SolverConfig (solver.hpp:35-65); precision uses CustomPrecision values."""
+
+    def __init__(self, precision: int = 0, pivot_strategy: int = 1, serial_nd: bool = True,
+                 max_panel_width: int = 8, shift_retry_epsilon: float = 1e-8):
+        self.precision = int(precision)
+        self.pivot_strategy = int(pivot_strategy)
+        self.serial_nd = bool(serial_nd)
+        self.max_panel_width = int(max_panel_width)
+        self.shift_retry_epsilon = float(shift_retry_epsilon)
+
+
+class CustomSolverError(RuntimeError):
+    def __init__(self, status: int, text: str, detail: str):
+        super().__init__(f"custom solver {text}" + (f": {detail}" if detail else ""))
+        self.status = status
+
+
+class LinearSolver:
+    def __init__(self, config: SolverConfig | None = None):
+        self._lib = _capi.load()
+        c = config or SolverConfig()
+        cfg = _capi.ClsConfig(c.precision, 0, c.pivot_strategy, int(c.serial_nd), c.max_panel_width,
+                              c.shift_retry_epsilon)
+        h = C.c_void_p()
+        st = self._lib.cls_create(C.byref(cfg), C.byref(h))
+        if st:
+            raise CustomSolverError(st, self._lib.cls_status_string(st).decode(), "")
+        self._h = h
+        self.n = 0
+        self.batch = 0
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            self._lib.cls_destroy(h)
+            self._h = None
+
+    def _check(self, st: int) -> None:
+        if st:
+            raise CustomSolverError(st, self._lib.cls_status_string(st).decode(),
+                                    self._lib.cls_last_error(self._h).decode())
+
+    def set_data(self, row_ptr, col_idx) -> None:
+        try:
+            import torch
+            is_dev = isinstance(row_ptr, torch.Tensor) and row_ptr.is_cuda
+        except ImportError:
+            is_dev = False
+        if is_dev:
+            n = row_ptr.numel() - 1
+            self._check(self._lib.cls_set_data(self._h, n, col_idx.numel(), row_ptr.data_ptr(), col_idx.data_ptr(), 1))
+        else:
+            rp = np.ascontiguousarray(row_ptr, dtype=np.int32)
+            ci = np.ascontiguousarray(col_idx, dtype=np.int32)
+            n = rp.size - 1
+            self._check(self._lib.cls_set_data(self._h, n, ci.size, rp.ctypes.data_as(C.c_void_p),
+                                               ci.ctypes.data_as(C.c_void_p), 0))
+        self.n = n
+
+    def analyze(self) -> None:
+        self._check(self._lib.cls_analyze(self._h))
+
+    def analyze_host(self) -> None:
+        """Symbolic analysis without device memory (plan introspection only)."""
+        self._check(self._lib.cls_analyze_host(self._h))
+
+    def setup(self, batch: int = 1) -> None:
+        self._check(self._lib.cls_setup(self._h, batch))
+        self.batch = batch
+
+    def set_stream(self, stream) -> None:
+        self._check(self._lib.cls_set_stream(self._h, C.c_void_p(int(stream))))
+
+    @staticmethod
+    def _vt(t) -> int:
+        import torch
+        if t.dtype == torch.float64:
+            return 0
+        if t.dtype == torch.float32:
+            return 1
+        raise ValueError("values must be float64 or float32")
+
+    def factorize(self, values) -> None:
+        self._check(self._lib.cls_factorize(self._h, values.data_ptr(), self._vt(values)))
+
+    def solve(self, rhs, out=None, transpose: bool = False):
+        import torch
+        if out is None:
+            out = torch.empty_like(rhs)
+        fn = self._lib.cls_solve_transpose if transpose else self._lib.cls_solve
+        self._check(fn(self._h, rhs.data_ptr(), self._vt(rhs), out.data_ptr(), self._vt(out)))
+        return out
+
+    def solve_transpose(self, rhs, out=None):
+        return self.solve(rhs, out, transpose=True)
+
+    def singular_flags(self) -> np.ndarray:
+        out = np.zeros(self.batch, dtype=np.int32)
+        self._check(self._lib.cls_singular_flags(self._h, out.ctypes.data_as(C.c_void_p), self.batch))
+        return out
+
+    def plan_array(self, name: str) -> np.ndarray:
+        ln = C.c_int64(0)
+        self._check(self._lib.cls_plan_array(self._h, name.encode(), None, 0, C.byref(ln)))
+        out = np.zeros(ln.value, dtype=np.int32)
+        self._check(self._lib.cls_plan_array(self._h, name.encode(), out.ctypes.data_as(C.c_void_p), out.size,
+                                             C.byref(ln)))
+        return out
