@@ -1,0 +1,347 @@
+"""Benchmark: converged Newton-Raphson solves/s, 2,000-bus grid x 1,024 load scenarios.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+
+One step = one batched Newton solve of every scenario of the batch to
+||F||_inf <= 1e-8 pu (max 10 iterations) on the synthetic 2,000-bus grid
+(400 PV, 1,599 PQ, Jacobian 3,598 x 3,598), per-bus load factors U(0.8, 1.2).
+
+value   : converged solves/s of the mixed-precision engine (FP32 Jacobian and
+          factors, FP64 mismatch / state / convergence test), inputs resident in
+          HBM, device time from CUDA events on the solve stream.
+fp64    : the plain FP64 flat-start engine path on the same batch (the metric's
+          denominator); "speedup_vs_fp64" = value / fp64.value.
+e2e     : the same mixed solve through the public API (cupf.NewtonSolver.
+          solve_batch) with host numpy buffers: H2D of Sbus/V0 and D2H of V and
+          the per-scenario results inside the timed region.
+Multi-GPU (torchrun): every rank solves its own batch (weak scaling, no
+collective on the data path); value = all converged solves / max rank time.
+--impl reference: the reference's own CPU NewtonSolver (cpu-klu path compiled
+from its sources, KLU replaced by the oracle LU) on all host cores, on a
+bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+for _p in (ROOT / "gpu-powerflow_b200", ROOT):
+    if str(_p) not in sys.path:
+        sys.path.insert(0, str(_p))
+
+import numpy as np  # noqa: E402
+
+METRIC = "NR solves/sec at ||F||inf<=1e-8 pu: plain FP64 vs mixed+warm-start, 1 B200"
+UNIT = "converged solves/s"
+BATCH = 1024
+TOL = 1e-8
+MAX_ITER = 10
+
+
+def _peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": float(d["hbm_gbs"]), "bf16_tflops": float(d["bf16_tflops"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback"}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+                out = ""
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in getattr(self, "lines", []):
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def _dist():
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1 and not dist.is_initialized():
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def _barrier(world: int) -> None:
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def _reduce(value: float, op: str, world: int, device) -> float:
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def factor_bytes_per_scenario(solver, elem: int) -> int:
+    """Algorithmic bytes of one factorization for one scenario: read J (elem * nnzJ),
+    read F (8 * dimF), write the U rows (elem * sum nc*fsz) and y (elem * dimF)."""
+    inf = solver.info()
+    fsz = solver.plan_array("fp_fsz").astype(np.int64)
+    nc = solver.plan_array("fp_nc").astype(np.int64)
+    return int(elem * inf["nnz_jacobian"] + 8 * inf["dim_f"] + elem * int((nc * fsz).sum()) + elem * inf["dim_f"])
+
+
+def make_solver(grid, compute):
+    import cupf
+    o = cupf.NewtonOptions()
+    o.backend = cupf.BackendKind.CUDA
+    o.compute = compute
+    o.custom.serial_nd = True
+    s = cupf.NewtonSolver(o)
+    s.initialize(grid.indptr, grid.indices, grid.data, grid.n_bus, grid.n_bus, grid.pv, grid.pq)
+    return s
+
+
+def run_engine(args) -> None:
+    import torch
+
+    import cupf
+    from cupf import grids
+
+    world, rank, local = _dist()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    g = grids.grid_2000()
+    B = args.batch
+    sbus_h = g.scenarios(B, seed=9100 + rank)
+    v0_h = g.flat_start(B)
+    sbus = torch.tensor(sbus_h, device=dev)
+    v0 = torch.tensor(v0_h, device=dev)
+    cfg = cupf.NRConfig()
+    cfg.tolerance = TOL
+    cfg.max_iter = MAX_ITER
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
+
+    def timed(solver, steps: int, warmup: int):
+        stream = torch.cuda.current_stream(dev)
+        for _ in range(warmup):
+            solver.solve_batch_device(sbus, v0, config=cfg)
+        _barrier(world)
+        torch.cuda.synchronize(dev)
+        times, conv, iters = [], 0, 0
+        for _ in range(steps):
+            flush.fill_(1.0)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            v, fm, it = solver.solve_batch_device(sbus, v0, config=cfg)
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+            conv += int((fm <= TOL).sum().item())
+            iters = it
+        torch.cuda.synchronize(dev)
+        _barrier(world)
+        return times, conv, iters, solver.info()["last_kernel_launches"]
+
+    mixed = make_solver(g, cupf.ComputePolicy.Mixed)
+    fp64 = make_solver(g, cupf.ComputePolicy.FP64)
+
+    with ClockSampler(local) as clk:
+        t_mix, conv_mix, it_mix, launches = timed(mixed, args.steps, args.warmup)
+    t_64, conv_64, it_64, _ = timed(fp64, args.steps, args.warmup)
+
+    ms_mix = statistics.mean(t_mix)
+    ms_mix_max = _reduce(ms_mix, "max", world, dev)
+    conv_total = _reduce(conv_mix / args.steps, "sum", world, dev)
+    value = conv_total / (ms_mix_max / 1e3)
+    ms_64 = _reduce(statistics.mean(t_64), "max", world, dev)
+    value_64 = _reduce(conv_64 / args.steps, "sum", world, dev) / (ms_64 / 1e3)
+
+    # e2e: public API with host buffers (H2D + D2H inside the timed region)
+    for _ in range(args.warmup):
+        mixed.solve_batch(g.indptr, g.indices, g.data, g.n_bus, g.n_bus, sbus_h, v0_h, g.pv, g.pq, cfg)
+    _barrier(world)
+    torch.cuda.synchronize(dev)
+    t_e2e, conv_e2e = [], 0
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        r = mixed.solve_batch(g.indptr, g.indices, g.data, g.n_bus, g.n_bus, sbus_h, v0_h, g.pv, g.pq, cfg)
+        t_e2e.append((time.perf_counter() - t0) * 1e3)
+        conv_e2e += int(r.converged_numpy.sum())
+    ms_e2e = _reduce(statistics.mean(t_e2e), "max", world, dev)
+    e2e_value = _reduce(conv_e2e / args.steps, "sum", world, dev) / (ms_e2e / 1e3)
+    h2d = 2 * B * g.n_bus * 16
+    d2h = B * g.n_bus * 16 + B * (4 + 8 + 1)
+
+    # roofline of the dominant kernel (the front factorization): stage timers
+    # over one extra profiled solve, outside the timed region
+    mixed.set_profiling(True)
+    flush.fill_(1.0)
+    mixed.solve_batch_device(sbus, v0, config=cfg)
+    st = mixed.stage_times()
+    mixed.set_profiling(False)
+    fact_ms, fact_launches = st["factorize"]
+    n_fact = max(1, it_mix - 1)
+    per_fact_ms = fact_ms / n_fact
+    fbytes = factor_bytes_per_scenario(mixed, 4) * B
+    peaks = _peaks()
+    achieved = fbytes / (per_fact_ms / 1e3) / 1e9
+    traffic = None
+    tr_file = ROOT / "profiles" / "factor_traffic.json"
+    if tr_file.exists():
+        try:
+            traffic = json.loads(tr_file.read_text()).get("bytes_per_factorization_b1024")
+        except Exception:
+            traffic = None
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(g, args.cpu_sample)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_mix_max, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 factors / f64 state",
+            "data": "synthetic: seeded 2,000-bus grid, per-bus load factors U(0.8,1.2)",
+            "config": {"workload": "2000-bus x 1024-scenario batched NR, mixed precision, flat start",
+                       "grid_buses": g.n_bus, "jacobian_dim": g.dim_f, "batch_per_gpu": B, "tolerance": TOL,
+                       "max_iter": MAX_ITER, "warm_start": "none", "l2": "256 MB buffer written between steps",
+                       "iterations": int(it_mix), "converged_per_step": conv_mix / args.steps},
+            "fp64": {"value": round(value_64, 1), "ms_per_step": round(ms_64, 4), "iterations": int(it_64),
+                     "converged_per_step": conv_64 / args.steps},
+            "speedup_vs_fp64": round(value / value_64, 3) if value_64 else None,
+            "e2e": {"value": round(e2e_value, 1), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "ms_per_step": round(ms_e2e, 4)},
+            "roofline": {"kernel": "k_front_factor (all levels of one factorization)", "bound": "hbm",
+                         "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                         "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": traffic,
+                         "algorithmic_bytes": fbytes, "ms_per_launch_group": round(per_fact_ms, 4),
+                         "peak_source": peaks["source"]},
+            "stage_ms_per_solve": {k: round(v[0], 4) for k, v in st.items()},
+            "cpu_baseline": cpu,
+            "gpu_launches": int(launches) * args.steps,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def cpu_baseline(g, sample: int) -> dict:
+    """The reference's own CPU path (or the oracle port) on all host cores."""
+    from oracle import oracle as orc
+    threads = os.cpu_count() or 1
+    S = g.scenarios(sample, seed=4242)
+    V0 = g.flat_start(sample)
+    kind = "reference" if orc.reference_available() else "port"
+    solver = orc.Reference() if kind == "reference" else orc.Oracle()
+    t0 = time.perf_counter()
+    r = solver.solve_many(g, S, V0, TOL, MAX_ITER, threads)
+    dt = time.perf_counter() - t0
+    conv = int((r["final_mismatch"] <= TOL).sum())
+    return {"value": round(conv / dt, 2), "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": f"{sample} scenarios of the 2,000-bus workload, one solver per thread, "
+                      f"{'reference cpu-klu NewtonSolver (KLU replaced by the oracle LU)' if kind == 'reference' else 'oracle C port'}"}
+
+
+def run_reference(args) -> None:
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from cupf import grids
+    g = grids.grid_2000()
+    cb = None
+    vals = []
+    for _ in range(args.warmup):
+        cpu_baseline(g, max(8, args.cpu_sample // 8))
+    for _ in range(args.steps):
+        cb = cpu_baseline(g, args.cpu_sample)
+        vals.append(cb["value"])
+    v = statistics.mean(vals)
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": round(v, 2), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * args.cpu_sample / v, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic: seeded 2,000-bus grid, per-bus load factors U(0.8,1.2)",
+        "config": {"workload": "2000-bus batched NR on the reference CPU path, bounded sample",
+                   "sample_scenarios_per_step": args.cpu_sample, "tolerance": TOL, "max_iter": MAX_ITER},
+        "cpu_baseline": cb, "e2e": {"value": round(v, 2), "unit": UNIT, "h2d_bytes_per_step": 0,
+                                     "d2h_bytes_per_step": 0}}))
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--batch", type=int, default=BATCH)
+    ap.add_argument("--cpu-sample", type=int, default=512)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_engine(args)
+
+
+if __name__ == "__main__":
+    main()

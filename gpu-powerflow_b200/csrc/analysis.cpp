@@ -548,6 +548,55 @@ FactorProgram build_factor_program(const SymbolicPlan& sp) {
       fp.crow_ptr[fr + 1] = static_cast<int32_t>(fp.crow_child.size());
     }
   }
+  // Dense-front assembly entries (sorted by destination) and warp chunks.
+  {
+    fp.fe_ptr.assign(P + 1, 0);
+    fp.fe_split.assign((size_t)P * (kFeChunks + 1), 0);
+    std::vector<std::vector<int32_t>> owned(P);
+    for (int32_t q = 0; q < sp.nnz; ++q) owned[sp.a_owner[q]].push_back(q);
+    std::vector<std::vector<int32_t>> kids(P);
+    for (int32_t c = 0; c < P; ++c)
+      if (sp.panel_parent[c] >= 0) kids[sp.panel_parent[c]].push_back(c);
+    struct Ent {
+      int32_t dst;
+      int64_t src;
+    };
+    std::vector<Ent> ents;
+    for (int32_t p = 0; p < P; ++p) {
+      ents.clear();
+      const int32_t fs = fp.fsz[p], nc = fp.nc[p], rw = fs + 1;
+      for (int32_t q : owned[p]) ents.push_back({sp.a_row[q] * rw + sp.a_col[q], (int64_t)q});
+      for (int32_t i = 0; i < nc; ++i)
+        ents.push_back({i * rw + fs, (int64_t(2) << kFeKindShift) | (int64_t)sp.perm[sp.panel_first[p] + i]});
+      for (int32_t c : kids[p]) {
+        const int32_t ucc = fp.fsz[c] - fp.nc[c];
+        const int32_t* al = sp.asm_local.data() + sp.asm_ptr[c];
+        for (int32_t r = 0; r < ucc; ++r)
+          for (int32_t cc = 0; cc <= ucc; ++cc) {
+            const int32_t col = cc < ucc ? al[cc] : fs;
+            const int64_t idx = fp.cb_off[c] + (int64_t)r * (ucc + 1) + cc;
+            ents.push_back({al[r] * rw + col, (int64_t(1) << kFeKindShift) | idx});
+          }
+      }
+      std::stable_sort(ents.begin(), ents.end(), [](const Ent& a, const Ent& b) { return a.dst < b.dst; });
+      const int64_t base = (int64_t)fp.fe_dst.size();
+      for (const Ent& e : ents) {
+        fp.fe_dst.push_back(e.dst);
+        fp.fe_src.push_back(e.src);
+      }
+      fp.fe_ptr[p + 1] = (int64_t)fp.fe_dst.size();
+      // chunk cuts at destination boundaries, about equal entry counts
+      const int64_t n = (int64_t)ents.size();
+      int64_t* split = fp.fe_split.data() + (size_t)p * (kFeChunks + 1);
+      split[0] = base;
+      for (int w = 1; w < kFeChunks; ++w) {
+        int64_t cut = std::max<int64_t>(split[w - 1] - base, n * w / kFeChunks);
+        while (cut > 0 && cut < n && ents[cut].dst == ents[cut - 1].dst) ++cut;
+        split[w] = base + std::min(cut, n);
+      }
+      split[kFeChunks] = base + n;
+    }
+  }
   // Level work lists, fronts ordered by size inside a level so that warps of
   // one block tend to take the same code path.
   fp.level_ptr = sp.level_ptr;

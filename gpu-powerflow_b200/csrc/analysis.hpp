@@ -95,7 +95,20 @@ struct FactorProgram {
   std::vector<int32_t> perm, iperm;
   std::vector<int32_t> parent_panel;
   std::vector<int32_t> nchildren;
+  // Dense-front assembly program: for front p, entries [fe_ptr[p], fe_ptr[p+1])
+  // give a destination inside the (fsz x (fsz + 1)) front (last column = rhs)
+  // and a source: kind (bits 62-63) 0 = Jacobian CSR position, 1 = CB element
+  // (global index), 2 = mismatch row.  Sorted by destination; fe_split
+  // (kFeChunks + 1 per front) cuts the list at destination boundaries into
+  // chunks that different warps can accumulate without sharing a destination.
+  std::vector<int64_t> fe_ptr;
+  std::vector<int32_t> fe_dst;
+  std::vector<int64_t> fe_src;
+  std::vector<int64_t> fe_split;
 };
+
+constexpr int kFeChunks = 8;
+constexpr int kFeKindShift = 62;
 
 FactorProgram build_factor_program(const SymbolicPlan& sp);
 

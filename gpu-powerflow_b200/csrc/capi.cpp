@@ -92,6 +92,7 @@ bool copy_plan_array(const Engine& e, const char* name, int32_t* out, int64_t ca
   CUPF_ARR("fp_crow_r", fp.crow_r)
   CUPF_ARR("fp_level_ptr", fp.level_ptr)
   CUPF_ARR("fp_level_fronts", fp.level_fronts)
+  CUPF_ARR("fe_dst", fp.fe_dst)
   CUPF_ARR("jac_row_ptr", ja.row_ptr)
   CUPF_ARR("jac_col_idx", ja.col_idx)
   CUPF_ARR("map11", ja.map11)
@@ -581,6 +582,41 @@ pf_status pf_evaluate(pf_handle h, const double* V, const double* sbus, int32_t 
     if (!h->eng->initialized()) throw std::runtime_error("pf_evaluate: initialize() must be called first");
     h->eng->evaluate_host(V, sbus, batch, F, J);
   })
+}
+
+pf_status pf_set_profiling(pf_handle h, int32_t enabled) {
+  if (!h || !h->eng) return PF_INVALID_ARGUMENT;
+  h->eng->set_profiling(enabled != 0);
+  return PF_OK;
+}
+
+pf_status pf_stage_times(pf_handle h, double* times_ms, int64_t* launches) {
+  if (!h || !h->eng) return PF_INVALID_ARGUMENT;
+  h->eng->stage_times_ms(times_ms, launches);
+  return PF_OK;
+}
+
+pf_status pf_plan_array64(pf_handle h, const char* name, int64_t* out, int64_t capacity, int64_t* len) {
+  if (!h || !h->eng || h->eng->dim() <= 0) return PF_INVALID_ARGUMENT;
+  const auto& fp = h->eng->program();
+  const std::string n(name ? name : "");
+  const std::vector<int64_t>* v = nullptr;
+  if (n == "fe_split") v = &fp.fe_split;
+  if (n == "fe_src") v = &fp.fe_src;
+  if (n == "fe_ptr") v = &fp.fe_ptr;
+  if (n == "u_off") v = &fp.u_off;
+  if (n == "l_off") v = &fp.l_off;
+  if (n == "cb_off") v = &fp.cb_off;
+  if (!v) {
+    h->err = "unknown int64 plan array: " + n;
+    return PF_INVALID_ARGUMENT;
+  }
+  if (len) *len = (int64_t)v->size();
+  if (out) {
+    if (capacity < (int64_t)v->size()) return PF_INVALID_ARGUMENT;
+    if (!v->empty()) std::memcpy(out, v->data(), v->size() * sizeof(int64_t));
+  }
+  return PF_OK;
 }
 
 pf_status pf_singular_flags(pf_handle h, int32_t* out_host, int32_t batch) {

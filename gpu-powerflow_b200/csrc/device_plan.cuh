@@ -37,6 +37,10 @@ struct DevPlan {
   const int* perm = nullptr;   // permuted index -> Jacobian row
   const int* iperm = nullptr;  // Jacobian row -> permuted index
   const int* level_fronts = nullptr;
+  // dense-front assembly program (analysis.hpp FactorProgram::fe_*)
+  const long long* fe_split = nullptr;  // 9 per front
+  const int* fe_dst = nullptr;
+  const long long* fe_src = nullptr;
 };
 
 // Ybus and the Jacobian maps of one grid.

@@ -93,7 +93,7 @@ struct Engine::Impl {
   DBuf y_ptr, y_col, y_row, y_re, y_im, map11, map21, map12, map22, bus_fa, bus_fm, pv, pq, jt_ptr, jt_row, jt_q;
   // factor program
   DBuf fsz, nc, first, front_ptr, front_rows, u_off, l_off, cb_off, tv_off, arow_ptr, arow_q, arow_col, crow_ptr,
-      crow_child, crow_r, asm_ptr, asm_local, perm, iperm, level_fronts;
+      crow_child, crow_r, asm_ptr, asm_local, perm, iperm, level_fronts, fe_split, fe_dst, fe_src;
   std::vector<LevelLaunch> levels;
   int64_t tv_total = 0;
   DevGrid g;
@@ -101,19 +101,36 @@ struct Engine::Impl {
   // workspace
   int Bp_cap = 0, B = 0, Bp = 0;
   DBuf v_re, v_im, va, vm, s_re, s_im, i_re, i_im, F, norm, sing;
-  DBuf J, U, L, CB, Y, X;
+  DBuf J, U, L, CB, Y, X, front_scratch;
+  size_t front_scratch_elems = 0;
   DBuf stage_in, stage_out, fin;
   DBuf G, R, lam, dlam, TV, W, Z, Jd;
   unsigned long long* h_norm = nullptr;
   double* h_final = nullptr;
   int h_cap = 0;
   cudaStream_t own = nullptr;
+  // stage timers
+  std::vector<cudaEvent_t> ev_pool;
+  size_t ev_used = 0;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_pairs;
+  cudaEvent_t ev_open[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  double stage_ms[5] = {0, 0, 0, 0, 0};
+  int64_t stage_launches[5] = {0, 0, 0, 0, 0};
+  cudaEvent_t next_event() {
+    if (ev_used == ev_pool.size()) {
+      cudaEvent_t e;
+      cudaEventCreate(&e);
+      ev_pool.push_back(e);
+    }
+    return ev_pool[ev_used++];
+  }
   // graph of one iteration tail (+ the next mismatch), per batch
   cudaGraphExec_t exec = nullptr;
   int graph_Bp = -1;
   bool graph_double = false;
 
   ~Impl() {
+    for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
     if (exec) cudaGraphExecDestroy(exec);
     if (h_norm) cudaFreeHost(h_norm);
     if (h_final) cudaFreeHost(h_final);
@@ -269,6 +286,9 @@ void Engine::upload_plan() {
   d.perm.upload(fp_.perm);
   d.iperm.upload(fp_.iperm);
   d.level_fronts.upload(fp_.level_fronts);
+  d.fe_split.upload(to_ll(fp_.fe_split));
+  d.fe_dst.upload(fp_.fe_dst);
+  d.fe_src.upload(to_ll(fp_.fe_src));
   d.levels.clear();
   for (int32_t L = 0; L < fp_.num_levels; ++L) {
     LevelLaunch lv;
@@ -307,6 +327,9 @@ void Engine::upload_plan() {
   pl.perm = d.perm.as<int>();
   pl.iperm = d.iperm.as<int>();
   pl.level_fronts = d.level_fronts.as<int>();
+  pl.fe_split = d.fe_split.as<long long>();
+  pl.fe_dst = d.fe_dst.as<int>();
+  pl.fe_src = d.fe_src.as<long long>();
   if (!d.own) CUPF_CUDA(cudaStreamCreateWithFlags(&d.own, cudaStreamNonBlocking));
   if (d.exec) {
     cudaGraphExecDestroy(d.exec);
@@ -385,6 +408,15 @@ void Engine::ensure_workspace(int32_t B) {
     d.CB.reserve((size_t)std::max<int64_t>(fp_.cb_total, 1) * Bp * es);
     d.Y.reserve(dim * Bp * es);
     d.X.reserve(dim * Bp * es);
+    // dense fronts of levels too large for shared memory live in global scratch
+    size_t scratch = 0;
+    const size_t cap = front_smem_capacity(es);
+    for (const auto& lv : d.levels) {
+      const size_t elems = (size_t)lv.max_fsz * (lv.max_fsz + 1);
+      if (elems > cap) scratch = std::max(scratch, elems * lv.count * (Bp / kWarp));
+    }
+    d.front_scratch_elems = scratch;
+    if (scratch) d.front_scratch.reserve(scratch * kWarp * es);
     d.Bp_cap = Bp;
     if (d.exec) {
       cudaGraphExecDestroy(d.exec);
@@ -407,6 +439,45 @@ void Engine::ensure_workspace(int32_t B) {
   }
 }
 
+void Engine::stage_begin(int stage, cudaStream_t s) {
+  if (!profiling_) return;
+  auto& d = *d_;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  cudaStreamIsCapturing(s, &cs);
+  if (cs != cudaStreamCaptureStatusNone) return;
+  d.ev_open[stage] = d.next_event();
+  cudaEventRecord(d.ev_open[stage], s);
+}
+
+void Engine::stage_end(int stage, cudaStream_t s) {
+  if (!profiling_) return;
+  auto& d = *d_;
+  if (!d.ev_open[stage]) return;
+  cudaEvent_t e = d.next_event();
+  cudaEventRecord(e, s);
+  d.ev_pairs.push_back({stage, {d.ev_open[stage], e}});
+  d.ev_open[stage] = nullptr;
+}
+
+void Engine::collect_stage_times() {
+  auto& d = *d_;
+  for (auto& pr : d.ev_pairs) {
+    float ms = 0.f;
+    cudaEventSynchronize(pr.second.second);
+    cudaEventElapsedTime(&ms, pr.second.first, pr.second.second);
+    d.stage_ms[pr.first] += ms;
+  }
+  d.ev_pairs.clear();
+  d.ev_used = 0;
+}
+
+void Engine::stage_times_ms(double* out5, int64_t* launches5) const {
+  for (int i = 0; i < 5; ++i) {
+    if (out5) out5[i] = d_->stage_ms[i];
+    if (launches5) launches5[i] = d_->stage_launches[i];
+  }
+}
+
 template <typename T>
 void Engine::factor_all(cudaStream_t s, int store_l, const void* J) {
   auto& d = *d_;
@@ -424,11 +495,16 @@ void Engine::factor_all(cudaStream_t s, int store_l, const void* J) {
   a.eps = cfg_.shift_epsilon;
   a.static_pivot = (cfg_.static_pivot && cfg_.shift_epsilon > 0.0) ? 1 : 0;
   a.sing = d.sing.as<int>();
+  a.front_scratch = d.front_scratch_elems ? d.front_scratch.as<T>() : nullptr;
+  a.front_scratch_elems = d.front_scratch_elems;
+  stage_begin(2, s);
   for (const auto& lv : d.levels) {
     launch_factor_level<T, T>(lv, a, s);
     debug_check(s, "factor level");
     ++launches_;
+    ++d.stage_launches[2];
   }
+  stage_end(2, s);
 }
 
 template <typename T>
@@ -441,25 +517,34 @@ void Engine::backward_all(cudaStream_t s) {
   a.U = d.U.as<T>();
   a.Y = d.Y.as<T>();
   a.X = d.X.as<T>();
+  stage_begin(3, s);
   for (int L = (int)d.levels.size() - 1; L >= 0; --L) {
     launch_backward_level<T>(d.levels[L], a, s);
     debug_check(s, "backward level");
     ++launches_;
+    ++d.stage_launches[3];
   }
+  stage_end(3, s);
 }
 
 template <typename T>
 void Engine::iteration_tail(cudaStream_t s, int store_l) {
   auto& d = *d_;
   const DevState st = d.state();
+  stage_begin(1, s);
   launch_jacobian<T>(d.g, st, d.J.as<T>(), s);
+  stage_end(1, s);
   debug_check(s, "jacobian");
   ++launches_;
+  ++d.stage_launches[1];
   factor_all<T>(s, store_l, d.J.p);
   backward_all<T>(s);
+  stage_begin(4, s);
   launch_voltage_update<T>(d.g, d.pl, st, d.X.as<T>(), s);
+  stage_end(4, s);
   debug_check(s, "voltage update");
   ++launches_;
+  ++d.stage_launches[4];
 }
 
 template <typename T>
@@ -474,9 +559,18 @@ SolveStats Engine::run_loop(double tol, int32_t max_iter, int32_t prepare_adjoin
   for (int b = 0; b < d.B; ++b) d.h_final[b] = 0.0;
   int completed = 0;
   double gmax = 0.0;
+  for (int i = 0; i < 5; ++i) {
+    d.stage_ms[i] = 0.0;
+    d.stage_launches[i] = 0;
+  }
+  d.ev_pairs.clear();
+  d.ev_used = 0;
   if (max_iter > 0) {
+    stage_begin(0, s);
     launch_ibus_mismatch(d.g, st, s);
+    stage_end(0, s);
     ++launches_;
+    ++d.stage_launches[0];
   }
   const bool use_graph = cfg_.use_cuda_graph != 0;
   for (int it = 0; it < max_iter; ++it) {
@@ -517,8 +611,11 @@ SolveStats Engine::run_loop(double tol, int32_t max_iter, int32_t prepare_adjoin
     } else {
       iteration_tail<T>(s, 0);
       if (it + 1 < max_iter) {
+        stage_begin(0, s);
         launch_ibus_mismatch(d.g, st, s);
+        stage_end(0, s);
         ++launches_;
+        ++d.stage_launches[0];
       }
     }
   }
@@ -539,6 +636,7 @@ SolveStats Engine::run_loop(double tol, int32_t max_iter, int32_t prepare_adjoin
   if (d_final) CUPF_CUDA(cudaMemcpyAsync(d_final, d.h_final, d.B * sizeof(double), cudaMemcpyHostToDevice, s));
   CUPF_CUDA(cudaStreamSynchronize(s));
   CUPF_CUDA(cudaGetLastError());
+  if (profiling_) collect_stage_times();
   return stats;
 }
 

@@ -101,6 +101,12 @@ class Engine {
   std::vector<int32_t> singular_flags() const;  // per scenario of the last factorization
   // kernel launches issued by the last solve (for reporting)
   int64_t last_launches() const { return launches_; }
+  // Stage timers (the reference's NR.iteration.* StageScope labels,
+  // newton_solver.cpp:521-553) measured with CUDA events on the solve stream.
+  // Stages: 0 mismatch (ibus+mismatch+norm), 1 jacobian, 2 factorize,
+  // 3 solve, 4 voltage_update.  Enabling adds event records, no host syncs.
+  void set_profiling(bool on) { profiling_ = on; }
+  void stage_times_ms(double* out5, int64_t* launches5) const;
 
  private:
   struct Impl;
@@ -113,6 +119,10 @@ class Engine {
   bool adjoint_ready_ = false;
   int32_t B_ = 0;
   int64_t launches_ = 0;
+  bool profiling_ = false;
+  void stage_begin(int stage, cudaStream_t s);
+  void stage_end(int stage, cudaStream_t s);
+  void collect_stage_times();
 
   void ensure_workspace(int32_t B);
   void upload_plan();

@@ -31,7 +31,13 @@ struct FactorArgs {
   double eps = 1e-8;
   int static_pivot = 1;
   int* sing = nullptr;
+  T* front_scratch = nullptr;       // global dense fronts for levels whose front exceeds shared memory
+  size_t front_scratch_elems = 0;   // capacity in elements per scenario lane group (x 32)
 };
+
+// Front elements [fsz][fsz + 1] beyond which a level's dense fronts live in
+// global scratch instead of shared memory (227 KB per block).
+inline size_t front_smem_capacity(size_t elem_bytes) { return (227u * 1024u) / (32u * elem_bytes); }
 
 template <typename T>
 struct SweepArgs {

@@ -54,97 +54,98 @@ __device__ __forceinline__ T guarded_pivot(T piv, bool static_pivot, double eps,
 
 // ---------------------------------------------------------------------------
 // Factor + forward substitution of one level of the front tree.
-//   U  [u_total][Bp]  : pivot rows k of every front, fsz entries (L11 left of
-//                       the diagonal, U11 | U12 from it)
-//   L  [l_total][Bp]  : L21 rows (only when store_l; needed by the adjoint)
-//   CB [cb_total][Bp] : uc rows of uc + 1 entries (last = rhs update)
+//
+// One block = one front x 32 scenarios (lane = scenario).  The block
+// assembles the dense front [fsz][fsz + 1] (last column = right-hand side) in
+// shared memory from the front's destination-sorted source list -- original
+// Jacobian entries, the mismatch rows of its pivots and its children's
+// contribution blocks -- each warp accumulating its own destination chunk with
+// eight independent loads in flight, then runs the right-looking LU over the
+// nc pivot columns with the rows split across the warps, and writes
+//   U  [u_total][Bp]  : pivot rows k (L11 left of the diagonal, U11 | U12 from it)
+//   L  [l_total][Bp]  : L21 rows (only when store_l; the adjoint needs them)
+//   CB [cb_total][Bp] : uc rows of uc + 1 entries (last = right-hand-side update)
 //   Y  [dim][Bp]      : y = L^-1 P F at the pivot rows (permuted order)
+// Fronts whose dense block does not fit the shared-memory budget use a
+// caller-provided global scratch area (front_scratch), same code.
 // ---------------------------------------------------------------------------
-template <typename T, typename TJ, int FMAX, int NCMAX>
-__global__ void __launch_bounds__(kFactorWarps * kWarp)
-    k_factor_level(DevPlan pl, int level_begin, int level_count, int groups, int Bp, int ub_rows,
-                   const TJ* __restrict__ J, const double* __restrict__ F, T* __restrict__ U, T* __restrict__ L,
-                   T* __restrict__ CB, T* __restrict__ Y, int store_l, double eps, int static_pivot,
-                   int* __restrict__ sing) {
+template <typename T, typename TJ>
+__global__ void __launch_bounds__(256)
+    k_front_factor(DevPlan pl, int level_begin, int groups, int Bp, int front_elems, const TJ* __restrict__ J,
+                   const double* __restrict__ F, T* __restrict__ U, T* __restrict__ L, T* __restrict__ CB,
+                   T* __restrict__ Y, int store_l, double eps, int static_pivot, int* __restrict__ sing,
+                   T* __restrict__ front_scratch) {
   extern __shared__ unsigned char smem_raw[];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const long item = (long)blockIdx.x * (blockDim.x >> 5) + warp;
-  if (item >= (long)level_count * groups) return;
+  const int W = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int item = blockIdx.x;
   const int p = pl.level_fronts[level_begin + item / groups];
-  const int g = (int)(item % groups);
-  const size_t b = (size_t)g * kWarp + lane;
+  const size_t b = (size_t)(item % groups) * kWarp + lane;
+  const int fs = pl.fsz[p], nc = pl.nc[p], uc = fs - nc, rw = fs + 1;
+  T* Fm = front_scratch ? front_scratch + (size_t)item * front_elems * kWarp : reinterpret_cast<T*>(smem_raw);
 
-  constexpr int RW = FMAX + 1;  // row width incl. the rhs slot
-  T* ub = reinterpret_cast<T*>(smem_raw) + (size_t)warp * (ub_rows + 1) * RW * kWarp;
-  T* rb = ub + (size_t)ub_rows * RW * kWarp;
+  for (int e = threadIdx.x; e < fs * rw * kWarp; e += blockDim.x) Fm[e] = T(0);
+  __syncthreads();
 
-  const int fs = pl.fsz[p], nc = pl.nc[p], uc = fs - nc;
-  const int fr0 = pl.front_ptr[p], first = pl.first[p];
-  const long long uo = pl.u_off[p], lo = pl.l_off[p], co = pl.cb_off[p];
+  // ---- assembly ----
+  const long long* split = pl.fe_split + (size_t)p * 9;
+  for (int ch = warp; ch < 8; ch += W) {
+    const long long e1 = split[ch + 1];
+    for (long long e = split[ch]; e < e1; e += 8) {
+      T v[8];
+      int d[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        v[u] = T(0);
+        d[u] = -1;
+        if (e + u < e1) {
+          const long long src = pl.fe_src[e + u];
+          d[u] = pl.fe_dst[e + u];
+          const int kind = (int)((unsigned long long)src >> 62);
+          const size_t idx = (size_t)(src & 0x3FFFFFFFFFFFFFFFll);
+          v[u] = kind == 0 ? static_cast<T>(J[idx * Bp + b])
+                           : (kind == 1 ? CB[idx * Bp + b] : static_cast<T>(F[idx * Bp + b]));
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+        if (d[u] >= 0) Fm[(size_t)d[u] * kWarp + lane] += v[u];
+    }
+  }
+  __syncthreads();
+
+  // ---- right-looking LU over the pivot columns ----
   bool shifted = false;
-
-  for (int i = 0; i < fs; ++i) {
-    // ---- assemble row i: original entries, children's CB rows, rhs ----
-#pragma unroll
-    for (int j = 0; j < RW; ++j) rb[j * kWarp + lane] = T(0);
-    for (int e = pl.arow_ptr[fr0 + i]; e < pl.arow_ptr[fr0 + i + 1]; ++e)
-      rb[pl.arow_col[e] * kWarp + lane] += static_cast<T>(J[(size_t)pl.arow_q[e] * Bp + b]);
-    if (i < nc) rb[FMAX * kWarp + lane] = static_cast<T>(F[(size_t)pl.perm[first + i] * Bp + b]);
-    for (int e = pl.crow_ptr[fr0 + i]; e < pl.crow_ptr[fr0 + i + 1]; ++e) {
-      const int c = pl.crow_child[e], r = pl.crow_r[e];
-      const int ucc = pl.fsz[c] - pl.nc[c];
-      const T* src = CB + (size_t)(pl.cb_off[c] + (long long)r * (ucc + 1)) * Bp + b;
-      const int* al = pl.asm_local + pl.asm_ptr[c];
-      for (int cc = 0; cc < ucc; ++cc) rb[al[cc] * kWarp + lane] += src[(size_t)cc * Bp];
-      rb[FMAX * kWarp + lane] += src[(size_t)ucc * Bp];
+  for (int k = 0; k < nc; ++k) {
+    T* Fk = Fm + (size_t)k * rw * kWarp + lane;
+    if (warp == 0) Fk[k * kWarp] = guarded_pivot(Fk[k * kWarp], static_pivot != 0, eps, shifted);
+    __syncthreads();
+    const T piv = Fk[k * kWarp];
+    for (int i = k + 1 + warp; i < fs; i += W) {
+      T* Fi = Fm + (size_t)i * rw * kWarp + lane;
+      const T l = Fi[k * kWarp] / piv;
+      Fi[k * kWarp] = l;
+      for (int j = k + 1; j < rw; ++j) Fi[j * kWarp] -= l * Fk[j * kWarp];
     }
-    T row[RW];
-#pragma unroll
-    for (int j = 0; j < RW; ++j) row[j] = rb[j * kWarp + lane];
+    __syncthreads();
+  }
 
-    // ---- eliminate with the previous pivot rows ----
-    const int kmax = i < nc ? i : nc;
-#pragma unroll
-    for (int k = 0; k < NCMAX; ++k) {
-      if (k < kmax) {
-        const T* uk = ub + (size_t)k * RW * kWarp + lane;
-        const T l = row[k] / uk[k * kWarp];
-        row[k] = l;
-#pragma unroll
-        for (int j = k + 1; j < FMAX; ++j)
-          if (j < fs) row[j] -= l * uk[j * kWarp];
-        row[FMAX] -= l * uk[FMAX * kWarp];
-      }
+  // ---- write U, y, L21, CB ----
+  const long long uo = pl.u_off[p], lo = pl.l_off[p], co = pl.cb_off[p];
+  const int first = pl.first[p];
+  for (int e = warp; e < nc * fs; e += W) {
+    const int k = e / fs, j = e - k * fs;
+    U[(size_t)(uo + e) * Bp + b] = Fm[(size_t)(k * rw + j) * kWarp + lane];
+  }
+  for (int k = warp; k < nc; k += W) Y[(size_t)(first + k) * Bp + b] = Fm[(size_t)(k * rw + fs) * kWarp + lane];
+  if (store_l) {
+    for (int e = warp; e < uc * nc; e += W) {
+      const int ii = e / nc, j = e - ii * nc;
+      L[(size_t)(lo + e) * Bp + b] = Fm[(size_t)((nc + ii) * rw + j) * kWarp + lane];
     }
-
-    if (i < nc) {
-      // ---- pivot row: guard the pivot, keep it for later rows, write U / y ----
-#pragma unroll
-      for (int k = 0; k < NCMAX; ++k)
-        if (k == i) row[k] = guarded_pivot(row[k], static_pivot != 0, eps, shifted);
-      T* ui = ub + (size_t)i * RW * kWarp + lane;
-#pragma unroll
-      for (int j = 0; j < RW; ++j) ui[j * kWarp] = row[j];
-      T* urow = U + (size_t)(uo + (long long)i * fs) * Bp + b;
-#pragma unroll
-      for (int j = 0; j < FMAX; ++j)
-        if (j < fs) urow[(size_t)j * Bp] = row[j];
-      Y[(size_t)(first + i) * Bp + b] = row[FMAX];
-    } else {
-      // ---- contribution row: L21 part (optional) and CB part + rhs update ----
-      const int ii = i - nc;
-      if (store_l) {
-        T* lrow = L + (size_t)(lo + (long long)ii * nc) * Bp + b;
-#pragma unroll
-        for (int j = 0; j < NCMAX; ++j)
-          if (j < nc) lrow[(size_t)j * Bp] = row[j];
-      }
-      T* cbrow = CB + (size_t)(co + (long long)ii * (uc + 1)) * Bp + b;
-#pragma unroll
-      for (int j = 0; j < FMAX; ++j)
-        if (j >= nc && j < fs) cbrow[(size_t)(j - nc) * Bp] = row[j];
-      cbrow[(size_t)uc * Bp] = row[FMAX];
-    }
+  }
+  for (int e = warp; e < uc * (uc + 1); e += W) {
+    const int ii = e / (uc + 1), jj = e - ii * (uc + 1);
+    CB[(size_t)(co + e) * Bp + b] = Fm[(size_t)((nc + ii) * rw + nc + jj) * kWarp + lane];
   }
   if (shifted) sing[b] = 1;
 }
@@ -339,27 +340,6 @@ inline int bucket_of(int fmax) {
   return -1;
 }
 
-template <typename T, typename TJ, int FMAX, int NCMAX>
-void launch_factor_t(const LevelLaunch& lv, const FactorArgs<T, TJ>& a, cudaStream_t s) {
-  constexpr int RW = FMAX + 1;
-  // per warp: the level's pivot rows plus one assembly row, 32 scenarios wide
-  const size_t per_warp = (size_t)(lv.max_nc + 1) * RW * kWarp * sizeof(T);
-  const int warps = (int)std::min<size_t>(kFactorWarps, kSmemLimit / per_warp);
-  if (warps < 1) throw std::runtime_error("front too large for the shared-memory budget of the factor kernel");
-  const size_t smem = per_warp * warps;
-  auto kern = k_factor_level<T, TJ, FMAX, NCMAX>;
-  static size_t configured = 0;
-  if (smem > configured) {
-    const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) throw std::runtime_error(std::string("factor kernel smem attribute: ") + cudaGetErrorString(e));
-    configured = smem;
-  }
-  const long items = (long)lv.count * a.groups;
-  const unsigned blocks = (unsigned)((items + warps - 1) / warps);
-  kern<<<blocks, warps * kWarp, smem, s>>>(a.plan, lv.begin, lv.count, a.groups, a.Bp, lv.max_nc, a.J, a.F, a.U,
-                                          a.L, a.CB, a.Y, a.store_l, a.eps, a.static_pivot, a.sing);
-}
-
 template <typename T, int FMAX, int NCMAX>
 void launch_backward_t(const LevelLaunch& lv, const SweepArgs<T>& a, cudaStream_t s) {
   const long items = (long)lv.count * a.groups;
@@ -406,13 +386,27 @@ void launch_lt_t(const LevelLaunch& lv, const AdjointSweepArgs<T>& a, cudaStream
 template <typename T, typename TJ>
 void launch_factor_level(const LevelLaunch& lv, const FactorArgs<T, TJ>& a, cudaStream_t s) {
   if (lv.count == 0) return;
-  if (lv.max_nc <= 8) {
-#define CALL(F, N) launch_factor_t<T, TJ, (F < 8 ? 8 : F), N>(lv, a, s)
-    CUPF_BUCKET_SWITCH(8, CALL)
-#undef CALL
-  } else {
-    throw std::runtime_error("panels wider than 8 columns are not supported (max_panel_width <= 8)");
+  const int fmax = lv.max_fsz;
+  const size_t elems = (size_t)fmax * (fmax + 1);
+  const size_t smem = elems * kWarp * sizeof(T);
+  const int warps = fmax <= 8 ? 2 : (fmax <= 20 ? 4 : 8);
+  const bool in_smem = smem <= kSmemLimit;
+  auto kern = k_front_factor<T, TJ>;
+  if (in_smem) {
+    static size_t configured = 0;
+    if (smem > configured) {
+      const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess)
+        throw std::runtime_error(std::string("factor kernel smem attribute: ") + cudaGetErrorString(e));
+      configured = smem;
+    }
+  } else if (!a.front_scratch || a.front_scratch_elems < elems * (size_t)lv.count * a.groups) {
+    throw std::runtime_error("front larger than the shared-memory budget and no scratch area provided");
   }
+  const unsigned blocks = (unsigned)((long)lv.count * a.groups);
+  kern<<<blocks, warps * kWarp, in_smem ? smem : 0, s>>>(a.plan, lv.begin, a.groups, a.Bp, (int)elems, a.J, a.F, a.U,
+                                                        a.L, a.CB, a.Y, a.store_l, a.eps, a.static_pivot, a.sing,
+                                                        in_smem ? nullptr : a.front_scratch);
 }
 
 template <typename T>

@@ -480,6 +480,14 @@ class NewtonSolver:
         _check(self._lib, self._h, self._lib.pf_plan_array(self._h, name.encode(), _ptr(out), out.size, C.byref(ln)))
         return out
 
+    def plan_array64(self, name: str) -> np.ndarray:
+        ln = C.c_int64(0)
+        _check(self._lib, self._h, self._lib.pf_plan_array64(self._h, name.encode(), None, 0, C.byref(ln)))
+        out = np.zeros(ln.value, dtype=np.int64)
+        _check(self._lib, self._h, self._lib.pf_plan_array64(self._h, name.encode(), _ptr(out), out.size,
+                                                             C.byref(ln)))
+        return out
+
     def evaluate(self, V, sbus) -> tuple[np.ndarray, np.ndarray]:
         """Mismatch F [batch, dim_f] and Jacobian values [batch, nnz] at host states (verification)."""
         V, sbus = _c128(np.atleast_2d(V)), _c128(np.atleast_2d(sbus))
@@ -489,6 +497,18 @@ class NewtonSolver:
         J = np.zeros((B, inf["nnz_jacobian"]))
         _check(self._lib, self._h, self._lib.pf_evaluate(self._h, _ptr(V), _ptr(sbus), B, _ptr(F), _ptr(J)))
         return F, J
+
+    STAGES = ("mismatch", "jacobian", "factorize", "solve", "voltage_update")
+
+    def set_profiling(self, on: bool = True) -> None:
+        _check(self._lib, self._h, self._lib.pf_set_profiling(self._h, int(bool(on))))
+
+    def stage_times(self) -> dict:
+        """{stage: (ms, launches)} of the last solve (profiling must be on)."""
+        t = np.zeros(5)
+        n = np.zeros(5, dtype=np.int64)
+        _check(self._lib, self._h, self._lib.pf_stage_times(self._h, _ptr(t), _ptr(n)))
+        return {k: (float(t[i]), int(n[i])) for i, k in enumerate(self.STAGES)}
 
     def singular_flags(self, batch: int) -> np.ndarray:
         out = np.zeros(batch, dtype=np.int32)

@@ -60,7 +60,7 @@ EXPORTS = [
     "cls_plan_array",
     "pf_create", "pf_destroy", "pf_last_error", "pf_initialize", "pf_analyze_host", "pf_solve_batch", "pf_solve_batch_device",
     "pf_solve_forward_device", "pf_solve_backward_device", "pf_solve_adjoint", "pf_info", "pf_plan_array",
-    "pf_evaluate", "pf_singular_flags",
+    "pf_evaluate", "pf_set_profiling", "pf_stage_times", "pf_plan_array64", "pf_singular_flags",
 ]
 
 _vp = C.c_void_p
@@ -103,6 +103,9 @@ def _declare(lib: C.CDLL) -> None:
         "pf_info": ([_vp, _p(PfInfo)], _i32),
         "pf_plan_array": ([_vp, C.c_char_p, _vp, _i64, _p(_i64)], _i32),
         "pf_evaluate": ([_vp, _vp, _vp, _i32, _vp, _vp], _i32),
+        "pf_set_profiling": ([_vp, _i32], _i32),
+        "pf_plan_array64": ([_vp, C.c_char_p, _vp, _i64, _p(_i64)], _i32),
+        "pf_stage_times": ([_vp, _vp, _vp], _i32),
         "pf_singular_flags": ([_vp, _vp, _i32], _i32),
     }
     for name, (args, res) in s.items():

@@ -237,6 +237,15 @@ pf_status pf_plan_array(pf_handle h, const char* name, int32_t* out, int64_t cap
  * complex, sbus [batch][n_bus] complex; outputs F [batch][dim_f] and J
  * [batch][nnz_jacobian] (CSR order of "jac_col_idx"), both double. */
 pf_status pf_evaluate(pf_handle h, const double* V, const double* sbus, int32_t batch, double* F, double* J);
+/* Stage timers of the last solve (the reference's NR.iteration.* stage
+ * labels, newton_solver.cpp:521-553): times_ms[5] and launches[5] for
+ * 0 mismatch, 1 jacobian, 2 factorize, 3 solve, 4 voltage_update, measured
+ * with CUDA events on the solve stream when enabled (no extra host syncs). */
+pf_status pf_set_profiling(pf_handle h, int32_t enabled);
+pf_status pf_stage_times(pf_handle h, double* times_ms, int64_t* launches);
+/* int64 plan arrays of the engine's factor program: "fe_split", "fe_src",
+ * "u_off", "l_off", "cb_off" (same calling convention as pf_plan_array). */
+pf_status pf_plan_array64(pf_handle h, const char* name, int64_t* out, int64_t capacity, int64_t* len);
 /* Per-scenario static-pivot flags of the last factorization. */
 pf_status pf_singular_flags(pf_handle h, int32_t* out_host, int32_t batch);
 

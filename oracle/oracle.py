@@ -165,6 +165,9 @@ class Reference:
         L.ref_jacobian_analysis.argtypes = [C.c_int, _i32p, _i32p, _f64p, _i32p, C.c_int, _i32p, C.c_int,
                                             C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_void_p, C.c_void_p,
                                             C.c_void_p]
+        L.ref_nr_solve_many.restype = C.c_int
+        L.ref_nr_solve_many.argtypes = [C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p, C.c_int, _i32p, C.c_int, _i32p,
+                                        C.c_int, C.c_double, C.c_int, C.c_int, _f64p, _i32p, _f64p]
         L.ref_symbolic_run.restype = C.c_void_p
         L.ref_symbolic_run.argtypes = [C.c_int, _i32p, _i32p, C.c_int, C.c_int, C.c_int]
         L.ref_symbolic_len.restype = C.c_int
@@ -188,6 +191,19 @@ class Reference:
                                         pq.size, tol, max_iter, v, C.byref(it), C.byref(fm), C.byref(cv)))
         return {"V": v.view(np.complex128).copy(), "iterations": it.value, "final_mismatch": fm.value,
                 "converged": bool(cv.value)}
+
+    def solve_many(self, g, sbus, v0, tol: float = 1e-8, max_iter: int = 50, threads: int = 1) -> dict:
+        ip, ix, pv, pq = _i32(g.indptr), _i32(g.indices), _i32(g.pv), _i32(g.pq)
+        sbus = np.ascontiguousarray(sbus, dtype=np.complex128)
+        v0 = np.ascontiguousarray(v0, dtype=np.complex128)
+        b = sbus.shape[0]
+        v = np.zeros(2 * g.n_bus * b)
+        its = np.zeros(b, np.int32)
+        fm = np.zeros(b)
+        self._err(self.lib.ref_nr_solve_many(g.n_bus, ip, ix, _cplx(g.data), sbus.reshape(-1).view(np.float64),
+                                             v0.reshape(-1).view(np.float64), b, pv, pv.size, pq, pq.size, tol,
+                                             max_iter, threads, v, its, fm))
+        return {"V": v.view(np.complex128).reshape(b, g.n_bus), "iterations": its, "final_mismatch": fm}
 
     def adjoint(self, g, sbus, v0, grad_va, grad_vm, tol: float = 1e-8, max_iter: int = 50) -> dict:
         ip, ix, pv, pq = _i32(g.indptr), _i32(g.indices), _i32(g.pv), _i32(g.pq)

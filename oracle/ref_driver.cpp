@@ -13,6 +13,7 @@
 #include <cstring>
 #include <exception>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "newton_solver/core/newton_solver.hpp"
@@ -93,6 +94,51 @@ int ref_nr_adjoint(int n_bus, const int32_t* indptr, const int32_t* indices, con
     g_error = e.what();
     return 1;
   }
+}
+
+// `count` independent cases spread over `threads` host threads, one reference
+// NewtonSolver per thread (the CPU pipeline is batch-1 only, pipeline.hpp:121).
+// sbus / v0 rows have stride 2 * n_bus doubles.
+int ref_nr_solve_many(int n_bus, const int32_t* indptr, const int32_t* indices, const double* ydata,
+                      const double* sbus, const double* v0, int count, const int32_t* pv, int n_pv,
+                      const int32_t* pq, int n_pq, double tol, int max_iter, int threads, double* v_out,
+                      int32_t* iterations, double* final_mismatch) {
+  if (threads < 1) threads = 1;
+  std::vector<std::thread> pool;
+  std::vector<std::string> errs(threads);
+  for (int t = 0; t < threads; ++t) {
+    pool.emplace_back([&, t] {
+      try {
+        NewtonOptions opts;
+        opts.backend = BackendKind::CPU;
+        NewtonSolver solver(opts);
+        const YbusView y = make_view(n_bus, indptr, indices, ydata);
+        solver.initialize(y, pv, n_pv, pq, n_pq);
+        NRConfig cfg;
+        cfg.tolerance = tol;
+        cfg.max_iter = max_iter;
+        const size_t stride = 2 * (size_t)n_bus;
+        for (int c = t; c < count; c += threads) {
+          NRResult res;
+          solver.solve(y, reinterpret_cast<const std::complex<double>*>(sbus + c * stride),
+                       reinterpret_cast<const std::complex<double>*>(v0 + c * stride), pv, n_pv, pq, n_pq, cfg,
+                       SolveOptions{}, res);
+          if (v_out) std::memcpy(v_out + c * stride, res.V.data(), sizeof(double) * stride);
+          if (iterations) iterations[c] = res.iterations;
+          if (final_mismatch) final_mismatch[c] = res.final_mismatch;
+        }
+      } catch (const std::exception& e) {
+        errs[t] = e.what();
+      }
+    });
+  }
+  for (auto& th : pool) th.join();
+  for (auto& e : errs)
+    if (!e.empty()) {
+      g_error = e;
+      return 1;
+    }
+  return 0;
 }
 
 // make_jacobian_indexing + JacobianPatternGenerator + JacobianMapBuilder
