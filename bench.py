@@ -26,7 +26,6 @@ import argparse
 import json
 import os
 import statistics
-import subprocess
 import sys
 import time
 from pathlib import Path
@@ -54,53 +53,55 @@ def _peaks() -> dict:
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and throttle reasons sampled by NVML from a background thread
+    during the timed region (200 ms period; NVML reads only, no settings)."""
 
-    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"),
+               ("hw_power_brake", "nvmlClocksEventReasonHwPowerBrakeSlowdown"))
 
-    def __init__(self, index: int):
-        self.index = index
-        self.proc = None
+    def __init__(self, index: int, period: float = 0.2):
+        self.index, self.period = index, period
+        self.sm, self.reasons, self.max_mhz = [], set(), None
+        self._stop = None
 
     def __enter__(self):
+        import threading
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            import pynvml as nv
+            nv.nvmlInit()
+            h = nv.nvmlDeviceGetHandleByIndex(self.index)
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
         except Exception:
-            self.proc = None
+            return self
+        self._stop = threading.Event()
+
+        def run():
+            while True:
+                try:
+                    self.sm.append(float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)))
+                    bits = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    for name, attr in self.REASONS:
+                        if bits & getattr(nv, attr, 0):
+                            self.reasons.add(name)
+                except Exception:
+                    pass
+                if self._stop.wait(self.period):
+                    break
+        self._thread = threading.Thread(target=run, daemon=True)
+        self._thread.start()
         return self
 
     def __exit__(self, *a):
-        self.lines = []
-        if self.proc is not None:
-            self.proc.terminate()
-            try:
-                out, _ = self.proc.communicate(timeout=5)
-            except Exception:
-                self.proc.kill()
-                out = ""
-            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+        if self._stop is not None:
+            self._stop.set()
+            self._thread.join(timeout=5)
 
     def summary(self) -> dict:
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in getattr(self, "lines", []):
-            f = [x.strip() for x in ln.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                mx = float(f[2])
-            except ValueError:
-                continue
-            for nm, v in zip(names, f[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(nm)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        return {"sm_mhz": statistics.median(self.sm) if self.sm else None, "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(self.sm)}
 
 
 def _dist():
@@ -199,7 +200,7 @@ def run_engine(args) -> None:
 
     with ClockSampler(local) as clk:
         t_mix, conv_mix, it_mix, launches = timed(mixed, args.steps, args.warmup)
-    t_64, conv_64, it_64, _ = timed(fp64, args.steps, args.warmup)
+        t_64, conv_64, it_64, _ = timed(fp64, args.steps, args.warmup)
 
     ms_mix = statistics.mean(t_mix)
     ms_mix_max = _reduce(ms_mix, "max", world, dev)
@@ -208,7 +209,10 @@ def run_engine(args) -> None:
     ms_64 = _reduce(statistics.mean(t_64), "max", world, dev)
     value_64 = _reduce(conv_64 / args.steps, "sum", world, dev) / (ms_64 / 1e3)
 
-    # e2e: public API with host buffers (H2D + D2H inside the timed region)
+    # e2e: public API with pinned host buffers (H2D + D2H inside the timed region)
+    sbus_p = torch.from_numpy(sbus_h).pin_memory()
+    v0_p = torch.from_numpy(v0_h).pin_memory()
+    sbus_h, v0_h = sbus_p.numpy(), v0_p.numpy()
     for _ in range(args.warmup):
         mixed.solve_batch(g.indptr, g.indices, g.data, g.n_bus, g.n_bus, sbus_h, v0_h, g.pv, g.pq, cfg)
     _barrier(world)

@@ -7,6 +7,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <numeric>
 #include <stdexcept>
 #include <string>
@@ -135,6 +136,11 @@ namespace {
 
 using Graph = std::pair<std::vector<idx_t>, std::vector<idx_t>>;  // (xadj, adjncy)
 
+// METIS keeps its random-number state in globals: two engines analysing at the
+// same time from different threads would race and could get different
+// orderings, so every METIS call holds this lock.
+std::mutex g_metis_mutex;
+
 void metis_options(idx_t* opt, int seed) {
   METIS_SetDefaultOptions(opt);
   opt[METIS_OPTION_NUMBERING] = 0;
@@ -152,7 +158,12 @@ std::vector<int32_t> nodend(const Graph& g, int seed) {
   idx_t opt[METIS_NOPTIONS];
   metis_options(opt, seed);
   std::vector<idx_t> xa(g.first), ad(g.second), p(n), ip(n);
-  if (METIS_NodeND(&nv, xa.data(), ad.data(), nullptr, opt, p.data(), ip.data()) != METIS_OK) return perm;
+  int st;
+  {
+    std::lock_guard<std::mutex> lock(g_metis_mutex);
+    st = METIS_NodeND(&nv, xa.data(), ad.data(), nullptr, opt, p.data(), ip.data());
+  }
+  if (st != METIS_OK) return perm;
   for (int32_t i = 0; i < n; ++i) perm[i] = static_cast<int32_t>(p[i]);
   return perm;
 }
@@ -190,8 +201,12 @@ std::vector<int32_t> nd_recurse(const Graph& g, int depth, int base_thr, int see
   idx_t opt[METIS_NOPTIONS];
   metis_options(opt, seed);
   std::vector<idx_t> xa(g.first), ad(g.second);
-  if (METIS_ComputeVertexSeparator(&nv, xa.data(), ad.data(), nullptr, opt, &sep, part.data()) != METIS_OK)
-    return nodend(g, seed);
+  int st;
+  {
+    std::lock_guard<std::mutex> lock(g_metis_mutex);
+    st = METIS_ComputeVertexSeparator(&nv, xa.data(), ad.data(), nullptr, opt, &sep, part.data());
+  }
+  if (st != METIS_OK) return nodend(g, seed);
   std::vector<int32_t> m0, m1;
   const Graph g0 = induced(g, part, 0, m0);
   const Graph g1 = induced(g, part, 1, m1);

@@ -62,7 +62,7 @@ typedef struct {
   int32_t matching;             /* 0 = None */
   int32_t pivot_strategy;       /* CLS_PIVOT_* */
   int32_t serial_nd;            /* 1 = one METIS_NodeND call, 0 = separator recursion */
-  int32_t max_panel_width;      /* 1..16 */
+  int32_t max_panel_width;      /* 1..8 (front kernels are built for panels of at most 8 pivots) */
   double shift_retry_epsilon;   /* static-shift threshold and magnitude */
 } cls_config;
 

@@ -395,6 +395,10 @@ int METIS_SetDefaultOptions(orc_idx_t* options);
 int METIS_NodeND(orc_idx_t* nvtxs, orc_idx_t* xadj, orc_idx_t* adjncy, orc_idx_t* vwgt,
                  orc_idx_t* options, orc_idx_t* perm, orc_idx_t* iperm);
 
+/* METIS keeps its random-number state in globals, so concurrent calls from
+ * several threads race and can return different orderings: serialize them. */
+static pthread_mutex_t g_metis_lock = PTHREAD_MUTEX_INITIALIZER;
+
 int orc_nd_order(int n, const int32_t* Ap, const int32_t* Ai, int32_t* perm) {
   /* symmetric adjacency without the diagonal, sorted + deduplicated */
   int32_t* deg = (int32_t*)calloc(n + 1, sizeof(int32_t));
@@ -438,7 +442,10 @@ int orc_nd_order(int n, const int32_t* Ap, const int32_t* Ai, int32_t* perm) {
     orc_idx_t nv = n;
     orc_idx_t* p = (orc_idx_t*)malloc(sizeof(orc_idx_t) * n);
     orc_idx_t* ip = (orc_idx_t*)malloc(sizeof(orc_idx_t) * n);
-    if (METIS_NodeND(&nv, xadj, adjncy, NULL, opt, p, ip) != 1) {
+    pthread_mutex_lock(&g_metis_lock);
+    const int st = METIS_NodeND(&nv, xadj, adjncy, NULL, opt, p, ip);
+    pthread_mutex_unlock(&g_metis_lock);
+    if (st != 1) {
       for (int i = 0; i < n; ++i) perm[i] = i;
       rc = 1;
     } else {

@@ -1,0 +1,138 @@
+"""Regenerate the golden fixtures in this folder.
+
+    python tests/golden/make_golden.py [--ref-root PATH]
+
+Every number here comes from the REFERENCE itself, built from its own sources
+by oracle/Makefile into oracle/_ref/libcupf_ref.so (its CPU NewtonSolver,
+cuPF/cpp/src/newton_solver/core/newton_solver.cpp, and its symbolic analysis,
+custom_linear_solver/src/analyze/pipeline.cpp + lower.cu host code), or from the
+reference's own linear-system datasets
+(custom_linear_solver/tests/datasets/power/<case>/{J.mtx,F.mtx}).
+
+Outputs:
+  two_bus.npz            reference NR on the analytic 2-bus case
+                         (cuPF/tests/unit/small_cases.cpp:9-31)
+  nr_<grid>.npz          reference NR (V, iterations, final mismatch) on seeded
+                         scenarios of the synthetic grids, tol 1e-8 / max 10 and
+                         tol 1e-12 / max 30
+  adjoint_<grid>.npz     reference solve_adjoint (lambda, grad_p, grad_q) at the
+                         converged state for seeded dL/dVa, dL/dVm
+  jacobian_118.npz       reference Jacobian pattern + scatter maps (118-bus)
+  symbolic_118.npz       every reference symbolic-plan array for the 118-bus
+                         Jacobian (serial nested dissection)
+  linsys_<case>.npz      the reference datasets' J (CSR) and F
+  hashes.json            sha256 of every Jacobian-analysis and symbolic-plan
+                         array for all synthetic grids and dataset patterns
+"""
+from __future__ import annotations
+
+import argparse
+import hashlib
+import json
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ROOT = HERE.parent.parent
+for p in (ROOT / "gpu-powerflow_b200", ROOT):
+    if str(p) not in sys.path:
+        sys.path.insert(0, str(p))
+
+from cupf import grids as G  # noqa: E402
+from oracle import oracle as orc  # noqa: E402
+
+DATASETS = ("case118", "case1354pegase")
+SYMBOLIC_KEYS = ("perm", "iperm", "parent", "Lp", "Li_sorted", "panel_first", "panel_ncols", "panel_width",
+                 "panel_of", "front_ptr", "front_rows", "panel_parent", "asm_ptr", "asm_idx", "asm_local",
+                 "plevel", "panel_level_ptr", "plcols_level", "front_off", "a_pos_csr", "graph_xadj",
+                 "graph_adjncy", "sym_col_ptr", "sym_row_idx")
+JAC_KEYS = ("row_ptr", "col_idx", "map11", "map21", "map12", "map22", "diag11", "diag21", "diag12", "diag22")
+
+
+def digest(a) -> str:
+    return hashlib.sha256(np.ascontiguousarray(np.asarray(a), dtype=np.int64).tobytes()).hexdigest()
+
+
+class _Case:
+    """Minimal grid-like view of the 2-bus case for the oracle wrappers."""
+
+    def __init__(self, c: dict):
+        self.indptr, self.indices, self.data = c["indptr"], c["indices"], c["data"]
+        self.pv, self.pq, self.n_bus = c["pv"], c["pq"], 2
+        self.dim_f = self.pv.size + 2 * self.pq.size
+
+
+def read_mtx(path: Path):
+    import scipy.io
+    import scipy.sparse as sp
+
+    m = scipy.io.mmread(str(path))
+    if sp.issparse(m):
+        m = sp.csr_matrix(m)
+        m.sort_indices()
+        return m
+    return np.asarray(m).reshape(-1)
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref-root", default="/root/reference")
+    args = ap.parse_args()
+    ref = orc.Reference()
+    hashes: dict = {}
+
+    c2 = G.two_bus_case()
+    g2 = _Case(c2)
+    r = ref.solve(g2, c2["sbus"], c2["v0"], 1e-8, 20)
+    np.savez(HERE / "two_bus.npz", V=r["V"], iterations=r["iterations"], final_mismatch=r["final_mismatch"],
+             expected=c2["expected_v"])
+
+    grids = {"118": G.grid_118, "500": G.grid_500, "2000": G.grid_2000, "10000": G.grid_10000}
+    for name, mk in grids.items():
+        g = mk()
+        ja = ref.jacobian_analysis(g)
+        sym = ref.symbolic(ja["row_ptr"], ja["col_idx"], parallel_nd=False)
+        hashes[f"grid{name}"] = {"jacobian": {k: digest(ja[k]) for k in JAC_KEYS},
+                                 "symbolic": {k: digest(sym[k]) for k in SYMBOLIC_KEYS},
+                                 "front_total": int(sym["front_total"][0]), "dim": int(ja["row_ptr"].size - 1),
+                                 "nnz": int(ja["col_idx"].size)}
+        if name == "118":
+            np.savez_compressed(HERE / "jacobian_118.npz", **{k: ja[k] for k in JAC_KEYS})
+            np.savez_compressed(HERE / "symbolic_118.npz", **{k: sym[k] for k in SYMBOLIC_KEYS})
+        if name in ("118", "2000"):
+            nsc = 4 if name == "118" else 2
+            S = g.scenarios(nsc, seed=777)
+            out = {"sbus": S, "v0": g.flat_start(nsc)}
+            for tag, tol, mi in (("t8", 1e-8, 10), ("t12", 1e-12, 30)):
+                rs = [ref.solve(g, S[b], out["v0"][b], tol, mi) for b in range(nsc)]
+                out[f"V_{tag}"] = np.stack([x["V"] for x in rs])
+                out[f"it_{tag}"] = np.array([x["iterations"] for x in rs], np.int32)
+                out[f"fm_{tag}"] = np.array([x["final_mismatch"] for x in rs])
+            np.savez_compressed(HERE / f"nr_{name}.npz", **out)
+            rng = np.random.default_rng(31 + int(name))
+            ga, gm = rng.standard_normal(g.n_bus), rng.standard_normal(g.n_bus)
+            ad = ref.adjoint(g, S[0], out["v0"][0], ga, gm, 1e-12, 30)
+            np.savez_compressed(HERE / f"adjoint_{name}.npz", sbus=S[0], v0=out["v0"][0], grad_va=ga, grad_vm=gm,
+                                V=ad["V"], lam=ad["lambda"], grad_p=ad["grad_p"], grad_q=ad["grad_q"],
+                                residual=ad["residual"])
+
+    droot = Path(args.ref_root) / "custom_linear_solver/tests/datasets/power"
+    for case in DATASETS:
+        J = read_mtx(droot / case / "J.mtx")
+        F = read_mtx(droot / case / "F.mtx")
+        meta = json.loads((droot / case / "metadata.json").read_text())
+        rp, ci = J.indptr.astype(np.int32), J.indices.astype(np.int32)
+        np.savez_compressed(HERE / f"linsys_{case}.npz", row_ptr=rp, col_idx=ci, values=J.data, F=F,
+                            mismatch_inf_norm=meta["mismatch_inf_norm"])
+        sym = ref.symbolic(rp, ci, parallel_nd=False)
+        hashes[case] = {"symbolic": {k: digest(sym[k]) for k in SYMBOLIC_KEYS},
+                        "front_total": int(sym["front_total"][0]), "dim": int(rp.size - 1), "nnz": int(ci.size)}
+
+    (HERE / "hashes.json").write_text(json.dumps(hashes, indent=1, sort_keys=True) + "\n")
+    print("golden fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main()

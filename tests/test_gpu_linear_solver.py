@@ -1,0 +1,130 @@
+"""The batched sparse solver (cls_* ABI, custom_linear_solver::Solver phases) on
+the reference's own linear-system datasets: real Newton Jacobians of case118
+and case1354pegase (custom_linear_solver/tests/datasets/power/<case>/J.mtx, F.mtx).
+
+The reference checks these with a relative residual (run_custom_solver.cu); the
+same check here, plus agreement with a FP64 SuperLU solve.
+"""
+from pathlib import Path
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+import scipy.sparse.linalg as spla
+
+import cupf
+from conftest import gpu_available
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not gpu_available(), reason="needs a CUDA device")]
+GOLD = Path(__file__).resolve().parent / "golden"
+
+
+def load(case):
+    d = np.load(GOLD / f"linsys_{case}.npz")
+    n = d["row_ptr"].size - 1
+    A = sp.csr_matrix((d["values"], d["col_idx"], d["row_ptr"]), shape=(n, n))
+    return d, A
+
+
+def batch_values(d, B, rng):
+    """B value sets on the same pattern: the dataset J with +-2 % perturbations."""
+    base = d["values"]
+    v = np.repeat(base[None, :], B, axis=0)
+    if B > 1:
+        v[1:] *= 1.0 + 0.02 * rng.uniform(-1, 1, size=(B - 1, base.size))
+    return v
+
+
+@pytest.mark.parametrize("case", ["case118", "case1354pegase"])
+@pytest.mark.parametrize("precision,tol", [(cupf.CustomPrecision.FP64, 1e-11), (cupf.CustomPrecision.FP32, 2e-4)])
+def test_factor_solve_residual(case, precision, tol):
+    import torch
+
+    d, A = load(case)
+    rng = np.random.default_rng(1)
+    B = 35
+    vals = batch_values(d, B, rng)
+    rhs = np.repeat(d["F"][None, :], B, axis=0) + 0.1 * rng.standard_normal((B, A.shape[0]))
+    ls = cupf.LinearSolver(cupf.SolverConfig(precision=int(precision), serial_nd=True))
+    ls.set_data(d["row_ptr"], d["col_idx"])
+    ls.analyze()
+    ls.setup(B)
+    dt = torch.float64 if precision == cupf.CustomPrecision.FP64 else torch.float32
+    ls.factorize(torch.tensor(vals, dtype=dt, device="cuda"))
+    x = ls.solve(torch.tensor(rhs, dtype=torch.float64, device="cuda")).cpu().numpy()
+    xt = ls.solve_transpose(torch.tensor(rhs, dtype=torch.float64, device="cuda")).cpu().numpy()
+    assert not ls.singular_flags().any()
+    for b in range(B):
+        Ab = sp.csr_matrix((vals[b], d["col_idx"], d["row_ptr"]), shape=A.shape)
+        r = np.linalg.norm(Ab @ x[b] - rhs[b]) / np.linalg.norm(rhs[b])
+        rt = np.linalg.norm(Ab.T @ xt[b] - rhs[b]) / np.linalg.norm(rhs[b])
+        assert r <= tol and rt <= tol, (b, r, rt)
+    if precision == cupf.CustomPrecision.FP64:
+        ref = spla.spsolve(sp.csc_matrix(A), rhs[0])
+        assert np.abs(x[0] - ref).max() <= 1e-9 * np.abs(ref).max()
+
+
+def test_float32_solution_buffers():
+    """rhs/solution type pairs f64/f32 and f32/f32 (solver.cpp:192-210)."""
+    import torch
+
+    d, A = load("case118")
+    ls = cupf.LinearSolver(cupf.SolverConfig(precision=int(cupf.CustomPrecision.FP32)))
+    ls.set_data(d["row_ptr"], d["col_idx"])
+    ls.analyze()
+    ls.setup(2)
+    ls.factorize(torch.tensor(np.stack([d["values"]] * 2), dtype=torch.float32, device="cuda"))
+    rhs = torch.tensor(np.stack([d["F"]] * 2), dtype=torch.float64, device="cuda")
+    x64 = ls.solve(rhs).cpu().numpy()
+    x32 = ls.solve(rhs, out=torch.empty(rhs.shape, dtype=torch.float32, device="cuda")).cpu().numpy()
+    xf = ls.solve(rhs.float()).cpu().numpy()
+    assert np.abs(x32 - x64).max() <= 1e-5 * np.abs(x64).max()
+    assert np.abs(xf - x64).max() <= 1e-3 * np.abs(x64).max()
+
+
+def test_device_pattern_upload():
+    import torch
+
+    d, A = load("case118")
+    ls = cupf.LinearSolver(cupf.SolverConfig(precision=int(cupf.CustomPrecision.FP64)))
+    ls.set_data(torch.tensor(d["row_ptr"], device="cuda"), torch.tensor(d["col_idx"], device="cuda"))
+    ls.analyze()
+    ls.setup(1)
+    ls.factorize(torch.tensor(d["values"][None, :], device="cuda"))
+    x = ls.solve(torch.tensor(d["F"][None, :], device="cuda")).cpu().numpy()[0]
+    assert np.linalg.norm(A @ x - d["F"]) <= 1e-11 * np.linalg.norm(d["F"])
+
+
+def test_zero_pivot_sets_singular_flag():
+    """A structurally present but numerically zero row: the static diagonal shift
+    (PivotStrategy::StaticDiagonalShift) replaces the zero pivot and flags the
+    scenario, the other scenarios stay unflagged."""
+    import torch
+
+    d, A = load("case118")
+    vals = np.stack([d["values"]] * 3)
+    r0, r1 = d["row_ptr"][5], d["row_ptr"][6]
+    vals[1, r0:r1] = 0.0
+    ls = cupf.LinearSolver(cupf.SolverConfig(precision=int(cupf.CustomPrecision.FP64)))
+    ls.set_data(d["row_ptr"], d["col_idx"])
+    ls.analyze()
+    ls.setup(3)
+    ls.factorize(torch.tensor(vals, device="cuda"))
+    flags = ls.singular_flags()
+    assert flags[1] != 0 and flags[0] == 0 and flags[2] == 0
+    x = ls.solve(torch.tensor(np.stack([d["F"]] * 3), device="cuda")).cpu().numpy()
+    assert np.isfinite(x[0]).all() and np.isfinite(x[2]).all()
+
+
+def test_state_errors():
+    import torch
+
+    d, _ = load("case118")
+    ls = cupf.LinearSolver()
+    ls.set_data(d["row_ptr"], d["col_idx"])
+    ls.analyze()
+    ls.setup(2)
+    with pytest.raises(cupf.linear_solver.CustomSolverError):
+        ls.solve(torch.zeros((2, 181), dtype=torch.float64, device="cuda"))  # before factorize
+    with pytest.raises(ValueError):
+        ls.factorize(torch.zeros((2, d["col_idx"].size), dtype=torch.int32, device="cuda"))

@@ -1,0 +1,210 @@
+"""Batched Newton-Raphson on the GPU against the oracle and the reference's goldens.
+
+Bars: V within 1e-8 of the FP64 oracle run to 1e-12; with FP64 factors the
+iteration counts equal the oracle's on the same stopping rule (the NR loop
+semantics of newton_solver.cpp:245-342: iterations = norm evaluations,
+convergence tested before the Jacobian, final mismatch = last evaluated norm).
+"""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import cupf
+from cupf import grids as G
+from conftest import gpu_available
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not gpu_available(), reason="needs a CUDA device")]
+GOLD = Path(__file__).resolve().parent / "golden"
+POLICIES = {"FP64": cupf.ComputePolicy.FP64, "FP32": cupf.ComputePolicy.FP32, "Mixed": cupf.ComputePolicy.Mixed}
+
+
+def make_solver(g, compute, graph=False, serial_nd=True):
+    o = cupf.NewtonOptions()
+    o.backend = cupf.BackendKind.CUDA
+    o.compute = compute
+    o.use_cuda_graph = graph
+    o.custom.serial_nd = serial_nd
+    s = cupf.NewtonSolver(o)
+    s.initialize(g.indptr, g.indices, g.data, g.n_bus, g.n_bus, g.pv, g.pq)
+    return s
+
+
+def cfg(tol=1e-8, max_iter=10):
+    c = cupf.NRConfig()
+    c.tolerance = tol
+    c.max_iter = max_iter
+    return c
+
+
+def solve(s, g, S, V0, c):
+    return s.solve_batch(g.indptr, g.indices, g.data, g.n_bus, g.n_bus, S, V0, g.pv, g.pq, c)
+
+
+class TwoBus:
+    def __init__(self):
+        c = G.two_bus_case()
+        self.c = c
+        self.indptr, self.indices, self.data = c["indptr"], c["indices"], c["data"]
+        self.pv, self.pq, self.n_bus = c["pv"], c["pq"], 2
+
+
+@pytest.mark.parametrize("policy", list(POLICIES))
+@pytest.mark.parametrize("graph", [False, True])
+def test_two_bus(policy, graph):
+    """cuPF/tests/unit/test_minimal_solver.cpp:100-346 (FP64/FP32/Mixed, batch 2, graph)."""
+    g = TwoBus()
+    s = make_solver(g, POLICIES[policy], graph=graph)
+    S = np.stack([g.c["sbus"]] * 2)
+    V0 = np.stack([g.c["v0"]] * 2)
+    r = solve(s, g, S, V0, cfg(1e-10, 20))
+    assert r.converged_numpy.all()
+    assert np.abs(r.V_numpy - g.c["expected_v"][None, :]).max() <= 1e-8
+    single = s.solve(g.indptr, g.indices, g.data, 2, 2, g.c["sbus"], g.c["v0"], g.pv, g.pq, cfg(1e-10, 20))
+    assert single.converged and abs(single.V_numpy - g.c["expected_v"]).max() <= 1e-8
+
+
+@pytest.mark.parametrize("policy", list(POLICIES))
+def test_118_matches_oracle(oracle, policy):
+    g = G.grid_118()
+    B = 40  # more than one warp of scenarios, ragged last warp
+    S = g.scenarios(B, seed=17)
+    V0 = g.flat_start(B)
+    s = make_solver(g, POLICIES[policy])
+    r = solve(s, g, S, V0, cfg())
+    assert r.converged_numpy.all()
+    for b in range(0, B, 7):
+        tight = oracle.solve(g, S[b], V0[b], tol=1e-12, max_iter=30)
+        assert np.abs(r.V_numpy[b] - tight["V"]).max() <= 1e-8
+        same = oracle.solve(g, S[b], V0[b], tol=1e-8, max_iter=10)
+        if policy == "FP64":
+            assert r.iterations_numpy[b] == same["iterations"]
+            assert r.final_mismatch_numpy[b] == pytest.approx(same["final_mismatch"], rel=1e-3, abs=1e-13)
+        assert r.final_mismatch_numpy[b] <= 1e-8
+
+
+def test_118_matches_reference_golden():
+    """The reference CPU NewtonSolver's answers (tests/golden/nr_118.npz)."""
+    g = G.grid_118()
+    gold = np.load(GOLD / "nr_118.npz")
+    s = make_solver(g, cupf.ComputePolicy.FP64)
+    r = solve(s, g, gold["sbus"], gold["v0"], cfg(1e-8, 10))
+    assert np.array_equal(r.iterations_numpy, gold["it_t8"])
+    assert np.abs(r.V_numpy - gold["V_t8"]).max() <= 1e-10
+    r12 = solve(s, g, gold["sbus"], gold["v0"], cfg(1e-12, 30))
+    assert np.abs(r12.V_numpy - gold["V_t12"]).max() <= 1e-11
+
+
+@pytest.mark.parametrize("policy", ["FP64", "Mixed"])
+def test_2000_matches_oracle(oracle, policy):
+    g = G.grid_2000()
+    B = 96
+    S = g.scenarios(B, seed=23)
+    V0 = g.flat_start(B)
+    s = make_solver(g, POLICIES[policy])
+    r = solve(s, g, S, V0, cfg())
+    assert r.converged_numpy.all()
+    for b in (0, 31, 32, 95):
+        tight = oracle.solve(g, S[b], V0[b], tol=1e-12, max_iter=30)
+        assert np.abs(r.V_numpy[b] - tight["V"]).max() <= 1e-8
+        if policy == "FP64":
+            assert r.iterations_numpy[b] == oracle.solve(g, S[b], V0[b], 1e-8, 10)["iterations"]
+
+
+def test_2000_matches_reference_golden():
+    g = G.grid_2000()
+    gold = np.load(GOLD / "nr_2000.npz")
+    s = make_solver(g, cupf.ComputePolicy.Mixed)
+    r = solve(s, g, gold["sbus"], gold["v0"], cfg(1e-8, 10))
+    assert r.converged_numpy.all()
+    assert np.abs(r.V_numpy - gold["V_t12"]).max() <= 1e-8
+
+
+def test_10000_mixed_matches_oracle(oracle):
+    g = G.grid_10000()
+    B = 64
+    S = g.scenarios(B, seed=29)
+    V0 = g.flat_start(B)
+    s = make_solver(g, cupf.ComputePolicy.Mixed)
+    r = solve(s, g, S, V0, cfg())
+    assert r.converged_numpy.all()
+    for b in (0, 63):
+        tight = oracle.solve(g, S[b], V0[b], tol=1e-12, max_iter=30)
+        assert np.abs(r.V_numpy[b] - tight["V"]).max() <= 1e-8
+
+
+def test_identical_rows_agree():
+    """test_cpu_solver.cpp:355-359: batch rows of the same case agree."""
+    g = G.grid_118()
+    S = np.repeat(g.scenarios(1, seed=3), 37, axis=0)
+    s = make_solver(g, cupf.ComputePolicy.Mixed)
+    r = solve(s, g, S, g.flat_start(37), cfg())
+    assert np.abs(r.V_numpy - r.V_numpy[0:1]).max() == 0.0
+    assert len(set(r.iterations_numpy.tolist())) == 1
+
+
+def test_graph_mode_matches_stream_mode():
+    g = G.grid_2000()
+    S = g.scenarios(64, seed=41)
+    V0 = g.flat_start(64)
+    a = solve(make_solver(g, cupf.ComputePolicy.Mixed), g, S, V0, cfg())
+    b = solve(make_solver(g, cupf.ComputePolicy.Mixed, graph=True), g, S, V0, cfg())
+    assert np.array_equal(a.V_numpy, b.V_numpy)
+    assert np.array_equal(a.iterations_numpy, b.iterations_numpy)
+
+
+def test_not_converged_reports_last_norm(oracle):
+    """max_iter too small: converged False and final_mismatch = the last norm evaluated."""
+    g = G.grid_118()
+    S = g.scenarios(4, seed=5)
+    V0 = g.flat_start(4)
+    s = make_solver(g, cupf.ComputePolicy.FP64)
+    r = solve(s, g, S, V0, cfg(1e-8, 2))
+    assert not r.converged_numpy.any()
+    assert (r.iterations_numpy == 2).all()
+    for b in range(4):
+        o = oracle.solve(g, S[b], V0[b], tol=1e-8, max_iter=2)
+        assert r.final_mismatch_numpy[b] == pytest.approx(o["final_mismatch"], rel=1e-9)
+        assert np.abs(r.V_numpy[b] - o["V"]).max() <= 1e-12
+
+
+def test_device_entry_point_matches_host():
+    import torch
+
+    g = G.grid_2000()
+    S = g.scenarios(33, seed=8)
+    V0 = g.flat_start(33)
+    s = make_solver(g, cupf.ComputePolicy.Mixed)
+    host = solve(s, g, S, V0, cfg())
+    v, fm, it = s.solve_batch_device(torch.tensor(S, device="cuda"), torch.tensor(V0, device="cuda"), config=cfg())
+    assert np.array_equal(v.cpu().numpy(), host.V_numpy)
+    assert np.array_equal(fm.cpu().numpy(), host.final_mismatch_numpy)
+
+
+def test_evaluate_matches_oracle(oracle):
+    """Mismatch F and Jacobian values at arbitrary states (FP64 kernels)."""
+    g = G.grid_2000()
+    rng = np.random.default_rng(4)
+    B = 3
+    V = (1 + 0.05 * rng.standard_normal((B, g.n_bus))) * np.exp(1j * 0.1 * rng.standard_normal((B, g.n_bus)))
+    S = g.scenarios(B, seed=9)
+    s = make_solver(g, cupf.ComputePolicy.FP64)
+    F, J = s.evaluate(V, S)
+    for b in range(B):
+        Fo, _ = oracle.mismatch(g, S[b], V[b])
+        Jo = oracle.jacobian_values(g, V[b])
+        assert np.abs(F[b] - Fo).max() <= 1e-12 * max(1.0, np.abs(Fo).max())
+        assert np.abs(J[b] - Jo).max() <= 1e-12 * np.abs(Jo).max()
+
+
+def test_stage_profiling_counts_launches():
+    g = G.grid_118()
+    s = make_solver(g, cupf.ComputePolicy.Mixed)
+    s.set_profiling(True)
+    r = solve(s, g, g.scenarios(8), g.flat_start(8), cfg())
+    st = s.stage_times()
+    s.set_profiling(False)
+    it = int(r.iterations_numpy[0])
+    assert st["mismatch"][1] == it
+    assert st["jacobian"][1] == it - 1
+    assert all(v[0] >= 0.0 for v in st.values())
