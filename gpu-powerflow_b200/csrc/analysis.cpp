@@ -582,7 +582,7 @@ FactorProgram build_factor_program(const SymbolicPlan& sp) {
       const int32_t fs = fp.fsz[p], nc = fp.nc[p], rw = fs + 1;
       for (int32_t q : owned[p]) ents.push_back({sp.a_row[q] * rw + sp.a_col[q], (int64_t)q});
       for (int32_t i = 0; i < nc; ++i)
-        ents.push_back({i * rw + fs, (int64_t(2) << kFeKindShift) | (int64_t)sp.perm[sp.panel_first[p] + i]});
+        ents.push_back({i * rw + fs, (int64_t(2) << kFeKindShift) | (int64_t)(sp.panel_first[p] + i)});
       for (int32_t c : kids[p]) {
         const int32_t ucc = fp.fsz[c] - fp.nc[c];
         const int32_t* al = sp.asm_local.data() + sp.asm_ptr[c];

@@ -98,7 +98,9 @@ struct FactorProgram {
   // Dense-front assembly program: for front p, entries [fe_ptr[p], fe_ptr[p+1])
   // give a destination inside the (fsz x (fsz + 1)) front (last column = rhs)
   // and a source: kind (bits 62-63) 0 = Jacobian CSR position, 1 = CB element
-  // (global index), 2 = mismatch row.  Sorted by destination; fe_split
+  // (global index), 2 = mismatch row (pivot-order index).  Sorted by
+  // destination, stable (J entries, mismatch rows, then children in order);
+  // fe_split
   // (kFeChunks + 1 per front) cuts the list at destination boundaries into
   // chunks that different warps can accumulate without sharing a destination.
   std::vector<int64_t> fe_ptr;

@@ -57,6 +57,8 @@ struct DevGrid {
   const int* map22 = nullptr;
   const int* bus_fa = nullptr;  // bus -> angle row (P equation), -1 for slack
   const int* bus_fm = nullptr;  // bus -> magnitude row (Q equation), -1 for slack/PV
+  const int* bus_fa_p = nullptr;  // the same rows in the factor's pivot order (iperm applied)
+  const int* bus_fm_p = nullptr;
   const int* pv = nullptr;
   const int* pq = nullptr;
   const int* jt_ptr = nullptr;  // J^T as CSR over J's CSR positions: column j of J
@@ -76,6 +78,8 @@ struct DevState {
   double* i_re = nullptr;
   double* i_im = nullptr;
   double* F = nullptr;
+  void* Fp = nullptr;   // F again, in pivot order and the factor's type (the LU's right-hand side)
+  int fp_double = 0;    // Fp holds double (FP64 factors) or float
   unsigned long long* norm_bits = nullptr;  // [Bp] max |F| per scenario as IEEE bits
   int* sing = nullptr;                      // [Bp] static-pivot shift applied
 };

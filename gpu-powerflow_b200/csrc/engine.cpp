@@ -90,7 +90,8 @@ std::vector<long long> to_ll(const std::vector<T>& v) {
 
 struct Engine::Impl {
   // grid
-  DBuf y_ptr, y_col, y_row, y_re, y_im, map11, map21, map12, map22, bus_fa, bus_fm, pv, pq, jt_ptr, jt_row, jt_q;
+  DBuf y_ptr, y_col, y_row, y_re, y_im, map11, map21, map12, map22, bus_fa, bus_fm, bus_fa_p, bus_fm_p, pv, pq,
+      jt_ptr, jt_row, jt_q;
   // factor program
   DBuf fsz, nc, first, front_ptr, front_rows, u_off, l_off, cb_off, tv_off, arow_ptr, arow_q, arow_col, crow_ptr,
       crow_child, crow_r, asm_ptr, asm_local, perm, iperm, level_fronts, fe_split, fe_dst, fe_src;
@@ -100,7 +101,8 @@ struct Engine::Impl {
   DevPlan pl;
   // workspace
   int Bp_cap = 0, B = 0, Bp = 0;
-  DBuf v_re, v_im, va, vm, s_re, s_im, i_re, i_im, F, norm, sing;
+  DBuf v_re, v_im, va, vm, s_re, s_im, i_re, i_im, F, Fp, norm, sing;
+  bool fp_double = false;
   DBuf J, U, L, CB, Y, X, front_scratch;
   size_t front_scratch_elems = 0;
   DBuf stage_in, stage_out, fin;
@@ -150,6 +152,8 @@ struct Engine::Impl {
     st.i_re = i_re.as<double>();
     st.i_im = i_im.as<double>();
     st.F = F.as<double>();
+    st.Fp = Fp.p;
+    st.fp_double = fp_double ? 1 : 0;
     st.norm_bits = norm.as<unsigned long long>();
     st.sing = sing.as<int>();
     return st;
@@ -193,6 +197,15 @@ void Engine::initialize(int32_t n_bus, const int32_t* indptr, const int32_t* ind
   d.map22.upload(ja_.map22);
   d.bus_fa.upload(ja_.row_pvpq);
   d.bus_fm.upload(ja_.row_pq);
+  {
+    std::vector<int32_t> fa_p(n_bus, -1), fm_p(n_bus, -1);
+    for (int32_t i = 0; i < n_bus; ++i) {
+      if (ja_.row_pvpq[i] >= 0) fa_p[i] = fp_.iperm[ja_.row_pvpq[i]];
+      if (ja_.row_pq[i] >= 0) fm_p[i] = fp_.iperm[ja_.row_pq[i]];
+    }
+    d.bus_fa_p.upload(fa_p);
+    d.bus_fm_p.upload(fm_p);
+  }
   d.pv.upload(std::vector<int32_t>(pv, pv + n_pv));
   d.pq.upload(std::vector<int32_t>(pq, pq + n_pq));
   // J^T as CSR over J's positions (csr_transpose.cpp:257-289, own layout)
@@ -231,6 +244,8 @@ void Engine::initialize(int32_t n_bus, const int32_t* indptr, const int32_t* ind
   g.map22 = d.map22.as<int>();
   g.bus_fa = d.bus_fa.as<int>();
   g.bus_fm = d.bus_fm.as<int>();
+  g.bus_fa_p = d.bus_fa_p.as<int>();
+  g.bus_fm_p = d.bus_fm_p.as<int>();
   g.pv = d.pv.as<int>();
   g.pq = d.pq.as<int>();
   g.jt_ptr = d.jt_ptr.as<int>();
@@ -299,6 +314,8 @@ void Engine::upload_plan() {
     for (int32_t q = lv.begin; q < lv.begin + lv.count; ++q) {
       lv.max_fsz = std::max(lv.max_fsz, fp_.fsz[fp_.level_fronts[q]]);
       lv.max_nc = std::max(lv.max_nc, fp_.nc[fp_.level_fronts[q]]);
+      const int32_t f = fp_.level_fronts[q];
+      lv.max_src = std::max<int>(lv.max_src, (int)(fp_.fe_ptr[f + 1] - fp_.fe_ptr[f]));
     }
     d.levels.push_back(lv);
   }
@@ -349,7 +366,7 @@ void Engine::analyze_host(int32_t n_bus, const int32_t* indptr, const int32_t* i
   so.serial_nd = cfg_.serial_nd != 0;
   sp_ = analyze_symbolic(ja_.dim, ja_.row_ptr.data(), ja_.col_idx.data(), so);
   fp_ = build_factor_program(sp_);
-  if (fp_.max_fsz > 128) throw std::runtime_error("initialize: a front exceeds 128 rows (unsupported)");
+  if (fp_.max_fsz > 64) throw std::runtime_error("initialize: a front exceeds 64 rows (unsupported)");
 }
 
 void Engine::analyze_matrix_host(int32_t n, int32_t nnz, const int32_t* row_ptr, const int32_t* col_idx) {
@@ -382,7 +399,7 @@ void Engine::initialize_matrix(int32_t n, int32_t nnz, const int32_t* row_ptr, c
   so.serial_nd = cfg_.serial_nd != 0;
   sp_ = analyze_symbolic(n, row_ptr, col_idx, so);
   fp_ = build_factor_program(sp_);
-  if (fp_.max_fsz > 128) throw std::runtime_error("Analyze: a front exceeds 128 rows (unsupported)");
+  if (fp_.max_fsz > 64) throw std::runtime_error("Analyze: a front exceeds 64 rows (unsupported)");
   upload_plan();
   initialized_ = true;
   adjoint_ready_ = false;
@@ -400,6 +417,12 @@ void Engine::ensure_workspace(int32_t B) {
     const size_t es = factor_is_double() ? sizeof(double) : sizeof(float);
     for (DBuf* b : {&d.v_re, &d.v_im, &d.va, &d.vm, &d.s_re, &d.s_im, &d.i_re, &d.i_im}) b->reserve(n * Bp * 8);
     d.F.reserve(dim * Bp * 8);
+    d.Fp.reserve(dim * Bp * es);
+    d.fp_double = factor_is_double();
+    if (d.fp_double)
+      configure_front_kernels<double, double>();
+    else
+      configure_front_kernels<float, float>();
     d.norm.reserve(Bp * 8);
     d.sing.reserve(Bp * 4);
     d.J.reserve((size_t)ja_.nnz * Bp * es);
@@ -410,10 +433,9 @@ void Engine::ensure_workspace(int32_t B) {
     d.X.reserve(dim * Bp * es);
     // dense fronts of levels too large for shared memory live in global scratch
     size_t scratch = 0;
-    const size_t cap = front_smem_capacity(es);
     for (const auto& lv : d.levels) {
       const size_t elems = (size_t)lv.max_fsz * (lv.max_fsz + 1);
-      if (elems > cap) scratch = std::max(scratch, elems * lv.count * (Bp / kWarp));
+      if (!front_fits_smem(lv, es)) scratch = std::max(scratch, elems * lv.count * (Bp / kWarp));
     }
     d.front_scratch_elems = scratch;
     if (scratch) d.front_scratch.reserve(scratch * kWarp * es);
@@ -486,7 +508,7 @@ void Engine::factor_all(cudaStream_t s, int store_l, const void* J) {
   a.groups = d.Bp / kWarp;
   a.Bp = d.Bp;
   a.J = static_cast<const T*>(J);
-  a.F = d.F.as<double>();
+  a.Fp = d.Fp.as<T>();
   a.U = d.U.as<T>();
   a.L = d.L.as<T>();
   a.CB = d.CB.as<T>();
@@ -794,6 +816,7 @@ void Engine::factorize_values(const void* d_values, int32_t values_is_double, in
       launch_batch_to_rows<float, float>(static_cast<const float*>(d_values), d.J.as<float>(), ja_.nnz, B, d.Bp, s);
   }
   CUPF_CUDA(cudaMemsetAsync(d.F.p, 0, (size_t)ja_.dim * d.Bp * 8, s));
+  CUPF_CUDA(cudaMemsetAsync(d.Fp.p, 0, (size_t)ja_.dim * d.Bp * (dbl ? 8 : 4), s));
   CUPF_CUDA(cudaMemsetAsync(d.sing.p, 0, d.Bp * sizeof(int), s));
   if (dbl) factor_all<double>(s, 1, d.J.p);
   else factor_all<float>(s, 1, d.J.p);

@@ -15,6 +15,7 @@ struct LevelLaunch {
   int count = 0;   // fronts in the level
   int max_fsz = 0; // largest front of the level (selects the register bucket)
   int max_nc = 0;  // widest panel of the level
+  int max_src = 0; // longest assembly source list of the level
 };
 
 template <typename T, typename TJ>
@@ -22,7 +23,7 @@ struct FactorArgs {
   DevPlan plan;
   int groups = 0, Bp = 0;
   const TJ* J = nullptr;
-  const double* F = nullptr;
+  const T* Fp = nullptr;  // right-hand side rows in pivot order
   T* U = nullptr;
   T* L = nullptr;
   T* CB = nullptr;
@@ -35,9 +36,44 @@ struct FactorArgs {
   size_t front_scratch_elems = 0;   // capacity in elements per scenario lane group (x 32)
 };
 
-// Front elements [fsz][fsz + 1] beyond which a level's dense fronts live in
-// global scratch instead of shared memory (227 KB per block).
-inline size_t front_smem_capacity(size_t elem_bytes) { return (227u * 1024u) / (32u * elem_bytes); }
+constexpr size_t kSmemLimit = 227 * 1024;  // opt-in dynamic shared memory per block on sm_100
+
+// Shared-memory plan of one factor-level launch (same for every block):
+// staged source list (src, dst), staged source rows, dense front.
+struct FrontSmem {
+  int chunk = 0;        // staged source rows per buffer
+  int nbuf = 1;         // 1, or 2 when a front's sources need more than one chunk
+  int idx_cap = 0;      // source entries whose (src, dst) are staged
+  size_t idx_bytes = 0, stage_bytes = 0, front_bytes = 0;
+  size_t total() const { return idx_bytes + stage_bytes + front_bytes; }
+};
+
+// The whole source list staged at once when it fits next to the dense front,
+// else two alternating chunk buffers of 128 / 64 / 32 rows.  With
+// front_in_smem = false the dense front lives in global scratch.
+inline FrontSmem plan_front_smem(const LevelLaunch& lv, size_t elem_bytes, bool front_in_smem) {
+  FrontSmem sm;
+  const size_t row = 32 * elem_bytes;
+  sm.idx_cap = lv.max_src > 0 ? lv.max_src : 1;
+  sm.idx_bytes = ((size_t)sm.idx_cap * (sizeof(long long) + sizeof(int)) + 15) / 16 * 16;
+  sm.front_bytes = front_in_smem ? (size_t)lv.max_fsz * (lv.max_fsz + 1) * row : 0;
+  sm.chunk = sm.idx_cap;
+  sm.nbuf = 1;
+  sm.stage_bytes = (size_t)sm.chunk * row;
+  for (int c : {128, 64, 32}) {
+    if (sm.total() <= kSmemLimit) break;
+    if (c >= sm.chunk && sm.nbuf == 1) continue;
+    sm.chunk = c;
+    sm.nbuf = 2;
+    sm.stage_bytes = 2 * (size_t)c * row;
+  }
+  return sm;
+}
+
+// True when a level's dense fronts fit in shared memory next to the staging.
+inline bool front_fits_smem(const LevelLaunch& lv, size_t elem_bytes) {
+  return plan_front_smem(lv, elem_bytes, true).total() <= kSmemLimit;
+}
 
 template <typename T>
 struct SweepArgs {
@@ -60,6 +96,8 @@ struct AdjointSweepArgs {
   T* Z = nullptr;             // L^T solution (permuted order)
 };
 
+template <typename T, typename TJ>
+void configure_front_kernels();
 template <typename T, typename TJ>
 void launch_factor_level(const LevelLaunch& lv, const FactorArgs<T, TJ>& a, cudaStream_t s);
 template <typename T>

@@ -27,6 +27,8 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <mutex>
+#include <set>
 #include <stdexcept>
 #include <string>
 
@@ -37,7 +39,6 @@ namespace cupf_b200 {
 namespace {
 
 constexpr int kFactorWarps = 4;       // independent (front, scenario-group) items per block, at most
-constexpr size_t kSmemLimit = 227 * 1024;  // opt-in dynamic shared memory per block on sm_100
 
 template <typename T>
 __device__ __forceinline__ T guarded_pivot(T piv, bool static_pivot, double eps, bool& shifted) {
@@ -52,100 +53,244 @@ __device__ __forceinline__ T guarded_pivot(T piv, bool static_pivot, double eps,
   return piv;
 }
 
+// Opt a kernel into the full 227 KB of dynamic shared memory, once per
+// (device, kernel); the attribute is per device and per function.
+inline void allow_full_smem(const void* fn) {
+  static std::mutex mu;
+  static std::set<std::pair<int, const void*>> done;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) throw std::runtime_error("cudaGetDevice failed");
+  std::lock_guard<std::mutex> lock(mu);
+  if (done.count({dev, fn})) return;
+  const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemLimit);
+  if (e != cudaSuccess) throw std::runtime_error(std::string("shared-memory attribute: ") + cudaGetErrorString(e));
+  done.insert({dev, fn});
+}
+
+inline void check_launch(const char* what) {
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) throw std::runtime_error(std::string(what) + " launch: " + cudaGetErrorString(e));
+}
+
+// ---------------------------------------------------------------------------
+// Asynchronous global -> shared copies (cp.async, sm_80+ form; the copy
+// completes in the background and cp.async.wait_group is a hardware wait, so
+// no software spin is involved).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+  const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
 // ---------------------------------------------------------------------------
 // Factor + forward substitution of one level of the front tree.
 //
-// One block = one front x 32 scenarios (lane = scenario).  The block
-// assembles the dense front [fsz][fsz + 1] (last column = right-hand side) in
-// shared memory from the front's destination-sorted source list -- original
-// Jacobian entries, the mismatch rows of its pivots and its children's
-// contribution blocks -- each warp accumulating its own destination chunk with
-// eight independent loads in flight, then runs the right-looking LU over the
-// nc pivot columns with the rows split across the warps, and writes
-//   U  [u_total][Bp]  : pivot rows k (L11 left of the diagonal, U11 | U12 from it)
-//   L  [l_total][Bp]  : L21 rows (only when store_l; the adjoint needs them)
-//   CB [cb_total][Bp] : uc rows of uc + 1 entries (last = right-hand-side update)
-//   Y  [dim][Bp]      : y = L^-1 P F at the pivot rows (permuted order)
-// Fronts whose dense block does not fit the shared-memory budget use a
+// One block = one front x 32 scenarios (lane = scenario).  Three phases:
+//  1. staging: the front's destination-sorted source list (indices) is copied
+//     into shared memory, then every source row -- 32 scenarios of one
+//     Jacobian entry or one child contribution-block element, a contiguous
+//     128 B (fp32) / 256 B (fp64) segment of the [element][Bp] arrays -- is
+//     requested with cp.async in one sweep, so a front costs two memory round
+//     trips however many sources it has (large lists go through two
+//     alternating buffers, chunk by chunk);
+//  2. assembly into the dense front [fsz][fsz + 1] (last column = right-hand
+//     side, seeded with the pivots' mismatch rows), each warp owning whole
+//     destinations so the sums run in list order without atomics;
+//  3. right-looking LU over the nc pivot columns with the rows split across
+//     the warps, then
+//       U  [u_total][Bp]  : pivot rows k (L11 left of the diagonal, U11 | U12 from it)
+//       L  [l_total][Bp]  : L21 rows (only when store_l; the adjoint needs them)
+//       CB [cb_total][Bp] : uc rows of uc + 1 entries (last = right-hand-side update)
+//       Y  [dim][Bp]      : y = L^-1 P F at the pivot rows (permuted order)
+// Fronts whose dense block does not fit next to the staging buffers live in a
 // caller-provided global scratch area (front_scratch), same code.
 // ---------------------------------------------------------------------------
-template <typename T, typename TJ>
+template <typename T, typename TJ, int FMAX, bool SMEM_FRONT>
 __global__ void __launch_bounds__(256)
-    k_front_factor(DevPlan pl, int level_begin, int groups, int Bp, int front_elems, const TJ* __restrict__ J,
-                   const double* __restrict__ F, T* __restrict__ U, T* __restrict__ L, T* __restrict__ CB,
-                   T* __restrict__ Y, int store_l, double eps, int static_pivot, int* __restrict__ sing,
-                   T* __restrict__ front_scratch) {
-  extern __shared__ unsigned char smem_raw[];
+    k_front_factor(DevPlan pl, int level_begin, int groups, int Bp, int front_elems, FrontSmem sm,
+                   const TJ* __restrict__ J, const T* __restrict__ Fp, T* __restrict__ U, T* __restrict__ L,
+                   T* __restrict__ CB, T* __restrict__ Y, int store_l, double eps, int static_pivot,
+                   int* __restrict__ sing, T* __restrict__ front_scratch) {
+  static_assert(sizeof(TJ) == sizeof(T), "Jacobian and factor rows are staged in the same slots");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int kRowBytes = kWarp * sizeof(T);
+  constexpr int kPieces = kRowBytes / 16;  // 16-byte cp.async pieces per source row
   const int W = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int item = blockIdx.x;
   const int p = pl.level_fronts[level_begin + item / groups];
-  const size_t b = (size_t)(item % groups) * kWarp + lane;
+  const int grp = item - (item / groups) * groups;
+  const size_t col0 = (size_t)grp * kWarp;
   const int fs = pl.fsz[p], nc = pl.nc[p], uc = fs - nc, rw = fs + 1;
-  T* Fm = front_scratch ? front_scratch + (size_t)item * front_elems * kWarp : reinterpret_cast<T*>(smem_raw);
+  const long long* split = pl.fe_split + (size_t)p * 9;
+  const long long e0 = split[0];
+  const int nsrc = (int)(split[8] - e0);
 
+  long long* s_src = reinterpret_cast<long long*>(smem_raw);
+  int* s_dst = reinterpret_cast<int*>(smem_raw + (size_t)sm.idx_cap * sizeof(long long));
+  unsigned char* stage = smem_raw + sm.idx_bytes;
+  T* Fm;
+  if constexpr (SMEM_FRONT)
+    Fm = reinterpret_cast<T*>(smem_raw + sm.idx_bytes + sm.stage_bytes);
+  else
+    Fm = front_scratch + (size_t)item * front_elems * kWarp;
+
+  // phase 1a: source list -> shared memory (the dense front is zeroed meanwhile)
+  for (int e = threadIdx.x; e < nsrc; e += blockDim.x) {
+    cp_async8(s_src + e, pl.fe_src + e0 + e);
+    cp_async4(s_dst + e, pl.fe_dst + e0 + e);
+  }
+  cp_async_commit();
   for (int e = threadIdx.x; e < fs * rw * kWarp; e += blockDim.x) Fm[e] = T(0);
+  cp_async_wait<0>();
   __syncthreads();
 
-  // ---- assembly ----
-  const long long* split = pl.fe_split + (size_t)p * 9;
-  for (int ch = warp; ch < 8; ch += W) {
-    const long long e1 = split[ch + 1];
-    for (long long e = split[ch]; e < e1; e += 8) {
+  // phase 1b: request the source rows (Jacobian entries, right-hand-side rows,
+  // children's contribution-block elements), one row per thread, chunk by chunk
+  const int nchunks = (nsrc + sm.chunk - 1) / sm.chunk;
+  auto issue = [&](int c) {
+    const int cs = c * sm.chunk, ce = min(nsrc, cs + sm.chunk);
+    unsigned char* buf = stage + (size_t)(c % sm.nbuf) * sm.chunk * kRowBytes;
+    for (int e = cs + (int)threadIdx.x; e < ce; e += blockDim.x) {
+      const unsigned long long src = (unsigned long long)s_src[e];
+      const int kind = (int)(src >> 62);
+      const size_t off = (size_t)(src & 0x3FFFFFFFFFFFFFFFull) * Bp + col0;
+      const unsigned char* g = kind == 0   ? reinterpret_cast<const unsigned char*>(J + off)
+                               : kind == 1 ? reinterpret_cast<const unsigned char*>(CB + off)
+                                           : reinterpret_cast<const unsigned char*>(Fp + off);
+      unsigned char* d = buf + (size_t)(e - cs) * kRowBytes;
+#pragma unroll
+      for (int piece = 0; piece < kPieces; ++piece) cp_async16(d + piece * 16, g + piece * 16);
+    }
+    cp_async_commit();
+  };
+  if (nchunks > 0) issue(0);
+  if (nchunks > 1) issue(1);
+
+  // phase 2: assembly.  Warp w owns the destination-disjoint range
+  // [split[8w/W], split[8(w+1)/W]); consecutive entries with one destination
+  // are summed in a register (in list order) and stored once.
+  const int A = (int)(split[warp * 8 / W] - e0), Z = (int)(split[(warp + 1) * 8 / W] - e0);
+  int cur = -1;
+  T acc = T(0);
+  for (int c = 0; c < nchunks; ++c) {
+    if (c + 1 < nchunks)
+      cp_async_wait<1>();
+    else
+      cp_async_wait<0>();
+    __syncthreads();
+    const int cs = c * sm.chunk, ce = min(nsrc, cs + sm.chunk);
+    const T* buf = reinterpret_cast<const T*>(stage + (size_t)(c % sm.nbuf) * sm.chunk * kRowBytes) + lane;
+    const int a = max(cs, A), z = min(ce, Z);
+    for (int e = a; e < z; e += 8) {
       T v[8];
       int d[8];
 #pragma unroll
       for (int u = 0; u < 8; ++u) {
-        v[u] = T(0);
-        d[u] = -1;
-        if (e + u < e1) {
-          const long long src = pl.fe_src[e + u];
-          d[u] = pl.fe_dst[e + u];
-          const int kind = (int)((unsigned long long)src >> 62);
-          const size_t idx = (size_t)(src & 0x3FFFFFFFFFFFFFFFll);
-          v[u] = kind == 0 ? static_cast<T>(J[idx * Bp + b])
-                           : (kind == 1 ? CB[idx * Bp + b] : static_cast<T>(F[idx * Bp + b]));
+        const bool in = e + u < z;
+        d[u] = in ? s_dst[e + u] : -1;
+        v[u] = in ? buf[(e + u - cs) * kWarp] : T(0);
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        if (d[u] >= 0) {
+          if (d[u] != cur) {
+            if (cur >= 0) Fm[cur * kWarp + lane] = acc;
+            cur = d[u];
+            acc = T(0);
+          }
+          acc += v[u];
+        }
+      }
+    }
+    __syncthreads();
+    if (c + 2 < nchunks) issue(c + 2);
+  }
+  if (cur >= 0) Fm[cur * kWarp + lane] = acc;
+  __syncthreads();
+
+  // phase 3a: the nc pivot rows, eliminated in order by warp 0 (row k applies
+  // the final rows m < k, then its pivot is guarded); the row lives in registers
+  bool shifted = false;
+  T* Fl = Fm + lane;
+  if (warp == 0) {
+    for (int k = 0; k < nc; ++k) {
+      T* Rk = Fl + k * rw * kWarp;
+      T r[FMAX + 1];
+#pragma unroll
+      for (int j = 0; j <= FMAX; ++j) r[j] = j < rw ? Rk[j * kWarp] : T(0);
+#pragma unroll
+      for (int m = 0; m < 8; ++m) {
+        if (m < k) {
+          const T* Um = Fl + m * rw * kWarp;
+          const T l = r[m] / Um[m * kWarp];
+          r[m] = l;
+#pragma unroll
+          for (int j = m + 1; j <= FMAX; ++j)
+            if (j < rw) r[j] -= l * Um[j * kWarp];
         }
       }
 #pragma unroll
-      for (int u = 0; u < 8; ++u)
-        if (d[u] >= 0) Fm[(size_t)d[u] * kWarp + lane] += v[u];
+      for (int j = 0; j < 8; ++j)
+        if (j == k) r[j] = guarded_pivot(r[j], static_pivot != 0, eps, shifted);
+#pragma unroll
+      for (int j = 0; j <= FMAX; ++j)
+        if (j < rw) Rk[j * kWarp] = r[j];
     }
   }
   __syncthreads();
 
-  // ---- right-looking LU over the pivot columns ----
-  bool shifted = false;
-  for (int k = 0; k < nc; ++k) {
-    T* Fk = Fm + (size_t)k * rw * kWarp + lane;
-    if (warp == 0) Fk[k * kWarp] = guarded_pivot(Fk[k * kWarp], static_pivot != 0, eps, shifted);
-    __syncthreads();
-    const T piv = Fk[k * kWarp];
-    for (int i = k + 1 + warp; i < fs; i += W) {
-      T* Fi = Fm + (size_t)i * rw * kWarp + lane;
-      const T l = Fi[k * kWarp] / piv;
-      Fi[k * kWarp] = l;
-      for (int j = k + 1; j < rw; ++j) Fi[j * kWarp] -= l * Fk[j * kWarp];
-    }
-    __syncthreads();
-  }
-
-  // ---- write U, y, L21, CB ----
+  // phase 3b: outputs of the pivot rows (U rows, y) ...
+  const size_t b = col0 + lane;
   const long long uo = pl.u_off[p], lo = pl.l_off[p], co = pl.cb_off[p];
   const int first = pl.first[p];
-  for (int e = warp; e < nc * fs; e += W) {
-    const int k = e / fs, j = e - k * fs;
-    U[(size_t)(uo + e) * Bp + b] = Fm[(size_t)(k * rw + j) * kWarp + lane];
+  {
+    T* Ub = U + (size_t)uo * Bp + b;
+    for (int k = 0; k < nc; ++k)
+      for (int j = warp; j < fs; j += W) Ub[(size_t)(k * fs + j) * Bp] = Fl[(k * rw + j) * kWarp];
+    for (int k = warp; k < nc; k += W) Y[(size_t)(first + k) * Bp + b] = Fl[(k * rw + fs) * kWarp];
   }
-  for (int k = warp; k < nc; k += W) Y[(size_t)(first + k) * Bp + b] = Fm[(size_t)(k * rw + fs) * kWarp + lane];
-  if (store_l) {
-    for (int e = warp; e < uc * nc; e += W) {
-      const int ii = e / nc, j = e - ii * nc;
-      L[(size_t)(lo + e) * Bp + b] = Fm[(size_t)((nc + ii) * rw + j) * kWarp + lane];
+  // ... and the uc non-pivot rows, independent of each other: row i applies
+  // the nc pivot rows in registers and goes straight out as L21 | CB
+  for (int i = nc + warp; i < fs; i += W) {
+    const int ii = i - nc;
+    const T* Ri = Fl + i * rw * kWarp;
+    T r[FMAX + 1];
+#pragma unroll
+    for (int j = 0; j <= FMAX; ++j) r[j] = j < rw ? Ri[j * kWarp] : T(0);
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      if (m < nc) {
+        const T* Um = Fl + m * rw * kWarp;
+        const T l = r[m] / Um[m * kWarp];
+        r[m] = l;
+#pragma unroll
+        for (int j = m + 1; j <= FMAX; ++j)
+          if (j < rw) r[j] -= l * Um[j * kWarp];
+      }
     }
-  }
-  for (int e = warp; e < uc * (uc + 1); e += W) {
-    const int ii = e / (uc + 1), jj = e - ii * (uc + 1);
-    CB[(size_t)(co + e) * Bp + b] = Fm[(size_t)((nc + ii) * rw + nc + jj) * kWarp + lane];
+    if (store_l) {
+      T* Lb = L + (size_t)(lo + (long long)ii * nc) * Bp + b;
+#pragma unroll
+      for (int m = 0; m < 8; ++m)
+        if (m < nc) Lb[(size_t)m * Bp] = r[m];
+    }
+    T* Cb = CB + (size_t)(co + (long long)ii * (uc + 1)) * Bp + b;
+#pragma unroll
+    for (int j = 0; j <= FMAX; ++j)
+      if (j >= nc && j < rw) Cb[(size_t)(j - nc) * Bp] = r[j];
   }
   if (shifted) sing[b] = 1;
 }
@@ -153,33 +298,56 @@ __global__ void __launch_bounds__(256)
 // ---------------------------------------------------------------------------
 // Backward substitution U x = y of one level (root first).  X is in permuted
 // order; a front reads the x of its CB rows, which belong to ancestors.
+// One warp = one front x 32 scenarios.  The warp stages its front's U rows
+// (contiguous elements) and the x rows of its CB rows (gathered through
+// front_rows) with cp.async, then solves the nc pivots from shared memory.
 // ---------------------------------------------------------------------------
-template <typename T, int FMAX, int NCMAX>
-__global__ void __launch_bounds__(128)
-    k_backward_level(DevPlan pl, int level_begin, int level_count, int groups, int Bp, const T* __restrict__ U,
-                     const T* __restrict__ Y, T* __restrict__ X) {
+template <typename T>
+__global__ void __launch_bounds__(256)
+    k_backward_level(DevPlan pl, int level_begin, int level_count, int groups, int Bp, int warp_elems,
+                     const T* __restrict__ U, const T* __restrict__ Y, T* __restrict__ X) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int kPieces = kWarp * sizeof(T) / 16;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const long item = (long)blockIdx.x * (blockDim.x >> 5) + warp;
   if (item >= (long)level_count * groups) return;
   const int p = pl.level_fronts[level_begin + item / groups];
-  const size_t b = (size_t)(item % groups) * kWarp + lane;
-  const int fs = pl.fsz[p], nc = pl.nc[p];
+  const size_t col0 = (size_t)(item % groups) * kWarp;
+  const size_t b = col0 + lane;
+  const int fs = pl.fsz[p], nc = pl.nc[p], uc = fs - nc;
   const int fr0 = pl.front_ptr[p], first = pl.first[p];
   const long long uo = pl.u_off[p];
-  T xs[FMAX];
+  T* Us = reinterpret_cast<T*>(smem_raw) + (size_t)warp * warp_elems * kWarp;  // [nc * fs][32]
+  T* Xs = Us + (size_t)nc * fs * kWarp;                                         // [fs][32]
+  // U rows: contiguous elements uo .. uo + nc * fs
+  for (int t = lane; t < nc * fs * kPieces; t += kWarp) {
+    const int e = t / kPieces, piece = t % kPieces;
+    cp_async16(reinterpret_cast<unsigned char*>(Us + (size_t)e * kWarp) + piece * 16,
+               reinterpret_cast<const unsigned char*>(U + (size_t)(uo + e) * Bp + col0) + piece * 16);
+  }
+  // x of the CB rows: lane j fetches row front_rows[fr0 + nc + j]
+  for (int j = lane; j < uc; j += kWarp) {
+    const size_t row = (size_t)pl.front_rows[fr0 + nc + j];
 #pragma unroll
-  for (int j = 0; j < FMAX; ++j)
-    xs[j] = (j >= nc && j < fs) ? X[(size_t)pl.front_rows[fr0 + j] * Bp + b] : T(0);
+    for (int piece = 0; piece < kPieces; ++piece)
+      cp_async16(reinterpret_cast<unsigned char*>(Xs + (size_t)(nc + j) * kWarp) + piece * 16,
+                 reinterpret_cast<const unsigned char*>(X + row * Bp + col0) + piece * 16);
+  }
+  cp_async_commit();
+  T yk[8];
 #pragma unroll
-  for (int k = NCMAX - 1; k >= 0; --k) {
+  for (int k = 0; k < 8; ++k) yk[k] = k < nc ? Y[(size_t)(first + k) * Bp + b] : T(0);
+  cp_async_wait<0>();
+  __syncwarp();
+#pragma unroll
+  for (int k = 7; k >= 0; --k) {
     if (k < nc) {
-      const T* urow = U + (size_t)(uo + (long long)k * fs) * Bp + b;
-      T s = Y[(size_t)(first + k) * Bp + b];
-#pragma unroll
-      for (int j = k + 1; j < FMAX; ++j)
-        if (j < fs) s -= urow[(size_t)j * Bp] * xs[j];
-      xs[k] = s / urow[(size_t)k * Bp];
-      X[(size_t)(first + k) * Bp + b] = xs[k];
+      const T* urow = Us + (size_t)k * fs * kWarp + lane;
+      T s = yk[k];
+      for (int j = k + 1; j < fs; ++j) s -= urow[(size_t)j * kWarp] * Xs[(size_t)j * kWarp + lane];
+      const T xk = s / urow[(size_t)k * kWarp];
+      Xs[(size_t)k * kWarp + lane] = xk;
+      X[(size_t)(first + k) * Bp + b] = xk;
     }
   }
 }
@@ -341,13 +509,6 @@ inline int bucket_of(int fmax) {
 }
 
 template <typename T, int FMAX, int NCMAX>
-void launch_backward_t(const LevelLaunch& lv, const SweepArgs<T>& a, cudaStream_t s) {
-  const long items = (long)lv.count * a.groups;
-  const unsigned blocks = (unsigned)((items + 3) / 4);
-  k_backward_level<T, FMAX, NCMAX><<<blocks, 128, 0, s>>>(a.plan, lv.begin, lv.count, a.groups, a.Bp, a.U, a.Y, a.X);
-}
-
-template <typename T, int FMAX, int NCMAX>
 void launch_lf_t(const LevelLaunch& lv, const AdjointSweepArgs<T>& a, cudaStream_t s) {
   const long items = (long)lv.count * a.groups;
   const unsigned blocks = (unsigned)((items + 3) / 4);
@@ -383,42 +544,78 @@ void launch_lt_t(const LevelLaunch& lv, const AdjointSweepArgs<T>& a, cudaStream
 
 }  // namespace
 
+template <typename T, typename TJ, int FMAX>
+void launch_factor_t(const LevelLaunch& lv, const FactorArgs<T, TJ>& a, cudaStream_t s) {
+  const int fmax = lv.max_fsz;
+  const size_t elems = (size_t)fmax * (fmax + 1);
+  FrontSmem sm = plan_front_smem(lv, sizeof(T), true);
+  const bool in_smem = sm.total() <= kSmemLimit;
+  if (!in_smem) {
+    sm = plan_front_smem(lv, sizeof(T), false);
+    if (sm.total() > kSmemLimit) throw std::runtime_error("factor level: source staging exceeds shared memory");
+    if (!a.front_scratch || a.front_scratch_elems < elems * (size_t)lv.count * a.groups)
+      throw std::runtime_error("front larger than the shared-memory budget and no scratch area provided");
+  }
+  const long items = (long)lv.count * a.groups;
+  // latency-bound levels (few fronts): every warp of the block helps; wide
+  // levels: warps by front size so that more blocks stay resident
+  int warps = fmax <= 10 ? 1 : (fmax <= 16 ? 2 : (fmax <= 24 ? 4 : 8));
+  if (items < 4L * 148) warps = 8;
+  const size_t smem = sm.total();
+  auto run = [&](auto kern) {
+    allow_full_smem(reinterpret_cast<const void*>(kern));
+    kern<<<(unsigned)items, warps * kWarp, smem, s>>>(a.plan, lv.begin, a.groups, a.Bp, (int)elems, sm, a.J, a.Fp,
+                                                      a.U, a.L, a.CB, a.Y, a.store_l, a.eps, a.static_pivot, a.sing,
+                                                      a.front_scratch);
+    check_launch("front factor");
+  };
+  if (in_smem) run(k_front_factor<T, TJ, FMAX, true>);
+  else run(k_front_factor<T, TJ, FMAX, false>);
+}
+
+// Opt every front kernel of this precision into the full dynamic shared
+// memory up front (outside any stream capture).
+template <typename T, typename TJ>
+void configure_front_kernels() {
+  allow_full_smem(reinterpret_cast<const void*>(k_backward_level<T>));
+#define CUPF_ALLOW(F)                                                                  \
+  allow_full_smem(reinterpret_cast<const void*>(k_front_factor<T, TJ, F, true>));    \
+  allow_full_smem(reinterpret_cast<const void*>(k_front_factor<T, TJ, F, false>));
+  CUPF_ALLOW(8) CUPF_ALLOW(16) CUPF_ALLOW(24) CUPF_ALLOW(32) CUPF_ALLOW(48) CUPF_ALLOW(64)
+#undef CUPF_ALLOW
+}
+
 template <typename T, typename TJ>
 void launch_factor_level(const LevelLaunch& lv, const FactorArgs<T, TJ>& a, cudaStream_t s) {
   if (lv.count == 0) return;
-  const int fmax = lv.max_fsz;
-  const size_t elems = (size_t)fmax * (fmax + 1);
-  const size_t smem = elems * kWarp * sizeof(T);
-  const int warps = fmax <= 8 ? 2 : (fmax <= 20 ? 4 : 8);
-  const bool in_smem = smem <= kSmemLimit;
-  auto kern = k_front_factor<T, TJ>;
-  if (in_smem) {
-    static size_t configured = 0;
-    if (smem > configured) {
-      const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e != cudaSuccess)
-        throw std::runtime_error(std::string("factor kernel smem attribute: ") + cudaGetErrorString(e));
-      configured = smem;
-    }
-  } else if (!a.front_scratch || a.front_scratch_elems < elems * (size_t)lv.count * a.groups) {
-    throw std::runtime_error("front larger than the shared-memory budget and no scratch area provided");
-  }
-  const unsigned blocks = (unsigned)((long)lv.count * a.groups);
-  kern<<<blocks, warps * kWarp, in_smem ? smem : 0, s>>>(a.plan, lv.begin, a.groups, a.Bp, (int)elems, a.J, a.F, a.U,
-                                                        a.L, a.CB, a.Y, a.store_l, a.eps, a.static_pivot, a.sing,
-                                                        in_smem ? nullptr : a.front_scratch);
+  if (lv.max_nc > 8) throw std::runtime_error("panels wider than 8 columns are not supported (max_panel_width <= 8)");
+  const int f = lv.max_fsz;
+  if (f <= 8) launch_factor_t<T, TJ, 8>(lv, a, s);
+  else if (f <= 16) launch_factor_t<T, TJ, 16>(lv, a, s);
+  else if (f <= 24) launch_factor_t<T, TJ, 24>(lv, a, s);
+  else if (f <= 32) launch_factor_t<T, TJ, 32>(lv, a, s);
+  else if (f <= 48) launch_factor_t<T, TJ, 48>(lv, a, s);
+  else if (f <= 64) launch_factor_t<T, TJ, 64>(lv, a, s);
+  else throw std::runtime_error("front larger than 64 rows is not supported");
 }
 
 template <typename T>
 void launch_backward_level(const LevelLaunch& lv, const SweepArgs<T>& a, cudaStream_t s) {
   if (lv.count == 0) return;
-  if (lv.max_nc <= 8) {
-#define CALL(F, N) launch_backward_t<T, (F < 8 ? 8 : F), N>(lv, a, s)
-    CUPF_BUCKET_SWITCH(8, CALL)
-#undef CALL
-  } else {
-    throw std::runtime_error("panels wider than 8 columns are not supported (max_panel_width <= 8)");
-  }
+  if (lv.max_nc > 8) throw std::runtime_error("panels wider than 8 columns are not supported (max_panel_width <= 8)");
+  const int warp_elems = lv.max_nc * lv.max_fsz + lv.max_fsz;
+  const size_t per_warp = (size_t)warp_elems * kWarp * sizeof(T);
+  int wpb = (int)std::min<size_t>(8, kSmemLimit / per_warp);
+  if (wpb < 1) throw std::runtime_error("backward level: front exceeds shared memory");
+  const long items = (long)lv.count * a.groups;
+  wpb = (int)std::min<long>(wpb, std::max<long>(1, items / 148));
+  wpb = std::max(1, std::min(wpb, 4));
+  const size_t smem = per_warp * wpb;
+  auto kern = k_backward_level<T>;
+  allow_full_smem(reinterpret_cast<const void*>(kern));
+  const unsigned blocks = (unsigned)((items + wpb - 1) / wpb);
+  kern<<<blocks, wpb * kWarp, smem, s>>>(a.plan, lv.begin, lv.count, a.groups, a.Bp, warp_elems, a.U, a.Y, a.X);
+  check_launch("backward sweep");
 }
 
 template <typename T>

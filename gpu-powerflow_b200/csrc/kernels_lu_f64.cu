@@ -3,6 +3,7 @@
 #include "kernels_lu.cuh"
 
 namespace cupf_b200 {
+template void configure_front_kernels<double, double>();
 template void launch_factor_level<double, double>(const LevelLaunch&, const FactorArgs<double, double>&,
                                                   cudaStream_t);
 template void launch_backward_level<double>(const LevelLaunch&, const SweepArgs<double>&, cudaStream_t);

@@ -59,6 +59,16 @@ __global__ void k_ibus_mismatch(DevGrid g, DevState st) {
       st.F[(size_t)fm * Bp + b] = mi;
       nmax = dmax_nan(nmax, fabs(mi), bad);
     }
+    if (st.Fp) {
+      const int pa = g.bus_fa_p[i], pm = g.bus_fm_p[i];
+      if (st.fp_double) {
+        if (pa >= 0) static_cast<double*>(st.Fp)[(size_t)pa * Bp + b] = mr;
+        if (pm >= 0) static_cast<double*>(st.Fp)[(size_t)pm * Bp + b] = mi;
+      } else {
+        if (pa >= 0) static_cast<float*>(st.Fp)[(size_t)pa * Bp + b] = static_cast<float>(mr);
+        if (pm >= 0) static_cast<float*>(st.Fp)[(size_t)pm * Bp + b] = static_cast<float>(mi);
+      }
+    }
   }
   __shared__ double red[kRows][kWarp];
   __shared__ int redbad[kRows][kWarp];
