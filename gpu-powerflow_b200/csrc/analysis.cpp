@@ -622,6 +622,22 @@ FactorProgram build_factor_program(const SymbolicPlan& sp) {
     std::stable_sort(b, e, [&](int32_t a, int32_t c) { return fp.fsz[a] < fp.fsz[c]; });
     for (auto it = b; it != e; ++it) fp.level_max_fsz[L] = std::max(fp.level_max_fsz[L], fp.fsz[*it]);
   }
+  // Per-front launch records in level order (24 int32 each, one
+  // 96-byte line per front): everything a front kernel needs before staging.
+  fp.front_meta.assign((size_t)P * 24, 0);
+  for (int32_t q = 0; q < P; ++q) {
+    const int32_t p = fp.level_fronts[q];
+    int32_t* m = fp.front_meta.data() + (size_t)q * 24;
+    m[0] = fp.fsz[p];
+    m[1] = fp.nc[p];
+    m[2] = fp.first[p];
+    m[3] = p;
+    const int64_t wide[4] = {fp.fe_ptr[p], fp.u_off[p], fp.l_off[p], fp.cb_off[p]};
+    std::memcpy(m + 4, wide, sizeof(wide));
+    const int64_t* split = fp.fe_split.data() + (size_t)p * (kFeChunks + 1);
+    for (int w = 1; w <= kFeChunks; ++w) m[11 + w] = (int32_t)(split[w] - split[0]);
+    m[20] = fp.front_ptr[p];
+  }
   return fp;
 }
 

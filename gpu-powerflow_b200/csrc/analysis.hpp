@@ -107,6 +107,10 @@ struct FactorProgram {
   std::vector<int32_t> fe_dst;
   std::vector<int64_t> fe_src;
   std::vector<int64_t> fe_split;
+  // Launch records in level order (24 int32 per front): fs, nc, first, p,
+  // fe start, u_off, l_off, cb_off (int64 as two int32), the 8 fe_split cuts
+  // relative to the fe start, front_ptr.
+  std::vector<int32_t> front_meta;
 };
 
 constexpr int kFeChunks = 8;

@@ -93,6 +93,7 @@ bool copy_plan_array(const Engine& e, const char* name, int32_t* out, int64_t ca
   CUPF_ARR("fp_level_ptr", fp.level_ptr)
   CUPF_ARR("fp_level_fronts", fp.level_fronts)
   CUPF_ARR("fe_dst", fp.fe_dst)
+  CUPF_ARR("front_meta", fp.front_meta)
   CUPF_ARR("jac_row_ptr", ja.row_ptr)
   CUPF_ARR("jac_col_idx", ja.col_idx)
   CUPF_ARR("map11", ja.map11)

@@ -13,6 +13,7 @@
 namespace cupf_b200 {
 
 constexpr int kWarp = 32;
+constexpr int kFrontMetaInts = 24;  // int32 per front launch record (front_meta)
 
 // The factor program of one grid (see analysis.hpp FactorProgram).
 struct DevPlan {
@@ -41,7 +42,44 @@ struct DevPlan {
   const long long* fe_split = nullptr;  // 9 per front
   const int* fe_dst = nullptr;
   const long long* fe_src = nullptr;
+  const int* front_meta = nullptr;  // 24 int32 per front, in level order
 };
+
+// One front's launch record (front_meta), read with six 16-byte loads.
+struct FrontMeta {
+  int fs, nc, first, p, fr0;
+  long long e0, uo, lo, co;
+  int split[9];  // assembly-list cuts relative to e0 (split[0] = 0)
+};
+
+__device__ __forceinline__ long long meta_ll(int lo, int hi) {
+  return (long long)(((unsigned long long)(unsigned)hi << 32) | (unsigned)lo);
+}
+
+__device__ __forceinline__ FrontMeta load_front_meta(const int* meta, int q) {
+  const int4* m4 = reinterpret_cast<const int4*>(meta) + (size_t)q * 6;
+  const int4 a = m4[0], b = m4[1], c = m4[2], d = m4[3], e = m4[4], f = m4[5];
+  FrontMeta m;
+  m.fs = a.x;
+  m.nc = a.y;
+  m.first = a.z;
+  m.p = a.w;
+  m.e0 = meta_ll(b.x, b.y);
+  m.uo = meta_ll(b.z, b.w);
+  m.lo = meta_ll(c.x, c.y);
+  m.co = meta_ll(c.z, c.w);
+  m.split[0] = 0;
+  m.split[1] = d.x;
+  m.split[2] = d.y;
+  m.split[3] = d.z;
+  m.split[4] = d.w;
+  m.split[5] = e.x;
+  m.split[6] = e.y;
+  m.split[7] = e.z;
+  m.split[8] = e.w;
+  m.fr0 = f.x;
+  return m;
+}
 
 // Ybus and the Jacobian maps of one grid.
 struct DevGrid {

@@ -94,7 +94,7 @@ struct Engine::Impl {
       jt_ptr, jt_row, jt_q;
   // factor program
   DBuf fsz, nc, first, front_ptr, front_rows, u_off, l_off, cb_off, tv_off, arow_ptr, arow_q, arow_col, crow_ptr,
-      crow_child, crow_r, asm_ptr, asm_local, perm, iperm, level_fronts, fe_split, fe_dst, fe_src;
+      crow_child, crow_r, asm_ptr, asm_local, perm, iperm, level_fronts, fe_split, fe_dst, fe_src, front_meta;
   std::vector<LevelLaunch> levels;
   int64_t tv_total = 0;
   DevGrid g;
@@ -304,20 +304,38 @@ void Engine::upload_plan() {
   d.fe_split.upload(to_ll(fp_.fe_split));
   d.fe_dst.upload(fp_.fe_dst);
   d.fe_src.upload(to_ll(fp_.fe_src));
+  d.front_meta.upload(fp_.front_meta);
+  // Launch list: each level of the front tree, cut into runs of similar front
+  // size (fronts are size-sorted inside a level) when both sides of a cut
+  // hold enough fronts to fill the GPU, so that the shared memory of a launch
+  // is sized for its own fronts rather than the level's largest.
   d.levels.clear();
+  auto bucket = [](int32_t f) {
+    for (int32_t c : {6, 8, 10, 12, 16, 20, 24, 32, 48, 64})
+      if (f <= c) return c;
+    return 1 << 30;
+  };
+  constexpr int32_t kMinRun = 64;
   for (int32_t L = 0; L < fp_.num_levels; ++L) {
-    LevelLaunch lv;
-    lv.begin = fp_.level_ptr[L];
-    lv.count = fp_.level_ptr[L + 1] - fp_.level_ptr[L];
-    lv.max_fsz = 0;
-    lv.max_nc = 0;
-    for (int32_t q = lv.begin; q < lv.begin + lv.count; ++q) {
-      lv.max_fsz = std::max(lv.max_fsz, fp_.fsz[fp_.level_fronts[q]]);
-      lv.max_nc = std::max(lv.max_nc, fp_.nc[fp_.level_fronts[q]]);
-      const int32_t f = fp_.level_fronts[q];
-      lv.max_src = std::max<int>(lv.max_src, (int)(fp_.fe_ptr[f + 1] - fp_.fe_ptr[f]));
+    const int32_t b0 = fp_.level_ptr[L], b1 = fp_.level_ptr[L + 1];
+    std::vector<int32_t> cuts{b0};
+    for (int32_t q = b0 + 1; q < b1; ++q) {
+      if (bucket(fp_.fsz[fp_.level_fronts[q]]) == bucket(fp_.fsz[fp_.level_fronts[q - 1]])) continue;
+      if (q - cuts.back() >= kMinRun && b1 - q >= kMinRun) cuts.push_back(q);
     }
-    d.levels.push_back(lv);
+    cuts.push_back(b1);
+    for (size_t c = 0; c + 1 < cuts.size(); ++c) {
+      LevelLaunch lv;
+      lv.begin = cuts[c];
+      lv.count = cuts[c + 1] - cuts[c];
+      for (int32_t q = lv.begin; q < lv.begin + lv.count; ++q) {
+        const int32_t f = fp_.level_fronts[q];
+        lv.max_fsz = std::max(lv.max_fsz, fp_.fsz[f]);
+        lv.max_nc = std::max(lv.max_nc, fp_.nc[f]);
+        lv.max_src = std::max<int>(lv.max_src, (int)(fp_.fe_ptr[f + 1] - fp_.fe_ptr[f]));
+      }
+      d.levels.push_back(lv);
+    }
   }
 
   DevPlan& pl = d.pl;
@@ -347,6 +365,7 @@ void Engine::upload_plan() {
   pl.fe_split = d.fe_split.as<long long>();
   pl.fe_dst = d.fe_dst.as<int>();
   pl.fe_src = d.fe_src.as<long long>();
+  pl.front_meta = d.front_meta.as<int>();
   if (!d.own) CUPF_CUDA(cudaStreamCreateWithFlags(&d.own, cudaStreamNonBlocking));
   if (d.exec) {
     cudaGraphExecDestroy(d.exec);

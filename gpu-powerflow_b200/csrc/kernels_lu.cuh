@@ -130,13 +130,13 @@ __global__ void __launch_bounds__(256)
   constexpr int kPieces = kRowBytes / 16;  // 16-byte cp.async pieces per source row
   const int W = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int item = blockIdx.x;
-  const int p = pl.level_fronts[level_begin + item / groups];
+  const int q = level_begin + item / groups;
   const int grp = item - (item / groups) * groups;
   const size_t col0 = (size_t)grp * kWarp;
-  const int fs = pl.fsz[p], nc = pl.nc[p], uc = fs - nc, rw = fs + 1;
-  const long long* split = pl.fe_split + (size_t)p * 9;
-  const long long e0 = split[0];
-  const int nsrc = (int)(split[8] - e0);
+  const FrontMeta m = load_front_meta(pl.front_meta, q);
+  const int fs = m.fs, nc = m.nc, uc = fs - nc, rw = fs + 1;
+  const long long e0 = m.e0;
+  const int nsrc = m.split[8];
 
   long long* s_src = reinterpret_cast<long long*>(smem_raw);
   int* s_dst = reinterpret_cast<int*>(smem_raw + (size_t)sm.idx_cap * sizeof(long long));
@@ -153,7 +153,12 @@ __global__ void __launch_bounds__(256)
     cp_async4(s_dst + e, pl.fe_dst + e0 + e);
   }
   cp_async_commit();
-  for (int e = threadIdx.x; e < fs * rw * kWarp; e += blockDim.x) Fm[e] = T(0);
+  {
+    // fs * rw * 32 elements is a multiple of 16 bytes: zero with 16-byte stores
+    float4* z4 = reinterpret_cast<float4*>(Fm);
+    const int n4 = fs * rw * kWarp * (int)sizeof(T) / 16;
+    for (int e = threadIdx.x; e < n4; e += blockDim.x) z4[e] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
   cp_async_wait<0>();
   __syncthreads();
 
@@ -182,7 +187,9 @@ __global__ void __launch_bounds__(256)
   // phase 2: assembly.  Warp w owns the destination-disjoint range
   // [split[8w/W], split[8(w+1)/W]); consecutive entries with one destination
   // are summed in a register (in list order) and stored once.
-  const int A = (int)(split[warp * 8 / W] - e0), Z = (int)(split[(warp + 1) * 8 / W] - e0);
+  const int wa = warp * 8 / W, wz = (warp + 1) * 8 / W;
+  const int A = wa == 0 ? 0 : pl.front_meta[(size_t)q * kFrontMetaInts + 11 + wa];
+  const int Z = pl.front_meta[(size_t)q * kFrontMetaInts + 11 + wz];
   int cur = -1;
   T acc = T(0);
   for (int c = 0; c < nchunks; ++c) {
@@ -254,12 +261,15 @@ __global__ void __launch_bounds__(256)
 
   // phase 3b: outputs of the pivot rows (U rows, y) ...
   const size_t b = col0 + lane;
-  const long long uo = pl.u_off[p], lo = pl.l_off[p], co = pl.cb_off[p];
-  const int first = pl.first[p];
+  const long long uo = m.uo, lo = m.lo, co = m.co;
+  const int first = m.first;
   {
-    T* Ub = U + (size_t)uo * Bp + b;
-    for (int k = 0; k < nc; ++k)
-      for (int j = warp; j < fs; j += W) Ub[(size_t)(k * fs + j) * Bp] = Fl[(k * rw + j) * kWarp];
+    const size_t step = (size_t)W * Bp;
+    for (int k = 0; k < nc; ++k) {
+      T* Ub = U + (size_t)(uo + (long long)k * fs + warp) * Bp + b;
+      const T* src = Fl + (k * rw + warp) * kWarp;
+      for (int j = warp; j < fs; j += W, Ub += step, src += W * kWarp) *Ub = *src;
+    }
     for (int k = warp; k < nc; k += W) Y[(size_t)(first + k) * Bp + b] = Fl[(k * rw + fs) * kWarp];
   }
   // ... and the uc non-pivot rows, independent of each other: row i applies
@@ -311,12 +321,13 @@ __global__ void __launch_bounds__(256)
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const long item = (long)blockIdx.x * (blockDim.x >> 5) + warp;
   if (item >= (long)level_count * groups) return;
-  const int p = pl.level_fronts[level_begin + item / groups];
+  const int q = level_begin + (int)(item / groups);
   const size_t col0 = (size_t)(item % groups) * kWarp;
   const size_t b = col0 + lane;
-  const int fs = pl.fsz[p], nc = pl.nc[p], uc = fs - nc;
-  const int fr0 = pl.front_ptr[p], first = pl.first[p];
-  const long long uo = pl.u_off[p];
+  const FrontMeta m = load_front_meta(pl.front_meta, q);
+  const int fs = m.fs, nc = m.nc, uc = fs - nc;
+  const int fr0 = m.fr0, first = m.first;
+  const long long uo = m.uo;
   T* Us = reinterpret_cast<T*>(smem_raw) + (size_t)warp * warp_elems * kWarp;  // [nc * fs][32]
   T* Xs = Us + (size_t)nc * fs * kWarp;                                         // [fs][32]
   // U rows: contiguous elements uo .. uo + nc * fs

@@ -147,3 +147,22 @@ def test_analysis_is_deterministic_across_threads():
     for t in ts:
         t.join()
     assert all(np.array_equal(out[0], o) for o in out[1:])
+
+
+def test_front_launch_records(analyzed):
+    """front_meta: one 24-int32 record per front in level order, consistent
+    with the plan arrays it summarises (the kernels read only the record)."""
+    s = analyzed("2000")
+    meta = s.plan_array("front_meta").reshape(-1, 24)
+    lf = s.plan_array("fp_level_fronts")
+    fsz, nc = s.plan_array("fp_fsz"), s.plan_array("fp_nc")
+    front_ptr = s.plan_array("front_ptr")
+    fe_ptr, u_off, cb_off = s.plan_array64("fe_ptr"), s.plan_array64("u_off"), s.plan_array64("cb_off")
+    split = s.plan_array64("fe_split").reshape(-1, 9)
+    wide = meta[:, 4:12].copy().view(np.int64)
+    assert np.array_equal(meta[:, 3], lf)
+    assert np.array_equal(meta[:, 0], fsz[lf]) and np.array_equal(meta[:, 1], nc[lf])
+    assert np.array_equal(wide[:, 0], fe_ptr[lf]) and np.array_equal(wide[:, 1], u_off[lf])
+    assert np.array_equal(wide[:, 3], cb_off[lf])
+    assert np.array_equal(meta[:, 12:20], (split[lf, 1:] - split[lf, :1]).astype(np.int32))
+    assert np.array_equal(meta[:, 20], front_ptr[lf])
