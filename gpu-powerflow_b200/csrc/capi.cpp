@@ -114,6 +114,13 @@ bool copy_plan_array(const Engine& e, const char* name, int32_t* out, int64_t ca
   return true;
 }
 
+// Stream of a device-pointer entry point: the caller's stream, where NULL is
+// the legacy default stream (torch's default stream reports handle 0), so
+// the engine's kernels stay ordered with the caller's earlier work on it.
+cudaStream_t caller_stream(void* stream) {
+  return stream ? static_cast<cudaStream_t>(stream) : cudaStreamLegacy;
+}
+
 const char* dtype_expected(const pf_options& o) { return o.compute == PF_COMPUTE_FP64 ? "float64" : "float32"; }
 
 }  // namespace
@@ -413,7 +420,34 @@ pf_status pf_solve_batch_device(pf_handle h, const double* sbus, int64_t sbus_st
     const pf_nr_config cfg = config ? *config : pf_nr_config{1e-8, 50};
     const int prep = solve_options ? solve_options->prepare_adjoint_cache : 0;
     const auto st = h->eng->solve_batch_device(sbus, sbus_stride, V0, V0_stride, batch, cfg.tolerance, cfg.max_iter,
-                                               prep, V_out, final_mismatch, static_cast<cudaStream_t>(stream));
+                                               prep, V_out, final_mismatch, caller_stream(stream));
+    if (result) {
+      std::memset(result, 0, sizeof(*result));
+      result->n_bus = h->n_bus;
+      result->batch_size = batch;
+      result->dim_f = h->eng->dim();
+      result->success = 1;
+      result->iterations = st.iterations;
+      result->max_final_mismatch = st.max_final_mismatch;
+      result->all_converged = st.all_converged;
+    }
+  })
+}
+
+pf_status pf_solve_batch_warm_device(pf_handle h, const double* sbus, int64_t sbus_stride, const double* V0,
+                                     int64_t V0_stride, const float* pred, int64_t pred_ld, int32_t batch,
+                                     const pf_nr_config* config, const pf_solve_options* solve_options,
+                                     double* V_out, double* final_mismatch, void* stream, pf_adjoint_result* result) {
+  if (!h || !h->eng) return PF_INVALID_ARGUMENT;
+  PF_TRY(h, {
+    if (!sbus || !V0 || !pred) throw std::invalid_argument("sbus/V0/pred must not be null");
+    if (sbus_stride < h->n_bus || (V0_stride != 0 && V0_stride < h->n_bus))
+      throw std::invalid_argument("stride must be at least n_bus (V0_stride 0 = one V0 row for every scenario)");
+    const pf_nr_config cfg = config ? *config : pf_nr_config{1e-8, 50};
+    const int prep = solve_options ? solve_options->prepare_adjoint_cache : 0;
+    const auto st = h->eng->solve_batch_warm_device(sbus, sbus_stride, V0, V0_stride, pred, pred_ld, batch,
+                                                    cfg.tolerance, cfg.max_iter, prep, V_out, final_mismatch,
+                                                    caller_stream(stream));
     if (result) {
       std::memset(result, 0, sizeof(*result));
       result->n_bus = h->n_bus;
@@ -447,7 +481,7 @@ pf_status pf_solve_forward_device(pf_handle h, const void* sbus_base_re, const v
     const int prep = solve_options ? solve_options->prepare_adjoint_cache : 0;
     const auto st = h->eng->solve_from_load(sbus_base_re, sbus_base_im, load_p, load_q, v0_va, v0_vm, batched_v0,
                                             va_out, vm_out, batch, want == "float64", cfg.tolerance, cfg.max_iter,
-                                            prep, static_cast<cudaStream_t>(stream), nullptr);
+                                            prep, caller_stream(stream), nullptr);
     if (result) {
       std::memset(result, 0, sizeof(*result));
       result->n_bus = n_bus;
@@ -473,7 +507,7 @@ pf_status pf_solve_backward_device(pf_handle h, const void* grad_va, const void*
     if (!grad_load_p || !grad_load_q) throw std::invalid_argument("output gradients must not be null");
     (void)options;
     const double res = h->eng->solve_adjoint_device(grad_va, grad_vm, grad_load_p, grad_load_q, nullptr, batch,
-                                                    want == "float64", static_cast<cudaStream_t>(stream));
+                                                    want == "float64", caller_stream(stream));
     if (result) {
       std::memset(result, 0, sizeof(*result));
       result->n_bus = n_bus;

@@ -15,6 +15,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <limits>
 #include <stdexcept>
 #include <string>
 
@@ -624,7 +625,13 @@ SolveStats Engine::run_loop(double tol, int32_t max_iter, int32_t prepare_adjoin
       double v;
       std::memcpy(&v, &d.h_norm[b], sizeof(double));
       d.h_final[b] = v;
-      if (!std::isfinite(v)) finite = false;
+      if (!std::isfinite(v)) {
+        if (tolerate_nonfinite_) {  // warm-started solves: the scenario failed, its fallback solves it
+          d.h_final[b] = std::numeric_limits<double>::infinity();
+          continue;
+        }
+        finite = false;
+      }
       gmax = std::max(gmax, v);
     }
     if (debug_sync()) std::fprintf(stderr, "[cupf] iteration %d max ||F||inf = %.3e\n", it, gmax);
@@ -724,6 +731,33 @@ SolveStats Engine::solve_batch_device(const double* d_sbus, int64_t sbus_stride,
                                       : run_loop<float>(tol, max_iter, prepare_adjoint, s, d_final_mismatch);
   if (d_v_out) launch_pack_voltage(d.g, st, d_v_out, s);
   launches_ += 2;
+  CUPF_CUDA(cudaStreamSynchronize(s));
+  return out;
+}
+
+SolveStats Engine::solve_batch_warm_device(const double* d_sbus, int64_t sbus_stride, const double* d_v0,
+                                           int64_t v0_stride, const float* d_pred, int64_t pred_ld, int32_t B,
+                                           double tol, int32_t max_iter, int32_t prepare_adjoint, double* d_v_out,
+                                           double* d_final_mismatch, cudaStream_t stream) {
+  if (!d_pred) throw std::invalid_argument("solve_batch_warm: prediction must not be null");
+  if (pred_ld < ja_.dim) throw std::invalid_argument("solve_batch_warm: prediction row stride must be >= dim_f");
+  ensure_workspace(B);
+  auto& d = *d_;
+  cudaStream_t s = stream ? stream : d.own;
+  const DevState st = d.state();
+  launch_seed_state(d.g, st, d_sbus, sbus_stride, d_v0, v0_stride, s);
+  launch_apply_warm(d.g, st, d_pred, pred_ld, s);
+  // a poor prediction may send a scenario to infinity: it is reported as not
+  // converged (final mismatch = inf) instead of failing the whole batch
+  struct Tolerate {
+    bool& f;
+    explicit Tolerate(bool& x) : f(x) { f = true; }
+    ~Tolerate() { f = false; }
+  } tolerate(tolerate_nonfinite_);
+  SolveStats out = factor_is_double() ? run_loop<double>(tol, max_iter, prepare_adjoint, s, d_final_mismatch)
+                                      : run_loop<float>(tol, max_iter, prepare_adjoint, s, d_final_mismatch);
+  if (d_v_out) launch_pack_voltage(d.g, st, d_v_out, s);
+  launches_ += 3;
   CUPF_CUDA(cudaStreamSynchronize(s));
   return out;
 }

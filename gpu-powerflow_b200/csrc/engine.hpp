@@ -70,6 +70,11 @@ class Engine {
   SolveStats solve_batch_device(const double* d_sbus, int64_t sbus_stride, const double* d_v0, int64_t v0_stride,
                                 int32_t B, double tol, int32_t max_iter, int32_t prepare_adjoint, double* d_v_out,
                                 double* d_final_mismatch, cudaStream_t stream);
+  // solve_batch_device from a predicted state (Jacobian-row order, fp32)
+  SolveStats solve_batch_warm_device(const double* d_sbus, int64_t sbus_stride, const double* d_v0, int64_t v0_stride,
+                                     const float* d_pred, int64_t pred_ld, int32_t B, double tol, int32_t max_iter,
+                                     int32_t prepare_adjoint, double* d_v_out, double* d_final_mismatch,
+                                     cudaStream_t stream);
   // torch-style: Sbus = base - load, V0 = (va0, vm0); base/v0 shared [n] or
   // v0 batched [B][n]; outputs Va/Vm [B][n]; float or double per is_double.
   SolveStats solve_from_load(const void* base_re, const void* base_im, const void* load_p, const void* load_q,
@@ -120,6 +125,7 @@ class Engine {
   int32_t B_ = 0;
   int64_t launches_ = 0;
   bool profiling_ = false;
+  bool tolerate_nonfinite_ = false;  // set during warm-started solves
   void stage_begin(int stage, cudaStream_t s);
   void stage_end(int stage, cudaStream_t s);
   void collect_stage_times();

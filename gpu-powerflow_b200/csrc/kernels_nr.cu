@@ -167,6 +167,30 @@ __global__ void k_voltage_update(DevGrid g, DevPlan pl, DevState st, const T* __
 // Layout conversions through a 32 x 32 shared tile: host arrays are
 // scenario-major [B][stride], the engine is bus-major [n][Bp].
 // Pad scenarios (B <= b < Bp) replicate scenario B - 1.
+// Warm start: overwrite the seeded angles / magnitudes with a prediction
+// given in Jacobian-row order (pred[b][row]: Va at the angle rows of the PV
+// and PQ buses, Vm at the magnitude rows of the PQ buses) and rebuild V.
+__global__ void k_apply_warm(DevGrid g, DevState st, const float* __restrict__ pred, long long ld) {
+  const int lane = threadIdx.x, wy = threadIdx.y;
+  const int Bp = st.Bp;
+  const int b = blockIdx.y * kWarp + lane;
+  const long long bb = b < st.B ? b : st.B - 1;
+  for (int i = blockIdx.x * kRows + wy; i < g.n_bus; i += gridDim.x * kRows) {
+    const int fa = g.bus_fa[i], fm = g.bus_fm[i];
+    if (fa < 0 && fm < 0) continue;
+    const size_t o = (size_t)i * Bp + b;
+    double va = st.va[o], vm = st.vm[o];
+    if (fa >= 0) va = (double)pred[bb * ld + fa];
+    if (fm >= 0) vm = (double)pred[bb * ld + fm];
+    st.va[o] = va;
+    st.vm[o] = vm;
+    double sn, cs;
+    sincos(va, &sn, &cs);
+    st.v_re[o] = vm * cs;
+    st.v_im[o] = vm * sn;
+  }
+}
+
 // ---------------------------------------------------------------------------
 __global__ void k_seed_state(DevGrid g, DevState st, const double* __restrict__ sbus_c, long long sbus_stride,
                              const double* __restrict__ v0_c, long long v0_stride) {
@@ -410,6 +434,10 @@ void launch_seed_state(const DevGrid& g, const DevState& st, const double* sbus_
                        const double* v0_c, long long v0_stride, cudaStream_t s) {
   dim3 grid((g.n_bus + kWarp - 1) / kWarp, st.Bp / kWarp);
   k_seed_state<<<grid, dim3(kWarp, kRows), 0, s>>>(g, st, sbus_c, sbus_stride, v0_c, v0_stride);
+}
+
+void launch_apply_warm(const DevGrid& g, const DevState& st, const float* pred, long long ld, cudaStream_t s) {
+  k_apply_warm<<<rows_grid(g.n_bus, st.Bp), dim3(kWarp, kRows), 0, s>>>(g, st, pred, ld);
 }
 
 void launch_pack_voltage(const DevGrid& g, const DevState& st, double* v_c, cudaStream_t s) {

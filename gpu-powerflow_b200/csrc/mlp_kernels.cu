@@ -1,0 +1,519 @@
+// mlp_kernels.cu -- BF16 training and inference kernels of the warm-start MLP.
+//
+// The network predicts each scenario's Newton starting point (Va, Vm) from its
+// loads.  Its dense layers are GEMM-shaped, so they run on the 5th-generation
+// tensor cores:
+//
+//   k_gemm_bf16   C[M,N] = A[M,K] * B[N,K]^T, A and B bf16 and K-contiguous,
+//                 fp32 accumulation in tensor memory.  One CTA computes a
+//                 128 x 128 tile: a producer thread streams 128 x 64 tiles of
+//                 A and B into shared memory with TMA (128-byte swizzle,
+//                 4-stage mbarrier ring), an MMA thread issues tcgen05.mma
+//                 (M = 128, N = 128, K = 16 per instruction) into a 128-column
+//                 TMEM accumulator, and the four warps read the accumulator
+//                 back (tcgen05.ld 32x32b) for a fused epilogue:
+//                   EPI_F32        out = acc                         (fp32)
+//                   EPI_BIAS_F32   out = acc + bias                  (fp32)
+//                   EPI_BIAS_GELU  z = acc + bias; aux = z; out = gelu(z)  (bf16)
+//                   EPI_DGELU      out = acc * gelu'(aux)            (bf16)
+//                 Every mbarrier wait is bounded; on a timeout the kernel
+//                 raises the error flag, still waits (bounded) for its own
+//                 MMAs and frees its TMEM before returning.
+//
+// plus the small element-wise and reduction kernels of a training step
+// (transpose, loss gradient, bias gradient, Adam).  GELU is the exact
+// erf form, 0.5 z (1 + erf(z / sqrt 2)).
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <tuple>
+
+#include "cupf_mlp.h"
+
+namespace cupf_b200 {
+namespace {
+
+constexpr int kBM = 128, kBN = 128, kBK = 64, kStages = 4, kThreads = 128;
+constexpr uint32_t kTileBytes = kBM * kBK * 2;  // 16 KB per operand tile (kBN == kBM)
+constexpr long long kSpinLimit = 1ll << 22;    // mbarrier polls before a wait gives up
+constexpr size_t kGemmSmem = 1024 + 2 * kStages * kTileBytes + 256;
+
+enum { EPI_F32 = 0, EPI_BIAS_F32 = 1, EPI_BIAS_GELU = 2, EPI_DGELU = 3 };
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// ---- mbarrier ----
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(done)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+// bounded wait: false when the phase did not complete within kSpinLimit polls
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  for (long long i = 0; i < kSpinLimit; ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
+// ---- TMA ----
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];\n" ::"r"(
+          smem_u32(dst)),
+      "l"(map), "r"(smem_u32(bar)), "r"(x), "r"(y)
+      : "memory");
+}
+
+// ---- tcgen05 ----
+__device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(slot)),
+               "r"(ncols)
+               : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(taddr), "r"(ncols) : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
+__device__ __forceinline__ void tc_mma(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d),
+      "l"(a), "l"(b), "r"(idesc), "r"(acc)
+      : "memory");
+}
+__device__ __forceinline__ void tc_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(smem_u32(bar))
+               : "memory");
+}
+// 32 consecutive fp32 columns of this thread's TMEM lane
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+        "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// Shared-memory matrix descriptor of a K-major bf16 tile written by TMA with
+// the 128-byte swizzle: rows of 64 elements (128 B), 8-row groups 1024 B apart.
+__device__ __forceinline__ uint64_t smem_desc_sw128(const void* tile) {
+  const uint64_t addr = smem_u32(tile);
+  uint64_t d = 0;
+  d |= (addr >> 4) & 0x3FFFull;      // start address
+  d |= (uint64_t)1 << 16;            // leading byte offset (unused for swizzled K-major)
+  d |= (uint64_t)(1024 >> 4) << 32;  // stride byte offset: next 8-row group
+  d |= (uint64_t)1 << 46;            // descriptor version for tcgen05
+  d |= (uint64_t)2 << 61;            // 128-byte swizzle
+  return d;
+}
+
+// Instruction descriptor: bf16 x bf16 -> fp32, both operands K-major, M x N.
+__host__ __device__ constexpr uint32_t idesc_bf16(int m, int n) {
+  return (1u << 4)                     // D format fp32
+         | (1u << 7)                   // A format bf16
+         | (1u << 10)                  // B format bf16
+         | ((uint32_t)(n >> 3) << 17)  // N / 8
+         | ((uint32_t)(m >> 4) << 24); // M / 16
+}
+
+__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+__device__ __forceinline__ float gelu_grad(float z) {
+  return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) + z * 0.3989422804014327f * expf(-0.5f * z * z);
+}
+
+struct GemmArgs {
+  int M, N, K;
+  void* out;           // [M][ldo] fp32 or bf16
+  long long ldo;
+  const float* bias;   // [N]
+  __nv_bfloat16* aux;  // [M][ldaux] pre-activations (written by EPI_BIAS_GELU, read by EPI_DGELU)
+  long long ldaux;
+  int epi;
+  int* error;
+};
+
+__global__ void __launch_bounds__(kThreads, 1)
+    k_gemm_bf16(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, GemmArgs g) {
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base =
+      reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  unsigned char* sA = base;
+  unsigned char* sB = base + kStages * kTileBytes;
+  uint64_t* full = reinterpret_cast<uint64_t*>(base + 2 * kStages * kTileBytes);
+  uint64_t* empty = full + kStages;
+  uint64_t* done = empty + kStages;
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int m0 = blockIdx.y * kBM, n0 = blockIdx.x * kBN;
+  const int nk = g.K / kBK;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(full + s, 1);
+      mbar_init(empty + s, 1);
+    }
+    mbar_init(done, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (warp == 0) tmem_alloc(tslot, kBN);
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tslot;
+  bool ok = true;
+
+  if (threadIdx.x == 0) {
+    // producer: stage s holds k-block kb; refill it once the MMAs of kb - kStages are done
+    for (int kb = 0; kb < nk; ++kb) {
+      const int s = kb % kStages;
+      if (kb >= kStages && !mbar_wait(empty + s, ((kb / kStages) - 1) & 1)) {
+        ok = false;
+        break;
+      }
+      mbar_expect_tx(full + s, 2 * kTileBytes);
+      tma_load_2d(sA + s * kTileBytes, &ta, kb * kBK, m0, full + s);
+      tma_load_2d(sB + s * kTileBytes, &tb, kb * kBK, n0, full + s);
+    }
+  } else if (threadIdx.x == 32) {
+    // MMA issuer
+    constexpr uint32_t idesc = idesc_bf16(kBM, kBN);
+    for (int kb = 0; kb < nk; ++kb) {
+      const int s = kb % kStages;
+      if (!mbar_wait(full + s, (kb / kStages) & 1)) {
+        ok = false;
+        break;
+      }
+      tc_fence_after();
+      const uint64_t da = smem_desc_sw128(sA + s * kTileBytes), db = smem_desc_sw128(sB + s * kTileBytes);
+#pragma unroll
+      for (int k = 0; k < kBK / 16; ++k)  // K = 16 per instruction: advance 32 bytes inside the swizzled row
+        tc_mma(tmem, da + (uint64_t)(2 * k), db + (uint64_t)(2 * k), idesc, (kb > 0 || k > 0) ? 1u : 0u);
+      tc_commit(empty + s);
+    }
+    tc_commit(done);  // arrives once every MMA issued above has completed
+  }
+  if (!ok) atomicExch(g.error, 1);
+
+  // every lane waits, then the warp agrees, so the .sync.aligned loads below
+  // run warp-converged
+  const bool have = __all_sync(0xffffffffu, mbar_wait(done, 0));
+  tc_fence_after();
+  if (!have) {
+    if (threadIdx.x == 0) atomicExch(g.error, 2);
+  } else {
+    const int row = m0 + warp * 32 + lane;
+    const uint32_t tl = tmem + ((uint32_t)(warp * 32) << 16);
+    for (int c0 = 0; c0 < kBN; c0 += 32) {
+      float v[32];
+      tmem_ld32(tl + (uint32_t)c0, v);
+      const int col = n0 + c0;
+      if (g.epi == EPI_F32 || g.epi == EPI_BIAS_F32) {
+        if (g.epi == EPI_BIAS_F32)
+#pragma unroll
+          for (int i = 0; i < 32; ++i) v[i] += g.bias[col + i];
+        float4* o = reinterpret_cast<float4*>(static_cast<float*>(g.out) + (size_t)row * g.ldo + col);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) o[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+      } else {
+        __nv_bfloat16* aux = g.aux + (size_t)row * g.ldaux + col;
+        __align__(16) __nv_bfloat16 ob[32];
+        if (g.epi == EPI_BIAS_GELU) {
+          __align__(16) __nv_bfloat16 zb[32];
+#pragma unroll
+          for (int i = 0; i < 32; ++i) {
+            const float z = v[i] + g.bias[col + i];
+            zb[i] = __float2bfloat16(z);
+            ob[i] = __float2bfloat16(gelu(z));
+          }
+#pragma unroll
+          for (int i = 0; i < 4; ++i) reinterpret_cast<uint4*>(aux)[i] = reinterpret_cast<const uint4*>(zb)[i];
+        } else {  // EPI_DGELU
+          __align__(16) __nv_bfloat16 zb[32];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) reinterpret_cast<uint4*>(zb)[i] = reinterpret_cast<const uint4*>(aux)[i];
+#pragma unroll
+          for (int i = 0; i < 32; ++i) ob[i] = __float2bfloat16(v[i] * gelu_grad(__bfloat162float(zb[i])));
+        }
+        uint4* o = reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(g.out) + (size_t)row * g.ldo + col);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) o[i] = reinterpret_cast<const uint4*>(ob)[i];
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, kBN);
+}
+
+// ---- element-wise / reduction kernels ----
+
+// out[c][r] = in[r][c] for a rows x cols bf16 matrix with row stride ld (32 x 32 tiles through shared memory)
+__global__ void k_transpose_bf16(const __nv_bfloat16* __restrict__ in, long long ld, __nv_bfloat16* __restrict__ out,
+                                 int rows, int cols) {
+  __shared__ __nv_bfloat16 t[32][33];
+  const int c = blockIdx.x * 32 + threadIdx.x;
+  for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+    const int r = blockIdx.y * 32 + i;
+    if (r < rows && c < cols) t[i][threadIdx.x] = in[(size_t)r * ld + c];
+  }
+  __syncthreads();
+  const int r = blockIdx.y * 32 + threadIdx.x;
+  for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+    const int cc = blockIdx.x * 32 + i;
+    if (r < rows && cc < cols) out[(size_t)cc * rows + r] = t[threadIdx.x][i];
+  }
+}
+
+// features: x[b][k] = bf16((raw[b][k] - mean[k]) * inv_std[k]) for k < n_in, 0 for n_in <= k < width
+// (x has row stride ldx)
+__global__ void k_standardize(const float* __restrict__ raw, const float* __restrict__ mean,
+                              const float* __restrict__ inv_std, __nv_bfloat16* __restrict__ x, long long ldx, int B,
+                              int n_in, int width) {
+  const long long n = (long long)B * width;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(i % width);
+    const long long b = i / width;
+    x[b * ldx + k] = __float2bfloat16(k < n_in ? (raw[b * n_in + k] - mean[k]) * inv_std[k] : 0.0f);
+  }
+}
+
+// mean-squared-error gradient on the first n_out columns:
+// g = 2 (pred - target) / (B n_out) in bf16 (0 in padding), loss += sum (pred - target)^2 / (B n_out)
+__global__ void k_mse_grad(const float* __restrict__ pred, int ld, const float* __restrict__ target, int n_out, int B,
+                           __nv_bfloat16* __restrict__ grad, float* __restrict__ loss) {
+  const long long n = (long long)B * ld;
+  const float scale = 1.0f / ((float)B * (float)n_out);
+  float local = 0.0f;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(i % ld);
+    const long long b = i / ld;
+    float gval = 0.0f;
+    if (k < n_out) {
+      const float d = pred[i] - target[b * n_out + k];
+      gval = 2.0f * d * scale;
+      local += d * d * scale;
+    }
+    grad[i] = __float2bfloat16(gval);
+  }
+  for (int o = 16; o > 0; o >>= 1) local += __shfl_xor_sync(0xffffffffu, local, o);
+  if ((threadIdx.x & 31) == 0 && loss) atomicAdd(loss, local);
+}
+
+// column sums of a bf16 [rows][cols] matrix into fp32 [cols]
+__global__ void k_col_sum_bf16(const __nv_bfloat16* __restrict__ g, int rows, int cols, float* __restrict__ out) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= cols) return;
+  float s = 0.0f;
+  for (int r = 0; r < rows; ++r) s += __bfloat162float(g[(size_t)r * cols + c]);
+  out[c] = s;
+}
+
+// Adam on fp32 master weights; refreshes the bf16 copy used by the GEMMs.
+__global__ void k_adam(float* __restrict__ w, const float* __restrict__ grad, float* __restrict__ m,
+                       float* __restrict__ v, __nv_bfloat16* __restrict__ w16, long long n, float lr, float b1,
+                       float b2, float eps, float bc1, float bc2, float weight_decay) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float gi = grad[i] + weight_decay * w[i];
+    const float mi = b1 * m[i] + (1.0f - b1) * gi;
+    const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    const float wi = w[i] - lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
+    w[i] = wi;
+    if (w16) w16[i] = __float2bfloat16(wi);
+  }
+}
+
+// ---- host side ----
+
+thread_local std::string g_err;
+
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiled encoder() {
+  static EncodeTiled fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiled>(p);
+  });
+  if (!fn) throw std::runtime_error("cuTensorMapEncodeTiled is not available");
+  return fn;
+}
+
+// [rows][k] bf16 with row stride ld, K contiguous, boxes of 128 rows x 64 elements, 128-byte swizzle
+CUtensorMap make_map(const void* ptr, int rows, int k, long long ld) {
+  CUtensorMap m;
+  const cuuint64_t dims[2] = {(cuuint64_t)k, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
+  const cuuint32_t box[2] = {(cuuint32_t)kBK, (cuuint32_t)kBM};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = encoder()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(ptr), dims, strides, box,
+                               estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) throw std::runtime_error("cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+  return m;
+}
+
+int* error_flag() {
+  static std::mutex mu;
+  static std::map<int, int*> flags;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lock(mu);
+  int*& f = flags[dev];
+  if (!f) {
+    if (cudaMalloc(&f, sizeof(int)) != cudaSuccess) throw std::runtime_error("error flag allocation failed");
+    cudaMemset(f, 0, sizeof(int));
+  }
+  return f;
+}
+
+void configure_gemm() {
+  static std::mutex mu;
+  static std::map<int, bool> done;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lock(mu);
+  if (done[dev]) return;
+  const cudaError_t e = cudaFuncSetAttribute(k_gemm_bf16, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem);
+  if (e != cudaSuccess) throw std::runtime_error(std::string("gemm smem attribute: ") + cudaGetErrorString(e));
+  done[dev] = true;
+}
+
+unsigned grid1d(long long n) { return (unsigned)std::min<long long>((n + 255) / 256, 148LL * 16); }
+
+template <typename F>
+int guarded(F&& f) {
+  try {
+    f();
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+      g_err = cudaGetErrorString(e);
+      return 2;
+    }
+    return 0;
+  } catch (const std::exception& ex) {
+    g_err = ex.what();
+    return 1;
+  }
+}
+
+}  // namespace
+}  // namespace cupf_b200
+
+using namespace cupf_b200;
+
+extern "C" {
+
+const char* mlp_last_error() { return g_err.c_str(); }
+
+int mlp_gemm_bf16(const void* A, long long lda, const void* B, long long ldb, int M, int N, int K, int epi,
+                  void* out, long long ldo, const float* bias, void* aux, long long ldaux, void* stream) {
+  return guarded([&] {
+    if (M <= 0 || N <= 0 || K <= 0 || M % kBM || N % kBN || K % kBK)
+      throw std::invalid_argument("mlp_gemm_bf16: M and N must be multiples of 128, K of 64");
+    if (epi < EPI_F32 || epi > EPI_DGELU) throw std::invalid_argument("mlp_gemm_bf16: unknown epilogue");
+    if ((epi == EPI_BIAS_F32 || epi == EPI_BIAS_GELU) && !bias) throw std::invalid_argument("mlp_gemm_bf16: bias missing");
+    if ((epi == EPI_BIAS_GELU || epi == EPI_DGELU) && (!aux || ldaux < N))
+      throw std::invalid_argument("mlp_gemm_bf16: aux missing");
+    if (lda < K || ldb < K || ldo < N || lda % 8 || ldb % 8 || ldo % 8)
+      throw std::invalid_argument("mlp_gemm_bf16: leading dimensions must be >= the row length and multiples of 8");
+    if ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B) | reinterpret_cast<uintptr_t>(out)) & 15)
+      throw std::invalid_argument("mlp_gemm_bf16: operands must be 16-byte aligned");
+    configure_gemm();
+    const CUtensorMap ta = make_map(A, M, K, lda), tb = make_map(B, N, K, ldb);
+    GemmArgs g{M, N, K, out, ldo, bias, static_cast<__nv_bfloat16*>(aux), ldaux, epi, error_flag()};
+    k_gemm_bf16<<<dim3(N / kBN, M / kBM), kThreads, kGemmSmem, static_cast<cudaStream_t>(stream)>>>(ta, tb, g);
+  });
+}
+
+int mlp_error_flag(int* out_host, int reset) {
+  return guarded([&] {
+    int* f = error_flag();
+    if (cudaMemcpy(out_host, f, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+      throw std::runtime_error("error flag read failed");
+    if (reset) cudaMemset(f, 0, sizeof(int));
+  });
+}
+
+int mlp_transpose_bf16(const void* in, long long ld, void* out, int rows, int cols, void* stream) {
+  return guarded([&] {
+    if (ld < cols) throw std::invalid_argument("mlp_transpose_bf16: ld must be >= cols");
+    dim3 grid((cols + 31) / 32, (rows + 31) / 32);
+    k_transpose_bf16<<<grid, dim3(32, 8), 0, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<const __nv_bfloat16*>(in), ld, static_cast<__nv_bfloat16*>(out), rows, cols);
+  });
+}
+
+int mlp_standardize(const float* raw, const float* mean, const float* inv_std, void* x, long long ldx, int B,
+                    int n_in, int width, void* stream) {
+  return guarded([&] {
+    if (ldx < width || width < n_in) throw std::invalid_argument("mlp_standardize: need n_in <= width <= ldx");
+    k_standardize<<<grid1d((long long)B * width), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        raw, mean, inv_std, static_cast<__nv_bfloat16*>(x), ldx, B, n_in, width);
+  });
+}
+
+int mlp_mse_grad(const float* pred, int ld, const float* target, int n_out, int B, void* grad, float* loss,
+                 void* stream) {
+  return guarded([&] {
+    k_mse_grad<<<grid1d((long long)B * ld), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        pred, ld, target, n_out, B, static_cast<__nv_bfloat16*>(grad), loss);
+  });
+}
+
+int mlp_col_sum_bf16(const void* g, int rows, int cols, float* out, void* stream) {
+  return guarded([&] {
+    k_col_sum_bf16<<<(cols + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<const __nv_bfloat16*>(g), rows, cols, out);
+  });
+}
+
+int mlp_adam(float* w, const float* grad, float* m, float* v, void* w_bf16, long long n, float lr, float b1, float b2,
+             float eps, int step, float weight_decay, void* stream) {
+  return guarded([&] {
+    const float bc1 = 1.0f - std::pow(b1, (float)step), bc2 = 1.0f - std::pow(b2, (float)step);
+    k_adam<<<grid1d(n), 256, 0, static_cast<cudaStream_t>(stream)>>>(w, grad, m, v, static_cast<__nv_bfloat16*>(w_bf16),
+                                                                      n, lr, b1, b2, eps, bc1, bc2, weight_decay);
+  });
+}
+
+}  // extern "C"

@@ -468,6 +468,28 @@ class NewtonSolver:
             fm.data_ptr(), C.c_void_p(stream), C.byref(raw)))
         return v_out, fm, raw.iterations
 
+    def solve_batch_warm_device(self, sbus, v0, pred, v_out=None, config=None, solve_options=None):
+        """Device-resident solve from a predicted state: pred is a float32 CUDA
+        tensor [batch, >= dim_f] in Jacobian-row order (Va at the PV and PQ
+        angle rows, Vm at the PQ magnitude rows); v0 complex128 [n_bus] (one
+        row for every scenario) or [batch, n_bus] supplies the other buses."""
+        import torch
+
+        B, n = sbus.shape
+        if pred.dtype != torch.float32 or pred.dim() != 2 or pred.shape[0] != B or not pred.is_contiguous():
+            raise ValueError("pred must be a contiguous float32 tensor [batch, >= dim_f]")
+        v0_stride = 0 if v0.dim() == 1 else n
+        if v_out is None:
+            v_out = torch.empty_like(sbus)
+        fm = torch.empty(B, dtype=torch.float64, device=sbus.device)
+        stream = torch.cuda.current_stream(sbus.device).cuda_stream
+        raw = _capi.PfAdjointResult()
+        cfg, so = _nr_config(config), _solve_options(solve_options)
+        _check(self._lib, self._h, self._lib.pf_solve_batch_warm_device(
+            self._h, sbus.data_ptr(), n, v0.data_ptr(), v0_stride, pred.data_ptr(), pred.shape[1], B, C.byref(cfg),
+            C.byref(so), v_out.data_ptr(), fm.data_ptr(), C.c_void_p(stream), C.byref(raw)))
+        return v_out, fm, raw.iterations
+
     def info(self) -> dict:
         inf = _capi.PfInfo()
         _check(self._lib, self._h, self._lib.pf_info(self._h, C.byref(inf)))

@@ -59,8 +59,14 @@ EXPORTS = [
     "cls_solve", "cls_solve_transpose", "cls_singular_flags", "cls_status_string", "cls_last_error",
     "cls_plan_array",
     "pf_create", "pf_destroy", "pf_last_error", "pf_initialize", "pf_analyze_host", "pf_solve_batch", "pf_solve_batch_device",
-    "pf_solve_forward_device", "pf_solve_backward_device", "pf_solve_adjoint", "pf_info", "pf_plan_array",
+    "pf_solve_batch_warm_device", "pf_solve_forward_device", "pf_solve_backward_device", "pf_solve_adjoint",
+    "pf_info", "pf_plan_array",
     "pf_evaluate", "pf_set_profiling", "pf_stage_times", "pf_plan_array64", "pf_singular_flags",
+]
+# exported symbols of include/cupf_mlp.h (warm-start network kernels)
+MLP_EXPORTS = [
+    "mlp_last_error", "mlp_gemm_bf16", "mlp_error_flag", "mlp_transpose_bf16", "mlp_standardize", "mlp_mse_grad",
+    "mlp_col_sum_bf16", "mlp_adam",
 ]
 
 _vp = C.c_void_p
@@ -94,6 +100,8 @@ def _declare(lib: C.CDLL) -> None:
                             _p(PfNRConfig), _p(PfSolveOptions), _vp, _vp, _vp, _vp], _i32),
         "pf_solve_batch_device": ([_vp, _vp, _i64, _vp, _i64, _i32, _p(PfNRConfig), _p(PfSolveOptions), _vp, _vp,
                                    _vp, _p(PfAdjointResult)], _i32),
+        "pf_solve_batch_warm_device": ([_vp, _vp, _i64, _vp, _i64, _vp, _i64, _i32, _p(PfNRConfig),
+                                        _p(PfSolveOptions), _vp, _vp, _vp, _p(PfAdjointResult)], _i32),
         "pf_solve_forward_device": ([_vp, _vp, _vp, _vp, _vp, _vp, _vp, _i32, _vp, _vp, _i32, _i32, C.c_char_p,
                                      _p(PfNRConfig), _p(PfSolveOptions), _vp, _p(PfAdjointResult)], _i32),
         "pf_solve_backward_device": ([_vp, _vp, _vp, _vp, _vp, _i32, _i32, C.c_char_p, _p(PfAdjointOptions), _vp,
@@ -107,6 +115,15 @@ def _declare(lib: C.CDLL) -> None:
         "pf_plan_array64": ([_vp, C.c_char_p, _vp, _i64, _p(_i64)], _i32),
         "pf_stage_times": ([_vp, _vp, _vp], _i32),
         "pf_singular_flags": ([_vp, _vp, _i32], _i32),
+        "mlp_last_error": ([], C.c_char_p),
+        "mlp_gemm_bf16": ([_vp, _i64, _vp, _i64, _i32, _i32, _i32, _i32, _vp, _i64, _vp, _vp, _i64, _vp], _i32),
+        "mlp_error_flag": ([_p(_i32), _i32], _i32),
+        "mlp_transpose_bf16": ([_vp, _i64, _vp, _i32, _i32, _vp], _i32),
+        "mlp_standardize": ([_vp, _vp, _vp, _vp, _i64, _i32, _i32, _i32, _vp], _i32),
+        "mlp_mse_grad": ([_vp, _i32, _vp, _i32, _i32, _vp, _vp, _vp], _i32),
+        "mlp_col_sum_bf16": ([_vp, _i32, _i32, _vp, _vp], _i32),
+        "mlp_adam": ([_vp, _vp, _vp, _vp, _vp, _i64, C.c_float, C.c_float, C.c_float, C.c_float, _i32, C.c_float,
+                      _vp], _i32),
     }
     for name, (args, res) in s.items():
         f = getattr(lib, name)

@@ -1,0 +1,362 @@
+"""Learned warm start for batched Newton solves.
+
+A multilayer perceptron maps each scenario's loads (P and Q at every bus) and
+its PV voltage setpoints to a starting state: Va at the PV and PQ buses and
+Vm at the PQ buses, in the Jacobian-row order the engine's warm entry point
+reads (``NewtonSolver.solve_batch_warm_device``).  Newton then runs from that
+prediction to the same tolerance as from a flat start; scenarios that do not
+converge within the iteration cap are solved again from the flat start.
+
+The network is trained on solutions the engine itself produces, with the
+engine's own BF16 kernels (include/cupf_mlp.h): tcgen05 GEMMs with fused
+bias + GELU epilogues for the forward pass, GELU-derivative epilogues and
+transposed GEMMs for the backward pass, and Adam on FP32 master weights.
+torch only allocates the buffers.  Layer widths are padded to multiples of
+128 (the GEMM tile); padded rows and columns stay exactly zero.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import time
+
+import numpy as np
+
+from . import _capi
+
+EPI_F32, EPI_BIAS_F32, EPI_BIAS_GELU, EPI_DGELU = 0, 1, 2, 3
+
+
+def _round_up(x: int, m: int) -> int:
+    return (x + m - 1) // m * m
+
+
+def _ptr(t) -> C.c_void_p:
+    return C.c_void_p(t.data_ptr())
+
+
+class MLP:
+    """Dense GELU network with BF16 weights and activations, FP32 accumulation,
+    FP32 master weights (Adam).  All compute goes through the mlp_* kernels.
+
+    Hidden layers: a_{l+1} = gelu(a_l W_l^T + b_l).  With skip=True the output
+    layer reads [a_L | x] (the last hidden activation next to the standardized
+    input), so the dominant, nearly linear part of the load-to-state map has a
+    direct path and the GELU stack learns the nonlinear remainder."""
+
+    def __init__(self, n_in: int, n_out: int, hidden: int = 1024, layers: int = 3, seed: int = 0,
+                 device=None, skip: bool = True):
+        import torch
+
+        if hidden % 128:
+            raise ValueError("hidden width must be a multiple of 128")
+        self.lib = _capi.load()
+        self.torch = torch
+        self.dev = torch.device(device or "cuda")
+        self.n_in, self.n_out, self.hidden, self.layers, self.skip = n_in, n_out, hidden, layers, skip
+        self.k0, self.no = _round_up(n_in, 128), _round_up(n_out, 128)
+        self.cat_w = hidden + (self.k0 if skip else 0)   # width of the output layer's input
+        self.dims_in = [self.k0] + [hidden] * (layers - 1) + [self.cat_w]
+        self.dims_out = [hidden] * layers + [self.no]
+        gen = torch.Generator().manual_seed(seed)
+        self.W, self.b, self.W16, self.WT16, self.mW, self.vW, self.mb, self.vb = [], [], [], [], [], [], [], []
+        for i in range(layers + 1):
+            d_in, d_out = self.dims_in[i], self.dims_out[i]
+            real_out = n_out if i == layers else hidden
+            w = torch.zeros(d_out, d_in)
+            if i == 0:
+                w[:, :n_in] = torch.randn(d_out, n_in, generator=gen) * math.sqrt(2.0 / n_in)
+            elif i < layers:
+                w[:] = torch.randn(d_out, d_in, generator=gen) * math.sqrt(2.0 / hidden)
+            else:
+                fan = hidden + (n_in if skip else 0)
+                w[:real_out, :hidden] = torch.randn(real_out, hidden, generator=gen) * math.sqrt(1.0 / fan)
+                if skip:
+                    w[:real_out, hidden:hidden + n_in] = torch.randn(real_out, n_in, generator=gen) * math.sqrt(1.0 / fan)
+            w = w.to(self.dev)
+            self.W.append(w)
+            self.b.append(torch.zeros(d_out, device=self.dev))
+            self.W16.append(w.to(torch.bfloat16).contiguous())
+            self.WT16.append(torch.empty(d_in, d_out, dtype=torch.bfloat16, device=self.dev))
+            self.mW.append(torch.zeros_like(w))
+            self.vW.append(torch.zeros_like(w))
+            self.mb.append(torch.zeros(d_out, device=self.dev))
+            self.vb.append(torch.zeros(d_out, device=self.dev))
+        self._refresh_transposes()
+        self.step = 0
+        self._bufs: dict[int, dict] = {}
+
+    # -- low-level wrappers --
+    def _stream(self):
+        return C.c_void_p(self.torch.cuda.current_stream(self.dev).cuda_stream)
+
+    def _check(self, rc: int) -> None:
+        if rc:
+            raise RuntimeError("mlp kernel: " + self.lib.mlp_last_error().decode())
+
+    def gemm(self, A, B, out, epi: int, bias=None, aux=None) -> None:
+        """out = epilogue(A B^T); A [M, K], B [N, K], out [M, N]: 2-D views with unit column stride."""
+        M, K = A.shape
+        N = B.shape[0]
+        for t in (A, B, out) + ((aux,) if aux is not None else ()):
+            if t.stride(1) != 1:
+                raise ValueError("gemm operands need unit column stride")
+        self._check(self.lib.mlp_gemm_bf16(_ptr(A), A.stride(0), _ptr(B), B.stride(0), M, N, K, epi, _ptr(out),
+                                           out.stride(0), _ptr(bias) if bias is not None else None,
+                                           _ptr(aux) if aux is not None else None,
+                                           aux.stride(0) if aux is not None else 0, self._stream()))
+
+    def transpose(self, a, out) -> None:
+        r, c = a.shape
+        self._check(self.lib.mlp_transpose_bf16(_ptr(a), a.stride(0), _ptr(out), r, c, self._stream()))
+
+    def _refresh_transposes(self) -> None:
+        for i in range(1, self.layers + 1):
+            self.transpose(self.W16[i], self.WT16[i])
+
+    def buffers(self, B: int) -> dict:
+        if B % 128:
+            raise ValueError("batch must be a multiple of 128")
+        if B not in self._bufs:
+            t, d = self.torch, self.dev
+            bf = t.bfloat16
+            H, L = self.hidden, self.layers
+            cat = t.zeros(B, self.cat_w if self.skip else H, dtype=bf, device=d)
+            xbuf = cat[:, H:] if self.skip else t.zeros(B, self.k0, dtype=bf, device=d)
+            acts = [t.empty(B, H, dtype=bf, device=d) for _ in range(L - 1)] + [cat[:, :H]]
+            h = {"cat": cat, "x": xbuf, "a": acts,
+                 "z": [t.empty(B, H, dtype=bf, device=d) for _ in range(L)],
+                 "p": t.empty(B, self.no, device=d),
+                 "gp": t.empty(B, self.no, dtype=bf, device=d),
+                 "g": [t.empty(B, H, dtype=bf, device=d) for _ in range(2)],
+                 "gT": t.empty(max(self.no, H), B, dtype=bf, device=d),
+                 "actT": t.empty(max(self.dims_in), B, dtype=bf, device=d),
+                 "gW": [t.empty(self.dims_out[i], self.dims_in[i], device=d) for i in range(L + 1)],
+                 "gb": [t.empty(self.dims_out[i], device=d) for i in range(L + 1)],
+                 "loss": t.zeros(1, device=d)}
+            self._bufs[B] = h
+        return self._bufs[B]
+
+    def _layer_input(self, h: dict, i: int):
+        if i == 0:
+            return h["x"]
+        if i == self.layers:
+            return h["cat"] if self.skip else h["a"][-1]
+        return h["a"][i - 1]
+
+    # -- passes --
+    def forward(self, h: dict):
+        """Forward pass on the standardized features in h['x']; fp32 [B, no] outputs."""
+        for i in range(self.layers):
+            self.gemm(self._layer_input(h, i), self.W16[i], h["a"][i], EPI_BIAS_GELU, bias=self.b[i], aux=h["z"][i])
+        self.gemm(self._layer_input(h, self.layers), self.W16[self.layers], h["p"], EPI_BIAS_F32,
+                  bias=self.b[self.layers])
+        return h["p"]
+
+    def backward(self, h: dict, target) -> None:
+        """Gradients of the mean-squared error against target (fp32 [B, n_out])
+        into h['gW'] / h['gb']; the loss accumulates into h['loss']."""
+        B = h["p"].shape[0]
+        self._check(self.lib.mlp_mse_grad(_ptr(h["p"]), self.no, _ptr(target), self.n_out, B, _ptr(h["gp"]),
+                                          _ptr(h["loss"]), self._stream()))
+        g = h["gp"]
+        H = self.hidden
+        for i in range(self.layers, -1, -1):
+            d_out, d_in = self.dims_out[i], self.dims_in[i]
+            act = self._layer_input(h, i)
+            gT = h["gT"][:d_out]
+            actT = h["actT"][:d_in]
+            self.transpose(g, gT)
+            self.transpose(act, actT)
+            self.gemm(gT, actT, h["gW"][i], EPI_F32)                    # dW = g^T act
+            self._check(self.lib.mlp_col_sum_bf16(_ptr(g), B, d_out, _ptr(h["gb"][i]), self._stream()))
+            if i > 0:
+                gn = h["g"][i % 2]
+                # (g W)[:, hidden part] * gelu'(z): the rows of W^T that multiply a_{i-1}
+                self.gemm(g, self.WT16[i][:H], gn, EPI_DGELU, aux=h["z"][i - 1])
+                g = gn
+
+    def adam(self, h: dict, lr: float, b1: float = 0.9, b2: float = 0.999, eps: float = 1e-8,
+             wd: float = 0.0) -> None:
+        """One Adam step from the gradients in buffer set h; refreshes the bf16
+        weights and their transposes."""
+        self.step += 1
+        for i in range(self.layers + 1):
+            self._check(self.lib.mlp_adam(_ptr(self.W[i]), _ptr(h["gW"][i]), _ptr(self.mW[i]), _ptr(self.vW[i]),
+                                          _ptr(self.W16[i]), self.W[i].numel(), lr, b1, b2, eps, self.step, wd,
+                                          self._stream()))
+            self._check(self.lib.mlp_adam(_ptr(self.b[i]), _ptr(h["gb"][i]), _ptr(self.mb[i]), _ptr(self.vb[i]),
+                                          None, self.b[i].numel(), lr, b1, b2, eps, self.step, 0.0, self._stream()))
+        self._refresh_transposes()
+
+    def train_step(self, h: dict, target, lr: float) -> None:
+        """Forward, backward and Adam on the features already standardized in h['x']."""
+        self.forward(h)
+        self.backward(h, target)
+        self.adam(h, lr)
+
+    def standardize(self, h: dict, raw, mean, inv_std) -> None:
+        x = h["x"]
+        self._check(self.lib.mlp_standardize(_ptr(raw), _ptr(mean), _ptr(inv_std), _ptr(x), x.stride(0),
+                                             raw.shape[0], self.n_in, self.k0, self._stream()))
+
+    def error_flag(self) -> int:
+        v = C.c_int32(0)
+        self._check(self.lib.mlp_error_flag(C.byref(v), 1))
+        return v.value
+
+
+class WarmStart:
+    """Warm-start predictor for one grid (features: P and Q loads at every bus
+    and the PV setpoints; outputs: the Newton unknowns in Jacobian-row order)."""
+
+    def __init__(self, grid, hidden: int = 1024, layers: int = 3, seed: int = 0, device=None, skip: bool = True):
+        import torch
+
+        self.torch = torch
+        self.g = grid
+        self.dev = torch.device(device or "cuda")
+        self.n_pvpq = grid.pv.size + grid.pq.size
+        self.n_in = 2 * grid.n_bus + grid.pv.size
+        self.n_out = self.n_pvpq + grid.pq.size
+        self.mlp = MLP(self.n_in, self.n_out, hidden, layers, seed, self.dev, skip=skip)
+        self.pvpq = torch.tensor(np.concatenate([grid.pv, grid.pq]), dtype=torch.long, device=self.dev)
+        self.pq = torch.tensor(grid.pq, dtype=torch.long, device=self.dev)
+        self.vm_pv = torch.tensor(np.abs(grid.v0[grid.pv]), dtype=torch.float32, device=self.dev)
+        self.sgen = torch.tensor(grid.sgen, device=self.dev)
+        self.v0 = torch.tensor(grid.v0, device=self.dev)
+        self.x_mean = self.x_istd = self.y_mean = self.y_std = None
+        self.va_ref = None  # angles of the nominal-load solution: the unwrapping reference
+        self.history: list[float] = []
+
+    # -- data --
+    def features(self, sbus):
+        """Raw features fp32 [B, n_in] from Sbus (complex128 [B, n]): load = Sgen - Sbus."""
+        t = self.torch
+        load = self.sgen[None, :] - sbus
+        B = sbus.shape[0]
+        return t.cat([load.real.float(), load.imag.float(), self.vm_pv[None, :].expand(B, -1)], dim=1).contiguous()
+
+    def targets(self, V):
+        """Newton unknowns of solved states V [B, n]: Va at the PV+PQ buses and
+        Vm at the PQ buses.  Bus angles on a large grid span more than 2 pi, so
+        each angle is unwrapped to within pi of the nominal-load solution's
+        (Newton only sees V = Vm e^{j Va}, so any 2 pi offset is harmless)."""
+        t = self.torch
+        va = t.angle(V)
+        if self.va_ref is not None:
+            va = self.va_ref[None, :] + t.remainder(va - self.va_ref[None, :] + math.pi, 2 * math.pi) - math.pi
+        return t.cat([va[:, self.pvpq], t.abs(V)[:, self.pq]], dim=1).float().contiguous()
+
+    def set_reference(self, solver, tol: float = 1e-10, max_iter: int = 20) -> None:
+        """Solve the nominal-load case once; its angles anchor the unwrapping."""
+        import cupf
+
+        t = self.torch
+        S = t.tensor(self.g.sbus[None, :], device=self.dev)
+        V, fm, _ = solver.solve_batch_device(S, self.v0[None, :].contiguous(),
+                                             config=cupf.NRConfig(tolerance=tol, max_iter=max_iter))
+        if not bool((fm <= tol).all()):
+            raise RuntimeError("warm start: the nominal-load case did not converge")
+        self.va_ref = t.angle(V[0])
+        self.vref = V[0].clone()
+
+    def generate(self, solver, n: int, lo: float = 0.7, hi: float = 1.3, seed: int = 12345, tol: float = 1e-10,
+                 max_iter: int = 20, chunk: int = 8192, keep_all: bool = False):
+        """Solve n seeded scenarios with the engine; returns (features,
+        targets, keep) as CUDA tensors.  keep marks the converged solutions on
+        the regular branch (every PQ magnitude within 0.1 pu and every angle
+        within 2.5 rad of the nominal-load solution); unless keep_all, only
+        those rows are returned.  A heavily loaded scenario can converge to a
+        far solution, which would only teach the network outliers."""
+        import cupf
+
+        t = self.torch
+        cfg = cupf.NRConfig(tolerance=tol, max_iter=max_iter)
+        if self.va_ref is None:
+            self.set_reference(solver, tol, max_iter)
+        ref = self.targets(self.vref[None, :])[0]
+        rng = np.random.default_rng(seed)
+        xs, ys, ks = [], [], []
+        for c0 in range(0, n, chunk):
+            m = min(chunk, n - c0)
+            f = rng.uniform(lo, hi, size=(m, self.g.n_bus))
+            S = t.tensor(self.g.sgen[None, :] - f * self.g.sload[None, :], device=self.dev)
+            V, fm, _ = solver.solve_batch_device(S, self.v0[None, :].expand(m, -1).contiguous(), config=cfg)
+            y = self.targets(V)
+            dev = (y - ref[None, :]).abs()
+            keep = (fm <= tol) & (dev[:, : self.n_pvpq].amax(1) <= 2.5) & (dev[:, self.n_pvpq:].amax(1) <= 0.1)
+            x = self.features(S)
+            if not keep_all:
+                x, y = x[keep], y[keep]
+            xs.append(x)
+            ys.append(y)
+            ks.append(keep)
+        return t.cat(xs), t.cat(ys), t.cat(ks)
+
+    # -- training --
+    def fit(self, X, Y, epochs: int = 10, batch: int = 1024, lr: float = 1e-3, lr_min: float = 1e-5,
+            seed: int = 0, log=None):
+        t = self.torch
+        self.x_mean = X.mean(0)
+        self.x_istd = 1.0 / X.std(0).clamp_min(1e-6)
+        self.y_mean = Y.mean(0)
+        self.y_std = Y.std(0).clamp_min(1e-9)
+        Yn = ((Y - self.y_mean) / self.y_std).contiguous()
+        n = X.shape[0] // batch * batch
+        steps = epochs * (n // batch)
+        h = self.mlp.buffers(batch)
+        gen = t.Generator(device=self.dev).manual_seed(seed)
+        s = 0
+        t0 = time.perf_counter()
+        for ep in range(epochs):
+            perm = t.randperm(X.shape[0], generator=gen, device=self.dev)[:n]
+            h["loss"].zero_()
+            for k in range(0, n, batch):
+                idx = perm[k:k + batch]
+                self.mlp.standardize(h, X[idx].contiguous(), self.x_mean, self.x_istd)
+                lr_s = lr_min + 0.5 * (lr - lr_min) * (1 + math.cos(math.pi * s / max(1, steps)))
+                self.mlp.train_step(h, Yn[idx].contiguous(), lr_s)
+                s += 1
+            loss = float(h["loss"].item()) / (n // batch)
+            self.history.append(loss)
+            if not math.isfinite(loss):
+                raise RuntimeError(f"warm-start training diverged at epoch {ep}")
+            if log:
+                log(f"epoch {ep}: loss {loss:.3e} ({time.perf_counter() - t0:.1f} s)")
+        if self.mlp.error_flag():
+            raise RuntimeError("warm-start GEMM reported a wait timeout")
+        return self.history
+
+    # -- inference --
+    def predict(self, sbus):
+        """Predicted Newton unknowns fp32 [B, n_out] (B padded to 128 internally)."""
+        t = self.torch
+        B = sbus.shape[0]
+        Bp = _round_up(B, 128)
+        raw = self.features(sbus)
+        if Bp != B:
+            raw = t.cat([raw, raw[-1:].expand(Bp - B, -1)]).contiguous()
+        h = self.mlp.buffers(Bp)
+        self.mlp.standardize(h, raw, self.x_mean, self.x_istd)
+        out = self.mlp.forward(h)
+        return (out[:B, : self.n_out] * self.y_std + self.y_mean).contiguous()
+
+    def solve(self, solver, sbus, config=None):
+        """Warm-started batched solve with flat-start fallback.  Returns
+        (V, final_mismatch, iterations_warm, n_fallback)."""
+        import cupf
+
+        t = self.torch
+        cfg = config or cupf.NRConfig()
+        pred = self.predict(sbus)
+        V, fm, it = solver.solve_batch_warm_device(sbus, self.v0, pred, config=cfg)
+        # (a non-finite prediction only makes its scenario fail and fall back)
+        bad = (fm > cfg.tolerance).nonzero().flatten()
+        nb = int(bad.numel())
+        if nb:
+            Sb = sbus[bad].contiguous()
+            Vb, fmb, _ = solver.solve_batch_device(Sb, self.v0[None, :].expand(nb, -1).contiguous(), config=cfg)
+            V[bad] = Vb
+            fm[bad] = fmb
+        return V, fm, it, nb

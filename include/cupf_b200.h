@@ -21,6 +21,11 @@
  * (scenario b, element k) at b * stride + k.  Complex arrays are interleaved
  * (re, im) doubles, i.e. std::complex<double>.
  *
+ * Streams: the device-pointer entry points (pf_solve_*_device) run on the
+ * caller's `stream`; NULL means the legacy default stream, so the engine's
+ * kernels stay ordered with whatever the caller queued there before (torch
+ * reports its default stream as handle 0).
+ *
  * Errors: every function returns a status; *_last_error() gives the message.
  * PF_INVALID_ARGUMENT corresponds to the reference's std::invalid_argument,
  * PF_RUNTIME_ERROR to std::runtime_error.  Handles are not thread-safe.
@@ -197,6 +202,15 @@ pf_status pf_solve_batch_device(pf_handle h, const double* sbus, int64_t sbus_st
                                 int64_t V0_stride, int32_t batch, const pf_nr_config* config,
                                 const pf_solve_options* solve_options, double* V_out, double* final_mismatch,
                                 void* stream, pf_adjoint_result* result);
+/* New (learned warm start, no reference counterpart): pf_solve_batch_device
+ * started from a predicted state.  pred [batch][pred_ld] fp32 holds, in
+ * Jacobian-row order, Va at the angle rows (PV then PQ buses) and Vm at the
+ * magnitude rows (PQ buses); the other buses keep V0.  V0_stride 0 uses one
+ * V0 row for every scenario. */
+pf_status pf_solve_batch_warm_device(pf_handle h, const double* sbus, int64_t sbus_stride, const double* V0,
+                                     int64_t V0_stride, const float* pred, int64_t pred_ld, int32_t batch,
+                                     const pf_nr_config* config, const pf_solve_options* solve_options,
+                                     double* V_out, double* final_mismatch, void* stream, pf_adjoint_result* result);
 /* Replaces: NewtonSolver::solve_torch_forward (core/torch_bridge.cpp:309-482).
  * Device pointers: sbus_base_re/im, v0_va/vm [n_bus] (or [batch][n_bus] when
  * batched_v0 = 1, used for per-scenario warm starts), load_p/q and

@@ -1,0 +1,55 @@
+/*
+ * cupf_mlp.h -- C ABI of the warm-start network's BF16 kernels.
+ *
+ * No reference counterpart.  The reference has only a torch MLP analog in its
+ * PINN benchmark harness (benchmark/pinn/model.py:13-38).  The engine trains
+ * and runs its warm-start network with these kernels; the Python driver is
+ * gpu-powerflow_b200/cupf/warm_start.py.
+ *
+ * All pointers are device pointers; row-major matrices; bf16 = IEEE bfloat16.
+ * Every function returns 0 on success, 1 for an invalid argument, 2 for a
+ * CUDA error; mlp_last_error() gives the message.  Launches are asynchronous
+ * on `stream` (NULL = legacy default stream).
+ */
+#ifndef CUPF_MLP_H
+#define CUPF_MLP_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+const char* mlp_last_error(void);
+
+/* C[M][N] = A[M][K] * B[N][K]^T on the tcgen05 tensor cores (bf16 in, fp32
+ * accumulate).  M and N multiples of 128, K a multiple of 64; row strides
+ * lda, ldb, ldo (elements, multiples of 8, at least the row length); A, B and
+ * out 16-byte aligned.  epi: 0 out = C (fp32); 1 out = C + bias (fp32);
+ * 2 aux = C + bias, out = gelu(aux) (both bf16); 3 out = C * gelu'(aux)
+ * (bf16).  aux has row stride ldaux. */
+int mlp_gemm_bf16(const void* A, long long lda, const void* B, long long ldb, int M, int N, int K, int epi,
+                  void* out, long long ldo, const float* bias, void* aux, long long ldaux, void* stream);
+/* Device error flag of the GEMM (1 or 2 after a bounded wait gave up); copied
+ * to *out_host with a synchronising copy, optionally reset. */
+int mlp_error_flag(int* out_host, int reset);
+/* out[cols][rows] = in[rows][cols] (bf16; in has row stride ld). */
+int mlp_transpose_bf16(const void* in, long long ld, void* out, int rows, int cols, void* stream);
+/* x[b][k] = bf16((raw[b][k] - mean[k]) * inv_std[k]) for k < n_in, 0 for
+ * n_in <= k < width; x has row stride ldx >= width, raw [B][n_in] fp32. */
+int mlp_standardize(const float* raw, const float* mean, const float* inv_std, void* x, long long ldx, int B,
+                    int n_in, int width, void* stream);
+/* Mean-squared error on the first n_out of ld columns: grad (bf16 [B][ld]) and
+ * *loss += mean squared difference (fp32, may be NULL). */
+int mlp_mse_grad(const float* pred, int ld, const float* target, int n_out, int B, void* grad, float* loss,
+                 void* stream);
+/* out[c] = sum_r g[r][c] (g bf16 [rows][cols], out fp32). */
+int mlp_col_sum_bf16(const void* g, int rows, int cols, float* out, void* stream);
+/* Adam step on fp32 master weights w (n elements) with moments m, v; writes
+ * the bf16 copy w_bf16 when not NULL.  step counts from 1. */
+int mlp_adam(float* w, const float* grad, float* m, float* v, void* w_bf16, long long n, float lr, float b1, float b2,
+             float eps, int step, float weight_decay, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CUPF_MLP_H */

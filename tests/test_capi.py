@@ -13,13 +13,14 @@ from cupf import grids as G
 
 ROOT = Path(__file__).resolve().parent.parent
 HEADER = ROOT / "include" / "cupf_b200.h"
+MLP_HEADER = ROOT / "include" / "cupf_mlp.h"
 
 
-def declared_functions() -> list[str]:
-    text = HEADER.read_text()
+def declared_functions(header: Path = HEADER, prefixes: str = "pf|cls") -> list[str]:
+    text = header.read_text()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
     text = re.sub(r"//[^\n]*", "", text)
-    names = re.findall(r"\b((?:pf|cls)_[a-z0-9_]+)\s*\(", text)
+    names = re.findall(r"\b((?:" + prefixes + r")_[a-z0-9_]+)\s*\(", text)
     seen = []
     for n in names:
         if n not in seen:
@@ -37,6 +38,23 @@ def test_library_exports_every_declared_symbol():
 
 def test_binding_table_matches_header():
     assert set(_capi.EXPORTS) == set(declared_functions())
+
+
+def test_mlp_header_symbols_exported():
+    lib = _capi.load()
+    decl = declared_functions(MLP_HEADER, "mlp")
+    assert set(decl) == set(_capi.MLP_EXPORTS)
+    missing = [n for n in decl if not hasattr(lib, n)]
+    assert not missing, f"declared in cupf_mlp.h but not exported: {missing}"
+
+
+def test_mlp_gemm_rejects_bad_shapes():
+    """Shape checks run on the host, before any device work."""
+    lib = _capi.load()
+    assert lib.mlp_gemm_bf16(None, 64, None, 64, 100, 128, 64, 0, None, 128, None, None, 0, None) == 1
+    assert b"multiples" in lib.mlp_last_error()
+    assert lib.mlp_gemm_bf16(None, 64, None, 64, 128, 128, 64, 9, None, 128, None, None, 0, None) == 1
+    assert lib.mlp_gemm_bf16(None, 32, None, 64, 128, 128, 64, 0, None, 128, None, None, 0, None) == 1
 
 
 def test_library_is_the_in_tree_build():

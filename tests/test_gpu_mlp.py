@@ -1,0 +1,208 @@
+"""Warm-start network kernels (include/cupf_mlp.h) on the GPU: the tcgen05
+GEMM and its epilogues against torch fp32 products, a full training step's
+gradients against the CPU oracle (oracle/mlp_oracle.py), training
+convergence, and the warm start's iteration savings on a real grid."""
+import numpy as np
+import pytest
+
+from conftest import gpu_available
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not gpu_available(), reason="needs a CUDA device")]
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch
+    return torch
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
+
+
+@pytest.mark.parametrize("M,N,K", [(128, 128, 64), (256, 384, 1024), (384, 128, 4480)])
+def test_gemm_f32_matches_torch(torch, M, N, K):
+    from cupf.warm_start import MLP, EPI_F32, EPI_BIAS_F32
+
+    g = torch.Generator(device="cuda").manual_seed(M + N + K)
+    A = torch.randn(M, K, device="cuda", generator=g).to(torch.bfloat16)
+    B = torch.randn(N, K, device="cuda", generator=g).to(torch.bfloat16)
+    bias = torch.randn(N, device="cuda", generator=g)
+    net = MLP(64, 64, hidden=128, layers=1)
+    out = torch.empty(M, N, device="cuda")
+    net.gemm(A, B, out, EPI_F32)
+    ref = A.float() @ B.float().T
+    assert _rel(out.cpu().numpy(), ref.cpu().numpy()) < 1e-5
+    net.gemm(A, B, out, EPI_BIAS_F32, bias=bias)
+    assert _rel(out.cpu().numpy(), (ref + bias).cpu().numpy()) < 1e-5
+    assert net.error_flag() == 0
+
+
+def test_gemm_gelu_epilogues(torch):
+    from cupf.warm_start import MLP, EPI_BIAS_GELU, EPI_DGELU
+    from oracle.mlp_oracle import gelu, gelu_grad
+
+    M, N, K = 256, 256, 512
+    g = torch.Generator(device="cuda").manual_seed(7)
+    A = (0.1 * torch.randn(M, K, device="cuda", generator=g)).to(torch.bfloat16)
+    B = (0.1 * torch.randn(N, K, device="cuda", generator=g)).to(torch.bfloat16)
+    bias = 0.1 * torch.randn(N, device="cuda", generator=g)
+    net = MLP(64, 64, hidden=128, layers=1)
+    out = torch.empty(M, N, dtype=torch.bfloat16, device="cuda")
+    aux = torch.empty(M, N, dtype=torch.bfloat16, device="cuda")
+    net.gemm(A, B, out, EPI_BIAS_GELU, bias=bias, aux=aux)
+    z = (A.double() @ B.double().T + bias.double()).cpu().numpy()
+    assert np.abs(aux.float().cpu().numpy() - z).max() <= 1e-2 * np.abs(z).max()
+    assert np.abs(out.float().cpu().numpy() - gelu(z)).max() <= 1e-2 * np.abs(gelu(z)).max()
+    out2 = torch.empty(M, N, dtype=torch.bfloat16, device="cuda")
+    net.gemm(A, B, out2, EPI_DGELU, aux=aux)
+    acc = (A.double() @ B.double().T).cpu().numpy()
+    ref = acc * gelu_grad(aux.double().cpu().numpy())
+    assert np.abs(out2.float().cpu().numpy() - ref).max() <= 1e-2 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("skip", [False, True])
+def test_training_step_gradients_match_oracle(torch, skip):
+    """One forward + backward of a 2-hidden-layer network: every weight and
+    bias gradient against the CPU oracle (same bf16 rounding points)."""
+    from cupf.warm_start import MLP
+    from oracle import mlp_oracle as mo
+
+    n_in, n_out, B = 200, 150, 128
+    net = MLP(n_in, n_out, hidden=256, layers=2, seed=3, skip=skip)
+    rng = np.random.default_rng(0)
+    x = np.zeros((B, net.k0))
+    x[:, :n_in] = rng.standard_normal((B, n_in))
+    x = mo.bf16(x)
+    y = rng.standard_normal((B, n_out))
+    h = net.buffers(B)
+    h["x"].copy_(torch.tensor(x, dtype=torch.float32, device="cuda").to(torch.bfloat16))
+    yt = torch.tensor(y, dtype=torch.float32, device="cuda")
+    for i in range(len(net.b)):
+        net.b[i].copy_(0.05 * torch.randn(net.b[i].shape, device="cuda"))
+    net.forward(h)
+    h["loss"].zero_()
+    net.backward(h, yt)
+    Ws = [w16.double().cpu().numpy() for w16 in net.W16]
+    bs = [b.double().cpu().numpy() for b in net.b]
+    p, loss, dWs, dbs = mo.forward_backward(x, Ws, bs, y, n_out, skip=skip)
+    assert _rel(h["p"].cpu().numpy(), p) < 1e-3
+    assert abs(float(h["loss"].item()) - loss) <= 1e-3 * loss
+    for i in range(len(dWs)):
+        assert _rel(h["gW"][i].cpu().numpy(), dWs[i]) < 2e-2, i
+        assert _rel(h["gb"][i].cpu().numpy(), dbs[i]) < 2e-2, i
+    assert net.error_flag() == 0
+
+
+def test_training_reduces_loss(torch):
+    from cupf.warm_start import MLP
+
+    n_in, n_out, B = 128, 64, 256
+    net = MLP(n_in, n_out, hidden=256, layers=2, seed=1)
+    g = torch.Generator(device="cuda").manual_seed(5)
+    T = torch.randn(n_out, n_in, device="cuda", generator=g) / n_in ** 0.5
+    X = torch.randn(B * 8, n_in, device="cuda", generator=g)
+    Y = torch.tanh(X @ T.T)
+    h = net.buffers(B)
+    losses = []
+    for step in range(300):
+        k = (step % 8) * B
+        h["x"][:, :n_in] = X[k:k + B].to(torch.bfloat16)
+        h["loss"].zero_()
+        net.train_step(h, Y[k:k + B].contiguous(), 2e-3)
+        losses.append(float(h["loss"].item()))
+    assert np.mean(losses[-20:]) < 0.1 * np.mean(losses[:5])
+
+
+def test_warm_start_saves_newton_iterations(torch):
+    """Trained on engine solutions of a 118-bus grid (load scaling 0.7-1.3),
+    the network's starting point needs fewer Newton iterations than the flat
+    start on held-out scenarios, and reaches the same solution."""
+    import cupf
+    from cupf import grids as G
+    from cupf.warm_start import WarmStart
+
+    g = G.grid_118()
+    o = cupf.NewtonOptions()
+    o.backend = cupf.BackendKind.CUDA
+    o.compute = cupf.ComputePolicy.Mixed
+    o.custom.serial_nd = True
+    s = cupf.NewtonSolver(o)
+    s.initialize(g.indptr, g.indices, g.data, g.n_bus, g.n_bus, g.pv, g.pq)
+    ws = WarmStart(g, hidden=256, layers=2, seed=0)
+    X, Y, _ = ws.generate(s, 16384, seed=1)
+    ws.fit(X, Y, epochs=40, batch=512, lr=2e-3)
+    rng = np.random.default_rng(99)
+    f = rng.uniform(0.7, 1.3, size=(512, g.n_bus))
+    S = torch.tensor(g.sgen[None, :] - f * g.sload[None, :], device="cuda")
+    cfg = cupf.NRConfig(tolerance=1e-8, max_iter=10)
+    Vf, fmf, itf = s.solve_batch_device(S, ws.v0[None, :].expand(512, -1).contiguous(), config=cfg)
+    Vw, fmw, itw, nfb = ws.solve(s, S, cfg)
+    assert bool((fmw <= 1e-8).all()) and bool((fmf <= 1e-8).all())
+    assert itw < itf, (itw, itf)
+    assert float((Vw - Vf).abs().max()) <= 1e-7
+
+
+def test_warm_entry_point_exact_prediction_and_failed_row(torch):
+    """pf_solve_batch_warm_device: seeded with the exact solution a scenario
+    converges at the first norm evaluation; a non-finite prediction only fails
+    its own scenario (final mismatch inf), the rest of the batch converges."""
+    import cupf
+    from cupf import grids as G
+
+    g = G.grid_118()
+    o = cupf.NewtonOptions()
+    o.backend = cupf.BackendKind.CUDA
+    o.compute = cupf.ComputePolicy.FP64
+    o.custom.serial_nd = True
+    s = cupf.NewtonSolver(o)
+    s.initialize(g.indptr, g.indices, g.data, g.n_bus, g.n_bus, g.pv, g.pq)
+    B = 40
+    S = torch.tensor(g.scenarios(B, seed=4), device="cuda")
+    v0 = torch.tensor(g.v0, device="cuda")
+    cfg = cupf.NRConfig(tolerance=1e-10, max_iter=20)
+    V, fm, it = s.solve_batch_device(S, v0[None, :].expand(B, -1).contiguous(), config=cfg)
+    assert bool((fm <= 1e-10).all())
+    pvpq = torch.tensor(np.concatenate([g.pv, g.pq]), device="cuda")
+    pq = torch.tensor(g.pq, device="cuda")
+    pred = torch.cat([torch.angle(V)[:, pvpq], torch.abs(V)[:, pq]], 1).float().contiguous()
+    cfg8 = cupf.NRConfig(tolerance=1e-5, max_iter=10)
+    Vw, fmw, itw = s.solve_batch_warm_device(S, v0, pred, config=cfg8)
+    assert itw == 1 and bool((fmw <= 1e-5).all())
+    pred[3, 5] = float("nan")
+    Vw, fmw, itw = s.solve_batch_warm_device(S, v0, pred, config=cfg8)
+    assert np.isinf(fmw[3].item())
+    ok = torch.ones(B, dtype=torch.bool, device="cuda")
+    ok[3] = False
+    assert bool((fmw[ok] <= 1e-5).all())
+
+
+def test_device_entry_points_follow_the_callers_stream(torch):
+    """The prediction is written by work still queued on torch's default stream
+    (behind a GPU sleep) when the warm solve is called: the engine must run on
+    that same stream (handle 0 = legacy default stream), not on a private one."""
+    import cupf
+    from cupf import grids as G
+
+    g = G.grid_118()
+    o = cupf.NewtonOptions()
+    o.backend = cupf.BackendKind.CUDA
+    o.compute = cupf.ComputePolicy.Mixed
+    o.custom.serial_nd = True
+    s = cupf.NewtonSolver(o)
+    s.initialize(g.indptr, g.indices, g.data, g.n_bus, g.n_bus, g.pv, g.pq)
+    B = 64
+    S = torch.tensor(g.scenarios(B, seed=8), device="cuda")
+    v0 = torch.tensor(g.v0, device="cuda")
+    V, fm, _ = s.solve_batch_device(S, v0[None, :].expand(B, -1).contiguous(),
+                                    config=cupf.NRConfig(tolerance=1e-11, max_iter=20))
+    pvpq = torch.tensor(np.concatenate([g.pv, g.pq]), device="cuda")
+    pq = torch.tensor(g.pq, device="cuda")
+    exact = torch.cat([torch.angle(V)[:, pvpq], torch.abs(V)[:, pq]], 1).float().contiguous()
+    pred = torch.full_like(exact, float("nan"))
+    torch.cuda.synchronize()
+    assert torch.cuda.current_stream().cuda_stream == 0
+    torch.cuda._sleep(20_000_000)  # keep the default stream busy
+    pred.copy_(exact)              # queued behind the sleep
+    Vw, fmw, itw = s.solve_batch_warm_device(S, v0, pred, config=cupf.NRConfig(tolerance=1e-6, max_iter=10))
+    assert bool((fmw <= 1e-6).all()) and itw <= 2
