@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "engine.hpp"
+#include "static_scratch.hpp"
 
 using cupf_b200::Engine;
 using cupf_b200::EngineConfig;
@@ -236,6 +237,25 @@ cls_status cls_factorize(cls_handle h, const void* values, int32_t value_type) {
   try {
     h->eng->factorize_values(values, value_type == CLS_VALUE_FLOAT64, h->batch, h->stream);
     return CLS_SUCCESS;
+  } catch (const std::exception& e) {
+    h->err = e.what();
+    return CLS_FACTORIZATION_FAILED;
+  }
+}
+
+cls_status cls_factorize_static_scratch(cls_handle h, const void* values, int32_t value_type) {
+  if (!h || !h->analyzed) return CLS_INVALID_STATE;
+  if (!values) return CLS_INVALID_STATE;
+  if (value_type != CLS_VALUE_FLOAT64 && value_type != CLS_VALUE_FLOAT32) return CLS_INVALID_VALUE;
+  if (h->batch == 0) h->batch = 1;
+  try {
+    void* scratch = cupf_b200::static_front_scratch();
+    h->eng->factorize_values_static_scratch(values, value_type == CLS_VALUE_FLOAT64, h->batch, scratch,
+                                            cupf_b200::kStaticFrontScratchBytes, h->stream);
+    return CLS_SUCCESS;
+  } catch (const std::invalid_argument& e) {
+    h->err = e.what();
+    return CLS_INVALID_VALUE;
   } catch (const std::exception& e) {
     h->err = e.what();
     return CLS_FACTORIZATION_FAILED;

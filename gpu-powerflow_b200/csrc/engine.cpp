@@ -879,6 +879,80 @@ void Engine::factorize_values(const void* d_values, int32_t values_is_double, in
   CUPF_CUDA(cudaGetLastError());
 }
 
+// Factorization whose global front scratch is a caller-supplied fixed area
+// (the static scratch of cls_factorize_static_scratch).  Allocates nothing:
+// the handle's workspace must already hold this batch size, and the levels'
+// scratch need must fit the area.  No stage timers (their events are created
+// on demand).
+template <typename T>
+void Engine::factor_all_external(cudaStream_t s, const void* J, T* scratch, size_t scratch_elems) {
+  auto& d = *d_;
+  FactorArgs<T, T> a;
+  a.plan = d.pl;
+  a.groups = d.Bp / kWarp;
+  a.Bp = d.Bp;
+  a.J = static_cast<const T*>(J);
+  a.Fp = d.Fp.as<T>();
+  a.U = d.U.as<T>();
+  a.L = d.L.as<T>();
+  a.CB = d.CB.as<T>();
+  a.Y = d.Y.as<T>();
+  a.store_l = 1;
+  a.eps = cfg_.shift_epsilon;
+  a.static_pivot = (cfg_.static_pivot && cfg_.shift_epsilon > 0.0) ? 1 : 0;
+  a.sing = d.sing.as<int>();
+  a.front_scratch = scratch;
+  a.front_scratch_elems = scratch_elems;
+  for (const auto& lv : d.levels) {
+    launch_factor_level<T, T>(lv, a, s);
+    ++launches_;
+  }
+}
+
+void Engine::factorize_values_static_scratch(const void* d_values, int32_t values_is_double, int32_t B,
+                                             void* scratch, size_t scratch_bytes, cudaStream_t stream) {
+  if (!initialized_) throw std::runtime_error("Factorize: Analyze() must be called first");
+  if (B <= 0) throw std::invalid_argument("Factorize: batch size must be positive");
+  auto& d = *d_;
+  const int Bp = (B + kWarp - 1) / kWarp * kWarp;
+  if (Bp > d.Bp_cap)
+    throw std::runtime_error(
+        "Factorize (static scratch): the handle has no workspace for this batch size; this entry point allocates "
+        "nothing, so run one regular cls_factorize at this batch size (or larger) first");
+  const bool dbl = factor_is_double();
+  const size_t es = dbl ? sizeof(double) : sizeof(float);
+  size_t need = 0;  // elements x 32 lanes
+  for (const auto& lv : d.levels)
+    if (!front_fits_smem(lv, es)) need = std::max(need, (size_t)lv.max_fsz * (lv.max_fsz + 1) * lv.count * (Bp / kWarp));
+  if (need * kWarp * es > scratch_bytes)
+    throw std::invalid_argument("Factorize (static scratch): this batch needs " + std::to_string(need * kWarp * es) +
+                                " bytes of front scratch, the static area holds " + std::to_string(scratch_bytes));
+  d.B = B;
+  d.Bp = Bp;
+  cudaStream_t s = stream ? stream : d.own;
+  if (dbl) {
+    if (values_is_double)
+      launch_batch_to_rows<double, double>(static_cast<const double*>(d_values), d.J.as<double>(), ja_.nnz, B, d.Bp, s);
+    else
+      launch_batch_to_rows<float, double>(static_cast<const float*>(d_values), d.J.as<double>(), ja_.nnz, B, d.Bp, s);
+  } else {
+    if (values_is_double)
+      launch_batch_to_rows<double, float>(static_cast<const double*>(d_values), d.J.as<float>(), ja_.nnz, B, d.Bp, s);
+    else
+      launch_batch_to_rows<float, float>(static_cast<const float*>(d_values), d.J.as<float>(), ja_.nnz, B, d.Bp, s);
+  }
+  CUPF_CUDA(cudaMemsetAsync(d.F.p, 0, (size_t)ja_.dim * d.Bp * 8, s));
+  CUPF_CUDA(cudaMemsetAsync(d.Fp.p, 0, (size_t)ja_.dim * d.Bp * es, s));
+  CUPF_CUDA(cudaMemsetAsync(d.sing.p, 0, d.Bp * sizeof(int), s));
+  const size_t elems = scratch_bytes / (kWarp * es);
+  if (dbl) factor_all_external<double>(s, d.J.p, static_cast<double*>(scratch), elems);
+  else factor_all_external<float>(s, d.J.p, static_cast<float*>(scratch), elems);
+  B_ = B;
+  adjoint_ready_ = false;
+  CUPF_CUDA(cudaStreamSynchronize(s));
+  CUPF_CUDA(cudaGetLastError());
+}
+
 void Engine::solve_values(const void* d_rhs, int32_t rhs_is_double, void* d_x, int32_t x_is_double, int32_t B,
                           bool transpose, cudaStream_t stream) {
   if (B != B_) throw std::invalid_argument("Solve: batch size differs from the factorization");

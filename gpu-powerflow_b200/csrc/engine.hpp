@@ -88,6 +88,10 @@ class Engine {
 
   // Linear-solver boundary: factor caller-supplied Jacobian values and solve.
   void factorize_values(const void* d_values, int32_t values_is_double, int32_t B, cudaStream_t stream);
+  // factorize_values with the global front scratch in a fixed caller area;
+  // allocates nothing (the workspace must already hold batch B)
+  void factorize_values_static_scratch(const void* d_values, int32_t values_is_double, int32_t B, void* scratch,
+                                       size_t scratch_bytes, cudaStream_t stream);
   void solve_values(const void* d_rhs, int32_t rhs_is_double, void* d_x, int32_t x_is_double, int32_t B,
                     bool transpose, cudaStream_t stream);
 
@@ -126,6 +130,8 @@ class Engine {
   int64_t launches_ = 0;
   bool profiling_ = false;
   bool tolerate_nonfinite_ = false;  // set during warm-started solves
+  template <typename T>
+  void factor_all_external(cudaStream_t s, const void* J, T* scratch, size_t scratch_elems);
   void stage_begin(int stage, cudaStream_t s);
   void stage_end(int stage, cudaStream_t s);
   void collect_stage_times();

@@ -1,0 +1,17 @@
+// static_scratch.hpp -- the statically allocated front-scratch area (see
+// static_scratch.cu).
+#pragma once
+
+#include <cstddef>
+
+namespace cupf_b200 {
+
+// Size of the static front-scratch area on each device (8 MiB).
+constexpr size_t kStaticFrontScratchBytes = size_t(8) << 20;
+
+// Device address of the area on the current device.  The first call on each
+// device looks the symbol up (cudaGetSymbolAddress, with that device current)
+// and caches it; later calls only read the cache.  Throws on failure.
+void* static_front_scratch();
+
+}  // namespace cupf_b200

@@ -56,6 +56,7 @@ class PfInfo(C.Structure):
 # exported symbols, in the order include/cupf_b200.h declares them
 EXPORTS = [
     "cls_create", "cls_destroy", "cls_set_data", "cls_analyze", "cls_analyze_host", "cls_setup", "cls_set_stream", "cls_factorize",
+    "cls_factorize_static_scratch",
     "cls_solve", "cls_solve_transpose", "cls_singular_flags", "cls_status_string", "cls_last_error",
     "cls_plan_array",
     "pf_create", "pf_destroy", "pf_last_error", "pf_initialize", "pf_analyze_host", "pf_solve_batch", "pf_solve_batch_device",
@@ -85,6 +86,7 @@ def _declare(lib: C.CDLL) -> None:
         "cls_setup": ([_vp, _i32], _i32),
         "cls_set_stream": ([_vp, _vp], _i32),
         "cls_factorize": ([_vp, _vp, _i32], _i32),
+        "cls_factorize_static_scratch": ([_vp, _vp, _i32], _i32),
         "cls_solve": ([_vp, _vp, _i32, _vp, _i32], _i32),
         "cls_solve_transpose": ([_vp, _vp, _i32, _vp, _i32], _i32),
         "cls_singular_flags": ([_vp, _vp, _i32], _i32),

@@ -105,6 +105,11 @@ class LinearSolver:
     def factorize(self, values) -> None:
         self._check(self._lib.cls_factorize(self._h, values.data_ptr(), self._vt(values)))
 
+    def factorize_static_scratch(self, values) -> None:
+        """cls_factorize_static_scratch: same factorization, no device allocation
+        in the call (needs a prior regular factorize at this batch size)."""
+        self._check(self._lib.cls_factorize_static_scratch(self._h, values.data_ptr(), self._vt(values)))
+
     def solve(self, rhs, out=None, transpose: bool = False):
         import torch
         if out is None:

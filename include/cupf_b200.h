@@ -93,6 +93,20 @@ cls_status cls_set_stream(cls_handle h, void* stream);
 /* Replaces: Solver::SetValues + Factorize() (solver.hpp:91,102); device values
  * [batch][nnz] in CSR order. */
 cls_status cls_factorize(cls_handle h, const void* values, int32_t value_type);
+/* New, no reference counterpart: cls_factorize for callers that must not
+ * allocate device memory in the call (their memory is pooled or reserved
+ * up front, or they cannot afford the implicit synchronisation of an
+ * allocation).  The dense fronts that exceed shared memory use a fixed 8 MiB
+ * static device area instead of the handle's workspace.  The call allocates
+ * nothing; it therefore needs the handle's workspace to exist for this batch
+ * size already (one regular cls_factorize at this batch size or larger), and
+ * it rejects a batch whose front scratch exceeds 8 MiB (CLS_INVALID_VALUE,
+ * message in cls_last_error).  Nothing has to be zeroed beforehand.  The area
+ * is shared by all handles of the process on a device: calls must not
+ * overlap in time.  The first call on each device looks the area's address
+ * up (cudaGetSymbolAddress with that device current); make it before any
+ * stream capture. */
+cls_status cls_factorize_static_scratch(cls_handle h, const void* values, int32_t value_type);
 /* Replaces: Solver::SetRhs / SetSolution / Solve() (solver.hpp:93-94,103);
  * device rhs / solution [batch][n]; pairs f64/f64, f64/f32, f32/f32. */
 cls_status cls_solve(cls_handle h, const void* rhs, int32_t rhs_type, void* solution, int32_t solution_type);
