@@ -225,7 +225,7 @@ cls_status cls_setup(cls_handle h, int32_t batch_size) {
 
 cls_status cls_set_stream(cls_handle h, void* stream) {
   if (!h || !h->analyzed || h->batch == 0) return CLS_INVALID_STATE;
-  h->stream = static_cast<cudaStream_t>(stream);
+  h->stream = caller_stream(stream);
   return CLS_SUCCESS;
 }
 

@@ -91,7 +91,8 @@ class LinearSolver:
         self.batch = batch
 
     def set_stream(self, stream) -> None:
-        self._check(self._lib.cls_set_stream(self._h, C.c_void_p(int(stream))))
+        """cls_set_stream; 0 / None is the legacy default stream."""
+        self._check(self._lib.cls_set_stream(self._h, C.c_void_p(int(stream or 0))))
 
     @staticmethod
     def _vt(t) -> int:
@@ -102,12 +103,20 @@ class LinearSolver:
             return 1
         raise ValueError("values must be float64 or float32")
 
+    def _bind_stream(self, t) -> None:
+        """Run on torch's current stream of the tensor's device (ordered after
+        the work that produced the inputs)."""
+        import torch
+        self.set_stream(torch.cuda.current_stream(t.device).cuda_stream)
+
     def factorize(self, values) -> None:
+        self._bind_stream(values)
         self._check(self._lib.cls_factorize(self._h, values.data_ptr(), self._vt(values)))
 
     def factorize_static_scratch(self, values) -> None:
         """cls_factorize_static_scratch: same factorization, no device allocation
         in the call (needs a prior regular factorize at this batch size)."""
+        self._bind_stream(values)
         self._check(self._lib.cls_factorize_static_scratch(self._h, values.data_ptr(), self._vt(values)))
 
     def solve(self, rhs, out=None, transpose: bool = False):
@@ -115,6 +124,7 @@ class LinearSolver:
         if out is None:
             out = torch.empty_like(rhs)
         fn = self._lib.cls_solve_transpose if transpose else self._lib.cls_solve
+        self._bind_stream(rhs)
         self._check(fn(self._h, rhs.data_ptr(), self._vt(rhs), out.data_ptr(), self._vt(out)))
         return out
 

@@ -88,7 +88,9 @@ cls_status cls_analyze(cls_handle h);
 cls_status cls_analyze_host(cls_handle h);
 /* Replaces: Solver::Setup(batch_size) (solver.hpp:101) */
 cls_status cls_setup(cls_handle h, int32_t batch_size);
-/* Replaces: Solver::SetStream(void*) (solver.hpp:109) */
+/* Replaces: Solver::SetStream(void*) (solver.hpp:109).  NULL selects the
+ * legacy default stream; a handle never given a stream uses a private one
+ * (its factorize / solve calls synchronise that stream before returning). */
 cls_status cls_set_stream(cls_handle h, void* stream);
 /* Replaces: Solver::SetValues + Factorize() (solver.hpp:91,102); device values
  * [batch][nnz] in CSR order. */
