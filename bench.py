@@ -147,12 +147,13 @@ def factor_bytes_per_scenario(solver, elem: int) -> int:
     return int(elem * inf["nnz_jacobian"] + 8 * inf["dim_f"] + elem * int((nc * fsz).sum()) + elem * inf["dim_f"])
 
 
-def make_solver(grid, compute):
+def make_solver(grid, compute, graph: bool = True):
     import cupf
     o = cupf.NewtonOptions()
     o.backend = cupf.BackendKind.CUDA
     o.compute = compute
     o.custom.serial_nd = True
+    o.use_cuda_graph = graph  # one Newton iteration captured once, replayed per iteration
     s = cupf.NewtonSolver(o)
     s.initialize(grid.indptr, grid.indices, grid.data, grid.n_bus, grid.n_bus, grid.pv, grid.pq)
     return s
@@ -181,8 +182,8 @@ def run_engine(args) -> None:
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
     stream = torch.cuda.current_stream(dev)
 
-    mixed = make_solver(g, cupf.ComputePolicy.Mixed)
-    fp64 = make_solver(g, cupf.ComputePolicy.FP64)
+    mixed = make_solver(g, cupf.ComputePolicy.Mixed, graph=not args.no_graph)
+    fp64 = make_solver(g, cupf.ComputePolicy.FP64, graph=not args.no_graph)
 
     # learned warm start: trained before the timed region on engine solutions
     ws, warm_info = None, None
@@ -300,16 +301,19 @@ def run_engine(args) -> None:
     e2e_value = _reduce(conv_e2e / args.steps, "sum", world, dev) / (ms_e2e / 1e3)
 
     # roofline of the dominant kernel (the front factorization): stage timers
-    # over one extra profiled Mixed solve, outside the timed region
-    mixed.set_profiling(True)
+    # (CUDA events around each stage's launches) over one extra Mixed solve
+    # launched stage by stage, outside the timed region
+    prof = make_solver(g, cupf.ComputePolicy.Mixed, graph=False)
+    prof.solve_batch_device(sbus, v0, config=cfg)
+    prof.set_profiling(True)
     flush.fill_(1.0)
-    mixed.solve_batch_device(sbus, v0, config=cfg)
-    st = mixed.stage_times()
-    mixed.set_profiling(False)
+    prof.solve_batch_device(sbus, v0, config=cfg)
+    st = prof.stage_times()
+    prof.set_profiling(False)
     fact_ms, _ = st["factorize"]
     n_fact = max(1, r_mix["iters"] - 1)
     per_fact_ms = fact_ms / n_fact
-    fbytes = factor_bytes_per_scenario(mixed, 4) * B
+    fbytes = factor_bytes_per_scenario(prof, 4) * B
     peaks = _peaks()
     achieved = fbytes / (per_fact_ms / 1e3) / 1e9
     traffic = None
@@ -337,6 +341,7 @@ def run_engine(args) -> None:
                        "max_iter": MAX_ITER, "warm_start": warm_info or "none",
                        "l2": "256 MB buffer written between steps",
                        "iterations": int(head["iters"]), "converged_per_step": head["conv"],
+                       "cuda_graph": not args.no_graph,
                        "fallback_per_step": head["fallback"]},
             "fp64": {"value": round(value_64, 1), "ms_per_step": round(ms_64, 4), "iterations": int(r_64["iters"]),
                      "converged_per_step": r_64["conv"], "start": "flat"},
@@ -415,6 +420,7 @@ def main() -> None:
     ap.add_argument("--cpu-sample", type=int, default=512)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-warm", action="store_true", help="skip the learned warm start (flat start only)")
+    ap.add_argument("--no-graph", action="store_true", help="launch every kernel from the host (no CUDA graph)")
     ap.add_argument("--train", type=int, default=200000, help="warm-start training scenarios (engine-solved)")
     ap.add_argument("--epochs", type=int, default=40)
     args = ap.parse_args()

@@ -592,7 +592,8 @@ void configure_front_kernels() {
 #define CUPF_ALLOW(F)                                                                  \
   allow_full_smem(reinterpret_cast<const void*>(k_front_factor<T, TJ, F, true>));    \
   allow_full_smem(reinterpret_cast<const void*>(k_front_factor<T, TJ, F, false>));
-  CUPF_ALLOW(8) CUPF_ALLOW(16) CUPF_ALLOW(24) CUPF_ALLOW(32) CUPF_ALLOW(48) CUPF_ALLOW(64)
+  CUPF_ALLOW(8) CUPF_ALLOW(12) CUPF_ALLOW(16) CUPF_ALLOW(20) CUPF_ALLOW(24) CUPF_ALLOW(32) CUPF_ALLOW(48)
+  CUPF_ALLOW(64)
 #undef CUPF_ALLOW
 }
 
@@ -602,7 +603,9 @@ void launch_factor_level(const LevelLaunch& lv, const FactorArgs<T, TJ>& a, cuda
   if (lv.max_nc > 8) throw std::runtime_error("panels wider than 8 columns are not supported (max_panel_width <= 8)");
   const int f = lv.max_fsz;
   if (f <= 8) launch_factor_t<T, TJ, 8>(lv, a, s);
+  else if (f <= 12) launch_factor_t<T, TJ, 12>(lv, a, s);
   else if (f <= 16) launch_factor_t<T, TJ, 16>(lv, a, s);
+  else if (f <= 20) launch_factor_t<T, TJ, 20>(lv, a, s);
   else if (f <= 24) launch_factor_t<T, TJ, 24>(lv, a, s);
   else if (f <= 32) launch_factor_t<T, TJ, 32>(lv, a, s);
   else if (f <= 48) launch_factor_t<T, TJ, 48>(lv, a, s);
