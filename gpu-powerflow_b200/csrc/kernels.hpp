@@ -39,13 +39,14 @@ struct FactorArgs {
 constexpr size_t kSmemLimit = 227 * 1024;  // opt-in dynamic shared memory per block on sm_100
 
 // Shared-memory plan of one factor-level launch (same for every block):
-// staged source list (src, dst), staged source rows, dense front.
+// staged source list (src, dst), pivot reciprocals, staged source rows,
+// dense front.
 struct FrontSmem {
   int chunk = 0;        // staged source rows per buffer
   int nbuf = 1;         // 1, or 2 when a front's sources need more than one chunk
   int idx_cap = 0;      // source entries whose (src, dst) are staged
-  size_t idx_bytes = 0, stage_bytes = 0, front_bytes = 0;
-  size_t total() const { return idx_bytes + stage_bytes + front_bytes; }
+  size_t idx_bytes = 0, inv_bytes = 0, stage_bytes = 0, front_bytes = 0;
+  size_t total() const { return idx_bytes + inv_bytes + stage_bytes + front_bytes; }
 };
 
 // The whole source list staged at once when it fits next to the dense front,
@@ -56,6 +57,7 @@ inline FrontSmem plan_front_smem(const LevelLaunch& lv, size_t elem_bytes, bool 
   const size_t row = 32 * elem_bytes;
   sm.idx_cap = lv.max_src > 0 ? lv.max_src : 1;
   sm.idx_bytes = ((size_t)sm.idx_cap * (sizeof(long long) + sizeof(int)) + 15) / 16 * 16;
+  sm.inv_bytes = 8 * row;  // reciprocals of the (at most 8) pivots, per scenario lane
   sm.front_bytes = front_in_smem ? (size_t)lv.max_fsz * (lv.max_fsz + 1) * row : 0;
   sm.chunk = sm.idx_cap;
   sm.nbuf = 1;

@@ -140,10 +140,11 @@ __global__ void __launch_bounds__(256)
 
   long long* s_src = reinterpret_cast<long long*>(smem_raw);
   int* s_dst = reinterpret_cast<int*>(smem_raw + (size_t)sm.idx_cap * sizeof(long long));
-  unsigned char* stage = smem_raw + sm.idx_bytes;
+  T* s_inv = reinterpret_cast<T*>(smem_raw + sm.idx_bytes);  // [8][32] pivot reciprocals
+  unsigned char* stage = smem_raw + sm.idx_bytes + sm.inv_bytes;
   T* Fm;
   if constexpr (SMEM_FRONT)
-    Fm = reinterpret_cast<T*>(smem_raw + sm.idx_bytes + sm.stage_bytes);
+    Fm = reinterpret_cast<T*>(stage + sm.stage_bytes);
   else
     Fm = front_scratch + (size_t)item * front_elems * kWarp;
 
@@ -228,36 +229,74 @@ __global__ void __launch_bounds__(256)
   if (cur >= 0) Fm[cur * kWarp + lane] = acc;
   __syncthreads();
 
-  // phase 3a: the nc pivot rows, eliminated in order by warp 0 (row k applies
-  // the final rows m < k, then its pivot is guarded); the row lives in registers
+  // phase 3a: the nc pivot rows.  A pivot is guarded once and its reciprocal
+  // kept in s_inv, so every elimination is a multiply (l = a * (1 / u_kk)).
+  // With at least nc warps, warp k holds pivot row k in registers and the
+  // block runs the nc right-looking steps (warp m publishes its final row,
+  // warps k > m apply it); otherwise warp 0 eliminates the rows in order.
   bool shifted = false;
   T* Fl = Fm + lane;
-  if (warp == 0) {
-    for (int k = 0; k < nc; ++k) {
-      T* Rk = Fl + k * rw * kWarp;
-      T r[FMAX + 1];
+  T* inv_l = s_inv + lane;
+  if (W >= nc) {
+    T r[FMAX + 1];
+    const bool own = warp < nc;
+    if (own) {
+      const T* Rw = Fl + warp * rw * kWarp;
 #pragma unroll
-      for (int j = 0; j <= FMAX; ++j) r[j] = j < rw ? Rk[j * kWarp] : T(0);
-#pragma unroll
-      for (int m = 0; m < 8; ++m) {
-        if (m < k) {
-          const T* Um = Fl + m * rw * kWarp;
-          const T l = r[m] / Um[m * kWarp];
-          r[m] = l;
-#pragma unroll
-          for (int j = m + 1; j <= FMAX; ++j)
-            if (j < rw) r[j] -= l * Um[j * kWarp];
-        }
-      }
-#pragma unroll
-      for (int j = 0; j < 8; ++j)
-        if (j == k) r[j] = guarded_pivot(r[j], static_pivot != 0, eps, shifted);
-#pragma unroll
-      for (int j = 0; j <= FMAX; ++j)
-        if (j < rw) Rk[j * kWarp] = r[j];
+      for (int j = 0; j <= FMAX; ++j) r[j] = j < rw ? Rw[j * kWarp] : T(0);
     }
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      if (m >= nc) break;
+      if (warp == m) {
+        r[m] = guarded_pivot(r[m], static_pivot != 0, eps, shifted);
+        inv_l[m * kWarp] = T(1) / r[m];
+        T* Rm = Fl + m * rw * kWarp;
+#pragma unroll
+        for (int j = 0; j <= FMAX; ++j)
+          if (j < rw) Rm[j * kWarp] = r[j];
+      }
+      __syncthreads();
+      if (own && warp > m) {
+        const T* Um = Fl + m * rw * kWarp;
+        const T l = r[m] * inv_l[m * kWarp];
+        r[m] = l;
+#pragma unroll
+        for (int j = m + 1; j <= FMAX; ++j)
+          if (j < rw) r[j] -= l * Um[j * kWarp];
+      }
+    }
+  } else {
+    if (warp == 0) {
+      for (int k = 0; k < nc; ++k) {
+        T* Rk = Fl + (size_t)k * rw * kWarp;
+        T r[FMAX + 1];
+#pragma unroll
+        for (int j = 0; j <= FMAX; ++j) r[j] = j < rw ? Rk[(size_t)j * kWarp] : T(0);
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+          if (m < k) {
+            const T* Um = Fl + (size_t)m * rw * kWarp;
+            const T l = r[m] * inv_l[m * kWarp];
+            r[m] = l;
+#pragma unroll
+            for (int j = m + 1; j <= FMAX; ++j)
+              if (j < rw) r[j] -= l * Um[(size_t)j * kWarp];
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+          if (j == k) {
+            r[j] = guarded_pivot(r[j], static_pivot != 0, eps, shifted);
+            inv_l[j * kWarp] = T(1) / r[j];
+          }
+#pragma unroll
+        for (int j = 0; j <= FMAX; ++j)
+          if (j < rw) Rk[(size_t)j * kWarp] = r[j];
+      }
+    }
+    __syncthreads();
   }
-  __syncthreads();
 
   // phase 3b: outputs of the pivot rows (U rows, y) ...
   const size_t b = col0 + lane;
@@ -284,7 +323,7 @@ __global__ void __launch_bounds__(256)
     for (int m = 0; m < 8; ++m) {
       if (m < nc) {
         const T* Um = Fl + m * rw * kWarp;
-        const T l = r[m] / Um[m * kWarp];
+        const T l = r[m] * inv_l[m * kWarp];
         r[m] = l;
 #pragma unroll
         for (int j = m + 1; j <= FMAX; ++j)
