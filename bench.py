@@ -324,6 +324,8 @@ def run_engine(args) -> None:
         except Exception:
             traffic = None
 
+    extras = run_extras(args, dev) if (rank == 0 and world == 1 and not args.no_extra) else None
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(g, args.cpu_sample)
@@ -357,6 +359,7 @@ def run_engine(args) -> None:
                          "algorithmic_bytes": fbytes, "ms_per_factorization": round(per_fact_ms, 4),
                          "peak_source": peaks["source"]},
             "stage_ms_per_solve": {k: round(v[0], 4) for k, v in st.items()},
+            "other_configs": extras,
             "cpu_baseline": cpu,
             "gpu_launches": int(head["launches"]),
             "clocks": clk.summary(),
@@ -365,6 +368,88 @@ def run_engine(args) -> None:
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def run_extras(args, dev) -> dict:
+    """The other configurations of the workload, measured after the headline:
+    the uneven multi-grid batch and the differentiable 10,000-bus case."""
+    import torch
+
+    import cupf
+    from cupf import grids
+    from cupf.batching import UnevenBatch
+
+    out = {}
+    cfg = cupf.NRConfig(tolerance=TOL, max_iter=MAX_ITER)
+    # uneven batch: 118/500/2,000/10,000 buses x 256/128/96/32 instances, one
+    # engine and CUDA stream per grid, solved concurrently (mixed, flat start)
+    inst = grids.uneven_grids()
+    ub = UnevenBatch([g for g, _ in inst])
+    S = [torch.tensor(g.scenarios(c, seed=600 + i), device=dev) for i, (g, c) in enumerate(inst)]
+    V0 = [torch.tensor(g.flat_start(c), device=dev) for g, c in inst]
+    for _ in range(2):
+        ub.solve(S, V0, cfg)
+    res = {}
+    for mode, conc in (("concurrent", True), ("sequential", False)):
+        ts, conv = [], 0
+        for _ in range(3):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            r = ub.solve(S, V0, cfg, concurrent=conc)
+            e1.record()
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+            conv = sum(int((fm <= TOL).sum()) for _, fm, _ in r)
+        res[mode] = {"ms": round(statistics.mean(ts), 3), "converged": conv,
+                     "value": round(conv / (statistics.mean(ts) / 1e3), 1)}
+    out["uneven_batch"] = {"instances": sum(c for _, c in inst),
+                           "grids": [[g.n_bus, c] for g, c in inst], "unit": UNIT,
+                           "method": "one engine + CUDA stream per grid, host thread per grid", **res}
+    # differentiable large case: 10,000 buses x 64, mixed forward through the
+    # torch autograd wrapper, loss = sum (Vm - 1)^2, backward = adjoint J^T solve
+    g = grids.grid_10000()
+    o = cupf.NewtonOptions()
+    o.backend = cupf.BackendKind.CUDA
+    o.compute = cupf.ComputePolicy.Mixed
+    o.custom.serial_nd = True
+    s = cupf.NewtonSolver(o)
+    s.initialize(g.indptr, g.indices, g.data, g.n_bus, g.n_bus, g.pv, g.pq)
+    B = 64
+    lp, lq = g.load_scenarios(B, seed=808)
+    base_re = torch.tensor(g.sgen.real, device=dev, dtype=torch.float32)
+    base_im = torch.tensor(g.sgen.imag, device=dev, dtype=torch.float32)
+    v0 = torch.tensor(g.v0, device=dev)
+    va0, vm0 = torch.angle(v0).float(), torch.abs(v0).float()
+    c5cfg = cupf.NRConfig(tolerance=TOL, max_iter=20)
+    tf, tb = [], []
+    for rep in range(4):
+        load_p = torch.tensor(lp, device=dev, dtype=torch.float32, requires_grad=True)
+        load_q = torch.tensor(lq, device=dev, dtype=torch.float32, requires_grad=True)
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record()
+        va, vm = cupf.solve(load_p, load_q, s, sbus_base_re=base_re, sbus_base_im=base_im, v0_va=va0, v0_vm=vm0,
+                            config=c5cfg)
+        loss = ((vm - 1.0) ** 2).sum()
+        e1.record()
+        loss.backward()
+        e2.record()
+        e2.synchronize()
+        if rep:
+            tf.append(e0.elapsed_time(e1))
+            tb.append(e1.elapsed_time(e2))
+    from oracle.oracle import Oracle
+
+    orc = Oracle()
+    S0 = g.sgen - (lp[0] + 1j * lq[0])
+    V = orc.solve(g, S0, g.v0, tol=1e-12, max_iter=30)["V"]
+    a = orc.adjoint(g, V, np.zeros(g.n_bus), 2.0 * (np.abs(V) - 1.0))
+    gp = load_p.grad[0].double().cpu().numpy()
+    relp = float(np.abs(gp - a["grad_p"]).max() / np.abs(a["grad_p"]).max())
+    out["c5_10000x64"] = {"forward_ms": round(statistics.mean(tf), 3), "backward_ms": round(statistics.mean(tb), 3),
+                          "loss": float(loss.item()), "grad_p_rel_err_vs_fp64_oracle_adjoint": relp,
+                          "path": "cupf.solve (CuPFFunction), mixed, flat start; backward = J^T solve on the "
+                                  "final-state factors"}
+    return out
 
 
 def cpu_baseline(g, sample: int) -> dict:
@@ -421,6 +506,7 @@ def main() -> None:
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-warm", action="store_true", help="skip the learned warm start (flat start only)")
     ap.add_argument("--no-graph", action="store_true", help="launch every kernel from the host (no CUDA graph)")
+    ap.add_argument("--no-extra", action="store_true", help="skip the uneven-batch and 10,000-bus measurements")
     ap.add_argument("--train", type=int, default=200000, help="warm-start training scenarios (engine-solved)")
     ap.add_argument("--epochs", type=int, default=40)
     args = ap.parse_args()
