@@ -525,9 +525,9 @@ pf_status pf_solve_backward_device(pf_handle h, const void* grad_va, const void*
       throw std::invalid_argument("cupf::torch_api::solve_backward(): dtype must be " + want);
     if (n_bus != h->n_bus) throw std::invalid_argument("cupf::torch_api::solve_backward(): n_bus mismatch");
     if (!grad_load_p || !grad_load_q) throw std::invalid_argument("output gradients must not be null");
-    (void)options;
     const double res = h->eng->solve_adjoint_device(grad_va, grad_vm, grad_load_p, grad_load_q, nullptr, batch,
-                                                    want == "float64", caller_stream(stream));
+                                                    want == "float64", caller_stream(stream),
+                                                    options ? options->check_residual != 0 : true);
     if (result) {
       std::memset(result, 0, sizeof(*result));
       result->n_bus = n_bus;
@@ -584,7 +584,8 @@ pf_status pf_solve_adjoint(pf_handle h, const double* grad_va, int64_t grad_va_s
     } guard{{dga, dgm, dgp, dgq, dl}};
     cudaMemcpy(dga, ga.data(), bn, cudaMemcpyHostToDevice);
     cudaMemcpy(dgm, gm.data(), bn, cudaMemcpyHostToDevice);
-    const double res = h->eng->solve_adjoint_device(dga, dgm, dgp, dgq, dl, batch, 1, nullptr);
+    const double res = h->eng->solve_adjoint_device(dga, dgm, dgp, dgq, dl, batch, 1, cudaStreamLegacy,
+                                                    options ? options->check_residual != 0 : true);
     if (lambda) cudaMemcpy(lambda, dl, bd, cudaMemcpyDeviceToHost);
     if (grad_load_p) cudaMemcpy(grad_load_p, dgp, bn, cudaMemcpyDeviceToHost);
     if (grad_load_q) cudaMemcpy(grad_load_q, dgq, bn, cudaMemcpyDeviceToHost);

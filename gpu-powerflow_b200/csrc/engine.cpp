@@ -107,7 +107,7 @@ struct Engine::Impl {
   DBuf J, U, L, CB, Y, X, front_scratch;
   size_t front_scratch_elems = 0;
   DBuf stage_in, stage_out, fin;
-  DBuf G, R, lam, dlam, TV, W, Z, Jd;
+  DBuf G, R, lam, dlam, TV, W, Z, Jd, red;
   unsigned long long* h_norm = nullptr;
   double* h_final = nullptr;
   int h_cap = 0;
@@ -803,7 +803,8 @@ void Engine::transpose_solve(const double* d_G, double* d_lam, cudaStream_t s) {
 }
 
 double Engine::solve_adjoint_device(const void* grad_va, const void* grad_vm, void* grad_p, void* grad_q,
-                                    double* d_lambda, int32_t B, int32_t is_double, cudaStream_t stream) {
+                                    double* d_lambda, int32_t B, int32_t is_double, cudaStream_t stream,
+                                    bool residual) {
   if (!adjoint_ready_)
     throw std::runtime_error("NewtonSolver::solve_adjoint(): missing exact final-state adjoint cache");
   if (B != B_) throw std::invalid_argument("NewtonSolver::solve_adjoint(): batch_size does not match the last forward solve");
@@ -832,23 +833,26 @@ double Engine::solve_adjoint_device(const void* grad_va, const void* grad_vm, vo
     else transpose_solve<float>(d.R.as<double>(), d.dlam.as<double>(), s);
     launch_axpy(d.lam.as<double>(), d.dlam.as<double>(), (long long)(dim * Bp), s);
   }
-  launch_jt_residual(d.g, d.Bp, d.Jd.as<double>(), d.lam.as<double>(), d.G.as<double>(), d.R.as<double>(), s);
   launch_project_load_gradients(d.g, st, d.lam.as<double>(), grad_p, grad_q, is_double, s);
   if (d_lambda) launch_rows_to_batch<double, double>(d.lam.as<double>(), d_lambda, (int)dim, B, d.Bp, s);
-  // relative residual ||J^T lambda - g|| / ||g|| over the real scenarios
-  std::vector<double> hr(dim * Bp), hg(dim * Bp);
-  CUPF_CUDA(cudaMemcpyAsync(hr.data(), d.R.p, dim * Bp * 8, cudaMemcpyDeviceToHost, s));
-  CUPF_CUDA(cudaMemcpyAsync(hg.data(), d.G.p, dim * Bp * 8, cudaMemcpyDeviceToHost, s));
-  CUPF_CUDA(cudaStreamSynchronize(s));
+  double res = 0.0;
+  if (residual) {
+    // relative residual ||J^T lambda - g|| / ||g|| over the real scenarios,
+    // reduced on the device; two doubles come back
+    launch_jt_residual(d.g, d.Bp, d.Jd.as<double>(), d.lam.as<double>(), d.G.as<double>(), d.R.as<double>(), s);
+    d.red.reserve((2 + 2 * 296) * sizeof(double));
+    launch_sumsq2(d.R.as<double>(), d.G.as<double>(), (int)dim, B, d.Bp, d.red.as<double>(), s);
+    CUPF_CUDA(cudaMemcpyAsync(d.h_norm, d.red.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  }
   CUPF_CUDA(cudaGetLastError());
-  long double rr = 0.0L, gg = 0.0L;
-  for (size_t f = 0; f < dim; ++f)
-    for (int b = 0; b < B; ++b) {
-      rr += (long double)hr[f * Bp + b] * hr[f * Bp + b];
-      gg += (long double)hg[f * Bp + b] * hg[f * Bp + b];
-    }
-  const long double den = std::max(std::sqrt(std::max(gg, 1e-60L)), 1e-30L);
-  return (double)(std::sqrt(rr) / den);
+  if (residual) {
+    // without the norm the call stays stream-ordered and returns at once
+    CUPF_CUDA(cudaStreamSynchronize(s));
+    double sums[2];
+    std::memcpy(sums, d.h_norm, sizeof(sums));
+    res = std::sqrt(sums[0]) / std::max(std::sqrt(std::max(sums[1], 1e-60)), 1e-30);
+  }
+  return res;
 }
 
 void Engine::factorize_values(const void* d_values, int32_t values_is_double, int32_t B, cudaStream_t stream) {

@@ -83,8 +83,11 @@ class Engine {
                              cudaStream_t stream, double* d_final_mismatch);
   // Adjoint on the cached final-state factors: grads [B][n] device, outputs
   // grad_p / grad_q [B][n]; optional lambda [B][dimF] (double, device).
+  // The relative residual ||J^T lambda - g|| / ||g|| is returned when
+  // `residual` (else 0).
   double solve_adjoint_device(const void* grad_va, const void* grad_vm, void* grad_p, void* grad_q,
-                              double* d_lambda, int32_t B, int32_t is_double, cudaStream_t stream);
+                              double* d_lambda, int32_t B, int32_t is_double, cudaStream_t stream,
+                              bool residual = true);
 
   // Linear-solver boundary: factor caller-supplied Jacobian values and solve.
   void factorize_values(const void* d_values, int32_t values_is_double, int32_t B, cudaStream_t stream);

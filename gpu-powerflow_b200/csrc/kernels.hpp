@@ -144,6 +144,9 @@ void launch_project_load_gradients(const DevGrid& g, const DevState& st, const d
 void launch_jt_residual(const DevGrid& g, int Bp, const double* Jd, const double* lam, const double* G, double* R,
                         cudaStream_t s);
 void launch_axpy(double* y, const double* x, long long n, cudaStream_t s);
+// scratch[0] = sum r^2, scratch[1] = sum g^2 over f < dim, b < B of [dim][Bp]
+// arrays R and G; scratch holds 2 + 2 * 296 doubles
+void launch_sumsq2(const double* R, const double* G, int dim, int B, int Bp, double* scratch, cudaStream_t s);
 // [B][rows] (TS) -> [rows][Bp] (TD) and back; pad scenarios copy scenario B - 1
 template <typename TS, typename TD>
 void launch_batch_to_rows(const TS* src, TD* dst, int rows, int B, int Bp, cudaStream_t s);

@@ -365,6 +365,49 @@ __global__ void k_jt_residual(DevGrid g, int Bp, const double* __restrict__ Jd, 
   }
 }
 
+// Relative residual of the adjoint: per-block partial sums of r^2 and g^2
+// over the real scenarios (b < B) of two [dim][Bp] arrays, then one block
+// adds the partials in a fixed order (deterministic).
+constexpr int kNormBlocks = 296;
+__global__ void k_sumsq_partials(const double* __restrict__ R, const double* __restrict__ G, int dim, int B, int Bp,
+                                 double* __restrict__ partials) {
+  __shared__ double sr[256], sg[256];
+  double ar = 0.0, ag = 0.0;
+  const long long n = (long long)dim * B;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const long long f = i / B, b = i - f * B;
+    const double r = R[f * Bp + b], g = G[f * Bp + b];
+    ar += r * r;
+    ag += g * g;
+  }
+  sr[threadIdx.x] = ar;
+  sg[threadIdx.x] = ag;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      sr[threadIdx.x] += sr[threadIdx.x + o];
+      sg[threadIdx.x] += sg[threadIdx.x + o];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    partials[2 * blockIdx.x] = sr[0];
+    partials[2 * blockIdx.x + 1] = sg[0];
+  }
+}
+
+__global__ void k_sumsq_final(const double* __restrict__ partials, int nblocks, double* __restrict__ out) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    double r = 0.0, g = 0.0;
+    for (int i = 0; i < nblocks; ++i) {
+      r += partials[2 * i];
+      g += partials[2 * i + 1];
+    }
+    out[0] = r;
+    out[1] = g;
+  }
+}
+
 __global__ void k_axpy(double* y, const double* x, long long n) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     y[i] += x[i];
@@ -523,6 +566,11 @@ template void launch_batch_to_rows<float, double>(const float*, double*, int, in
 template void launch_rows_to_batch<double, double>(const double*, double*, int, int, int, cudaStream_t);
 template void launch_rows_to_batch<float, double>(const float*, double*, int, int, int, cudaStream_t);
 template void launch_rows_to_batch<double, float>(const double*, float*, int, int, int, cudaStream_t);
+
+void launch_sumsq2(const double* R, const double* G, int dim, int B, int Bp, double* scratch, cudaStream_t s) {
+  k_sumsq_partials<<<kNormBlocks, 256, 0, s>>>(R, G, dim, B, Bp, scratch + 2);
+  k_sumsq_final<<<1, 32, 0, s>>>(scratch + 2, kNormBlocks, scratch);
+}
 
 void launch_axpy(double* y, const double* x, long long n, cudaStream_t s) {
   long long blocks = (n + 255) / 256;
