@@ -63,6 +63,7 @@ EXPORTS = [
     "pf_solve_batch_warm_device", "pf_solve_forward_device", "pf_solve_backward_device", "pf_solve_adjoint",
     "pf_info", "pf_plan_array",
     "pf_evaluate", "pf_set_profiling", "pf_stage_times", "pf_plan_array64", "pf_singular_flags",
+    "pf_case_load", "pf_case_last_error", "pf_case_dims", "pf_case_name", "pf_case_copy", "pf_case_destroy",
 ]
 # exported symbols of include/cupf_mlp.h (warm-start network kernels)
 MLP_EXPORTS = [
@@ -117,6 +118,12 @@ def _declare(lib: C.CDLL) -> None:
         "pf_plan_array64": ([_vp, C.c_char_p, _vp, _i64, _p(_i64)], _i32),
         "pf_stage_times": ([_vp, _vp, _vp], _i32),
         "pf_singular_flags": ([_vp, _vp, _i32], _i32),
+        "pf_case_load": ([C.c_char_p, _p(_vp)], _i32),
+        "pf_case_last_error": ([], C.c_char_p),
+        "pf_case_dims": ([_vp, _p(_i32), _p(_i32), _p(_i32), _p(_i32), _p(_i32), _p(_i32)], _i32),
+        "pf_case_name": ([_vp], C.c_char_p),
+        "pf_case_copy": ([_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp], _i32),
+        "pf_case_destroy": ([_vp], None),
         "mlp_last_error": ([], C.c_char_p),
         "mlp_gemm_bf16": ([_vp, _i64, _vp, _i64, _i32, _i32, _i32, _i32, _vp, _i64, _vp, _vp, _i64, _vp], _i32),
         "mlp_error_flag": ([_p(_i32), _i32], _i32),

@@ -279,6 +279,30 @@ pf_status pf_plan_array64(pf_handle h, const char* name, int64_t* out, int64_t c
 /* Per-scenario static-pivot flags of the last factorization. */
 pf_status pf_singular_flags(pf_handle h, int32_t* out_host, int32_t batch);
 
+/* ---- Case I/O: the reference's dump-case directory format ----------------
+ * Replaces: cupf::tests::load_dump_case (cuPF/tests/dump_case_loader.cpp:210-232,
+ * dump_case_loader.hpp:14-42), the loader of the case directories that
+ * benchmark/common/matpower_data.py:341-359 (save_dump_case) writes:
+ * dump_Ybus.mtx (MatrixMarket coordinate complex), dump_Sbus.txt, dump_V.txt,
+ * dump_pv.txt, dump_pq.txt, and, when present, dump_Vref.txt.  Complex arrays
+ * come out interleaved (re, im) as double[2 * n]; Ybus as sorted CSR.
+ * pf_case_load returns PF_RUNTIME_ERROR with the reference's message (read
+ * with pf_case_last_error, per thread) for a missing directory or file,
+ * a malformed line, an unsupported header, an out-of-range entry or
+ * mismatched sizes. */
+typedef struct pf_case_s* pf_case;
+pf_status pf_case_load(const char* case_dir, pf_case* out);
+const char* pf_case_last_error(void);
+pf_status pf_case_dims(pf_case c, int32_t* rows, int32_t* cols, int32_t* nnz, int32_t* n_pv, int32_t* n_pq,
+                       int32_t* has_vref);
+/* Directory name of the case (DumpCaseData::case_name). */
+const char* pf_case_name(pf_case c);
+/* Copies the case into caller buffers sized by pf_case_dims; any pointer may
+ * be NULL to skip that array (vref must be NULL when has_vref is 0). */
+pf_status pf_case_copy(pf_case c, int32_t* indptr, int32_t* indices, double* ybus, double* sbus, double* v0,
+                       int32_t* pv, int32_t* pq, double* vref);
+void pf_case_destroy(pf_case c);
+
 #ifdef __cplusplus
 }
 #endif

@@ -178,6 +178,8 @@ class Reference:
         L.ref_symbolic_names.argtypes = [C.c_void_p, C.c_char_p, C.c_int]
         L.ref_symbolic_free.restype = None
         L.ref_symbolic_free.argtypes = [C.c_void_p]
+        L.ref_load_dump_case.restype = C.c_int
+        L.ref_load_dump_case.argtypes = [C.c_char_p] + [C.POINTER(C.c_int32)] * 4 + [C.c_void_p] * 7
 
     def _err(self, rc: int) -> None:
         if rc:
@@ -257,6 +259,24 @@ class Reference:
             return out
         finally:
             self.lib.ref_symbolic_free(h)
+
+
+    def load_dump_case(self, case_dir) -> dict:
+        """cupf::tests::load_dump_case (cuPF/tests/dump_case_loader.cpp:210-232)."""
+        rows, nnz, npv, npq = (C.c_int32(0) for _ in range(4))
+        d = str(case_dir).encode()
+        self._err(self.lib.ref_load_dump_case(d, C.byref(rows), C.byref(nnz), C.byref(npv), C.byref(npq),
+                                              *([None] * 7)))
+        n = rows.value
+        out = {"indptr": np.zeros(n + 1, np.int32), "indices": np.zeros(nnz.value, np.int32),
+               "ybus_data": np.zeros(nnz.value, np.complex128), "sbus": np.zeros(n, np.complex128),
+               "v0": np.zeros(n, np.complex128), "pv": np.zeros(npv.value, np.int32),
+               "pq": np.zeros(npq.value, np.int32)}
+        keys = ("indptr", "indices", "ybus_data", "sbus", "v0", "pv", "pq")
+        self._err(self.lib.ref_load_dump_case(d, C.byref(rows), C.byref(nnz), C.byref(npv), C.byref(npq),
+                                              *[out[k].ctypes.data for k in keys]))
+        out["rows"] = n
+        return out
 
 
 def reference_available() -> bool:

@@ -16,6 +16,7 @@
 #include <thread>
 #include <vector>
 
+#include "dump_case_loader.hpp"
 #include "newton_solver/core/newton_solver.hpp"
 #include "newton_solver/ops/jacobian/jacobian_analysis.hpp"
 
@@ -169,6 +170,31 @@ int ref_jacobian_analysis(int n_bus, const int32_t* indptr, const int32_t* indic
       std::memcpy(w, v->data(), sizeof(int32_t) * n_bus);
       w += n_bus;
     }
+    return 0;
+  } catch (const std::exception& e) {
+    g_error = e.what();
+    return 1;
+  }
+}
+
+// cupf::tests::load_dump_case (cuPF/tests/dump_case_loader.cpp:210-232):
+// sizes when any output pointer is null, else the arrays (complex as re, im).
+int ref_load_dump_case(const char* dir, int32_t* rows, int32_t* nnz, int32_t* n_pv, int32_t* n_pq, int32_t* indptr,
+                       int32_t* indices, double* ydata, double* sbus, double* v0, int32_t* pv, int32_t* pq) {
+  try {
+    const auto d = cupf::tests::load_dump_case(dir);
+    *rows = d.rows;
+    *nnz = (int32_t)d.ybus_data.size();
+    *n_pv = (int32_t)d.pv.size();
+    *n_pq = (int32_t)d.pq.size();
+    if (!indptr || !indices || !ydata || !sbus || !v0 || !pv || !pq) return 0;
+    std::memcpy(indptr, d.indptr.data(), d.indptr.size() * sizeof(int32_t));
+    std::memcpy(indices, d.indices.data(), d.indices.size() * sizeof(int32_t));
+    std::memcpy(ydata, d.ybus_data.data(), d.ybus_data.size() * sizeof(std::complex<double>));
+    std::memcpy(sbus, d.sbus.data(), d.sbus.size() * sizeof(std::complex<double>));
+    std::memcpy(v0, d.v0.data(), d.v0.size() * sizeof(std::complex<double>));
+    if (!d.pv.empty()) std::memcpy(pv, d.pv.data(), d.pv.size() * sizeof(int32_t));
+    if (!d.pq.empty()) std::memcpy(pq, d.pq.data(), d.pq.size() * sizeof(int32_t));
     return 0;
   } catch (const std::exception& e) {
     g_error = e.what();

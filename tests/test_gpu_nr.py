@@ -232,3 +232,19 @@ def test_uneven_multi_grid_batch(oracle):
         s0 = S[i][0].cpu().numpy()
         ref = oracle.solve(g, s0, g.v0, tol=1e-12, max_iter=30)["V"]
         assert np.abs(V[0].cpu().numpy() - ref).max() <= 1e-8
+
+
+def test_dump_case_solves_like_the_grid(tmp_path):
+    """A grid written in the dump-case format and read back solves to the
+    same voltages, bit for bit, on the batch cupf_bench builds from a case
+    (load scale 1 + step * b, cuPF/tests/cupf_bench.cpp:188-198)."""
+    from cupf import case_io
+
+    g = G.grid_2000()
+    c = case_io.load_dump_case(case_io.save_grid(tmp_path, g))
+    S, V0 = case_io.replicate_scenarios(c, 40, load_scale_step=0.001)
+    s = make_solver(g, cupf.ComputePolicy.Mixed)
+    a = s.solve_batch(c.indptr, c.indices, c.ybus_data, c.rows, c.cols, S, V0, c.pv, c.pq, cfg())
+    b = solve(s, g, S, V0, cfg())
+    assert a.converged_numpy.all()
+    assert np.array_equal(a.V_numpy, b.V_numpy)
