@@ -454,6 +454,52 @@ pf_status pf_solve_batch_device(pf_handle h, const double* sbus, int64_t sbus_st
   })
 }
 
+pf_status pf_solve_batch_ybus(pf_handle h, const double* ybus_data, int64_t ybus_stride, const double* sbus,
+                              int64_t sbus_stride, const double* V0, int64_t V0_stride, int32_t batch,
+                              const pf_nr_config* config, const pf_solve_options* solve_options, double* V_out,
+                              int32_t* iterations, double* final_mismatch, uint8_t* converged) {
+  if (!h || !h->eng) return PF_INVALID_ARGUMENT;
+  PF_TRY(h, {
+    if (!h->eng->initialized()) throw std::runtime_error("NewtonSolver::solve_batch(): initialize() must be called first");
+    if (batch <= 0) throw std::invalid_argument("NewtonSolver::solve_batch(): batch_size must be positive");
+    if (!ybus_data) throw std::invalid_argument("per-scenario Ybus values must not be null");
+    if (ybus_stride < (int64_t)h->ind.size())
+      throw std::invalid_argument("per-scenario Ybus stride must be at least the Ybus nnz");
+    const pf_nr_config cfg = config ? *config : pf_nr_config{1e-8, 50};
+    const int prep = solve_options ? solve_options->prepare_adjoint_cache : 0;
+    h->eng->solve_batch_host(sbus, sbus_stride, V0, V0_stride, batch, cfg.tolerance, cfg.max_iter, prep, V_out,
+                             iterations, final_mismatch, converged, ybus_data, ybus_stride);
+  })
+}
+
+pf_status pf_solve_batch_ybus_device(pf_handle h, const double* ybus_data, int64_t ybus_stride, const double* sbus,
+                                     int64_t sbus_stride, const double* V0, int64_t V0_stride, int32_t batch,
+                                     const pf_nr_config* config, const pf_solve_options* solve_options,
+                                     double* V_out, double* final_mismatch, void* stream, pf_adjoint_result* result) {
+  if (!h || !h->eng) return PF_INVALID_ARGUMENT;
+  PF_TRY(h, {
+    if (!sbus || !V0 || !ybus_data) throw std::invalid_argument("sbus/V0/ybus must not be null");
+    if (sbus_stride < h->n_bus || V0_stride < h->n_bus) throw std::invalid_argument("stride must be at least n_bus");
+    if (ybus_stride < (int64_t)h->ind.size())
+      throw std::invalid_argument("per-scenario Ybus stride must be at least the Ybus nnz");
+    const pf_nr_config cfg = config ? *config : pf_nr_config{1e-8, 50};
+    const int prep = solve_options ? solve_options->prepare_adjoint_cache : 0;
+    const auto st = h->eng->solve_batch_device(sbus, sbus_stride, V0, V0_stride, batch, cfg.tolerance, cfg.max_iter,
+                                               prep, V_out, final_mismatch, caller_stream(stream), ybus_data,
+                                               ybus_stride);
+    if (result) {
+      std::memset(result, 0, sizeof(*result));
+      result->n_bus = h->n_bus;
+      result->batch_size = batch;
+      result->dim_f = h->eng->dim();
+      result->success = 1;
+      result->iterations = st.iterations;
+      result->max_final_mismatch = st.max_final_mismatch;
+      result->all_converged = st.all_converged;
+    }
+  })
+}
+
 pf_status pf_solve_batch_warm_device(pf_handle h, const double* sbus, int64_t sbus_stride, const double* V0,
                                      int64_t V0_stride, const float* pred, int64_t pred_ld, int32_t batch,
                                      const pf_nr_config* config, const pf_solve_options* solve_options,

@@ -120,6 +120,9 @@ struct DevState {
   int fp_double = 0;    // Fp holds double (FP64 factors) or float
   unsigned long long* norm_bits = nullptr;  // [Bp] max |F| per scenario as IEEE bits
   int* sing = nullptr;                      // [Bp] static-pivot shift applied
+  // per-scenario Ybus values [nnz_y][Bp] (null: every scenario uses DevGrid's)
+  const double* yb_re = nullptr;
+  const double* yb_im = nullptr;
 };
 
 }  // namespace cupf_b200

@@ -108,6 +108,9 @@ struct Engine::Impl {
   size_t front_scratch_elems = 0;
   DBuf stage_in, stage_out, fin;
   DBuf G, R, lam, dlam, TV, W, Z, Jd, red;
+  DBuf yb_re, yb_im;           // per-scenario Ybus values [nnz_y][Bp]
+  bool yb_active = false;      // the current batch uses them
+  const void* graph_yb = nullptr;  // yb pointer baked into the captured iteration
   unsigned long long* h_norm = nullptr;
   double* h_final = nullptr;
   int h_cap = 0;
@@ -157,6 +160,8 @@ struct Engine::Impl {
     st.fp_double = fp_double ? 1 : 0;
     st.norm_bits = norm.as<unsigned long long>();
     st.sing = sing.as<int>();
+    st.yb_re = yb_active ? yb_re.as<double>() : nullptr;
+    st.yb_im = yb_active ? yb_im.as<double>() : nullptr;
     return st;
   }
 };
@@ -638,7 +643,8 @@ SolveStats Engine::run_loop(double tol, int32_t max_iter, int32_t prepare_adjoin
     if (!finite) throw std::runtime_error("NewtonSolver: mismatch norm is not finite");
     if (gmax <= tol) break;
     if (use_graph) {
-      if (!d.exec || d.graph_Bp != d.Bp || d.graph_double != std::is_same<T, double>::value) {
+      if (!d.exec || d.graph_Bp != d.Bp || d.graph_double != std::is_same<T, double>::value ||
+          d.graph_yb != static_cast<const void*>(st.yb_re)) {
         if (d.exec) cudaGraphExecDestroy(d.exec);
         d.exec = nullptr;
         cudaStream_t cs = d.own;
@@ -652,6 +658,7 @@ SolveStats Engine::run_loop(double tol, int32_t max_iter, int32_t prepare_adjoin
         cudaGraphDestroy(graph);
         d.graph_Bp = d.Bp;
         d.graph_double = std::is_same<T, double>::value;
+        d.graph_yb = st.yb_re;
         launches_ = before;
       }
       CUPF_CUDA(cudaGraphLaunch(d.exec, s));
@@ -690,14 +697,16 @@ SolveStats Engine::run_loop(double tol, int32_t max_iter, int32_t prepare_adjoin
 
 SolveStats Engine::solve_batch_host(const double* sbus, int64_t sbus_stride, const double* v0, int64_t v0_stride,
                                     int32_t B, double tol, int32_t max_iter, int32_t prepare_adjoint, double* v_out,
-                                    int32_t* iterations, double* final_mismatch, uint8_t* converged) {
+                                    int32_t* iterations, double* final_mismatch, uint8_t* converged,
+                                    const double* ybus, int64_t ybus_stride) {
   if (!sbus || !v0) throw std::invalid_argument("NewtonSolver::solve_batch(): sbus/V0 must not be null");
   if (sbus_stride < ja_.n_bus) throw std::invalid_argument("NewtonSolver::solve_batch(): sbus stride must be at least n_bus");
   if (v0_stride < ja_.n_bus) throw std::invalid_argument("NewtonSolver::solve_batch(): V0 stride must be at least n_bus");
   ensure_workspace(B);
   auto& d = *d_;
   const size_t n = ja_.n_bus;
-  const size_t in_elems = 2 * ((size_t)B * sbus_stride + (size_t)B * v0_stride);
+  const size_t y_elems = ybus ? 2 * (size_t)B * ybus_stride : 0;
+  const size_t in_elems = 2 * ((size_t)B * sbus_stride + (size_t)B * v0_stride) + y_elems;
   d.stage_in.reserve(in_elems * sizeof(double));
   d.stage_out.reserve(2 * (size_t)B * n * sizeof(double));
   d.fin.reserve(std::max<size_t>(B, 1) * sizeof(double));
@@ -706,8 +715,10 @@ SolveStats Engine::solve_batch_host(const double* sbus, int64_t sbus_stride, con
   cudaStream_t s = d.own;
   CUPF_CUDA(cudaMemcpyAsync(din, sbus, 2 * (size_t)B * sbus_stride * sizeof(double), cudaMemcpyHostToDevice, s));
   CUPF_CUDA(cudaMemcpyAsync(dv0, v0, 2 * (size_t)B * v0_stride * sizeof(double), cudaMemcpyHostToDevice, s));
+  double* dyb = ybus ? dv0 + 2 * (size_t)B * v0_stride : nullptr;
+  if (ybus) CUPF_CUDA(cudaMemcpyAsync(dyb, ybus, y_elems * sizeof(double), cudaMemcpyHostToDevice, s));
   SolveStats st = solve_batch_device(din, sbus_stride, dv0, v0_stride, B, tol, max_iter, prepare_adjoint,
-                                     d.stage_out.as<double>(), nullptr, s);
+                                     d.stage_out.as<double>(), nullptr, s, dyb, ybus_stride);
   if (v_out)
     CUPF_CUDA(cudaMemcpyAsync(v_out, d.stage_out.p, 2 * (size_t)B * n * sizeof(double), cudaMemcpyDeviceToHost, s));
   CUPF_CUDA(cudaStreamSynchronize(s));
@@ -719,12 +730,28 @@ SolveStats Engine::solve_batch_host(const double* sbus, int64_t sbus_stride, con
   return st;
 }
 
+void Engine::use_scenario_ybus(const double* d_ybus, int64_t ybus_stride, int32_t B, cudaStream_t s) {
+  auto& d = *d_;
+  if (!d_ybus) {
+    d.yb_active = false;
+    return;
+  }
+  const int nnz = (int)ja_.map11.size();
+  if (ybus_stride < nnz) throw std::invalid_argument("solve_batch: per-scenario Ybus stride must be at least nnz");
+  d.yb_re.reserve((size_t)nnz * d.Bp * sizeof(double));
+  d.yb_im.reserve((size_t)nnz * d.Bp * sizeof(double));
+  launch_ybus_to_rows(d_ybus, ybus_stride, nnz, B, d.Bp, d.yb_re.as<double>(), d.yb_im.as<double>(), s);
+  d.yb_active = true;
+}
+
 SolveStats Engine::solve_batch_device(const double* d_sbus, int64_t sbus_stride, const double* d_v0, int64_t v0_stride,
                                       int32_t B, double tol, int32_t max_iter, int32_t prepare_adjoint,
-                                      double* d_v_out, double* d_final_mismatch, cudaStream_t stream) {
+                                      double* d_v_out, double* d_final_mismatch, cudaStream_t stream,
+                                      const double* d_ybus, int64_t ybus_stride) {
   ensure_workspace(B);
   auto& d = *d_;
   cudaStream_t s = stream ? stream : d.own;
+  use_scenario_ybus(d_ybus, ybus_stride, B, s);
   const DevState st = d.state();
   launch_seed_state(d.g, st, d_sbus, sbus_stride, d_v0, v0_stride, s);
   SolveStats out = factor_is_double() ? run_loop<double>(tol, max_iter, prepare_adjoint, s, d_final_mismatch)
@@ -744,6 +771,7 @@ SolveStats Engine::solve_batch_warm_device(const double* d_sbus, int64_t sbus_st
   ensure_workspace(B);
   auto& d = *d_;
   cudaStream_t s = stream ? stream : d.own;
+  use_scenario_ybus(nullptr, 0, B, s);
   const DevState st = d.state();
   launch_seed_state(d.g, st, d_sbus, sbus_stride, d_v0, v0_stride, s);
   launch_apply_warm(d.g, st, d_pred, pred_ld, s);
@@ -771,6 +799,7 @@ SolveStats Engine::solve_from_load(const void* base_re, const void* base_im, con
   ensure_workspace(B);
   auto& d = *d_;
   cudaStream_t s = stream ? stream : d.own;
+  use_scenario_ybus(nullptr, 0, B, s);
   const DevState st = d.state();
   if (batched_v0)
     launch_set_inputs_batched(d.g, st, base_re, base_im, load_p, load_q, va0, vm0, is_double, s);
@@ -1020,6 +1049,7 @@ void Engine::evaluate_host(const double* V, const double* sbus, int32_t B, doubl
   double* dv = ds + 2 * (size_t)B * n;
   CUPF_CUDA(cudaMemcpyAsync(ds, sbus, 2 * (size_t)B * n * sizeof(double), cudaMemcpyHostToDevice, s));
   CUPF_CUDA(cudaMemcpyAsync(dv, V, 2 * (size_t)B * n * sizeof(double), cudaMemcpyHostToDevice, s));
+  use_scenario_ybus(nullptr, 0, B, s);
   const DevState st = d.state();
   launch_seed_state(d.g, st, ds, (long long)n, dv, (long long)n, s);
   CUPF_CUDA(cudaMemsetAsync(d.norm.p, 0, d.Bp * sizeof(unsigned long long), s));

@@ -65,11 +65,15 @@ class Engine {
   // complex [B][stride]; outputs V [B][n] complex, per-scenario stats.
   SolveStats solve_batch_host(const double* sbus, int64_t sbus_stride, const double* v0, int64_t v0_stride,
                               int32_t B, double tol, int32_t max_iter, int32_t prepare_adjoint, double* v_out,
-                              int32_t* iterations, double* final_mismatch, uint8_t* converged);
-  // Same with device-resident inputs/outputs in the same host layout.
+                              int32_t* iterations, double* final_mismatch, uint8_t* converged,
+                              const double* ybus = nullptr, int64_t ybus_stride = 0);
+  // Same with device-resident inputs/outputs in the same host layout.  With
+  // d_ybus (complex [B][ybus_stride], CSR order of the analysed pattern) every
+  // scenario has its own Ybus values; otherwise all share the handle's.
   SolveStats solve_batch_device(const double* d_sbus, int64_t sbus_stride, const double* d_v0, int64_t v0_stride,
                                 int32_t B, double tol, int32_t max_iter, int32_t prepare_adjoint, double* d_v_out,
-                                double* d_final_mismatch, cudaStream_t stream);
+                                double* d_final_mismatch, cudaStream_t stream, const double* d_ybus = nullptr,
+                                int64_t ybus_stride = 0);
   // solve_batch_device from a predicted state (Jacobian-row order, fp32)
   SolveStats solve_batch_warm_device(const double* d_sbus, int64_t sbus_stride, const double* d_v0, int64_t v0_stride,
                                      const float* d_pred, int64_t pred_ld, int32_t B, double tol, int32_t max_iter,
@@ -141,6 +145,8 @@ class Engine {
 
   void ensure_workspace(int32_t B);
   void upload_plan();
+  // selects per-scenario (d_ybus != null) or shared Ybus values for this batch
+  void use_scenario_ybus(const double* d_ybus, int64_t ybus_stride, int32_t B, cudaStream_t s);
   template <typename T>
   SolveStats run_loop(double tol, int32_t max_iter, int32_t prepare_adjoint, cudaStream_t s, double* d_final);
   template <typename T>

@@ -146,6 +146,9 @@ void launch_jt_residual(const DevGrid& g, int Bp, const double* Jd, const double
 void launch_axpy(double* y, const double* x, long long n, cudaStream_t s);
 // scratch[0] = sum r^2, scratch[1] = sum g^2 over f < dim, b < B of [dim][Bp]
 // arrays R and G; scratch holds 2 + 2 * 296 doubles
+// Per-scenario Ybus values complex [B][stride] -> re/im [nnz][Bp]
+void launch_ybus_to_rows(const double* yc, long long stride, int nnz, int B, int Bp, double* yr, double* yi,
+                         cudaStream_t s);
 void launch_sumsq2(const double* R, const double* G, int dim, int B, int Bp, double* scratch, cudaStream_t s);
 // [B][rows] (TS) -> [rows][Bp] (TD) and back; pad scenarios copy scenario B - 1
 template <typename TS, typename TD>

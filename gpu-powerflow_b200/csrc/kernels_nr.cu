@@ -35,11 +35,15 @@ __global__ void k_ibus_mismatch(DevGrid g, DevState st) {
   const size_t b = (size_t)blockIdx.y * kWarp + lane;
   double nmax = 0.0;
   bool bad = false;
+  // Ybus value of entry k: shared y[k], or this scenario's yb[k * Bp + b]
+  const double* yre = st.yb_re ? st.yb_re + b : g.y_re;
+  const double* yim = st.yb_re ? st.yb_im + b : g.y_im;
+  const size_t ys = st.yb_re ? (size_t)Bp : 1;
   for (int i = blockIdx.x * kRows + wy; i < g.n_bus; i += gridDim.x * kRows) {
     double ir = 0.0, ii = 0.0;
     for (int k = g.y_ptr[i]; k < g.y_ptr[i + 1]; ++k) {
       const size_t c = (size_t)g.y_col[k] * Bp + b;
-      const double yr = g.y_re[k], yi = g.y_im[k];
+      const double yr = yre[k * ys], yi = yim[k * ys];
       const double vr = st.v_re[c], vi = st.v_im[c];
       ir += yr * vr - yi * vi;
       ii += yr * vi + yi * vr;
@@ -102,9 +106,12 @@ __global__ void k_jacobian(DevGrid g, DevState st, TJ* __restrict__ J) {
   const int lane = threadIdx.x, wy = threadIdx.y;
   const int Bp = st.Bp;
   const size_t b = (size_t)blockIdx.y * kWarp + lane;
+  const double* yre = st.yb_re ? st.yb_re + b : g.y_re;
+  const double* yim = st.yb_re ? st.yb_im + b : g.y_im;
+  const size_t ys = st.yb_re ? (size_t)Bp : 1;
   for (int k = blockIdx.x * kRows + wy; k < g.nnz_y; k += gridDim.x * kRows) {
     const int i = g.y_row[k], c = g.y_col[k];
-    const double yr = g.y_re[k], yi = g.y_im[k];
+    const double yr = yre[k * ys], yi = yim[k * ys];
     const size_t oi = (size_t)i * Bp + b, oc = (size_t)c * Bp + b;
     const double vir = st.v_re[oi], vii = st.v_im[oi];
     const double vcr = st.v_re[oc], vci = st.v_im[oc];
@@ -445,6 +452,32 @@ __global__ void k_rows_to_batch(const TS* __restrict__ src, TD* __restrict__ dst
   }
 }
 
+// Per-scenario Ybus values, complex [B][stride] (CSR order) -> re/im
+// [nnz][Bp]: 32 x 32 tiles through shared memory; padding scenarios repeat
+// the last one.
+__global__ void k_ybus_to_rows(const double* __restrict__ yc, long long stride, int nnz, int B, int Bp,
+                               double* __restrict__ yr, double* __restrict__ yi) {
+  __shared__ double tr[kWarp][kWarp + 1], ti[kWarp][kWarp + 1];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int k0 = blockIdx.x * kWarp, b0 = blockIdx.y * kWarp;
+  for (int r = ty; r < kWarp; r += kRows) {
+    const int bb = min(b0 + r, B - 1), k = k0 + tx;
+    if (k < nnz) {
+      const double* src = yc + 2 * ((size_t)bb * stride + k);
+      tr[r][tx] = src[0];
+      ti[r][tx] = src[1];
+    }
+  }
+  __syncthreads();
+  for (int r = ty; r < kWarp; r += kRows) {
+    const int k = k0 + r;
+    if (k < nnz) {
+      yr[(size_t)k * Bp + b0 + tx] = tr[tx][r];
+      yi[(size_t)k * Bp + b0 + tx] = ti[tx][r];
+    }
+  }
+}
+
 dim3 rows_grid(int rows, int Bp) {
   int bx = (rows + kRows * 4 - 1) / (kRows * 4);
   if (bx < 1) bx = 1;
@@ -576,6 +609,12 @@ void launch_axpy(double* y, const double* x, long long n, cudaStream_t s) {
   long long blocks = (n + 255) / 256;
   if (blocks > 4096) blocks = 4096;
   k_axpy<<<(unsigned)blocks, 256, 0, s>>>(y, x, n);
+}
+
+void launch_ybus_to_rows(const double* yc, long long stride, int nnz, int B, int Bp, double* yr, double* yi,
+                         cudaStream_t s) {
+  k_ybus_to_rows<<<dim3((nnz + kWarp - 1) / kWarp, Bp / kWarp), dim3(kWarp, kRows), 0, s>>>(yc, stride, nnz, B, Bp,
+                                                                                          yr, yi);
 }
 
 }  // namespace cupf_b200

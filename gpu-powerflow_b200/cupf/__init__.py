@@ -363,6 +363,15 @@ class NewtonSolver:
         fm = np.zeros(B, dtype=np.float64)
         cv = np.zeros(B, dtype=np.uint8)
         cfg, so = _nr_config(config), _solve_options(solve_options)
+        if dt.ndim == 2:
+            # per-scenario Ybus values [batch, nnz] on the initialized pattern
+            if dt.shape[0] != B or dt.shape[1] != ix.size:
+                raise ValueError("per-scenario Ybus data must be [batch, nnz]")
+            _check(self._lib, self._h, self._lib.pf_solve_batch_ybus(
+                self._h, _ptr(dt), dt.shape[1], _ptr(sbus), rows, _ptr(v0), rows, B, C.byref(cfg), C.byref(so),
+                _ptr(V), _ptr(its), _ptr(fm), _ptr(cv)))
+            self._batch = B
+            return NRBatchResult(V, rows, B, its, fm, cv)
         _check(self._lib, self._h, self._lib.pf_solve_batch(
             self._h, _ptr(ip), _ptr(ix), _ptr(dt), rows, cols, dt.size, _ptr(sbus), rows, _ptr(v0), rows, B,
             _ptr(pv), pv.size, _ptr(pq), pq.size, C.byref(cfg), C.byref(so), _ptr(V), _ptr(its), _ptr(fm), _ptr(cv)))
@@ -452,8 +461,10 @@ class NewtonSolver:
         return AdjointResult(raw, zero_copy=True)
 
     # -- engine extras --
-    def solve_batch_device(self, sbus, v0, v_out=None, config=None, solve_options=None):
-        """Device-resident solve: sbus / v0 are complex128 CUDA tensors [batch, n_bus]."""
+    def solve_batch_device(self, sbus, v0, v_out=None, config=None, solve_options=None, ybus=None):
+        """Device-resident solve: sbus / v0 are complex128 CUDA tensors [batch, n_bus];
+        ybus, when given, a complex128 CUDA tensor [batch, nnz] of per-scenario
+        Ybus values on the initialized pattern."""
         import torch
 
         B, n = sbus.shape
@@ -463,6 +474,13 @@ class NewtonSolver:
         stream = torch.cuda.current_stream(sbus.device).cuda_stream
         raw = _capi.PfAdjointResult()
         cfg, so = _nr_config(config), _solve_options(solve_options)
+        if ybus is not None:
+            if ybus.dtype != torch.complex128 or ybus.dim() != 2 or ybus.shape[0] != B or ybus.stride(1) != 1:
+                raise ValueError("ybus must be a complex128 tensor [batch, nnz] with contiguous rows")
+            _check(self._lib, self._h, self._lib.pf_solve_batch_ybus_device(
+                self._h, ybus.data_ptr(), ybus.stride(0), sbus.data_ptr(), n, v0.data_ptr(), n, B, C.byref(cfg),
+                C.byref(so), v_out.data_ptr(), fm.data_ptr(), C.c_void_p(stream), C.byref(raw)))
+            return v_out, fm, raw.iterations
         _check(self._lib, self._h, self._lib.pf_solve_batch_device(
             self._h, sbus.data_ptr(), n, v0.data_ptr(), n, B, C.byref(cfg), C.byref(so), v_out.data_ptr(),
             fm.data_ptr(), C.c_void_p(stream), C.byref(raw)))

@@ -60,6 +60,7 @@ EXPORTS = [
     "cls_solve", "cls_solve_transpose", "cls_singular_flags", "cls_status_string", "cls_last_error",
     "cls_plan_array",
     "pf_create", "pf_destroy", "pf_last_error", "pf_initialize", "pf_analyze_host", "pf_solve_batch", "pf_solve_batch_device",
+    "pf_solve_batch_ybus", "pf_solve_batch_ybus_device",
     "pf_solve_batch_warm_device", "pf_solve_forward_device", "pf_solve_backward_device", "pf_solve_adjoint",
     "pf_info", "pf_plan_array",
     "pf_evaluate", "pf_set_profiling", "pf_stage_times", "pf_plan_array64", "pf_singular_flags",
@@ -103,6 +104,10 @@ def _declare(lib: C.CDLL) -> None:
                             _p(PfNRConfig), _p(PfSolveOptions), _vp, _vp, _vp, _vp], _i32),
         "pf_solve_batch_device": ([_vp, _vp, _i64, _vp, _i64, _i32, _p(PfNRConfig), _p(PfSolveOptions), _vp, _vp,
                                    _vp, _p(PfAdjointResult)], _i32),
+        "pf_solve_batch_ybus": ([_vp, _vp, _i64, _vp, _i64, _vp, _i64, _i32, _p(PfNRConfig), _p(PfSolveOptions), _vp,
+                                 _vp, _vp, _vp], _i32),
+        "pf_solve_batch_ybus_device": ([_vp, _vp, _i64, _vp, _i64, _vp, _i64, _i32, _p(PfNRConfig),
+                                        _p(PfSolveOptions), _vp, _vp, _vp, _p(PfAdjointResult)], _i32),
         "pf_solve_batch_warm_device": ([_vp, _vp, _i64, _vp, _i64, _vp, _i64, _i32, _p(PfNRConfig),
                                         _p(PfSolveOptions), _vp, _vp, _vp, _p(PfAdjointResult)], _i32),
         "pf_solve_forward_device": ([_vp, _vp, _vp, _vp, _vp, _vp, _vp, _i32, _vp, _vp, _i32, _i32, C.c_char_p,

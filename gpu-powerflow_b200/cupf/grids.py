@@ -81,6 +81,32 @@ class Grid:
     def flat_start(self, batch: int) -> np.ndarray:
         return np.repeat(self.v0[None, :], batch, axis=0)
 
+    def branch_scaled_ybus(self, batch: int, lo: float = 0.9, hi: float = 1.1,
+                           seed: int | None = None) -> np.ndarray:
+        """Per-scenario Ybus values [batch, nnz] on this grid's pattern: the
+        series admittance between every connected bus pair is scaled by its
+        own U(lo, hi) factor (a parameter or contingency sweep; a factor of 0
+        takes the pair out of service).  With Y_ij = -y_ij and
+        Y_ii = sum_j y_ij + shunt_i, scaling y_ij by f gives
+        Y'_ij = f Y_ij and Y'_ii = Y_ii - (f - 1) Y_ij; shunts are kept."""
+        rng = np.random.default_rng(self.seed * 104729 + 5 if seed is None else seed)
+        rows = np.repeat(np.arange(self.n_bus), np.diff(self.indptr))
+        cols = self.indices.astype(np.int64)
+        off = rows != cols
+        lo_r, hi_c = np.minimum(rows, cols), np.maximum(rows, cols)
+        pair = lo_r * self.n_bus + hi_c
+        uniq, pid = np.unique(pair[off], return_inverse=True)
+        f = rng.uniform(lo, hi, size=(batch, uniq.size))
+        y = np.repeat(self.data[None, :], batch, axis=0)
+        fo = f[:, pid]                                   # factor of each off-diagonal entry
+        y[:, off] = self.data[off][None, :] * fo
+        dpos = np.flatnonzero(~off)                      # diagonal positions, one per row
+        drow = rows[dpos]
+        delta = np.zeros((batch, self.n_bus), np.complex128)
+        np.add.at(delta.T, rows[off], (-(fo - 1.0) * self.data[off][None, :]).T)
+        y[:, dpos] += delta[:, drow]
+        return y
+
 
 def _mst_edges(xy: np.ndarray) -> np.ndarray:
     """Euclidean MST (Kruskal over the Delaunay edges, which contain it)."""

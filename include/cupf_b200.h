@@ -218,6 +218,25 @@ pf_status pf_solve_batch_device(pf_handle h, const double* sbus, int64_t sbus_st
                                 int64_t V0_stride, int32_t batch, const pf_nr_config* config,
                                 const pf_solve_options* solve_options, double* V_out, double* final_mismatch,
                                 void* stream, pf_adjoint_result* result);
+/* Per-scenario Ybus values (contingency and parameter sweeps on one pattern).
+ * The reference's storage carries ybus_values_batched / ybus_value_stride
+ * (cuda_batched_storage.hpp:84-89, .cpp:262-293; solver_contexts.hpp:42-43)
+ * but its Ibus kernel rejects them (compute_ibus.cu:45-48) and
+ * newton_solver.cpp:294 always passes false.  Here ybus_data is complex
+ * [batch][ybus_stride] in the CSR order of the pattern given to
+ * pf_initialize (ybus_stride >= nnz); scenario b solves with row b.  The
+ * pattern, pv and pq are the initialized ones.  A later solve without these
+ * entry points uses the shared values again; an adjoint after this solve
+ * uses the per-scenario values of its forward solve.  Host buffers: */
+pf_status pf_solve_batch_ybus(pf_handle h, const double* ybus_data, int64_t ybus_stride, const double* sbus,
+                              int64_t sbus_stride, const double* V0, int64_t V0_stride, int32_t batch,
+                              const pf_nr_config* config, const pf_solve_options* solve_options, double* V_out,
+                              int32_t* iterations, double* final_mismatch, uint8_t* converged);
+/* ... device buffers (as pf_solve_batch_device): */
+pf_status pf_solve_batch_ybus_device(pf_handle h, const double* ybus_data, int64_t ybus_stride, const double* sbus,
+                                     int64_t sbus_stride, const double* V0, int64_t V0_stride, int32_t batch,
+                                     const pf_nr_config* config, const pf_solve_options* solve_options,
+                                     double* V_out, double* final_mismatch, void* stream, pf_adjoint_result* result);
 /* New (learned warm start, no reference counterpart): pf_solve_batch_device
  * started from a predicted state.  pred [batch][pred_ld] fp32 holds, in
  * Jacobian-row order, Va at the angle rows (PV then PQ buses) and Vm at the
