@@ -237,6 +237,96 @@ std::vector<int32_t> nd_order(const std::vector<int32_t>& xadj, const std::vecto
   return nodend(g, seed);
 }
 
+// Perfect structural matching row -> column by Hopcroft-Karp, in the search
+// order of StructuralMatchingFromCsc (analyze/pipeline.cpp:77-160): rows keep
+// their columns in ascending order; each phase runs a BFS from all unmatched
+// rows, then a depth-first augmentation from every unmatched row in row
+// order, trying its columns in order and restarting at the first column on
+// every call.  The depth-first search runs on an explicit stack (paths may be
+// as long as n).  Returns false when no perfect matching exists.
+bool structural_matching(int32_t n, const int32_t* row_ptr, const int32_t* col_idx, std::vector<int32_t>& row_to_col) {
+  // row -> columns ascending (the CSR may hold them in any order)
+  std::vector<int32_t> rp(n + 1, 0), adj;
+  {
+    std::vector<std::vector<int32_t>> rows(n);
+    for (int32_t r = 0; r < n; ++r)
+      for (int32_t k = row_ptr[r]; k < row_ptr[r + 1]; ++k)
+        if (col_idx[k] >= 0 && col_idx[k] < n) rows[r].push_back(col_idx[k]);
+    for (int32_t r = 0; r < n; ++r) {
+      std::sort(rows[r].begin(), rows[r].end());
+      rp[r + 1] = rp[r] + static_cast<int32_t>(rows[r].size());
+      adj.insert(adj.end(), rows[r].begin(), rows[r].end());
+    }
+  }
+  for (int32_t r = 0; r < n; ++r)
+    if (rp[r + 1] == rp[r]) return false;
+  row_to_col.assign(n, -1);
+  std::vector<int32_t> col_to_row(n, -1), dist(n, -1), q;
+  q.reserve(n);
+  auto bfs = [&]() {
+    q.clear();
+    bool found = false;
+    for (int32_t r = 0; r < n; ++r) {
+      if (row_to_col[r] < 0) {
+        dist[r] = 0;
+        q.push_back(r);
+      } else {
+        dist[r] = -1;
+      }
+    }
+    for (size_t h = 0; h < q.size(); ++h) {
+      const int32_t r = q[h];
+      for (int32_t p = rp[r]; p < rp[r + 1]; ++p) {
+        const int32_t rr = col_to_row[adj[p]];
+        if (rr < 0) {
+          found = true;
+        } else if (dist[rr] < 0) {
+          dist[rr] = dist[r] + 1;
+          q.push_back(rr);
+        }
+      }
+    }
+    return found;
+  };
+  struct Frame {
+    int32_t r, p;
+  };
+  std::vector<Frame> st;
+  auto augment = [&](int32_t r0) {
+    st.clear();
+    st.push_back({r0, rp[r0]});
+    while (!st.empty()) {
+      Frame& f = st.back();
+      if (f.p == rp[f.r + 1]) {  // every column tried: this row is a dead end
+        dist[f.r] = -1;
+        st.pop_back();
+        if (!st.empty()) ++st.back().p;
+        continue;
+      }
+      const int32_t c = adj[f.p];
+      const int32_t rr = col_to_row[c];
+      if (rr < 0) {  // free column: flip the path
+        for (size_t k = st.size(); k-- > 0;) {
+          const int32_t cc = adj[st[k].p];
+          row_to_col[st[k].r] = cc;
+          col_to_row[cc] = st[k].r;
+        }
+        return true;
+      }
+      if (dist[rr] == dist[f.r] + 1)
+        st.push_back({rr, rp[rr]});
+      else
+        ++f.p;
+    }
+    return false;
+  };
+  int32_t matched = 0;
+  while (bfs())
+    for (int32_t r = 0; r < n; ++r)
+      if (row_to_col[r] < 0 && augment(r)) ++matched;
+  return matched == n;
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -271,23 +361,62 @@ SymbolicPlan analyze_symbolic(int32_t n, const int32_t* row_ptr, const int32_t* 
     }
   }
 
-  // Ordering (pipeline.cpp:236-258, no structural matching).
-  sp.perm = nd_order(sp.graph_xadj, sp.graph_adjncy, n, opt.serial_nd, opt.metis_seed);
-  sp.iperm.assign(n, 0);
-  for (int32_t k = 0; k < n; ++k) sp.iperm[sp.perm[k]] = k;
+  // Optional structural matching, computed before the ordering as the
+  // reference does (pipeline.cpp:222-233).
+  if (opt.use_matching && !structural_matching(n, row_ptr, col_idx, sp.row_to_col))
+    throw std::runtime_error("analyze_symbolic: structural matching requested but no perfect matching exists");
 
-  // Relabelled graph: new column k holds old column perm[k], rows through
-  // iperm, in the old adjacency order (PermuteSymmetricPattern, pipeline.cpp:47-72).
-  sp.sym_col_ptr.assign(n + 1, 0);
-  for (int32_t k = 0; k < n; ++k) {
-    const int32_t o = sp.perm[k];
-    sp.sym_col_ptr[k + 1] = sp.sym_col_ptr[k] + (sp.graph_xadj[o + 1] - sp.graph_xadj[o]);
+  // Ordering (pipeline.cpp:236-258).  perm orders the rows; the columns
+  // follow the rows, or with a matching the matched column of each row:
+  // col_perm[k] = row_to_col[perm[k]], iperm = col_perm^-1.
+  sp.perm = nd_order(sp.graph_xadj, sp.graph_adjncy, n, opt.serial_nd, opt.metis_seed);
+  sp.row_iperm.assign(n, 0);
+  for (int32_t k = 0; k < n; ++k) sp.row_iperm[sp.perm[k]] = k;
+  if (opt.use_matching) {
+    sp.col_perm.assign(n, 0);
+    for (int32_t k = 0; k < n; ++k) sp.col_perm[k] = sp.row_to_col[sp.perm[k]];
+    sp.iperm.assign(n, 0);
+    for (int32_t k = 0; k < n; ++k) sp.iperm[sp.col_perm[k]] = k;
+  } else {
+    sp.col_perm = sp.perm;
+    sp.iperm = sp.row_iperm;
   }
-  sp.sym_row_idx.resize(sp.sym_col_ptr[n]);
-  for (int32_t k = 0; k < n; ++k) {
-    const int32_t o = sp.perm[k];
-    int32_t w = sp.sym_col_ptr[k];
-    for (int32_t p = sp.graph_xadj[o]; p < sp.graph_xadj[o + 1]; ++p) sp.sym_row_idx[w++] = sp.iperm[sp.graph_adjncy[p]];
+
+  if (opt.use_matching) {
+    // The permuted matrix is no longer structurally symmetric: its A + A^T
+    // graph is built afresh, neighbours ascending (pipeline.cpp:265-272 with
+    // BuildSymmetricGraphDevice on the ordered pattern).
+    std::vector<std::vector<int32_t>> adj(n);
+    for (int32_t r = 0; r < n; ++r)
+      for (int32_t k = row_ptr[r]; k < row_ptr[r + 1]; ++k) {
+        const int32_t i = sp.row_iperm[r], j = sp.iperm[col_idx[k]];
+        if (i == j) continue;
+        adj[i].push_back(j);
+        adj[j].push_back(i);
+      }
+    sp.sym_col_ptr.assign(n + 1, 0);
+    for (int32_t v = 0; v < n; ++v) {
+      auto& a = adj[v];
+      std::sort(a.begin(), a.end());
+      a.erase(std::unique(a.begin(), a.end()), a.end());
+      sp.sym_col_ptr[v + 1] = sp.sym_col_ptr[v] + static_cast<int32_t>(a.size());
+      sp.sym_row_idx.insert(sp.sym_row_idx.end(), a.begin(), a.end());
+    }
+  } else {
+    // Relabelled graph: new column k holds old column perm[k], rows through
+    // iperm, in the old adjacency order (PermuteSymmetricPattern, pipeline.cpp:47-72).
+    sp.sym_col_ptr.assign(n + 1, 0);
+    for (int32_t k = 0; k < n; ++k) {
+      const int32_t o = sp.perm[k];
+      sp.sym_col_ptr[k + 1] = sp.sym_col_ptr[k] + (sp.graph_xadj[o + 1] - sp.graph_xadj[o]);
+    }
+    sp.sym_row_idx.resize(sp.sym_col_ptr[n]);
+    for (int32_t k = 0; k < n; ++k) {
+      const int32_t o = sp.perm[k];
+      int32_t w = sp.sym_col_ptr[k];
+      for (int32_t p = sp.graph_xadj[o]; p < sp.graph_xadj[o + 1]; ++p)
+        sp.sym_row_idx[w++] = sp.iperm[sp.graph_adjncy[p]];
+    }
   }
 
   // Elimination tree with path compression (symbolic/elimination_tree.cpp:67-88).
@@ -450,7 +579,7 @@ SymbolicPlan analyze_symbolic(int32_t n, const int32_t* row_ptr, const int32_t* 
   sp.front_off[P] = static_cast<int32_t>(total);
   sp.front_total = total;
 
-  // Entry positions: entry (i, j) of P A P^T belongs to the panel of min(i, j);
+  // Entry positions: entry (i, j) of P_r A P_c^T belongs to the panel of min(i, j);
   // inside the front its row and column are the local indices of i and j
   // (BuildAPosDevice, lower.cu:35-62), reported per CSR entry.
   sp.a_pos_csr.assign(sp.nnz, -1);
@@ -459,7 +588,7 @@ SymbolicPlan analyze_symbolic(int32_t n, const int32_t* row_ptr, const int32_t* 
   sp.a_col.assign(sp.nnz, -1);
   for (int32_t r = 0; r < n; ++r)
     for (int32_t k = row_ptr[r]; k < row_ptr[r + 1]; ++k) {
-      const int32_t i = sp.iperm[r], j = sp.iperm[col_idx[k]];
+      const int32_t i = sp.row_iperm[r], j = sp.iperm[col_idx[k]];
       const int32_t mn = std::min(i, j), mx = std::max(i, j);
       const int32_t owner = sp.panel_of[mn];
       const int32_t first = sp.panel_first[owner], nc = sp.panel_ncols[owner];
@@ -498,6 +627,8 @@ FactorProgram build_factor_program(const SymbolicPlan& sp) {
   fp.asm_ptr = sp.asm_ptr;
   fp.perm = sp.perm;
   fp.iperm = sp.iperm;
+  fp.row_iperm = sp.row_iperm;
+  fp.col_perm = sp.col_perm;
   fp.parent_panel = sp.panel_parent;
   fp.fsz.resize(P);
   fp.nc.resize(P);

@@ -44,13 +44,16 @@ struct SymbolicOptions {
   int max_panel_width = 8;   // relaxed-panel cap (clamped to [1, 64])
   bool serial_nd = true;     // one METIS_NodeND call; false = separator recursion
   int metis_seed = 42;
+  bool use_matching = false;  // structural (Hopcroft-Karp) column matching
 };
 
 struct SymbolicPlan {
   int32_t n = 0, nnz = 0;
   // ordering
   std::vector<int32_t> graph_xadj, graph_adjncy;  // A + A^T without the diagonal
-  std::vector<int32_t> perm, iperm;               // perm[new] = old
+  std::vector<int32_t> perm, iperm;               // perm[new] = old row; iperm[old col] = new col
+  std::vector<int32_t> row_iperm, col_perm;       // iperm[old row] = new row; col_perm[new] = old col
+  std::vector<int32_t> row_to_col;                // structural matching (empty without)
   std::vector<int32_t> sym_col_ptr, sym_row_idx;  // relabelled graph
   // elimination tree + fill
   std::vector<int32_t> parent;
@@ -92,7 +95,8 @@ struct FactorProgram {
   std::vector<int32_t> asm_ptr;
   std::vector<int32_t> level_ptr, level_fronts;   // fronts by level, bucket-sorted inside a level
   std::vector<int32_t> level_max_fsz;
-  std::vector<int32_t> perm, iperm;
+  std::vector<int32_t> perm, iperm;          // row order; column inverse
+  std::vector<int32_t> row_iperm, col_perm;  // row inverse; column order
   std::vector<int32_t> parent_panel;
   std::vector<int32_t> nchildren;
   // Dense-front assembly program: for front p, entries [fe_ptr[p], fe_ptr[p+1])

@@ -45,6 +45,7 @@ EngineConfig engine_config(const cls_config& c, int32_t compute, int32_t use_gra
   e.factor_precision = c.precision;
   e.max_panel_width = c.max_panel_width;
   e.serial_nd = c.serial_nd;
+  e.use_matching = c.matching;
   e.static_pivot = c.pivot_strategy == CLS_PIVOT_STATIC_DIAGONAL_SHIFT ? 1 : 0;
   e.shift_epsilon = c.shift_retry_epsilon;
   e.use_cuda_graph = use_graph;
@@ -60,6 +61,9 @@ bool copy_plan_array(const Engine& e, const char* name, int32_t* out, int64_t ca
   if (n == key) v = &(vec);
   CUPF_ARR("perm", sp.perm)
   CUPF_ARR("iperm", sp.iperm)
+  CUPF_ARR("row_iperm", sp.row_iperm)
+  CUPF_ARR("col_perm", sp.col_perm)
+  CUPF_ARR("row_to_col", sp.row_to_col)
   CUPF_ARR("parent", sp.parent)
   CUPF_ARR("Lp", sp.Lp)
   CUPF_ARR("Li", sp.Li)
@@ -149,7 +153,8 @@ cls_status cls_create(const cls_config* config, cls_handle* out) {
   *out = nullptr;
   cls_config c{CLS_PRECISION_FP64, 0, CLS_PIVOT_STATIC_DIAGONAL_SHIFT, 1, 8, 1e-8};
   if (config) c = *config;
-  if (c.matching != 0 || c.max_panel_width < 1 || c.max_panel_width > 8) return CLS_INVALID_VALUE;
+  if ((c.matching != 0 && c.matching != 1) || c.max_panel_width < 1 || c.max_panel_width > 8)
+    return CLS_INVALID_VALUE;
   auto* h = new (std::nothrow) cls_solver_s();
   if (!h) return CLS_ALLOCATION_FAILED;
   h->cfg = c;
@@ -337,7 +342,8 @@ pf_status pf_create(const pf_options* options, pf_handle* out) {
       throw std::invalid_argument("NewtonSolver: this engine provides the custom CUDA linear solver only");
     if (o.compute != PF_COMPUTE_FP64 && o.compute != PF_COMPUTE_FP32 && o.compute != PF_COMPUTE_MIXED)
       throw std::invalid_argument("NewtonSolver: unsupported compute policy");
-    if (o.custom.matching != 0) throw std::invalid_argument("NewtonSolver: structural matching is not supported");
+    if (o.custom.matching != 0 && o.custom.matching != 1)
+      throw std::invalid_argument("NewtonSolver: matching must be None or Structural");
     cls_config c = o.custom;
     if (o.compute == PF_COMPUTE_FP64) c.precision = CLS_PRECISION_FP64;
     h->eng.reset(new Engine(engine_config(c, o.compute, o.use_cuda_graph)));

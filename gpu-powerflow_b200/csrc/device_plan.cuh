@@ -36,7 +36,9 @@ struct DevPlan {
   const int* asm_ptr = nullptr;
   const int* asm_local = nullptr;
   const int* perm = nullptr;   // permuted index -> Jacobian row
-  const int* iperm = nullptr;  // Jacobian row -> permuted index
+  const int* iperm = nullptr;  // Jacobian column -> permuted index
+  const int* row_iperm = nullptr;  // Jacobian row -> permuted index (= iperm without matching)
+  const int* col_perm = nullptr;   // permuted index -> Jacobian column (= perm without matching)
   const int* level_fronts = nullptr;
   // dense-front assembly program (analysis.hpp FactorProgram::fe_*)
   const long long* fe_split = nullptr;  // 9 per front

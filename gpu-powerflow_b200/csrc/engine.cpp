@@ -95,7 +95,7 @@ struct Engine::Impl {
       jt_ptr, jt_row, jt_q;
   // factor program
   DBuf fsz, nc, first, front_ptr, front_rows, u_off, l_off, cb_off, tv_off, arow_ptr, arow_q, arow_col, crow_ptr,
-      crow_child, crow_r, asm_ptr, asm_local, perm, iperm, level_fronts, fe_split, fe_dst, fe_src, front_meta;
+      crow_child, crow_r, asm_ptr, asm_local, perm, iperm, row_iperm, col_perm, level_fronts, fe_split, fe_dst, fe_src, front_meta;
   std::vector<LevelLaunch> levels;
   int64_t tv_total = 0;
   DevGrid g;
@@ -206,8 +206,9 @@ void Engine::initialize(int32_t n_bus, const int32_t* indptr, const int32_t* ind
   {
     std::vector<int32_t> fa_p(n_bus, -1), fm_p(n_bus, -1);
     for (int32_t i = 0; i < n_bus; ++i) {
-      if (ja_.row_pvpq[i] >= 0) fa_p[i] = fp_.iperm[ja_.row_pvpq[i]];
-      if (ja_.row_pq[i] >= 0) fm_p[i] = fp_.iperm[ja_.row_pq[i]];
+      // equation rows go where the row ordering puts them
+      if (ja_.row_pvpq[i] >= 0) fa_p[i] = fp_.row_iperm[ja_.row_pvpq[i]];
+      if (ja_.row_pq[i] >= 0) fm_p[i] = fp_.row_iperm[ja_.row_pq[i]];
     }
     d.bus_fa_p.upload(fa_p);
     d.bus_fm_p.upload(fm_p);
@@ -306,6 +307,8 @@ void Engine::upload_plan() {
   d.asm_local.upload(fp_.asm_local);
   d.perm.upload(fp_.perm);
   d.iperm.upload(fp_.iperm);
+  d.row_iperm.upload(fp_.row_iperm);
+  d.col_perm.upload(fp_.col_perm);
   d.level_fronts.upload(fp_.level_fronts);
   d.fe_split.upload(to_ll(fp_.fe_split));
   d.fe_dst.upload(fp_.fe_dst);
@@ -367,6 +370,8 @@ void Engine::upload_plan() {
   pl.asm_local = d.asm_local.as<int>();
   pl.perm = d.perm.as<int>();
   pl.iperm = d.iperm.as<int>();
+  pl.row_iperm = d.row_iperm.as<int>();
+  pl.col_perm = d.col_perm.as<int>();
   pl.level_fronts = d.level_fronts.as<int>();
   pl.fe_split = d.fe_split.as<long long>();
   pl.fe_dst = d.fe_dst.as<int>();
@@ -389,6 +394,7 @@ void Engine::analyze_host(int32_t n_bus, const int32_t* indptr, const int32_t* i
   SymbolicOptions so;
   so.max_panel_width = cfg_.max_panel_width;
   so.serial_nd = cfg_.serial_nd != 0;
+  so.use_matching = cfg_.use_matching != 0;
   sp_ = analyze_symbolic(ja_.dim, ja_.row_ptr.data(), ja_.col_idx.data(), so);
   fp_ = build_factor_program(sp_);
   if (fp_.max_fsz > 64) throw std::runtime_error("initialize: a front exceeds 64 rows (unsupported)");
@@ -407,6 +413,7 @@ void Engine::analyze_matrix_host(int32_t n, int32_t nnz, const int32_t* row_ptr,
   SymbolicOptions so;
   so.max_panel_width = cfg_.max_panel_width;
   so.serial_nd = cfg_.serial_nd != 0;
+  so.use_matching = cfg_.use_matching != 0;
   sp_ = analyze_symbolic(n, row_ptr, col_idx, so);
   fp_ = build_factor_program(sp_);
 }
@@ -422,6 +429,7 @@ void Engine::initialize_matrix(int32_t n, int32_t nnz, const int32_t* row_ptr, c
   SymbolicOptions so;
   so.max_panel_width = cfg_.max_panel_width;
   so.serial_nd = cfg_.serial_nd != 0;
+  so.use_matching = cfg_.use_matching != 0;
   sp_ = analyze_symbolic(n, row_ptr, col_idx, so);
   fp_ = build_factor_program(sp_);
   if (fp_.max_fsz > 64) throw std::runtime_error("Analyze: a front exceeds 64 rows (unsupported)");
@@ -828,7 +836,8 @@ void Engine::transpose_solve(const double* d_G, double* d_lam, cudaStream_t s) {
   a.Z = d.Z.as<T>();
   for (const auto& lv : d.levels) launch_ut_forward_level<T>(lv, a, s);
   for (int L = (int)d.levels.size() - 1; L >= 0; --L) launch_lt_backward_level<T>(d.levels[L], a, s);
-  launch_permuted_to_rows<T>(d.pl, ja_.dim, d.Bp, d.Z.as<T>(), d_lam, s);
+  // lambda is indexed by equation rows: undo the row ordering
+  launch_permuted_to_rows<T>(d.pl.row_iperm, ja_.dim, d.Bp, d.Z.as<T>(), d_lam, s);
 }
 
 double Engine::solve_adjoint_device(const void* grad_va, const void* grad_vm, void* grad_p, void* grad_q,
@@ -1027,7 +1036,8 @@ void Engine::solve_values(const void* d_rhs, int32_t rhs_is_double, void* d_x, i
     bk.Y = d.W.as<T>();
     bk.X = d.X.as<T>();
     for (int L = (int)d.levels.size() - 1; L >= 0; --L) launch_backward_level<T>(d.levels[L], bk, s);
-    launch_permuted_to_rows<T>(d.pl, (int)dim, (int)Bp, d.X.as<T>(), d.lam.as<double>(), s);
+    // x is indexed by columns: undo the column ordering
+    launch_permuted_to_rows<T>(d.pl.iperm, (int)dim, (int)Bp, d.X.as<T>(), d.lam.as<double>(), s);
   };
   if (dbl) run(double{});
   else run(float{});

@@ -137,7 +137,7 @@ void launch_copy_voltage_outputs(const DevGrid& g, const DevState& st, void* va_
 void launch_gather_adjoint_rhs(const DevGrid& g, const DevState& st, const void* grad_va, const void* grad_vm,
                                int is_double, double* G, cudaStream_t s);
 template <typename T>
-void launch_permuted_to_rows(const DevPlan& pl, int dim, int Bp, const T* Z, double* lam, cudaStream_t s);
+void launch_permuted_to_rows(const int* inv, int dim, int Bp, const T* Z, double* lam, cudaStream_t s);
 void launch_project_load_gradients(const DevGrid& g, const DevState& st, const double* lam, void* grad_p,
                                    void* grad_q, int is_double, cudaStream_t s);
 // r = g - J^T lambda, J given by its CSR values [nnz_j][Bp] (fp64)

@@ -491,7 +491,8 @@ __global__ void __launch_bounds__(128)
   for (int k = 0; k < NCMAX; ++k) {
     w[k] = T(0);
     if (k < nc) {
-      T s = static_cast<T>(G[(size_t)pl.perm[first + k] * Bp + b]) - t[k];
+      // J^T's right-hand side is indexed by Jacobian columns
+      T s = static_cast<T>(G[(size_t)pl.col_perm[first + k] * Bp + b]) - t[k];
 #pragma unroll
       for (int m = 0; m < k; ++m) s -= U[(size_t)(uo + (long long)m * fs + k) * Bp + b] * w[m];
       w[k] = s / U[(size_t)(uo + (long long)k * fs + k) * Bp + b];

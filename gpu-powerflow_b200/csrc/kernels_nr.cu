@@ -336,12 +336,15 @@ __global__ void k_gather_adjoint_rhs(DevGrid g, DevState st, const void* grad_va
   }
 }
 
+// lam[f] = Z[inv[f]]: a solution in pivot order back to Jacobian order
+// (inv = the column inverse for J x = b, the row inverse for J^T x = b)
 template <typename T>
-__global__ void k_permuted_to_rows(DevPlan pl, int dim, int Bp, const T* __restrict__ Z, double* __restrict__ lam) {
+__global__ void k_permuted_to_rows(const int* __restrict__ inv, int dim, int Bp, const T* __restrict__ Z,
+                                   double* __restrict__ lam) {
   const int lane = threadIdx.x, wy = threadIdx.y;
   const size_t b = (size_t)blockIdx.y * kWarp + lane;
   for (int f = blockIdx.x * kRows + wy; f < dim; f += gridDim.x * kRows)
-    lam[(size_t)f * Bp + b] = static_cast<double>(Z[(size_t)pl.iperm[f] * Bp + b]);
+    lam[(size_t)f * Bp + b] = static_cast<double>(Z[(size_t)inv[f] * Bp + b]);
 }
 
 // grad_load = -lambda at the bus's rows (adjoint_math.cpp:189-216)
@@ -561,11 +564,11 @@ void launch_gather_adjoint_rhs(const DevGrid& g, const DevState& st, const void*
 }
 
 template <typename T>
-void launch_permuted_to_rows(const DevPlan& pl, int dim, int Bp, const T* Z, double* lam, cudaStream_t s) {
-  k_permuted_to_rows<T><<<rows_grid(dim, Bp), dim3(kWarp, kRows), 0, s>>>(pl, dim, Bp, Z, lam);
+void launch_permuted_to_rows(const int* inv, int dim, int Bp, const T* Z, double* lam, cudaStream_t s) {
+  k_permuted_to_rows<T><<<rows_grid(dim, Bp), dim3(kWarp, kRows), 0, s>>>(inv, dim, Bp, Z, lam);
 }
-template void launch_permuted_to_rows<float>(const DevPlan&, int, int, const float*, double*, cudaStream_t);
-template void launch_permuted_to_rows<double>(const DevPlan&, int, int, const double*, double*, cudaStream_t);
+template void launch_permuted_to_rows<float>(const int*, int, int, const float*, double*, cudaStream_t);
+template void launch_permuted_to_rows<double>(const int*, int, int, const double*, double*, cudaStream_t);
 
 void launch_project_load_gradients(const DevGrid& g, const DevState& st, const double* lam, void* grad_p,
                                    void* grad_q, int is_double, cudaStream_t s) {

@@ -61,10 +61,14 @@ enum { CLS_LOCATION_HOST = 0, CLS_LOCATION_DEVICE = 1 };
 enum { CLS_PIVOT_NONE = 0, CLS_PIVOT_STATIC_DIAGONAL_SHIFT = 1 };
 
 /* SolverConfig / CustomSolverConfig (solver.hpp:35-65,
- * cuPF newton_solver_types.hpp:152-159).  matching must be 0 (None). */
+ * cuPF newton_solver_types.hpp:152-159).  matching 1 (Structural) computes a
+ * Hopcroft-Karp row -> column matching before the ordering and factors
+ * P_r A P_c^T with the columns following their matched rows
+ * (analyze/pipeline.cpp:77-160, 222-272); plan arrays "row_iperm",
+ * "col_perm" and "row_to_col" expose it. */
 typedef struct {
   int32_t precision;            /* CLS_PRECISION_*; TF32 runs the FP32 kernels */
-  int32_t matching;             /* 0 = None */
+  int32_t matching;             /* 0 = None, 1 = Structural */
   int32_t pivot_strategy;       /* CLS_PIVOT_* */
   int32_t serial_nd;            /* 1 = one METIS_NodeND call, 0 = separator recursion */
   int32_t max_panel_width;      /* 1..8 (front kernels are built for panels of at most 8 pivots) */

@@ -170,6 +170,8 @@ class Reference:
                                         C.c_int, C.c_double, C.c_int, C.c_int, _f64p, _i32p, _f64p]
         L.ref_symbolic_run.restype = C.c_void_p
         L.ref_symbolic_run.argtypes = [C.c_int, _i32p, _i32p, C.c_int, C.c_int, C.c_int]
+        L.ref_symbolic_run_m.restype = C.c_void_p
+        L.ref_symbolic_run_m.argtypes = [C.c_int, _i32p, _i32p, C.c_int, C.c_int, C.c_int, C.c_int]
         L.ref_symbolic_len.restype = C.c_int
         L.ref_symbolic_len.argtypes = [C.c_void_p, C.c_char_p]
         L.ref_symbolic_copy.restype = C.c_int
@@ -239,10 +241,11 @@ class Reference:
         return out
 
     def symbolic(self, row_ptr, col_idx, max_panel_width: int = 8, parallel_nd: bool = False,
-                 float_front: bool = True) -> dict:
+                 float_front: bool = True, use_matching: bool = False) -> dict:
         rp, ci = _i32(row_ptr), _i32(col_idx)
         n = rp.size - 1
-        h = self.lib.ref_symbolic_run(n, rp, ci, max_panel_width, int(parallel_nd), int(float_front))
+        h = self.lib.ref_symbolic_run_m(n, rp, ci, max_panel_width, int(parallel_nd), int(float_front),
+                                        int(use_matching))
         if not h:
             raise RuntimeError("reference symbolic analysis failed")
         try:

@@ -14,6 +14,12 @@
 //   * A + A^T adjacency = sorted unique directed edge keys, diagonal dropped;
 //   * column relabel new_col = iperm[old_col], rows through iperm;
 //   * a_pos[q] = front_off + r * fsz + c, reported in CSR order.
+// With structural matching (use_matching), the reference's own
+// StructuralMatchingFromCsc (pipeline.cpp:77-160) runs on that CSC, the rows
+// follow the ND order and the columns their matched rows, the permuted CSC
+// maps rows through row_iperm and columns through iperm (PermuteCscDeviceRc,
+// pattern_kernels.cu:405-460), and the Etree / fill graph is A' + A'^T of the
+// permuted matrix (pipeline.cpp:265-272).
 // Everything else -- METIS ND, Etree, FillPattern, RelaxedPanels,
 // ComputeMultifrontalSymbolic, panel levels, subtree/tier orders, assembly
 // map, arena layout -- is the reference's code.
@@ -39,8 +45,8 @@ struct RefSymbolic {
 
 extern "C" {
 
-void* ref_symbolic_run(int n, const int* csr_row_ptr, const int* csr_col_idx, int max_panel_width,
-                       int parallel_nd, int float_front) {
+void* ref_symbolic_run_m(int n, const int* csr_row_ptr, const int* csr_col_idx, int max_panel_width,
+                         int parallel_nd, int float_front, int use_matching) {
   using namespace custom_linear_solver;
   using namespace custom_linear_solver::plan;
   namespace sym = custom_linear_solver::symbolic;
@@ -82,6 +88,15 @@ void* ref_symbolic_run(int n, const int* csr_row_ptr, const int* csr_col_idx, in
   A["graph_xadj"] = xadj;
   A["graph_adjncy"] = adjncy;
 
+  std::vector<int> row_to_col;
+  if (use_matching) {
+    if (!StructuralMatchingFromCsc(n, cp, ci, row_to_col)) {
+      delete out;
+      return nullptr;
+    }
+    A["row_to_col"] = row_to_col;
+  }
+
   // 3. METIS nested dissection (reference code, seed 42)
   std::vector<int> perm(n, 0);
   {
@@ -91,26 +106,57 @@ void* ref_symbolic_run(int n, const int* csr_row_ptr, const int* csr_col_idx, in
       return nullptr;
     }
   }
-  std::vector<int> iperm(n);
-  for (int k = 0; k < n; ++k) iperm[perm[k]] = k;
+  std::vector<int> iperm(n), row_iperm(n);
+  if (use_matching) {
+    std::vector<int> col_perm(n);
+    for (int k = 0; k < n; ++k) col_perm[k] = row_to_col[perm[k]];
+    for (int k = 0; k < n; ++k) iperm[col_perm[k]] = k;
+    A["col_perm"] = col_perm;
+  } else {
+    for (int k = 0; k < n; ++k) iperm[perm[k]] = k;
+  }
+  for (int k = 0; k < n; ++k) row_iperm[perm[k]] = k;
   A["perm"] = perm;
   A["iperm"] = iperm;
+  A["row_iperm"] = row_iperm;
 
-  // 4. permuted CSC (new column iperm[old], rows through iperm, order kept)
+  // 4. permuted CSC (new column iperm[old], rows through row_iperm, order kept)
   std::vector<int> ocp(n + 1, 0), oci(nnz), osrc(nnz);
   for (int c = 0; c < n; ++c) ocp[iperm[c] + 1] = cp[c + 1] - cp[c];
   for (int c = 0; c < n; ++c) ocp[c + 1] += ocp[c];
   for (int c = 0; c < n; ++c) {
     const int nc = iperm[c];
     for (int off = 0; off < cp[c + 1] - cp[c]; ++off) {
-      oci[ocp[nc] + off] = iperm[ci[cp[c] + off]];
+      oci[ocp[nc] + off] = row_iperm[ci[cp[c] + off]];
       osrc[ocp[nc] + off] = src[cp[c] + off];
     }
   }
 
-  // 5. relabelled symmetric pattern (reference static helper)
+  // 5. symmetric pattern for Etree / fill: relabelled (reference static
+  // helper), or with matching A' + A'^T of the permuted CSC, sorted unique
   std::vector<int> scp, sri;
-  PermuteSymmetricPattern(n, xadj, adjncy, perm, iperm, scp, sri);
+  if (use_matching) {
+    std::vector<unsigned long long> ok;
+    ok.reserve(2 * (size_t)nnz);
+    for (int c = 0; c < n; ++c)
+      for (int q = ocp[c]; q < ocp[c + 1]; ++q) {
+        const int r = oci[q];
+        if (r == c) continue;
+        ok.push_back((unsigned long long)r * n + c);
+        ok.push_back((unsigned long long)c * n + r);
+      }
+    std::sort(ok.begin(), ok.end());
+    ok.erase(std::unique(ok.begin(), ok.end()), ok.end());
+    scp.assign(n + 1, 0);
+    sri.resize(ok.size());
+    for (size_t i = 0; i < ok.size(); ++i) {
+      scp[(int)(ok[i] / n) + 1]++;
+      sri[i] = (int)(ok[i] % n);
+    }
+    for (int v = 0; v < n; ++v) scp[v + 1] += scp[v];
+  } else {
+    PermuteSymmetricPattern(n, xadj, adjncy, perm, iperm, scp, sri);
+  }
   A["sym_col_ptr"] = scp;
   A["sym_row_idx"] = sri;
 
@@ -206,6 +252,11 @@ void* ref_symbolic_run(int n, const int* csr_row_ptr, const int* csr_col_idx, in
     }
   A["a_pos_csr"] = a_pos_csr;
   return out;
+}
+
+void* ref_symbolic_run(int n, const int* csr_row_ptr, const int* csr_col_idx, int max_panel_width,
+                       int parallel_nd, int float_front) {
+  return ref_symbolic_run_m(n, csr_row_ptr, csr_col_idx, max_panel_width, parallel_nd, float_front, 0);
 }
 
 int ref_symbolic_len(void* h, const char* name) {

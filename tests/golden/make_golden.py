@@ -48,7 +48,22 @@ SYMBOLIC_KEYS = ("perm", "iperm", "parent", "Lp", "Li_sorted", "panel_first", "p
                  "panel_of", "front_ptr", "front_rows", "panel_parent", "asm_ptr", "asm_idx", "asm_local",
                  "plevel", "panel_level_ptr", "plcols_level", "front_off", "a_pos_csr", "graph_xadj",
                  "graph_adjncy", "sym_col_ptr", "sym_row_idx")
+# with structural matching the plan also carries the matching and both inverses
+MATCHING_KEYS = SYMBOLIC_KEYS + ("row_iperm", "col_perm", "row_to_col")
 JAC_KEYS = ("row_ptr", "col_idx", "map11", "map21", "map12", "map22", "diag11", "diag21", "diag12", "diag22")
+
+
+ROWPERM_SEED = 118
+
+
+def row_permuted_pattern(row_ptr, col_idx, seed: int):
+    """CSR pattern with its rows in a seeded random order (columns kept)."""
+    n = row_ptr.size - 1
+    order = np.random.default_rng(seed).permutation(n)
+    lens = np.diff(row_ptr)[order]
+    rp = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    ci = np.concatenate([col_idx[row_ptr[r]:row_ptr[r + 1]] for r in order]).astype(np.int32)
+    return rp, ci
 
 
 def digest(a) -> str:
@@ -98,6 +113,8 @@ def main() -> None:
                                  "symbolic": {k: digest(sym[k]) for k in SYMBOLIC_KEYS},
                                  "front_total": int(sym["front_total"][0]), "dim": int(ja["row_ptr"].size - 1),
                                  "nnz": int(ja["col_idx"].size)}
+        symm = ref.symbolic(ja["row_ptr"], ja["col_idx"], parallel_nd=False, use_matching=True)
+        hashes[f"grid{name}"]["symbolic_matching"] = {k: digest(symm[k]) for k in MATCHING_KEYS}
         if name == "118":
             np.savez_compressed(HERE / "jacobian_118.npz", **{k: ja[k] for k in JAC_KEYS})
             np.savez_compressed(HERE / "symbolic_118.npz", **{k: sym[k] for k in SYMBOLIC_KEYS})
@@ -129,6 +146,16 @@ def main() -> None:
         sym = ref.symbolic(rp, ci, parallel_nd=False)
         hashes[case] = {"symbolic": {k: digest(sym[k]) for k in SYMBOLIC_KEYS},
                         "front_total": int(sym["front_total"][0]), "dim": int(rp.size - 1), "nnz": int(ci.size)}
+        symm = ref.symbolic(rp, ci, parallel_nd=False, use_matching=True)
+        hashes[case]["symbolic_matching"] = {k: digest(symm[k]) for k in MATCHING_KEYS}
+
+    # a pattern whose diagonal is structurally incomplete: case118's J with
+    # its rows shuffled (seeded); structural matching has to find columns
+    d = np.load(HERE / "linsys_case118.npz")
+    rp, ci = row_permuted_pattern(d["row_ptr"], d["col_idx"], ROWPERM_SEED)
+    symm = ref.symbolic(rp, ci, parallel_nd=False, use_matching=True)
+    hashes["case118_rowperm"] = {"symbolic_matching": {k: digest(symm[k]) for k in MATCHING_KEYS},
+                                 "seed": ROWPERM_SEED}
 
     (HERE / "hashes.json").write_text(json.dumps(hashes, indent=1, sort_keys=True) + "\n")
     print("golden fixtures written to", HERE)

@@ -166,3 +166,65 @@ def test_front_launch_records(analyzed):
     assert np.array_equal(wide[:, 3], cb_off[lf])
     assert np.array_equal(meta[:, 12:20], (split[lf, 1:] - split[lf, :1]).astype(np.int32))
     assert np.array_equal(meta[:, 20], front_ptr[lf])
+
+
+MATCHING = dict(SYMBOLIC, row_iperm="row_iperm", col_perm="col_perm", row_to_col="row_to_col")
+
+
+def _row_permuted(row_ptr, col_idx, seed):
+    """The rows of a CSR pattern in a seeded random order (tests/golden/make_golden.py)."""
+    n = row_ptr.size - 1
+    order = np.random.default_rng(seed).permutation(n)
+    lens = np.diff(row_ptr)[order]
+    rp = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    ci = np.concatenate([col_idx[row_ptr[r]:row_ptr[r + 1]] for r in order]).astype(np.int32)
+    return rp, ci
+
+
+@pytest.mark.parametrize("name", ["118", "2000", "10000"])
+def test_symbolic_plan_with_matching_bit_exact(name):
+    """Structural matching (CustomMatchingMode::Structural): the Hopcroft-Karp
+    matching, both permutations and every plan array equal the reference's
+    (analyze/pipeline.cpp:77-160, 222-272)."""
+    g = GRIDS[name]()
+    o = cupf.NewtonOptions()
+    o.backend = cupf.BackendKind.CUDA
+    o.custom.serial_nd = True
+    o.custom.matching = cupf.CustomMatchingMode.Structural
+    s = cupf.NewtonSolver(o)
+    s.analyze_host(g.indptr, g.indices, g.n_bus, g.pv, g.pq)
+    gold = HASHES[f"grid{name}"]["symbolic_matching"]
+    bad = [ours for ours, ref in MATCHING.items() if digest(s.plan_array(ours)) != gold[ref]]
+    assert not bad, f"arrays differing from the reference: {bad}"
+
+
+@pytest.mark.parametrize("case", ["case118", "case1354pegase", "case118_rowperm"])
+def test_linear_solver_matching_bit_exact(case):
+    """Matching on the reference datasets, and on case118's J with its rows
+    shuffled, where the diagonal is structurally incomplete and the matching
+    is not the identity."""
+    d = np.load(GOLD / f"linsys_{case.split('_')[0]}.npz")
+    rp, ci = d["row_ptr"], d["col_idx"]
+    if case.endswith("rowperm"):
+        rp, ci = _row_permuted(rp, ci, HASHES[case]["seed"])
+    ls = cupf.LinearSolver(cupf.SolverConfig(serial_nd=True, matching=1))
+    ls.set_data(rp, ci)
+    ls.analyze_host()
+    gold = HASHES[case]["symbolic_matching"]
+    bad = [ours for ours, ref in MATCHING.items() if digest(ls.plan_array(ours)) != gold[ref]]
+    assert not bad, f"arrays differing from the reference: {bad}"
+    if case.endswith("rowperm"):
+        r2c = ls.plan_array("row_to_col")
+        assert np.array_equal(np.sort(r2c), np.arange(rp.size - 1))
+        assert (r2c != np.arange(rp.size - 1)).any()
+
+
+def test_matching_fails_without_a_perfect_matching():
+    """Two rows whose only column is the same: no perfect matching exists; the
+    analysis fails (the reference's Analyze returns false there)."""
+    rp = np.array([0, 1, 2, 4], np.int32)
+    ci = np.array([0, 0, 1, 2], np.int32)
+    ls = cupf.LinearSolver(cupf.SolverConfig(serial_nd=True, matching=1))
+    ls.set_data(rp, ci)
+    with pytest.raises(Exception):
+        ls.analyze_host()

@@ -128,3 +128,84 @@ def test_state_errors():
         ls.solve(torch.zeros((2, 181), dtype=torch.float64, device="cuda"))  # before factorize
     with pytest.raises(ValueError):
         ls.factorize(torch.zeros((2, d["col_idx"].size), dtype=torch.int32, device="cuda"))
+
+
+def _row_permuted(d, seed):
+    """case118's J with its rows in a seeded random order: the diagonal is
+    structurally incomplete, so only a matching makes the pivots nonzero."""
+    rp0, ci0, v0 = d["row_ptr"], d["col_idx"], d["values"]
+    n = rp0.size - 1
+    order = np.random.default_rng(seed).permutation(n)
+    rp = np.concatenate([[0], np.cumsum(np.diff(rp0)[order])]).astype(np.int32)
+    ci = np.concatenate([ci0[rp0[r]:rp0[r + 1]] for r in order]).astype(np.int32)
+    v = np.concatenate([v0[rp0[r]:rp0[r + 1]] for r in order])
+    return rp, ci, v, order
+
+
+@pytest.mark.parametrize("precision,tol,tol_t", [(cupf.CustomPrecision.FP64, 1e-8, 1e-8)])
+def test_structural_matching_solves_a_row_permuted_system(precision, tol, tol_t):
+    """MatchingMode::Structural (analyze/pipeline.cpp:77-160, 222-272) on a
+    row-shuffled Jacobian (structurally zero diagonal entries; ordered
+    without a matching, its A + A^T graph fills in past the 64-row front
+    limit): factor, solve and transpose solve are accurate.  The matched
+    diagonal is not the Jacobian's own, so the unpivoted LU grows elements
+    (185x to 1,049x over these nine systems; the exact FP64 LU in this order
+    leaves relative residuals up to 1e-9 (solve) and 3e-9 (transpose)),
+    hence the looser bars than on the natural row order.  FP32 factors are
+    not tested on this system: an exact FP32 LU in the matched order already
+    leaves a 1 % residual (growth times FP32 roundoff), whatever the kernel;
+    the FP32 kernels share the permutation code checked here."""
+    import torch
+
+    d = np.load(GOLD / "linsys_case118.npz")
+    rp, ci, v, order = _row_permuted(d, 118)
+    n = rp.size - 1
+    A = sp.csr_matrix((v, ci, rp), shape=(n, n))
+    rng = np.random.default_rng(5)
+    B = 9
+    vals = np.repeat(v[None, :], B, axis=0) * (1.0 + 0.02 * rng.uniform(-1, 1, size=(B, v.size)))
+    rhs = rng.standard_normal((B, n))
+    dt = torch.float64 if precision == cupf.CustomPrecision.FP64 else torch.float32
+    ls = cupf.LinearSolver(cupf.SolverConfig(precision=int(precision), serial_nd=True, matching=1))
+    ls.set_data(rp, ci)
+    ls.analyze()
+    ls.setup(B)
+    ls.factorize(torch.tensor(vals, dtype=dt, device="cuda"))
+    assert not ls.singular_flags().any()
+    x = ls.solve(torch.tensor(rhs, device="cuda")).cpu().numpy()
+    xt = ls.solve_transpose(torch.tensor(rhs, device="cuda")).cpu().numpy()
+    for b in range(B):
+        Ab = sp.csr_matrix((vals[b], ci, rp), shape=A.shape)
+        assert np.linalg.norm(Ab @ x[b] - rhs[b]) <= tol * np.linalg.norm(rhs[b])
+        assert np.linalg.norm(Ab.T @ xt[b] - rhs[b]) <= tol_t * np.linalg.norm(rhs[b])
+
+
+def test_pivot_strategy_none_keeps_small_pivots():
+    """PivotStrategy::None (front_ops.cuh:147-161): a pivot below the shift
+    threshold is used as it is and no system is flagged; the default static
+    shift replaces it and flags the system."""
+    import torch
+
+    # a path 0 - 1 - 2 whose leaf 0 has the small diagonal: whatever the
+    # nested-dissection order, bus 0 is eliminated before its neighbour 1,
+    # so its pivot is 1e-4, below the 1e-3 threshold
+    n = 3
+    rp = np.array([0, 2, 5, 7], np.int32)
+    ci = np.array([0, 1, 0, 1, 2, 1, 2], np.int32)
+    vals = np.array([[1e-4, 1.0, 1.0, 2.0, 1.0, 1.0, 3.0]])
+    rhs = np.array([[1.0, 2.0, 3.0]])
+    A = sp.csr_matrix((vals[0], ci, rp), shape=(n, n))
+    exact = np.linalg.solve(A.toarray(), rhs[0])
+    out = {}
+    for strat in (0, 1):
+        ls = cupf.LinearSolver(cupf.SolverConfig(precision=0, serial_nd=True, pivot_strategy=strat,
+                                                 shift_retry_epsilon=1e-3))
+        ls.set_data(rp, ci)
+        ls.analyze()
+        ls.setup(1)
+        ls.factorize(torch.tensor(vals, device="cuda"))
+        out[strat] = (ls.solve(torch.tensor(rhs, device="cuda")).cpu().numpy()[0], ls.singular_flags()[0])
+    x0, f0 = out[0]
+    assert not f0 and np.abs(x0 - exact).max() <= 1e-9 * np.abs(exact).max()
+    x1, f1 = out[1]
+    assert f1 and np.abs(x1 - exact).max() > 1e-6 * np.abs(exact).max()

@@ -248,3 +248,21 @@ def test_dump_case_solves_like_the_grid(tmp_path):
     b = solve(s, g, S, V0, cfg())
     assert a.converged_numpy.all()
     assert np.array_equal(a.V_numpy, b.V_numpy)
+
+
+def test_structural_matching_gives_the_same_solution():
+    """CustomMatchingMode::Structural on a Newton Jacobian (its diagonal is
+    structurally full, so the matching is the identity): the same voltages,
+    bit for bit."""
+    g = G.grid_2000()
+    S, V0 = g.scenarios(40, seed=19), g.flat_start(40)
+    a = solve(make_solver(g, cupf.ComputePolicy.Mixed), g, S, V0, cfg())
+    o = cupf.NewtonOptions()
+    o.backend = cupf.BackendKind.CUDA
+    o.compute = cupf.ComputePolicy.Mixed
+    o.custom.serial_nd = True
+    o.custom.matching = cupf.CustomMatchingMode.Structural
+    s = cupf.NewtonSolver(o)
+    s.initialize(g.indptr, g.indices, g.data, g.n_bus, g.n_bus, g.pv, g.pq)
+    b = solve(s, g, S, V0, cfg())
+    assert np.array_equal(a.V_numpy, b.V_numpy)
