@@ -344,9 +344,13 @@ pf_status pf_create(const pf_options* options, pf_handle* out) {
       throw std::invalid_argument("NewtonSolver: unsupported compute policy");
     if (o.custom.matching != 0 && o.custom.matching != 1)
       throw std::invalid_argument("NewtonSolver: matching must be None or Structural");
+    if (o.cuda_jacobian < PF_JACOBIAN_EDGE || o.cuda_jacobian > PF_JACOBIAN_VERTEX_WARP)
+      throw std::invalid_argument("NewtonSolver: cuda_jacobian must be Edge, EdgeAtomic or VertexWarp");
     cls_config c = o.custom;
     if (o.compute == PF_COMPUTE_FP64) c.precision = CLS_PRECISION_FP64;
-    h->eng.reset(new Engine(engine_config(c, o.compute, o.use_cuda_graph)));
+    EngineConfig ec = engine_config(c, o.compute, o.use_cuda_graph);
+    ec.jacobian_kind = o.cuda_jacobian;
+    h->eng.reset(new Engine(ec));
   } catch (const std::exception& e) {
     // keep the handle so the caller can read the message, then report failure
     h->err = e.what();

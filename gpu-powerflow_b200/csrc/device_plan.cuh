@@ -86,9 +86,11 @@ __device__ __forceinline__ FrontMeta load_front_meta(const int* meta, int q) {
 // Ybus and the Jacobian maps of one grid.
 struct DevGrid {
   int n_bus = 0, nnz_y = 0, dim = 0, nnz_j = 0, n_pv = 0, n_pq = 0;
+  int jac_kind = 0;  // Jacobian fill: 0 edge, 1 edge with atomic diagonal sums, 2 vertex (one bus row per warp)
   const int* y_ptr = nullptr;
   const int* y_col = nullptr;
   const int* y_row = nullptr;
+  const int* y_diag = nullptr;  // position of the diagonal entry of each row, -1 if absent
   const double* y_re = nullptr;
   const double* y_im = nullptr;
   const int* map11 = nullptr;

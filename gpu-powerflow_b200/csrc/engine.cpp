@@ -91,7 +91,7 @@ std::vector<long long> to_ll(const std::vector<T>& v) {
 
 struct Engine::Impl {
   // grid
-  DBuf y_ptr, y_col, y_row, y_re, y_im, map11, map21, map12, map22, bus_fa, bus_fm, bus_fa_p, bus_fm_p, pv, pq,
+  DBuf y_ptr, y_col, y_row, y_diag, y_re, y_im, map11, map21, map12, map22, bus_fa, bus_fm, bus_fa_p, bus_fm_p, pv, pq,
       jt_ptr, jt_row, jt_q;
   // factor program
   DBuf fsz, nc, first, front_ptr, front_rows, u_off, l_off, cb_off, tv_off, arow_ptr, arow_q, arow_col, crow_ptr,
@@ -184,10 +184,14 @@ void Engine::initialize(int32_t n_bus, const int32_t* indptr, const int32_t* ind
 
   auto& d = *d_;
   const int32_t nnz_y = indptr[n_bus];
-  std::vector<int32_t> yptr(indptr, indptr + n_bus + 1), ycol(indices, indices + nnz_y), yrow(nnz_y);
+  std::vector<int32_t> yptr(indptr, indptr + n_bus + 1), ycol(indices, indices + nnz_y), yrow(nnz_y),
+      ydiag(n_bus, -1);
   std::vector<double> yre(nnz_y), yim(nnz_y);
   for (int32_t r = 0; r < n_bus; ++r)
-    for (int32_t k = indptr[r]; k < indptr[r + 1]; ++k) yrow[k] = r;
+    for (int32_t k = indptr[r]; k < indptr[r + 1]; ++k) {
+      yrow[k] = r;
+      if (indices[k] == r) ydiag[r] = k;
+    }
   for (int32_t k = 0; k < nnz_y; ++k) {
     yre[k] = ydata[2 * k];
     yim[k] = ydata[2 * k + 1];
@@ -195,6 +199,7 @@ void Engine::initialize(int32_t n_bus, const int32_t* indptr, const int32_t* ind
   d.y_ptr.upload(yptr);
   d.y_col.upload(ycol);
   d.y_row.upload(yrow);
+  d.y_diag.upload(ydiag);
   d.y_re.upload(yre);
   d.y_im.upload(yim);
   d.map11.upload(ja_.map11);
@@ -243,6 +248,8 @@ void Engine::initialize(int32_t n_bus, const int32_t* indptr, const int32_t* ind
   g.y_ptr = d.y_ptr.as<int>();
   g.y_col = d.y_col.as<int>();
   g.y_row = d.y_row.as<int>();
+  g.y_diag = d.y_diag.as<int>();
+  g.jac_kind = cfg_.jacobian_kind;
   g.y_re = d.y_re.as<double>();
   g.y_im = d.y_im.as<double>();
   g.map11 = d.map11.as<int>();

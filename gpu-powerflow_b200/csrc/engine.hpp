@@ -28,6 +28,7 @@ struct EngineConfig {
   int32_t max_panel_width = 8;
   int32_t serial_nd = 1;
   int32_t use_matching = 0;       // structural (Hopcroft-Karp) column matching
+  int32_t jacobian_kind = 0;      // CudaJacobianKind: 0 Edge, 1 EdgeAtomic, 2 VertexWarp
   int32_t static_pivot = 1;       // StaticDiagonalShift
   double shift_epsilon = 1e-8;    // threshold and replacement magnitude
   int32_t use_cuda_graph = 0;     // capture one iteration and replay it

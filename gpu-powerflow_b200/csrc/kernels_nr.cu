@@ -144,6 +144,136 @@ __global__ void k_jacobian(DevGrid g, DevState st, TJ* __restrict__ J) {
 }
 
 // ---------------------------------------------------------------------------
+// The two other fills of CudaJacobianKind (fill_jacobian_edge_atomic_kernel.hpp,
+// fill_jacobian_vertex_warp_kernel.hpp).  Both build the diagonal from the
+// edges instead of from Ibus:
+//   dS_i/dVa_i = sum_{c != i} j V_i conj(y_ic V_c)            (= -sum of the off-diagonal angle terms)
+//   dS_i/d|V_i| = sum_c conj(y_ic V_c) V_i / |V_i| + V_i conj(y_ii V_i / |V_i|)
+// The off-diagonal entries are those of k_jacobian.
+// ---------------------------------------------------------------------------
+struct EdgeTerms {
+  double var, vai, vmr, vmi;  // -j V_i conj(y V_c) and V_i conj(y V_c / |V_c|)
+  double dmr, dmi;            // conj(y V_c) V_i / |V_i|
+};
+
+__device__ __forceinline__ EdgeTerms edge_terms(double yr, double yi, double vir, double vii, double vcr, double vci) {
+  EdgeTerms t;
+  const double yvr = yr * vcr - yi * vci, yvi = yr * vci + yi * vcr;
+  t.var = vii * yvr - vir * yvi;
+  t.vai = -(vii * yvi + vir * yvr);
+  double mc = hypot(vcr, vci);
+  mc = mc < 1e-8 ? 1e-8 : mc;
+  const double ynr = yvr / mc, yni = yvi / mc;
+  t.vmr = vir * ynr + vii * yni;
+  t.vmi = vii * ynr - vir * yni;
+  double mi = hypot(vir, vii);
+  mi = mi < 1e-8 ? 1e-8 : mi;
+  const double nr = vir / mi, ni = vii / mi;
+  t.dmr = yvr * nr + yvi * ni;
+  t.dmi = yvr * ni - yvi * nr;
+  return t;
+}
+
+// Vertex fill: a warp takes one bus row for 32 scenarios and walks its Ybus
+// entries, storing the off-diagonal slots and summing the diagonal in
+// registers (each lane owns its scenario, so no reduction is needed).
+template <typename TJ>
+__global__ void k_jacobian_vertex(DevGrid g, DevState st, TJ* __restrict__ J) {
+  const int lane = threadIdx.x, wy = threadIdx.y;
+  const int Bp = st.Bp;
+  const size_t b = (size_t)blockIdx.y * kWarp + lane;
+  const double* yre = st.yb_re ? st.yb_re + b : g.y_re;
+  const double* yim = st.yb_re ? st.yb_im + b : g.y_im;
+  const size_t ys = st.yb_re ? (size_t)Bp : 1;
+  for (int i = blockIdx.x * kRows + wy; i < g.n_bus; i += gridDim.x * kRows) {
+    const size_t oi = (size_t)i * Bp + b;
+    const double vir = st.v_re[oi], vii = st.v_im[oi];
+    double d11 = 0.0, d21 = 0.0, d12 = 0.0, d22 = 0.0;
+    int kd = -1;
+    for (int k = g.y_ptr[i]; k < g.y_ptr[i + 1]; ++k) {
+      const int c = g.y_col[k];
+      const size_t oc = (size_t)c * Bp + b;
+      const EdgeTerms t = edge_terms(yre[k * ys], yim[k * ys], vir, vii, st.v_re[oc], st.v_im[oc]);
+      d12 += t.dmr;
+      d22 += t.dmi;
+      if (c == i) {
+        kd = k;
+        d12 += t.vmr;
+        d22 += t.vmi;
+        continue;
+      }
+      d11 -= t.var;
+      d21 -= t.vai;
+      const int p11 = g.map11[k], p21 = g.map21[k], p12 = g.map12[k], p22 = g.map22[k];
+      if (p11 >= 0) J[(size_t)p11 * Bp + b] = static_cast<TJ>(t.var);
+      if (p21 >= 0) J[(size_t)p21 * Bp + b] = static_cast<TJ>(t.vai);
+      if (p12 >= 0) J[(size_t)p12 * Bp + b] = static_cast<TJ>(t.vmr);
+      if (p22 >= 0) J[(size_t)p22 * Bp + b] = static_cast<TJ>(t.vmi);
+    }
+    if (kd >= 0) {
+      const int p11 = g.map11[kd], p21 = g.map21[kd], p12 = g.map12[kd], p22 = g.map22[kd];
+      if (p11 >= 0) J[(size_t)p11 * Bp + b] = static_cast<TJ>(d11);
+      if (p21 >= 0) J[(size_t)p21 * Bp + b] = static_cast<TJ>(d21);
+      if (p12 >= 0) J[(size_t)p12 * Bp + b] = static_cast<TJ>(d12);
+      if (p22 >= 0) J[(size_t)p22 * Bp + b] = static_cast<TJ>(d22);
+    }
+  }
+}
+
+// Edge fill with atomic diagonal accumulation: a warp takes one Ybus entry
+// for 32 scenarios, stores its off-diagonal slots and adds its share of the
+// row's diagonal with atomicAdd in the Jacobian's own type (the diagonal
+// slots are zeroed first).  The summation order of the diagonal depends on
+// scheduling, so results may differ in the last bits from run to run.
+template <typename TJ>
+__global__ void k_jacobian_zero_diag(DevGrid g, DevState st, TJ* __restrict__ J) {
+  const int lane = threadIdx.x, wy = threadIdx.y;
+  const int Bp = st.Bp;
+  const size_t b = (size_t)blockIdx.y * kWarp + lane;
+  for (int i = blockIdx.x * kRows + wy; i < g.n_bus; i += gridDim.x * kRows)
+    for (int k = g.y_ptr[i]; k < g.y_ptr[i + 1]; ++k)
+      if (g.y_col[k] == i) {
+        const int p[4] = {g.map11[k], g.map21[k], g.map12[k], g.map22[k]};
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          if (p[q] >= 0) J[(size_t)p[q] * Bp + b] = TJ(0);
+      }
+}
+
+template <typename TJ>
+__global__ void k_jacobian_edge_atomic(DevGrid g, DevState st, TJ* __restrict__ J) {
+  const int lane = threadIdx.x, wy = threadIdx.y;
+  const int Bp = st.Bp;
+  const size_t b = (size_t)blockIdx.y * kWarp + lane;
+  const double* yre = st.yb_re ? st.yb_re + b : g.y_re;
+  const double* yim = st.yb_re ? st.yb_im + b : g.y_im;
+  const size_t ys = st.yb_re ? (size_t)Bp : 1;
+  for (int k = blockIdx.x * kRows + wy; k < g.nnz_y; k += gridDim.x * kRows) {
+    const int i = g.y_row[k], c = g.y_col[k];
+    const size_t oi = (size_t)i * Bp + b, oc = (size_t)c * Bp + b;
+    const EdgeTerms t = edge_terms(yre[k * ys], yim[k * ys], st.v_re[oi], st.v_im[oi], st.v_re[oc], st.v_im[oc]);
+    const int kd = g.y_diag[i];
+    if (kd < 0) continue;
+    const int q11 = g.map11[kd], q21 = g.map21[kd], q12 = g.map12[kd], q22 = g.map22[kd];
+    double a12 = t.dmr, a22 = t.dmi;
+    if (c == i) {
+      a12 += t.vmr;
+      a22 += t.vmi;
+    } else {
+      const int p11 = g.map11[k], p21 = g.map21[k], p12 = g.map12[k], p22 = g.map22[k];
+      if (p11 >= 0) J[(size_t)p11 * Bp + b] = static_cast<TJ>(t.var);
+      if (p21 >= 0) J[(size_t)p21 * Bp + b] = static_cast<TJ>(t.vai);
+      if (p12 >= 0) J[(size_t)p12 * Bp + b] = static_cast<TJ>(t.vmr);
+      if (p22 >= 0) J[(size_t)p22 * Bp + b] = static_cast<TJ>(t.vmi);
+      if (q11 >= 0) atomicAdd(&J[(size_t)q11 * Bp + b], static_cast<TJ>(-t.var));
+      if (q21 >= 0) atomicAdd(&J[(size_t)q21 * Bp + b], static_cast<TJ>(-t.vai));
+    }
+    if (q12 >= 0) atomicAdd(&J[(size_t)q12 * Bp + b], static_cast<TJ>(a12));
+    if (q22 >= 0) atomicAdd(&J[(size_t)q22 * Bp + b], static_cast<TJ>(a22));
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Va/Vm -= dx at the pv/pq rows, V = Vm (cos Va + j sin Va)
 // (cuPF voltage_update_kernels.hpp:44-104).  dx is read from the permuted
 // solution X (x_perm[iperm[row]]).  The bus-0 thread clears the scenario's
@@ -495,6 +625,15 @@ void launch_ibus_mismatch(const DevGrid& g, const DevState& st, cudaStream_t s) 
 
 template <typename TJ>
 void launch_jacobian(const DevGrid& g, const DevState& st, TJ* J, cudaStream_t s) {
+  if (g.jac_kind == 2) {
+    k_jacobian_vertex<TJ><<<rows_grid(g.n_bus, st.Bp), dim3(kWarp, kRows), 0, s>>>(g, st, J);
+    return;
+  }
+  if (g.jac_kind == 1) {
+    k_jacobian_zero_diag<TJ><<<rows_grid(g.n_bus, st.Bp), dim3(kWarp, kRows), 0, s>>>(g, st, J);
+    k_jacobian_edge_atomic<TJ><<<rows_grid(g.nnz_y, st.Bp), dim3(kWarp, kRows), 0, s>>>(g, st, J);
+    return;
+  }
   k_jacobian<TJ><<<rows_grid(g.nnz_y, st.Bp), dim3(kWarp, kRows), 0, s>>>(g, st, J);
 }
 template void launch_jacobian<float>(const DevGrid&, const DevState&, float*, cudaStream_t);

@@ -150,7 +150,10 @@ typedef struct {
   int32_t backend;              /* only PF_BACKEND_CUDA is provided */
   int32_t compute;              /* PF_COMPUTE_* */
   int32_t cuda_linear_solver;   /* only PF_CUDA_SOLVER_CUSTOM is provided */
-  int32_t cuda_jacobian;        /* all kinds run the one fill kernel */
+  int32_t cuda_jacobian;        /* PF_JACOBIAN_*: EDGE writes each slot once and takes the diagonal
+                                   from Ibus; EDGE_ATOMIC sums the diagonal from the edges with
+                                   atomicAdd (last bits vary run to run); VERTEX_WARP sums each bus
+                                   row's diagonal in registers (fill_jacobian_*_kernel.hpp) */
   cls_config custom;
   int32_t use_cuda_graph;       /* capture one iteration, replay per step */
 } pf_options;
