@@ -130,16 +130,21 @@ struct Engine::Impl {
     }
     return ev_pool[ev_used++];
   }
-  // graph of one iteration tail (+ the next mismatch), per batch
+  // graph of a whole solve: the first mismatch and its test, then a WHILE
+  // node around (update, mismatch, test); per batch size, precision and Ybus
   cudaGraphExec_t exec = nullptr;
   int graph_Bp = -1;
   bool graph_double = false;
+  int64_t graph_body_launches = 0;
+  DBuf ctl, fin_dev;           // LoopCtl, final norms [Bp]
+  LoopCtl* h_ctl = nullptr;    // pinned
 
   ~Impl() {
     for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
     if (exec) cudaGraphExecDestroy(exec);
     if (h_norm) cudaFreeHost(h_norm);
     if (h_final) cudaFreeHost(h_final);
+    if (h_ctl) cudaFreeHost(h_ctl);
     if (own) cudaStreamDestroy(own);
   }
 
@@ -609,6 +614,81 @@ void Engine::iteration_tail(cudaStream_t s, int store_l) {
   ++d.stage_launches[4];
 }
 
+// Builds the graph of a whole solve for this batch size, precision and Ybus
+// source: [mismatch, test] -> WHILE(test says "update") { Jacobian, factor,
+// backward sweep, voltage update, mismatch, test }.  The test kernel sets the
+// WHILE node's condition (a CUDA graph conditional node), so the iterations
+// run back to back on the device and the host synchronises once per solve.
+template <typename T>
+void Engine::ensure_loop_graph(const DevState& st) {
+  auto& d = *d_;
+  const bool dbl = std::is_same<T, double>::value;
+  if (d.exec && d.graph_Bp == d.Bp && d.graph_double == dbl && d.graph_yb == static_cast<const void*>(st.yb_re))
+    return;
+  if (d.exec) cudaGraphExecDestroy(d.exec);
+  d.exec = nullptr;
+  d.graph_Bp = -1;
+  d.ctl.reserve(sizeof(LoopCtl));
+  d.fin_dev.reserve((size_t)d.Bp * sizeof(double));
+  if (!d.h_ctl) CUPF_CUDA(cudaMallocHost(&d.h_ctl, sizeof(LoopCtl)));
+  LoopCtl* ctl = d.ctl.as<LoopCtl>();
+  auto* norm = d.norm.as<unsigned long long>();
+  double* fin = d.fin_dev.as<double>();
+  cudaStream_t cs = d.own;
+  const int64_t before = launches_;
+  cudaGraph_t graph = nullptr;
+  CUPF_CUDA(cudaGraphCreate(&graph, 0));
+  bool capturing = false;
+  try {
+    cudaGraphConditionalHandle h;
+    CUPF_CUDA(cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault));
+    CUPF_CUDA(cudaStreamBeginCaptureToGraph(cs, graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    capturing = true;
+    launch_ibus_mismatch(d.g, st, cs);
+    launch_loop_check(h, ctl, norm, fin, cs);
+    cudaStreamCaptureStatus cst;
+    cudaGraph_t cap = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    CUPF_CUDA(cudaStreamGetCaptureInfo(cs, &cst, nullptr, &cap, &deps, &ndeps));
+    cudaGraphNodeParams p = {};
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = h;
+    p.conditional.type = cudaGraphCondTypeWhile;
+    p.conditional.size = 1;
+    cudaGraphNode_t wn;
+    CUPF_CUDA(cudaGraphAddNode(&wn, cap, deps, ndeps, &p));
+    CUPF_CUDA(cudaStreamUpdateCaptureDependencies(cs, &wn, 1, cudaStreamSetCaptureDependencies));
+    cudaGraph_t done = nullptr;
+    capturing = false;
+    CUPF_CUDA(cudaStreamEndCapture(cs, &done));
+    cudaGraph_t body = p.conditional.phGraph_out[0];
+    CUPF_CUDA(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    capturing = true;
+    const int64_t b0 = launches_;
+    iteration_tail<T>(cs, 0);
+    d.graph_body_launches = (launches_ - b0) + 2;
+    launch_ibus_mismatch(d.g, st, cs);
+    launch_loop_check(h, ctl, norm, fin, cs);
+    capturing = false;
+    CUPF_CUDA(cudaStreamEndCapture(cs, &done));
+    CUPF_CUDA(cudaGraphInstantiate(&d.exec, graph, 0));
+  } catch (...) {
+    if (capturing) {
+      cudaGraph_t g2 = nullptr;
+      cudaStreamEndCapture(cs, &g2);
+    }
+    cudaGraphDestroy(graph);
+    launches_ = before;
+    throw;
+  }
+  cudaGraphDestroy(graph);
+  d.graph_Bp = d.Bp;
+  d.graph_double = dbl;
+  d.graph_yb = st.yb_re;
+  launches_ = before;
+}
+
 template <typename T>
 SolveStats Engine::run_loop(double tol, int32_t max_iter, int32_t prepare_adjoint, cudaStream_t s, double* d_final) {
   auto& d = *d_;
@@ -627,15 +707,37 @@ SolveStats Engine::run_loop(double tol, int32_t max_iter, int32_t prepare_adjoin
   }
   d.ev_pairs.clear();
   d.ev_used = 0;
-  if (max_iter > 0) {
+  const bool use_graph = cfg_.use_cuda_graph != 0 && max_iter > 0;
+  if (use_graph) {
+    // the whole solve is one graph launch: no host round trip per iteration
+    ensure_loop_graph<T>(st);
+    LoopCtl* hc = d.h_ctl;
+    *hc = LoopCtl{};
+    hc->tol = tol;
+    hc->max_iter = max_iter;
+    hc->B = d.B;
+    hc->tolerate = tolerate_nonfinite_ ? 1 : 0;
+    CUPF_CUDA(cudaMemcpyAsync(d.ctl.p, hc, sizeof(LoopCtl), cudaMemcpyHostToDevice, s));
+    CUPF_CUDA(cudaGraphLaunch(d.exec, s));
+    CUPF_CUDA(cudaMemcpyAsync(hc, d.ctl.p, sizeof(LoopCtl), cudaMemcpyDeviceToHost, s));
+    CUPF_CUDA(cudaMemcpyAsync(d.h_final, d.fin_dev.p, d.B * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CUPF_CUDA(cudaStreamSynchronize(s));
+    completed = hc->completed;
+    gmax = hc->gmax;
+    // first mismatch + test, then per update: the body, plus the closing
+    // mismatch and test when the cap stopped the loop
+    const int64_t updates = (gmax <= tol || hc->status) ? completed - 1 : completed;
+    launches_ += 2 + updates * d.graph_body_launches;
+    if (debug_sync()) std::fprintf(stderr, "[cupf] %d norm evaluations, max ||F||inf = %.3e\n", completed, gmax);
+    if (hc->status) throw std::runtime_error("NewtonSolver: mismatch norm is not finite");
+  } else if (max_iter > 0) {
     stage_begin(0, s);
     launch_ibus_mismatch(d.g, st, s);
     stage_end(0, s);
     ++launches_;
     ++d.stage_launches[0];
   }
-  const bool use_graph = cfg_.use_cuda_graph != 0;
-  for (int it = 0; it < max_iter; ++it) {
+  for (int it = 0; it < (use_graph ? 0 : max_iter); ++it) {
     completed = it + 1;
     CUPF_CUDA(cudaMemcpyAsync(d.h_norm, d.norm.p, d.Bp * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
     CUPF_CUDA(cudaStreamSynchronize(s));
@@ -657,36 +759,13 @@ SolveStats Engine::run_loop(double tol, int32_t max_iter, int32_t prepare_adjoin
     if (debug_sync()) std::fprintf(stderr, "[cupf] iteration %d max ||F||inf = %.3e\n", it, gmax);
     if (!finite) throw std::runtime_error("NewtonSolver: mismatch norm is not finite");
     if (gmax <= tol) break;
-    if (use_graph) {
-      if (!d.exec || d.graph_Bp != d.Bp || d.graph_double != std::is_same<T, double>::value ||
-          d.graph_yb != static_cast<const void*>(st.yb_re)) {
-        if (d.exec) cudaGraphExecDestroy(d.exec);
-        d.exec = nullptr;
-        cudaStream_t cs = d.own;
-        cudaGraph_t graph;
-        const int64_t before = launches_;
-        CUPF_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-        iteration_tail<T>(cs, 0);
-        launch_ibus_mismatch(d.g, st, cs);
-        CUPF_CUDA(cudaStreamEndCapture(cs, &graph));
-        CUPF_CUDA(cudaGraphInstantiate(&d.exec, graph, 0));
-        cudaGraphDestroy(graph);
-        d.graph_Bp = d.Bp;
-        d.graph_double = std::is_same<T, double>::value;
-        d.graph_yb = st.yb_re;
-        launches_ = before;
-      }
-      CUPF_CUDA(cudaGraphLaunch(d.exec, s));
-      launches_ += 3 + 2 * (int64_t)d.levels.size();
-    } else {
-      iteration_tail<T>(s, 0);
-      if (it + 1 < max_iter) {
-        stage_begin(0, s);
-        launch_ibus_mismatch(d.g, st, s);
-        stage_end(0, s);
-        ++launches_;
-        ++d.stage_launches[0];
-      }
+    iteration_tail<T>(s, 0);
+    if (it + 1 < max_iter) {
+      stage_begin(0, s);
+      launch_ibus_mismatch(d.g, st, s);
+      stage_end(0, s);
+      ++launches_;
+      ++d.stage_launches[0];
     }
   }
   CUPF_CUDA(cudaGetLastError());

@@ -31,7 +31,7 @@ struct EngineConfig {
   int32_t jacobian_kind = 0;      // CudaJacobianKind: 0 Edge, 1 EdgeAtomic, 2 VertexWarp
   int32_t static_pivot = 1;       // StaticDiagonalShift
   double shift_epsilon = 1e-8;    // threshold and replacement magnitude
-  int32_t use_cuda_graph = 0;     // capture one iteration and replay it
+  int32_t use_cuda_graph = 0;     // run each solve as one graph (device-side convergence test)
   int32_t adjoint_refine_steps = 2;
 };
 
@@ -151,6 +151,8 @@ class Engine {
   void use_scenario_ybus(const double* d_ybus, int64_t ybus_stride, int32_t B, cudaStream_t s);
   template <typename T>
   SolveStats run_loop(double tol, int32_t max_iter, int32_t prepare_adjoint, cudaStream_t s, double* d_final);
+  template <typename T>
+  void ensure_loop_graph(const DevState& st);
   template <typename T>
   void iteration_tail(cudaStream_t s, int store_l);
   template <typename T>

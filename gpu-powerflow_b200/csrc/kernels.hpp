@@ -149,6 +149,23 @@ void launch_axpy(double* y, const double* x, long long n, cudaStream_t s);
 // Per-scenario Ybus values complex [B][stride] -> re/im [nnz][Bp]
 void launch_ybus_to_rows(const double* yc, long long stride, int nnz, int B, int Bp, double* yr, double* yi,
                          cudaStream_t s);
+// Convergence test of the device-side Newton loop (one CUDA graph per solve,
+// a WHILE node around the iteration).  The host writes tol / max_iter / B /
+// tolerate before each launch; the check kernel keeps the rest.
+struct LoopCtl {
+  double tol = 0.0;
+  int max_iter = 0;
+  int B = 0;
+  int tolerate = 0;   // a non-finite scenario norm ends that scenario (inf) instead of the solve
+  int completed = 0;  // norm evaluations so far
+  int status = 0;     // 1: a non-finite norm that was not tolerated
+  double gmax = 0.0;  // max over the batch of the last evaluated norms
+};
+// Reads the per-scenario norms of the last mismatch, records them as the
+// final mismatches, counts the evaluation and sets the loop's condition to
+// 1 (iterate again) or 0 (converged, iteration cap, or non-finite).
+void launch_loop_check(cudaGraphConditionalHandle h, LoopCtl* ctl, const unsigned long long* norm_bits,
+                       double* final_norm, cudaStream_t s);
 void launch_sumsq2(const double* R, const double* G, int dim, int B, int Bp, double* scratch, cudaStream_t s);
 // [B][rows] (TS) -> [rows][Bp] (TD) and back; pad scenarios copy scenario B - 1
 template <typename TS, typename TD>

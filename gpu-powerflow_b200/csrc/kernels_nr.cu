@@ -505,6 +505,63 @@ __global__ void k_jt_residual(DevGrid g, int Bp, const double* __restrict__ Jd, 
   }
 }
 
+// Convergence test of the device-side Newton loop, with the semantics of the
+// host loop of newton_solver.cpp:245-342: every iteration evaluates the norm
+// (the iteration count is the number of evaluations), stops when
+// max_b ||F_b||inf <= tol, and otherwise updates V, also after the last
+// allowed evaluation; a non-finite norm ends the solve with an error (or, for
+// warm-started solves, only that scenario).  The condition it sets means
+// "run one more update".  A mismatch evaluated after the cap was reached is
+// not counted.  One block; the max is reduced in a fixed order.
+constexpr int kCheckThreads = 1024;
+__global__ void __launch_bounds__(kCheckThreads)
+    k_loop_check(cudaGraphConditionalHandle h, LoopCtl* __restrict__ ctl,
+                 const unsigned long long* __restrict__ norm_bits, double* __restrict__ final_norm) {
+  __shared__ double sm[kCheckThreads / kWarp];
+  __shared__ int sb[kCheckThreads / kWarp];
+  if (ctl->completed >= ctl->max_iter) {  // the cap was reached before this evaluation
+    if (threadIdx.x == 0) cudaGraphSetConditional(h, 0u);
+    return;
+  }
+  const int B = ctl->B, tolerate = ctl->tolerate;
+  double m = 0.0;
+  int bad = 0;
+  for (int b = threadIdx.x; b < B; b += blockDim.x) {
+    const double v = __longlong_as_double((long long)norm_bits[b]);
+    const bool finite = v == v && v <= 1.7976931348623157e308;
+    if (!finite) {
+      final_norm[b] = tolerate ? __longlong_as_double(0x7FF0000000000000ll) : v;
+      if (!tolerate) bad = 1;
+      continue;
+    }
+    final_norm[b] = v;
+    m = v > m ? v : m;
+  }
+  for (int o = kWarp / 2; o > 0; o >>= 1) {
+    const double mo = __shfl_down_sync(0xffffffffu, m, o);
+    m = mo > m ? mo : m;
+    bad |= __shfl_down_sync(0xffffffffu, bad, o);
+  }
+  const int w = threadIdx.x / kWarp, l = threadIdx.x % kWarp;
+  if (l == 0) {
+    sm[w] = m;
+    sb[w] = bad;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int i = 1; i < (int)(blockDim.x / kWarp); ++i) {
+      m = sm[i] > m ? sm[i] : m;
+      bad |= sb[i];
+    }
+    const int done = ctl->completed + 1;
+    ctl->completed = done;
+    ctl->gmax = m;
+    if (bad) ctl->status = 1;
+    const bool stop = bad || m <= ctl->tol;
+    cudaGraphSetConditional(h, stop ? 0u : 1u);
+  }
+}
+
 // Relative residual of the adjoint: per-block partial sums of r^2 and g^2
 // over the real scenarios (b < B) of two [dim][Bp] arrays, then one block
 // adds the partials in a fixed order (deterministic).
@@ -757,6 +814,11 @@ void launch_ybus_to_rows(const double* yc, long long stride, int nnz, int B, int
                          cudaStream_t s) {
   k_ybus_to_rows<<<dim3((nnz + kWarp - 1) / kWarp, Bp / kWarp), dim3(kWarp, kRows), 0, s>>>(yc, stride, nnz, B, Bp,
                                                                                           yr, yi);
+}
+
+void launch_loop_check(cudaGraphConditionalHandle h, LoopCtl* ctl, const unsigned long long* norm_bits,
+                       double* final_norm, cudaStream_t s) {
+  k_loop_check<<<1, kCheckThreads, 0, s>>>(h, ctl, norm_bits, final_norm);
 }
 
 }  // namespace cupf_b200
