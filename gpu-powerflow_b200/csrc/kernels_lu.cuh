@@ -31,6 +31,7 @@
 #include <set>
 #include <stdexcept>
 #include <string>
+#include <utility>
 
 #include "device_plan.cuh"
 #include "kernels.hpp"
@@ -69,6 +70,38 @@ inline void allow_full_smem(const void* fn) {
 
 inline void check_launch(const char* what) {
   const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) throw std::runtime_error(std::string(what) + " launch: " + cudaGetErrorString(e));
+}
+
+// ---------------------------------------------------------------------------
+// Programmatic dependent launch between consecutive level kernels: a level
+// kernel lets the next one be scheduled as soon as all of its own blocks are
+// running (launch_dependents), and the next one runs the part of its work
+// that reads only the static plan (launch record, assembly list, zeroing its
+// shared-memory front) before it waits for the previous grid to finish and
+// its writes to be visible (griddepcontrol.wait, a hardware wait that ends
+// when that grid completes).  Launched without the attribute, both are
+// no-ops.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void chain_allow_next() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
+__device__ __forceinline__ void chain_wait_previous() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+
+// Launch with programmatic stream serialization (the kernel's prologue may
+// overlap the tail of the kernel before it on the stream).
+template <typename... KArgs, typename... Args>
+void launch_chained(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, const char* what,
+                    Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  const cudaError_t e = cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
   if (e != cudaSuccess) throw std::runtime_error(std::string(what) + " launch: " + cudaGetErrorString(e));
 }
 
@@ -133,6 +166,7 @@ __global__ void __launch_bounds__(256)
   const int q = level_begin + item / groups;
   const int grp = item - (item / groups) * groups;
   const size_t col0 = (size_t)grp * kWarp;
+  chain_allow_next();
   const FrontMeta m = load_front_meta(pl.front_meta, q);
   const int fs = m.fs, nc = m.nc, uc = fs - nc, rw = fs + 1;
   const long long e0 = m.e0;
@@ -154,12 +188,17 @@ __global__ void __launch_bounds__(256)
     cp_async4(s_dst + e, pl.fe_dst + e0 + e);
   }
   cp_async_commit();
-  {
-    // fs * rw * 32 elements is a multiple of 16 bytes: zero with 16-byte stores
+  // fs * rw * 32 elements is a multiple of 16 bytes: zero with 16-byte stores
+  auto zero_front = [&]() {
     float4* z4 = reinterpret_cast<float4*>(Fm);
     const int n4 = fs * rw * kWarp * (int)sizeof(T) / 16;
     for (int e = threadIdx.x; e < n4; e += blockDim.x) z4[e] = make_float4(0.f, 0.f, 0.f, 0.f);
-  }
+  };
+  if constexpr (SMEM_FRONT) zero_front();
+  // everything below reads what earlier kernels wrote (J, CB, Fp), and a
+  // global scratch front may still be in use by the previous level's blocks
+  chain_wait_previous();
+  if constexpr (!SMEM_FRONT) zero_front();
   cp_async_wait<0>();
   __syncthreads();
 
@@ -363,10 +402,12 @@ __global__ void __launch_bounds__(256)
   const int q = level_begin + (int)(item / groups);
   const size_t col0 = (size_t)(item % groups) * kWarp;
   const size_t b = col0 + lane;
+  chain_allow_next();
   const FrontMeta m = load_front_meta(pl.front_meta, q);
   const int fs = m.fs, nc = m.nc, uc = fs - nc;
   const int fr0 = m.fr0, first = m.first;
   const long long uo = m.uo;
+  chain_wait_previous();  // U, Y and the x of ancestors come from earlier kernels
   T* Us = reinterpret_cast<T*>(smem_raw) + (size_t)warp * warp_elems * kWarp;  // [nc * fs][32]
   T* Xs = Us + (size_t)nc * fs * kWarp;                                         // [fs][32]
   // U rows: contiguous elements uo .. uo + nc * fs
@@ -619,10 +660,9 @@ void launch_factor_t(const LevelLaunch& lv, const FactorArgs<T, TJ>& a, cudaStre
   const size_t smem = sm.total();
   auto run = [&](auto kern) {
     allow_full_smem(reinterpret_cast<const void*>(kern));
-    kern<<<(unsigned)items, warps * kWarp, smem, s>>>(a.plan, lv.begin, a.groups, a.Bp, (int)elems, sm, a.J, a.Fp,
-                                                      a.U, a.L, a.CB, a.Y, a.store_l, a.eps, a.static_pivot, a.sing,
-                                                      a.front_scratch);
-    check_launch("front factor");
+    launch_chained(kern, dim3((unsigned)items), dim3(warps * kWarp), smem, s, "front factor", a.plan, lv.begin,
+                   a.groups, a.Bp, (int)elems, sm, a.J, a.Fp, a.U, a.L, a.CB, a.Y, a.store_l, a.eps, a.static_pivot,
+                   a.sing, a.front_scratch);
   };
   if (in_smem) run(k_front_factor<T, TJ, FMAX, true>);
   else run(k_front_factor<T, TJ, FMAX, false>);
@@ -672,8 +712,8 @@ void launch_backward_level(const LevelLaunch& lv, const SweepArgs<T>& a, cudaStr
   auto kern = k_backward_level<T>;
   allow_full_smem(reinterpret_cast<const void*>(kern));
   const unsigned blocks = (unsigned)((items + wpb - 1) / wpb);
-  kern<<<blocks, wpb * kWarp, smem, s>>>(a.plan, lv.begin, lv.count, a.groups, a.Bp, warp_elems, a.U, a.Y, a.X);
-  check_launch("backward sweep");
+  launch_chained(kern, dim3(blocks), dim3(wpb * kWarp), smem, s, "backward sweep", a.plan, lv.begin, lv.count,
+                 a.groups, a.Bp, warp_elems, a.U, a.Y, a.X);
 }
 
 template <typename T>
