@@ -49,6 +49,11 @@ TOL = 1e-8
 MAX_ITER = 10
 
 
+
+# measured DRAM traffic of one Mixed factorization of the 2,000-bus grid at
+# 1,024 scenarios: 277.9 MB read + 11.9 MB written over its 19 level launches
+FACTOR_DRAM_BYTES_B1024 = 289_800_000
+
 def _peaks() -> dict:
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -316,13 +321,10 @@ def run_engine(args) -> None:
     fbytes = factor_bytes_per_scenario(prof, 4) * B
     peaks = _peaks()
     achieved = fbytes / (per_fact_ms / 1e3) / 1e9
-    traffic = None
-    tr_file = ROOT / "profiles" / "factor_traffic.json"
-    if tr_file.exists():
-        try:
-            traffic = json.loads(tr_file.read_text()).get("bytes_per_factorization_b1024")
-        except Exception:
-            traffic = None
+    # DRAM bytes (read + write) of the 19 level launches of one Mixed
+    # factorization at 1,024 scenarios, from one ncu capture of this workload
+    # (profiles/k_front_factor_2000x1024_levels.md); scaled by the batch
+    traffic = int(FACTOR_DRAM_BYTES_B1024 * B / 1024) if g.n_bus == 2000 else None
 
     extras = run_extras(args, dev) if (rank == 0 and world == 1 and not args.no_extra) else None
 
