@@ -119,10 +119,12 @@ __global__ void k_jacobian(DevGrid g, DevState st, TJ* __restrict__ J) {
     // -j V_i conj(y V_c)
     double var = vii * yvr - vir * yvi;
     double vai = -(vii * yvi + vir * yvr);
-    // V_i conj(y V_c / |V_c|)
-    double mc = hypot(vcr, vci);
+    // V_i conj(y V_c / |V_c|), with |V_c| the stored magnitude Vm_c (V is
+    // built as Vm e^{j Va}, so they agree to rounding); one reciprocal
+    double mc = st.vm[oc];
     mc = mc < 1e-8 ? 1e-8 : mc;
-    const double ynr = yvr / mc, yni = yvi / mc;
+    const double inv = 1.0 / mc;
+    const double ynr = yvr * inv, yni = yvi * inv;
     double vmr = vir * ynr + vii * yni;
     double vmi = vii * ynr - vir * yni;
     if (i == c) {
@@ -131,7 +133,7 @@ __global__ void k_jacobian(DevGrid g, DevState st, TJ* __restrict__ J) {
       var += -(vii * ir - vir * ii);
       vai += vir * ir + vii * ii;
       // conj(I) V / |V|
-      const double nr = vir / mc, ni = vii / mc;
+      const double nr = vir * inv, ni = vii * inv;
       vmr += ir * nr + ii * ni;
       vmi += ir * ni - ii * nr;
     }
