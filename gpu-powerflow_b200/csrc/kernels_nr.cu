@@ -103,6 +103,10 @@ __global__ void k_ibus_mismatch(DevGrid g, DevState st) {
 // ---------------------------------------------------------------------------
 template <typename TJ>
 __global__ void k_jacobian(DevGrid g, DevState st, TJ* __restrict__ J) {
+  // arithmetic in the Jacobian's own type, as the reference's fill does
+  // (fill_jacobian_edge_kernel.hpp:58-60: AccumScalar = JScalar); the FP64
+  // state is read and rounded once
+  using A = TJ;
   const int lane = threadIdx.x, wy = threadIdx.y;
   const int Bp = st.Bp;
   const size_t b = (size_t)blockIdx.y * kWarp + lane;
@@ -111,37 +115,37 @@ __global__ void k_jacobian(DevGrid g, DevState st, TJ* __restrict__ J) {
   const size_t ys = st.yb_re ? (size_t)Bp : 1;
   for (int k = blockIdx.x * kRows + wy; k < g.nnz_y; k += gridDim.x * kRows) {
     const int i = g.y_row[k], c = g.y_col[k];
-    const double yr = yre[k * ys], yi = yim[k * ys];
+    const A yr = static_cast<A>(yre[k * ys]), yi = static_cast<A>(yim[k * ys]);
     const size_t oi = (size_t)i * Bp + b, oc = (size_t)c * Bp + b;
-    const double vir = st.v_re[oi], vii = st.v_im[oi];
-    const double vcr = st.v_re[oc], vci = st.v_im[oc];
-    const double yvr = yr * vcr - yi * vci, yvi = yr * vci + yi * vcr;  // y V_c
+    const A vir = static_cast<A>(st.v_re[oi]), vii = static_cast<A>(st.v_im[oi]);
+    const A vcr = static_cast<A>(st.v_re[oc]), vci = static_cast<A>(st.v_im[oc]);
+    const A yvr = yr * vcr - yi * vci, yvi = yr * vci + yi * vcr;  // y V_c
     // -j V_i conj(y V_c)
-    double var = vii * yvr - vir * yvi;
-    double vai = -(vii * yvi + vir * yvr);
+    A var = vii * yvr - vir * yvi;
+    A vai = -(vii * yvi + vir * yvr);
     // V_i conj(y V_c / |V_c|), with |V_c| the stored magnitude Vm_c (V is
     // built as Vm e^{j Va}, so they agree to rounding); one reciprocal
-    double mc = st.vm[oc];
-    mc = mc < 1e-8 ? 1e-8 : mc;
-    const double inv = 1.0 / mc;
-    const double ynr = yvr * inv, yni = yvi * inv;
-    double vmr = vir * ynr + vii * yni;
-    double vmi = vii * ynr - vir * yni;
+    A mc = static_cast<A>(st.vm[oc]);
+    mc = mc < A(1e-8) ? A(1e-8) : mc;
+    const A inv = A(1) / mc;
+    const A ynr = yvr * inv, yni = yvi * inv;
+    A vmr = vir * ynr + vii * yni;
+    A vmi = vii * ynr - vir * yni;
     if (i == c) {
-      const double ir = st.i_re[oi], ii = st.i_im[oi];
+      const A ir = static_cast<A>(st.i_re[oi]), ii = static_cast<A>(st.i_im[oi]);
       // j V conj(I)
       var += -(vii * ir - vir * ii);
       vai += vir * ir + vii * ii;
       // conj(I) V / |V|
-      const double nr = vir * inv, ni = vii * inv;
+      const A nr = vir * inv, ni = vii * inv;
       vmr += ir * nr + ii * ni;
       vmi += ir * ni - ii * nr;
     }
     const int p11 = g.map11[k], p21 = g.map21[k], p12 = g.map12[k], p22 = g.map22[k];
-    if (p11 >= 0) J[(size_t)p11 * Bp + b] = static_cast<TJ>(var);
-    if (p21 >= 0) J[(size_t)p21 * Bp + b] = static_cast<TJ>(vai);
-    if (p12 >= 0) J[(size_t)p12 * Bp + b] = static_cast<TJ>(vmr);
-    if (p22 >= 0) J[(size_t)p22 * Bp + b] = static_cast<TJ>(vmi);
+    if (p11 >= 0) J[(size_t)p11 * Bp + b] = var;
+    if (p21 >= 0) J[(size_t)p21 * Bp + b] = vai;
+    if (p12 >= 0) J[(size_t)p12 * Bp + b] = vmr;
+    if (p22 >= 0) J[(size_t)p22 * Bp + b] = vmi;
   }
 }
 
