@@ -323,8 +323,7 @@ void Engine::upload_plan() {
   d.col_perm.upload(fp_.col_perm);
   d.level_fronts.upload(fp_.level_fronts);
   d.fe_split.upload(to_ll(fp_.fe_split));
-  d.fe_dst.upload(fp_.fe_dst);
-  d.fe_src.upload(to_ll(fp_.fe_src));
+
   d.front_meta.upload(fp_.front_meta);
   // Launch list: each level of the front tree, cut into runs of similar front
   // size (fronts are size-sorted inside a level) when both sides of a cut
@@ -357,6 +356,29 @@ void Engine::upload_plan() {
       }
       d.levels.push_back(lv);
     }
+  }
+  // source lists in launch order, each padded to its launch's longest
+  {
+    std::vector<long long> psrc;
+    std::vector<int32_t> pdst;
+    for (auto& lv : d.levels) {
+      lv.max_src = std::max(lv.max_src, 1);
+      lv.fe_base = (long long)psrc.size();
+      for (int32_t q = lv.begin; q < lv.begin + lv.count; ++q) {
+        const int32_t f = fp_.level_fronts[q];
+        const int64_t a = fp_.fe_ptr[f], z = fp_.fe_ptr[f + 1];
+        for (int64_t e = a; e < z; ++e) {
+          psrc.push_back(fp_.fe_src[e]);
+          pdst.push_back(fp_.fe_dst[e]);
+        }
+        for (int64_t e = z - a; e < lv.max_src; ++e) {
+          psrc.push_back(0);
+          pdst.push_back(-1);
+        }
+      }
+    }
+    d.fe_src.upload(psrc);
+    d.fe_dst.upload(pdst);
   }
 
   DevPlan& pl = d.pl;

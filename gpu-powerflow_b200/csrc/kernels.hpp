@@ -16,6 +16,10 @@ struct LevelLaunch {
   int max_fsz = 0; // largest front of the level (selects the register bucket)
   int max_nc = 0;  // widest panel of the level
   int max_src = 0; // longest assembly source list of the level
+  // the launch's source lists, padded to max_src entries each (front q of
+  // the launch starts at fe_base + (q - begin) * max_src), so a block finds
+  // its list without reading the launch record first
+  long long fe_base = 0;
 };
 
 template <typename T, typename TJ>

@@ -153,7 +153,8 @@ __device__ __forceinline__ void cp_async_wait() {
 // ---------------------------------------------------------------------------
 template <typename T, typename TJ, int FMAX, bool SMEM_FRONT>
 __global__ void __launch_bounds__(256)
-    k_front_factor(DevPlan pl, int level_begin, int groups, int Bp, int front_elems, FrontSmem sm,
+    k_front_factor(DevPlan pl, int level_begin, long long fe_base, int fe_pad, int groups, int Bp, int front_elems,
+                   FrontSmem sm,
                    const TJ* __restrict__ J, const T* __restrict__ Fp, T* __restrict__ U, T* __restrict__ L,
                    T* __restrict__ CB, T* __restrict__ Y, int store_l, double eps, int static_pivot,
                    int* __restrict__ sing, T* __restrict__ front_scratch) {
@@ -167,13 +168,23 @@ __global__ void __launch_bounds__(256)
   const int grp = item - (item / groups) * groups;
   const size_t col0 = (size_t)grp * kWarp;
   chain_allow_next();
-  const FrontMeta m = load_front_meta(pl.front_meta, q);
-  const int fs = m.fs, nc = m.nc, uc = fs - nc, rw = fs + 1;
-  const long long e0 = m.e0;
-  const int nsrc = m.split[8];
-
   long long* s_src = reinterpret_cast<long long*>(smem_raw);
   int* s_dst = reinterpret_cast<int*>(smem_raw + (size_t)sm.idx_cap * sizeof(long long));
+  // phase 1a: the source list -> shared memory.  Its place follows from the
+  // item alone (padded lists), so it is requested together with the launch
+  // record: one memory round trip for both.
+  {
+    const long long e0 = fe_base + (long long)(q - level_begin) * fe_pad;
+    for (int e = threadIdx.x; e < fe_pad; e += blockDim.x) {
+      cp_async8(s_src + e, pl.fe_src + e0 + e);
+      cp_async4(s_dst + e, pl.fe_dst + e0 + e);
+    }
+    cp_async_commit();
+  }
+  const FrontMeta m = load_front_meta(pl.front_meta, q);
+  const int fs = m.fs, nc = m.nc, uc = fs - nc, rw = fs + 1;
+  const int nsrc = m.split[8];
+
   T* s_inv = reinterpret_cast<T*>(smem_raw + sm.idx_bytes);  // [8][32] pivot reciprocals
   unsigned char* stage = smem_raw + sm.idx_bytes + sm.inv_bytes;
   T* Fm;
@@ -182,12 +193,7 @@ __global__ void __launch_bounds__(256)
   else
     Fm = front_scratch + (size_t)item * front_elems * kWarp;
 
-  // phase 1a: source list -> shared memory (the dense front is zeroed meanwhile)
-  for (int e = threadIdx.x; e < nsrc; e += blockDim.x) {
-    cp_async8(s_src + e, pl.fe_src + e0 + e);
-    cp_async4(s_dst + e, pl.fe_dst + e0 + e);
-  }
-  cp_async_commit();
+  // (the dense front is zeroed while the list arrives)
   // fs * rw * 32 elements is a multiple of 16 bytes: zero with 16-byte stores
   auto zero_front = [&]() {
     float4* z4 = reinterpret_cast<float4*>(Fm);
@@ -661,7 +667,7 @@ void launch_factor_t(const LevelLaunch& lv, const FactorArgs<T, TJ>& a, cudaStre
   auto run = [&](auto kern) {
     allow_full_smem(reinterpret_cast<const void*>(kern));
     launch_chained(kern, dim3((unsigned)items), dim3(warps * kWarp), smem, s, "front factor", a.plan, lv.begin,
-                   a.groups, a.Bp, (int)elems, sm, a.J, a.Fp, a.U, a.L, a.CB, a.Y, a.store_l, a.eps, a.static_pivot,
+                   lv.fe_base, lv.max_src, a.groups, a.Bp, (int)elems, sm, a.J, a.Fp, a.U, a.L, a.CB, a.Y, a.store_l, a.eps, a.static_pivot,
                    a.sing, a.front_scratch);
   };
   if (in_smem) run(k_front_factor<T, TJ, FMAX, true>);
