@@ -97,6 +97,11 @@ struct Engine::Impl {
   DBuf fsz, nc, first, front_ptr, front_rows, u_off, l_off, cb_off, tv_off, arow_ptr, arow_q, arow_col, crow_ptr,
       crow_child, crow_r, asm_ptr, asm_local, perm, iperm, row_iperm, col_perm, level_fronts, fe_split, fe_dst, fe_src, front_meta;
   std::vector<LevelLaunch> levels;
+  // backward sweep: the narrow top levels (launch-list entries from bw_first
+  // on) run as one launch over bw_bounds (descending level boundaries)
+  int bw_first = 0, bw_nlev = 0;
+  LevelLaunch bw_top;
+  DBuf bw_bounds;
   int64_t tv_total = 0;
   DevGrid g;
   DevPlan pl;
@@ -357,6 +362,32 @@ void Engine::upload_plan() {
       d.levels.push_back(lv);
     }
   }
+  // The top of the tree for the backward sweep: the trailing levels of at
+  // most kBackwardTopFronts fronts.
+  d.bw_first = (int)d.levels.size();
+  d.bw_nlev = 0;
+  d.bw_top = LevelLaunch{};
+  {
+    constexpr int32_t kBackwardTopFronts = 8;
+    int32_t Ls = fp_.num_levels;
+    while (Ls > 0 && fp_.level_ptr[Ls] - fp_.level_ptr[Ls - 1] <= kBackwardTopFronts) --Ls;
+    if (fp_.num_levels - Ls >= 2) {
+      std::vector<int32_t> bounds;
+      for (int32_t L = fp_.num_levels; L >= Ls; --L) bounds.push_back(fp_.level_ptr[L]);
+      d.bw_bounds.upload(bounds);
+      d.bw_nlev = fp_.num_levels - Ls;
+      LevelLaunch& t = d.bw_top;
+      t.begin = fp_.level_ptr[Ls];
+      t.count = fp_.P - t.begin;
+      for (int32_t q = t.begin; q < fp_.P; ++q) {
+        const int32_t f = fp_.level_fronts[q];
+        t.max_fsz = std::max(t.max_fsz, fp_.fsz[f]);
+        t.max_nc = std::max(t.max_nc, fp_.nc[f]);
+      }
+      d.bw_first = 0;
+      while (d.bw_first < (int)d.levels.size() && d.levels[d.bw_first].begin < t.begin) ++d.bw_first;
+    }
+  }
   // source lists in launch order, each padded to its launch's longest
   {
     std::vector<long long> psrc;
@@ -607,13 +638,29 @@ void Engine::backward_all(cudaStream_t s) {
   a.Y = d.Y.as<T>();
   a.X = d.X.as<T>();
   stage_begin(3, s);
-  for (int L = (int)d.levels.size() - 1; L >= 0; --L) {
+  const int64_t n = backward_levels<T>(a, s);
+  launches_ += n;
+  d.stage_launches[3] += n;
+  stage_end(3, s);
+}
+
+// Backward substitution over the whole tree, root first: the narrow top in
+// one launch, then level by level.  Returns the launches made.
+template <typename T>
+int64_t Engine::backward_levels(const SweepArgs<T>& a, cudaStream_t s) {
+  auto& d = *d_;
+  int64_t n = 0;
+  if (d.bw_nlev > 0) {
+    launch_backward_top<T>(d.bw_top, d.bw_bounds.as<int>(), d.bw_nlev, a, s);
+    debug_check(s, "backward tree top");
+    ++n;
+  }
+  for (int L = d.bw_first - 1; L >= 0; --L) {
     launch_backward_level<T>(d.levels[L], a, s);
     debug_check(s, "backward level");
-    ++launches_;
-    ++d.stage_launches[3];
+    ++n;
   }
-  stage_end(3, s);
+  return n;
 }
 
 template <typename T>
@@ -1143,7 +1190,7 @@ void Engine::solve_values(const void* d_rhs, int32_t rhs_is_double, void* d_x, i
     bk.U = d.U.as<T>();
     bk.Y = d.W.as<T>();
     bk.X = d.X.as<T>();
-    for (int L = (int)d.levels.size() - 1; L >= 0; --L) launch_backward_level<T>(d.levels[L], bk, s);
+    backward_levels<T>(bk, s);
     // x is indexed by columns: undo the column ordering
     launch_permuted_to_rows<T>(d.pl.iperm, (int)dim, (int)Bp, d.X.as<T>(), d.lam.as<double>(), s);
   };

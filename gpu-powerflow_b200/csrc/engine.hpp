@@ -16,6 +16,7 @@
 
 #include "analysis.hpp"
 #include "device_plan.cuh"
+#include "kernels.hpp"
 
 namespace cupf_b200 {
 
@@ -159,6 +160,8 @@ class Engine {
   void factor_all(cudaStream_t s, int store_l, const void* J);
   template <typename T>
   void backward_all(cudaStream_t s);
+  template <typename T>
+  int64_t backward_levels(const SweepArgs<T>& a, cudaStream_t s);
   template <typename T>
   void transpose_solve(const double* d_G, double* d_lam, cudaStream_t s);
 };

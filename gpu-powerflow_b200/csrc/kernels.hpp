@@ -108,6 +108,12 @@ template <typename T, typename TJ>
 void launch_factor_level(const LevelLaunch& lv, const FactorArgs<T, TJ>& a, cudaStream_t s);
 template <typename T>
 void launch_backward_level(const LevelLaunch& lv, const SweepArgs<T>& a, cudaStream_t s);
+// The narrow top levels as one launch (block = 32 scenarios walking the
+// levels root-down); lv_bounds: device array of nlev + 1 descending level
+// boundaries in level order; top: the levels' extent (max_fsz, max_nc).
+template <typename T>
+void launch_backward_top(const LevelLaunch& top, const int* lv_bounds, int nlev, const SweepArgs<T>& a,
+                         cudaStream_t s);
 template <typename T>
 void launch_ut_forward_level(const LevelLaunch& lv, const AdjointSweepArgs<T>& a, cudaStream_t s);
 // L y = P g for a rhs given after factorization (y written to a.W)

@@ -396,26 +396,20 @@ __global__ void __launch_bounds__(256)
 // (contiguous elements) and the x rows of its CB rows (gathered through
 // front_rows) with cp.async, then solves the nc pivots from shared memory.
 // ---------------------------------------------------------------------------
+// One front x 32 scenarios (starting at col0), by one warp, with its
+// staging area Us.
 template <typename T>
-__global__ void __launch_bounds__(256)
-    k_backward_level(DevPlan pl, int level_begin, int level_count, int groups, int Bp, int warp_elems,
-                     const T* __restrict__ U, const T* __restrict__ Y, T* __restrict__ X) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+__device__ __forceinline__ void backward_front(const DevPlan& pl, int q, size_t col0, int Bp, T* Us,
+                                               const T* __restrict__ U, const T* __restrict__ Y,
+                                               T* __restrict__ X) {
   constexpr int kPieces = kWarp * sizeof(T) / 16;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const long item = (long)blockIdx.x * (blockDim.x >> 5) + warp;
-  if (item >= (long)level_count * groups) return;
-  const int q = level_begin + (int)(item / groups);
-  const size_t col0 = (size_t)(item % groups) * kWarp;
+  const int lane = threadIdx.x & 31;
   const size_t b = col0 + lane;
-  chain_allow_next();
   const FrontMeta m = load_front_meta(pl.front_meta, q);
   const int fs = m.fs, nc = m.nc, uc = fs - nc;
   const int fr0 = m.fr0, first = m.first;
   const long long uo = m.uo;
-  chain_wait_previous();  // U, Y and the x of ancestors come from earlier kernels
-  T* Us = reinterpret_cast<T*>(smem_raw) + (size_t)warp * warp_elems * kWarp;  // [nc * fs][32]
-  T* Xs = Us + (size_t)nc * fs * kWarp;                                         // [fs][32]
+  T* Xs = Us + (size_t)nc * fs * kWarp;  // [fs][32]
   // U rows: contiguous elements uo .. uo + nc * fs
   for (int t = lane; t < nc * fs * kPieces; t += kWarp) {
     const int e = t / kPieces, piece = t % kPieces;
@@ -446,6 +440,46 @@ __global__ void __launch_bounds__(256)
       Xs[(size_t)k * kWarp + lane] = xk;
       X[(size_t)(first + k) * Bp + b] = xk;
     }
+  }
+  __syncwarp();  // the staging area is reused by the warp's next front
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256)
+    k_backward_level(DevPlan pl, int level_begin, int level_count, int groups, int Bp, int warp_elems,
+                     const T* __restrict__ U, const T* __restrict__ Y, T* __restrict__ X) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int warp = threadIdx.x >> 5;
+  const long item = (long)blockIdx.x * (blockDim.x >> 5) + warp;
+  if (item >= (long)level_count * groups) return;
+  const int q = level_begin + (int)(item / groups);
+  const size_t col0 = (size_t)(item % groups) * kWarp;
+  chain_allow_next();
+  chain_wait_previous();  // U, Y and the x of ancestors come from earlier kernels
+  T* Us = reinterpret_cast<T*>(smem_raw) + (size_t)warp * warp_elems * kWarp;  // [nc * fs][32]
+  backward_front<T>(pl, q, col0, Bp, Us, U, Y, X);
+}
+
+// The narrow top of the tree in one launch: block = one group of 32
+// scenarios, walking the levels from the root down; the warps of the block
+// share out each level's fronts and meet at a block barrier between levels
+// (the x a front reads come from its ancestors, written by this block).
+// lv_lo[t] .. lv_lo[t + 1]: level-order fronts of the t-th level from the
+// root (descending boundaries, nlev + 1 entries).
+template <typename T>
+__global__ void __launch_bounds__(256)
+    k_backward_top(DevPlan pl, const int* __restrict__ lv_bounds, int nlev, int Bp, int warp_elems,
+                   const T* __restrict__ U, const T* __restrict__ Y, T* __restrict__ X) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int W = blockDim.x >> 5, warp = threadIdx.x >> 5;
+  const size_t col0 = (size_t)blockIdx.x * kWarp;
+  chain_allow_next();
+  chain_wait_previous();
+  T* Us = reinterpret_cast<T*>(smem_raw) + (size_t)warp * warp_elems * kWarp;
+  for (int t = 0; t < nlev; ++t) {
+    const int hi = lv_bounds[t], lo = lv_bounds[t + 1];
+    for (int q = lo + warp; q < hi; q += W) backward_front<T>(pl, q, col0, Bp, Us, U, Y, X);
+    __syncthreads();
   }
 }
 
@@ -679,6 +713,7 @@ void launch_factor_t(const LevelLaunch& lv, const FactorArgs<T, TJ>& a, cudaStre
 template <typename T, typename TJ>
 void configure_front_kernels() {
   allow_full_smem(reinterpret_cast<const void*>(k_backward_level<T>));
+  allow_full_smem(reinterpret_cast<const void*>(k_backward_top<T>));
 #define CUPF_ALLOW(F)                                                                  \
   allow_full_smem(reinterpret_cast<const void*>(k_front_factor<T, TJ, F, true>));    \
   allow_full_smem(reinterpret_cast<const void*>(k_front_factor<T, TJ, F, false>));
@@ -720,6 +755,22 @@ void launch_backward_level(const LevelLaunch& lv, const SweepArgs<T>& a, cudaStr
   const unsigned blocks = (unsigned)((items + wpb - 1) / wpb);
   launch_chained(kern, dim3(blocks), dim3(wpb * kWarp), smem, s, "backward sweep", a.plan, lv.begin, lv.count,
                  a.groups, a.Bp, warp_elems, a.U, a.Y, a.X);
+}
+
+// The top levels [top.begin, top.begin + top.count) of the launch list given
+// by lv_bounds (device, descending level boundaries, nlev + 1 entries).
+template <typename T>
+void launch_backward_top(const LevelLaunch& top, const int* lv_bounds, int nlev, const SweepArgs<T>& a,
+                         cudaStream_t s) {
+  if (top.count == 0 || nlev == 0) return;
+  const int warp_elems = top.max_nc * top.max_fsz + top.max_fsz;
+  const size_t per_warp = (size_t)warp_elems * kWarp * sizeof(T);
+  const int wpb = (int)std::min<size_t>(4, kSmemLimit / per_warp);
+  if (wpb < 1) throw std::runtime_error("backward sweep: front exceeds shared memory");
+  auto kern = k_backward_top<T>;
+  allow_full_smem(reinterpret_cast<const void*>(kern));
+  launch_chained(kern, dim3((unsigned)a.groups), dim3(wpb * kWarp), per_warp * wpb, s, "backward sweep (tree top)",
+                 a.plan, lv_bounds, nlev, a.Bp, warp_elems, a.U, a.Y, a.X);
 }
 
 template <typename T>

@@ -6,6 +6,7 @@ namespace cupf_b200 {
 template void configure_front_kernels<double, double>();
 template void launch_factor_level<double, double>(const LevelLaunch&, const FactorArgs<double, double>&,
                                                   cudaStream_t);
+template void launch_backward_top<double>(const LevelLaunch&, const int*, int, const SweepArgs<double>&, cudaStream_t);
 template void launch_backward_level<double>(const LevelLaunch&, const SweepArgs<double>&, cudaStream_t);
 template void launch_ut_forward_level<double>(const LevelLaunch&, const AdjointSweepArgs<double>&, cudaStream_t);
 template void launch_l_forward_level<double>(const LevelLaunch&, const AdjointSweepArgs<double>&, cudaStream_t);
