@@ -511,7 +511,8 @@ pf_status pf_solve_batch_ybus_device(pf_handle h, const double* ybus_data, int64
 }
 
 pf_status pf_solve_batch_warm_device(pf_handle h, const double* sbus, int64_t sbus_stride, const double* V0,
-                                     int64_t V0_stride, const float* pred, int64_t pred_ld, int32_t batch,
+                                     int64_t V0_stride, const float* pred, int64_t pred_ld, const float* pred_scale,
+                                     const float* pred_shift, int32_t batch,
                                      const pf_nr_config* config, const pf_solve_options* solve_options,
                                      double* V_out, double* final_mismatch, void* stream, pf_adjoint_result* result) {
   if (!h || !h->eng) return PF_INVALID_ARGUMENT;
@@ -521,7 +522,10 @@ pf_status pf_solve_batch_warm_device(pf_handle h, const double* sbus, int64_t sb
       throw std::invalid_argument("stride must be at least n_bus (V0_stride 0 = one V0 row for every scenario)");
     const pf_nr_config cfg = config ? *config : pf_nr_config{1e-8, 50};
     const int prep = solve_options ? solve_options->prepare_adjoint_cache : 0;
-    const auto st = h->eng->solve_batch_warm_device(sbus, sbus_stride, V0, V0_stride, pred, pred_ld, batch,
+    if ((pred_scale == nullptr) != (pred_shift == nullptr))
+      throw std::invalid_argument("pred_scale and pred_shift must be given together");
+    const auto st = h->eng->solve_batch_warm_device(sbus, sbus_stride, V0, V0_stride, pred, pred_ld, pred_scale,
+                                                    pred_shift, batch,
                                                     cfg.tolerance, cfg.max_iter, prep, V_out, final_mismatch,
                                                     caller_stream(stream));
     if (result) {

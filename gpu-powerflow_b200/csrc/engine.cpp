@@ -770,6 +770,7 @@ SolveStats Engine::run_loop(double tol, int32_t max_iter, int32_t prepare_adjoin
   for (int b = 0; b < d.B; ++b) d.h_final[b] = 0.0;
   int completed = 0;
   double gmax = 0.0;
+  bool nonfinite = false;  // a tolerated scenario whose norm went non-finite
   for (int i = 0; i < 5; ++i) {
     d.stage_ms[i] = 0.0;
     d.stage_launches[i] = 0;
@@ -793,6 +794,7 @@ SolveStats Engine::run_loop(double tol, int32_t max_iter, int32_t prepare_adjoin
     CUPF_CUDA(cudaStreamSynchronize(s));
     completed = hc->completed;
     gmax = hc->gmax;
+    nonfinite = hc->nonfinite != 0;
     // first mismatch + test, then per update: the body, plus the closing
     // mismatch and test when the cap stopped the loop
     const int64_t updates = (gmax <= tol || hc->status) ? completed - 1 : completed;
@@ -811,6 +813,7 @@ SolveStats Engine::run_loop(double tol, int32_t max_iter, int32_t prepare_adjoin
     CUPF_CUDA(cudaMemcpyAsync(d.h_norm, d.norm.p, d.Bp * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
     CUPF_CUDA(cudaStreamSynchronize(s));
     gmax = 0.0;
+    nonfinite = false;
     bool finite = true;
     for (int b = 0; b < d.B; ++b) {
       double v;
@@ -819,6 +822,7 @@ SolveStats Engine::run_loop(double tol, int32_t max_iter, int32_t prepare_adjoin
       if (!std::isfinite(v)) {
         if (tolerate_nonfinite_) {  // warm-started solves: the scenario failed, its fallback solves it
           d.h_final[b] = std::numeric_limits<double>::infinity();
+          nonfinite = true;
           continue;
         }
         finite = false;
@@ -840,7 +844,7 @@ SolveStats Engine::run_loop(double tol, int32_t max_iter, int32_t prepare_adjoin
   CUPF_CUDA(cudaGetLastError());
   stats.iterations = completed;
   stats.max_final_mismatch = gmax;
-  stats.all_converged = (gmax <= tol) ? 1 : 0;
+  stats.all_converged = (gmax <= tol && !nonfinite) ? 1 : 0;
   if (prepare_adjoint) {
     // final-state factorization with L kept (newton_solver.cpp:388-491)
     CUPF_CUDA(cudaMemsetAsync(d.norm.p, 0, d.Bp * sizeof(unsigned long long), s));
@@ -926,7 +930,8 @@ SolveStats Engine::solve_batch_device(const double* d_sbus, int64_t sbus_stride,
 }
 
 SolveStats Engine::solve_batch_warm_device(const double* d_sbus, int64_t sbus_stride, const double* d_v0,
-                                           int64_t v0_stride, const float* d_pred, int64_t pred_ld, int32_t B,
+                                           int64_t v0_stride, const float* d_pred, int64_t pred_ld,
+                                           const float* d_scale, const float* d_shift, int32_t B,
                                            double tol, int32_t max_iter, int32_t prepare_adjoint, double* d_v_out,
                                            double* d_final_mismatch, cudaStream_t stream) {
   if (!d_pred) throw std::invalid_argument("solve_batch_warm: prediction must not be null");
@@ -937,7 +942,7 @@ SolveStats Engine::solve_batch_warm_device(const double* d_sbus, int64_t sbus_st
   use_scenario_ybus(nullptr, 0, B, s);
   const DevState st = d.state();
   launch_seed_state(d.g, st, d_sbus, sbus_stride, d_v0, v0_stride, s);
-  launch_apply_warm(d.g, st, d_pred, pred_ld, s);
+  launch_apply_warm(d.g, st, d_pred, pred_ld, d_scale, d_shift, s);
   // a poor prediction may send a scenario to infinity: it is reported as not
   // converged (final mismatch = inf) instead of failing the whole batch
   struct Tolerate {

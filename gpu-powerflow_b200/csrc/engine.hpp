@@ -79,7 +79,8 @@ class Engine {
                                 int64_t ybus_stride = 0);
   // solve_batch_device from a predicted state (Jacobian-row order, fp32)
   SolveStats solve_batch_warm_device(const double* d_sbus, int64_t sbus_stride, const double* d_v0, int64_t v0_stride,
-                                     const float* d_pred, int64_t pred_ld, int32_t B, double tol, int32_t max_iter,
+                                     const float* d_pred, int64_t pred_ld, const float* d_scale, const float* d_shift,
+                                     int32_t B, double tol, int32_t max_iter,
                                      int32_t prepare_adjoint, double* d_v_out, double* d_final_mismatch,
                                      cudaStream_t stream);
   // torch-style: Sbus = base - load, V0 = (va0, vm0); base/v0 shared [n] or

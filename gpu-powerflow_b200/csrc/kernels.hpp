@@ -133,7 +133,8 @@ void launch_seed_state(const DevGrid& g, const DevState& st, const double* sbus_
                        const double* v0_c, long long v0_stride, cudaStream_t s);
 void launch_pack_voltage(const DevGrid& g, const DevState& st, double* v_c, cudaStream_t s);
 // warm start from a prediction pred[B][ld] in Jacobian-row order (fp32)
-void launch_apply_warm(const DevGrid& g, const DevState& st, const float* pred, long long ld, cudaStream_t s);
+void launch_apply_warm(const DevGrid& g, const DevState& st, const float* pred, long long ld, const float* scale,
+                       const float* shift, cudaStream_t s);
 // torch-style inputs: base injection [n], loads [B][n], flat start [n]; dtype float or double
 void launch_set_inputs_from_load(const DevGrid& g, const DevState& st, const void* base_re, const void* base_im,
                                  const void* load_p, const void* load_q, const void* va0, const void* vm0,
@@ -169,6 +170,7 @@ struct LoopCtl {
   int tolerate = 0;   // a non-finite scenario norm ends that scenario (inf) instead of the solve
   int completed = 0;  // norm evaluations so far
   int status = 0;     // 1: a non-finite norm that was not tolerated
+  int nonfinite = 0;  // 1: some scenario's norm was non-finite (tolerated: that scenario failed)
   double gmax = 0.0;  // max over the batch of the last evaluated norms
 };
 // Reads the per-scenario norms of the last mismatch, records them as the

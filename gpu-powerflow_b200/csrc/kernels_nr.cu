@@ -313,7 +313,8 @@ __global__ void k_voltage_update(DevGrid g, DevPlan pl, DevState st, const T* __
 // Warm start: overwrite the seeded angles / magnitudes with a prediction
 // given in Jacobian-row order (pred[b][row]: Va at the angle rows of the PV
 // and PQ buses, Vm at the magnitude rows of the PQ buses) and rebuild V.
-__global__ void k_apply_warm(DevGrid g, DevState st, const float* __restrict__ pred, long long ld) {
+__global__ void k_apply_warm(DevGrid g, DevState st, const float* __restrict__ pred, long long ld,
+                             const float* __restrict__ scale, const float* __restrict__ shift) {
   const int lane = threadIdx.x, wy = threadIdx.y;
   const int Bp = st.Bp;
   const int b = blockIdx.y * kWarp + lane;
@@ -323,8 +324,8 @@ __global__ void k_apply_warm(DevGrid g, DevState st, const float* __restrict__ p
     if (fa < 0 && fm < 0) continue;
     const size_t o = (size_t)i * Bp + b;
     double va = st.va[o], vm = st.vm[o];
-    if (fa >= 0) va = (double)pred[bb * ld + fa];
-    if (fm >= 0) vm = (double)pred[bb * ld + fm];
+    if (fa >= 0) va = (double)(scale ? pred[bb * ld + fa] * scale[fa] + shift[fa] : pred[bb * ld + fa]);
+    if (fm >= 0) vm = (double)(scale ? pred[bb * ld + fm] * scale[fm] + shift[fm] : pred[bb * ld + fm]);
     st.va[o] = va;
     st.vm[o] = vm;
     double sn, cs;
@@ -531,13 +532,13 @@ __global__ void __launch_bounds__(kCheckThreads)
   }
   const int B = ctl->B, tolerate = ctl->tolerate;
   double m = 0.0;
-  int bad = 0;
+  int bad = 0;  // bit 0: a non-finite norm, bit 1: one that is not tolerated
   for (int b = threadIdx.x; b < B; b += blockDim.x) {
     const double v = __longlong_as_double((long long)norm_bits[b]);
     const bool finite = v == v && v <= 1.7976931348623157e308;
     if (!finite) {
       final_norm[b] = tolerate ? __longlong_as_double(0x7FF0000000000000ll) : v;
-      if (!tolerate) bad = 1;
+      bad |= tolerate ? 1 : 3;
       continue;
     }
     final_norm[b] = v;
@@ -562,8 +563,9 @@ __global__ void __launch_bounds__(kCheckThreads)
     const int done = ctl->completed + 1;
     ctl->completed = done;
     ctl->gmax = m;
-    if (bad) ctl->status = 1;
-    const bool stop = bad || m <= ctl->tol;
+    ctl->nonfinite = bad & 1;
+    if (bad & 2) ctl->status = 1;
+    const bool stop = (bad & 2) || m <= ctl->tol;
     cudaGraphSetConditional(h, stop ? 0u : 1u);
   }
 }
@@ -717,8 +719,9 @@ void launch_seed_state(const DevGrid& g, const DevState& st, const double* sbus_
   k_seed_state<<<grid, dim3(kWarp, kRows), 0, s>>>(g, st, sbus_c, sbus_stride, v0_c, v0_stride);
 }
 
-void launch_apply_warm(const DevGrid& g, const DevState& st, const float* pred, long long ld, cudaStream_t s) {
-  k_apply_warm<<<rows_grid(g.n_bus, st.Bp), dim3(kWarp, kRows), 0, s>>>(g, st, pred, ld);
+void launch_apply_warm(const DevGrid& g, const DevState& st, const float* pred, long long ld, const float* scale,
+                       const float* shift, cudaStream_t s) {
+  k_apply_warm<<<rows_grid(g.n_bus, st.Bp), dim3(kWarp, kRows), 0, s>>>(g, st, pred, ld, scale, shift);
 }
 
 void launch_pack_voltage(const DevGrid& g, const DevState& st, double* v_c, cudaStream_t s) {

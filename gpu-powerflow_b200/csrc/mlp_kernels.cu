@@ -247,7 +247,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
         for (int i = 0; i < 8; ++i) o[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
       } else {
-        __nv_bfloat16* aux = g.aux + (size_t)row * g.ldaux + col;
+        __nv_bfloat16* aux = g.aux ? g.aux + (size_t)row * g.ldaux + col : nullptr;
         __align__(16) __nv_bfloat16 ob[32];
         if (g.epi == EPI_BIAS_GELU) {
           __align__(16) __nv_bfloat16 zb[32];
@@ -257,8 +257,9 @@ __global__ void __launch_bounds__(kThreads, 1)
             zb[i] = __float2bfloat16(z);
             ob[i] = __float2bfloat16(gelu(z));
           }
+          if (aux)  // inference keeps no pre-activations
 #pragma unroll
-          for (int i = 0; i < 4; ++i) reinterpret_cast<uint4*>(aux)[i] = reinterpret_cast<const uint4*>(zb)[i];
+            for (int i = 0; i < 4; ++i) reinterpret_cast<uint4*>(aux)[i] = reinterpret_cast<const uint4*>(zb)[i];
         } else {  // EPI_DGELU
           __align__(16) __nv_bfloat16 zb[32];
 #pragma unroll
@@ -306,6 +307,35 @@ __global__ void k_standardize(const float* __restrict__ raw, const float* __rest
     const int k = (int)(i % width);
     const long long b = i / width;
     x[b * ldx + k] = __float2bfloat16(k < n_in ? (raw[b * n_in + k] - mean[k]) * inv_std[k] : 0.0f);
+  }
+}
+
+// Power-flow load features, standardized, straight from Sbus: column k is
+// Re(sgen_k - S_bk) for k < n, Im(sgen_{k-n} - S_b(k-n)) for n <= k < 2n,
+// extra[k - 2n] for the next n_extra columns (fixed inputs such as PV
+// setpoints), then zero padding to width.  Rows r >= B repeat row B - 1.
+__global__ void k_load_features(const double* __restrict__ sbus, long long sbus_stride, const double* __restrict__ sgen,
+                                const float* __restrict__ extra, int n, int n_extra, const float* __restrict__ mean,
+                                const float* __restrict__ inv_std, __nv_bfloat16* __restrict__ x, long long ldx,
+                                int B, int rows, int width) {
+  const int n_in = 2 * n + n_extra;
+  const long long total = (long long)rows * width;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(i % width);
+    const long long r = i / width;
+    const long long b = r < B ? r : B - 1;
+    float v = 0.0f;
+    if (k < n_in) {
+      double f;
+      if (k < n)
+        f = sgen[2 * k] - sbus[2 * (b * sbus_stride + k)];
+      else if (k < 2 * n)
+        f = sgen[2 * (k - n) + 1] - sbus[2 * (b * sbus_stride + k - n) + 1];
+      else
+        f = (double)extra[k - 2 * n];
+      v = ((float)f - mean[k]) * inv_std[k];
+    }
+    x[r * ldx + k] = __float2bfloat16(v);
   }
 }
 
@@ -452,8 +482,8 @@ int mlp_gemm_bf16(const void* A, long long lda, const void* B, long long ldb, in
       throw std::invalid_argument("mlp_gemm_bf16: M and N must be multiples of 128, K of 64");
     if (epi < EPI_F32 || epi > EPI_DGELU) throw std::invalid_argument("mlp_gemm_bf16: unknown epilogue");
     if ((epi == EPI_BIAS_F32 || epi == EPI_BIAS_GELU) && !bias) throw std::invalid_argument("mlp_gemm_bf16: bias missing");
-    if ((epi == EPI_BIAS_GELU || epi == EPI_DGELU) && (!aux || ldaux < N))
-      throw std::invalid_argument("mlp_gemm_bf16: aux missing");
+    if (epi == EPI_DGELU && (!aux || ldaux < N)) throw std::invalid_argument("mlp_gemm_bf16: aux missing");
+    if (epi == EPI_BIAS_GELU && aux && ldaux < N) throw std::invalid_argument("mlp_gemm_bf16: aux row stride < N");
     if (lda < K || ldb < K || ldo < N || lda % 8 || ldb % 8 || ldo % 8)
       throw std::invalid_argument("mlp_gemm_bf16: leading dimensions must be >= the row length and multiples of 8");
     if ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B) | reinterpret_cast<uintptr_t>(out)) & 15)
@@ -489,6 +519,20 @@ int mlp_standardize(const float* raw, const float* mean, const float* inv_std, v
     if (ldx < width || width < n_in) throw std::invalid_argument("mlp_standardize: need n_in <= width <= ldx");
     k_standardize<<<grid1d((long long)B * width), 256, 0, static_cast<cudaStream_t>(stream)>>>(
         raw, mean, inv_std, static_cast<__nv_bfloat16*>(x), ldx, B, n_in, width);
+  });
+}
+
+int mlp_load_features(const double* sbus, long long sbus_stride, const double* sgen, const float* extra, int n,
+                      int n_extra, const float* mean, const float* inv_std, void* x, long long ldx, int B, int rows,
+                      int width, void* stream) {
+  return guarded([&] {
+    if (!sbus || !sgen || !mean || !inv_std || !x || (n_extra > 0 && !extra))
+      throw std::invalid_argument("mlp_load_features: null pointer");
+    if (n <= 0 || n_extra < 0 || B <= 0 || rows < B || width < 2 * n + n_extra || ldx < width || sbus_stride < n)
+      throw std::invalid_argument("mlp_load_features: inconsistent sizes");
+    k_load_features<<<grid1d((long long)rows * width), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        sbus, sbus_stride, sgen, extra, n, n_extra, mean, inv_std, static_cast<__nv_bfloat16*>(x), ldx, B, rows,
+        width);
   });
 }
 

@@ -486,16 +486,22 @@ class NewtonSolver:
             fm.data_ptr(), C.c_void_p(stream), C.byref(raw)))
         return v_out, fm, raw.iterations
 
-    def solve_batch_warm_device(self, sbus, v0, pred, v_out=None, config=None, solve_options=None):
+    def solve_batch_warm_device(self, sbus, v0, pred, v_out=None, config=None, solve_options=None,
+                                pred_scale=None, pred_shift=None):
         """Device-resident solve from a predicted state: pred is a float32 CUDA
-        tensor [batch, >= dim_f] in Jacobian-row order (Va at the PV and PQ
-        angle rows, Vm at the PQ magnitude rows); v0 complex128 [n_bus] (one
-        row for every scenario) or [batch, n_bus] supplies the other buses."""
+        tensor [>= batch, >= dim_f] with unit column stride, in Jacobian-row
+        order (Va at the PV and PQ angle rows, Vm at the PQ magnitude rows),
+        mapped to the state by pred * pred_scale + pred_shift when those
+        (float32 [dim_f]) are given; v0 complex128 [n_bus] (one row for every
+        scenario) or [batch, n_bus] supplies the other buses.  Whether every
+        scenario converged is kept in self.last_all_converged."""
         import torch
 
         B, n = sbus.shape
-        if pred.dtype != torch.float32 or pred.dim() != 2 or pred.shape[0] != B or not pred.is_contiguous():
-            raise ValueError("pred must be a contiguous float32 tensor [batch, >= dim_f]")
+        if pred.dtype != torch.float32 or pred.dim() != 2 or pred.shape[0] < B or pred.stride(1) != 1:
+            raise ValueError("pred must be a float32 tensor [>= batch, >= dim_f] with unit column stride")
+        if (pred_scale is None) != (pred_shift is None):
+            raise ValueError("pred_scale and pred_shift go together")
         v0_stride = 0 if v0.dim() == 1 else n
         if v_out is None:
             v_out = torch.empty_like(sbus)
@@ -503,9 +509,12 @@ class NewtonSolver:
         stream = torch.cuda.current_stream(sbus.device).cuda_stream
         raw = _capi.PfAdjointResult()
         cfg, so = _nr_config(config), _solve_options(solve_options)
+        sc = pred_scale.data_ptr() if pred_scale is not None else None
+        sh = pred_shift.data_ptr() if pred_shift is not None else None
         _check(self._lib, self._h, self._lib.pf_solve_batch_warm_device(
-            self._h, sbus.data_ptr(), n, v0.data_ptr(), v0_stride, pred.data_ptr(), pred.shape[1], B, C.byref(cfg),
-            C.byref(so), v_out.data_ptr(), fm.data_ptr(), C.c_void_p(stream), C.byref(raw)))
+            self._h, sbus.data_ptr(), n, v0.data_ptr(), v0_stride, pred.data_ptr(), pred.stride(0), sc, sh, B,
+            C.byref(cfg), C.byref(so), v_out.data_ptr(), fm.data_ptr(), C.c_void_p(stream), C.byref(raw)))
+        self.last_all_converged = bool(raw.all_converged)
         return v_out, fm, raw.iterations
 
     def info(self) -> dict:

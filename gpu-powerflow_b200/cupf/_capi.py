@@ -69,7 +69,7 @@ EXPORTS = [
 # exported symbols of include/cupf_mlp.h (warm-start network kernels)
 MLP_EXPORTS = [
     "mlp_last_error", "mlp_gemm_bf16", "mlp_error_flag", "mlp_transpose_bf16", "mlp_standardize", "mlp_mse_grad",
-    "mlp_col_sum_bf16", "mlp_adam",
+    "mlp_col_sum_bf16", "mlp_adam", "mlp_load_features",
 ]
 
 _vp = C.c_void_p
@@ -108,7 +108,7 @@ def _declare(lib: C.CDLL) -> None:
                                  _vp, _vp, _vp], _i32),
         "pf_solve_batch_ybus_device": ([_vp, _vp, _i64, _vp, _i64, _vp, _i64, _i32, _p(PfNRConfig),
                                         _p(PfSolveOptions), _vp, _vp, _vp, _p(PfAdjointResult)], _i32),
-        "pf_solve_batch_warm_device": ([_vp, _vp, _i64, _vp, _i64, _vp, _i64, _i32, _p(PfNRConfig),
+        "pf_solve_batch_warm_device": ([_vp, _vp, _i64, _vp, _i64, _vp, _i64, _vp, _vp, _i32, _p(PfNRConfig),
                                         _p(PfSolveOptions), _vp, _vp, _vp, _p(PfAdjointResult)], _i32),
         "pf_solve_forward_device": ([_vp, _vp, _vp, _vp, _vp, _vp, _vp, _i32, _vp, _vp, _i32, _i32, C.c_char_p,
                                      _p(PfNRConfig), _p(PfSolveOptions), _vp, _p(PfAdjointResult)], _i32),
@@ -134,6 +134,7 @@ def _declare(lib: C.CDLL) -> None:
         "mlp_error_flag": ([_p(_i32), _i32], _i32),
         "mlp_transpose_bf16": ([_vp, _i64, _vp, _i32, _i32, _vp], _i32),
         "mlp_standardize": ([_vp, _vp, _vp, _vp, _i64, _i32, _i32, _i32, _vp], _i32),
+        "mlp_load_features": ([_vp, _i64, _vp, _vp, _i32, _i32, _vp, _vp, _vp, _i64, _i32, _i32, _i32, _vp], _i32),
         "mlp_mse_grad": ([_vp, _i32, _vp, _i32, _i32, _vp, _vp, _vp], _i32),
         "mlp_col_sum_bf16": ([_vp, _i32, _i32, _vp, _vp], _i32),
         "mlp_adam": ([_vp, _vp, _vp, _vp, _vp, _i64, C.c_float, C.c_float, C.c_float, C.c_float, _i32, C.c_float,

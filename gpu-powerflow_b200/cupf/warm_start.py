@@ -145,10 +145,13 @@ class MLP:
         return h["a"][i - 1]
 
     # -- passes --
-    def forward(self, h: dict):
-        """Forward pass on the standardized features in h['x']; fp32 [B, no] outputs."""
+    def forward(self, h: dict, keep_pre: bool = True):
+        """Forward pass on the standardized features in h['x']; fp32 [B, no]
+        outputs.  keep_pre=False (inference) skips storing the GELU
+        pre-activations that only the backward pass reads."""
         for i in range(self.layers):
-            self.gemm(self._layer_input(h, i), self.W16[i], h["a"][i], EPI_BIAS_GELU, bias=self.b[i], aux=h["z"][i])
+            self.gemm(self._layer_input(h, i), self.W16[i], h["a"][i], EPI_BIAS_GELU, bias=self.b[i],
+                      aux=h["z"][i] if keep_pre else None)
         self.gemm(self._layer_input(h, self.layers), self.W16[self.layers], h["p"], EPI_BIAS_F32,
                   bias=self.b[self.layers])
         return h["p"]
@@ -199,6 +202,18 @@ class MLP:
         x = h["x"]
         self._check(self.lib.mlp_standardize(_ptr(raw), _ptr(mean), _ptr(inv_std), _ptr(x), x.stride(0),
                                              raw.shape[0], self.n_in, self.k0, self._stream()))
+
+    def load_features(self, h: dict, sbus, sgen, extra, mean, inv_std) -> None:
+        """Standardized features of Sbus (complex128 [B, n]) straight into h['x']
+        (mlp_load_features: loads sgen - S, then the fixed extra inputs); the
+        rows past B repeat the last scenario."""
+        x = h["x"]
+        if sbus.stride(1) != 1:
+            sbus = sbus.contiguous()
+        B, n = sbus.shape
+        self._check(self.lib.mlp_load_features(_ptr(sbus), sbus.stride(0), _ptr(sgen), _ptr(extra), n, extra.numel(),
+                                               _ptr(mean), _ptr(inv_std), _ptr(x), x.stride(0), B, x.shape[0],
+                                               self.k0, self._stream()))
 
     def error_flag(self) -> int:
         v = C.c_int32(0)
@@ -329,17 +344,20 @@ class WarmStart:
         return self.history
 
     # -- inference --
-    def predict(self, sbus):
-        """Predicted Newton unknowns fp32 [B, n_out] (B padded to 128 internally)."""
-        t = self.torch
-        B = sbus.shape[0]
-        Bp = _round_up(B, 128)
-        raw = self.features(sbus)
-        if Bp != B:
-            raw = t.cat([raw, raw[-1:].expand(Bp - B, -1)]).contiguous()
+    def predict_standardized(self, sbus):
+        """Network output fp32 [B rounded up to 128, no], still standardized
+        (state = out * y_std + y_mean on the first n_out columns): the
+        features are built from Sbus by one kernel and no pre-activations
+        are kept."""
+        Bp = _round_up(sbus.shape[0], 128)
         h = self.mlp.buffers(Bp)
-        self.mlp.standardize(h, raw, self.x_mean, self.x_istd)
-        out = self.mlp.forward(h)
+        self.mlp.load_features(h, sbus, self.sgen, self.vm_pv, self.x_mean, self.x_istd)
+        return self.mlp.forward(h, keep_pre=False)
+
+    def predict(self, sbus):
+        """Predicted Newton unknowns fp32 [B, n_out]."""
+        B = sbus.shape[0]
+        out = self.predict_standardized(sbus)
         return (out[:B, : self.n_out] * self.y_std + self.y_mean).contiguous()
 
     def solve(self, solver, sbus, config=None):
@@ -347,10 +365,12 @@ class WarmStart:
         (V, final_mismatch, iterations_warm, n_fallback)."""
         import cupf
 
-        t = self.torch
         cfg = config or cupf.NRConfig()
-        pred = self.predict(sbus)
-        V, fm, it = solver.solve_batch_warm_device(sbus, self.v0, pred, config=cfg)
+        pred = self.predict_standardized(sbus)
+        V, fm, it = solver.solve_batch_warm_device(sbus, self.v0, pred, config=cfg, pred_scale=self.y_std,
+                                                   pred_shift=self.y_mean)
+        if solver.last_all_converged:  # known from the solve itself: no extra synchronisation
+            return V, fm, it, 0
         # (a non-finite prediction only makes its scenario fail and fall back)
         bad = (fm > cfg.tolerance).nonzero().flatten()
         nb = int(bad.numel())

@@ -248,9 +248,13 @@ pf_status pf_solve_batch_ybus_device(pf_handle h, const double* ybus_data, int64
  * started from a predicted state.  pred [batch][pred_ld] fp32 holds, in
  * Jacobian-row order, Va at the angle rows (PV then PQ buses) and Vm at the
  * magnitude rows (PQ buses); the other buses keep V0.  V0_stride 0 uses one
- * V0 row for every scenario. */
+ * V0 row for every scenario.  pred_scale / pred_shift (fp32 [dim_f] each,
+ * may be NULL together) map a standardized prediction to the state:
+ * value = pred * scale + shift per Jacobian row.  result->all_converged is 0
+ * whenever a scenario failed (final mismatch above tol or not finite). */
 pf_status pf_solve_batch_warm_device(pf_handle h, const double* sbus, int64_t sbus_stride, const double* V0,
-                                     int64_t V0_stride, const float* pred, int64_t pred_ld, int32_t batch,
+                                     int64_t V0_stride, const float* pred, int64_t pred_ld, const float* pred_scale,
+                                     const float* pred_shift, int32_t batch,
                                      const pf_nr_config* config, const pf_solve_options* solve_options,
                                      double* V_out, double* final_mismatch, void* stream, pf_adjoint_result* result);
 /* Replaces: NewtonSolver::solve_torch_forward (core/torch_bridge.cpp:309-482).

@@ -24,7 +24,8 @@ const char* mlp_last_error(void);
  * accumulate).  M and N multiples of 128, K a multiple of 64; row strides
  * lda, ldb, ldo (elements, multiples of 8, at least the row length); A, B and
  * out 16-byte aligned.  epi: 0 out = C (fp32); 1 out = C + bias (fp32);
- * 2 aux = C + bias, out = gelu(aux) (both bf16); 3 out = C * gelu'(aux)
+ * 2 aux = C + bias, out = gelu(aux) (both bf16; aux may be NULL when the
+ * pre-activations are not needed, as in inference); 3 out = C * gelu'(aux)
  * (bf16).  aux has row stride ldaux. */
 int mlp_gemm_bf16(const void* A, long long lda, const void* B, long long ldb, int M, int N, int K, int epi,
                   void* out, long long ldo, const float* bias, void* aux, long long ldaux, void* stream);
@@ -37,6 +38,15 @@ int mlp_transpose_bf16(const void* in, long long ld, void* out, int rows, int co
  * n_in <= k < width; x has row stride ldx >= width, raw [B][n_in] fp32. */
 int mlp_standardize(const float* raw, const float* mean, const float* inv_std, void* x, long long ldx, int B,
                     int n_in, int width, void* stream);
+/* Standardized power-flow load features straight from Sbus (complex128
+ * [B][sbus_stride]) and the grid's generation sgen (complex128 [n]):
+ * x[r][k] = bf16((f_k - mean[k]) * inv_std[k]) with f_k = Re(sgen_k - S_rk)
+ * for k < n, Im(sgen - S) at k - n for n <= k < 2n, extra[k - 2n] for the
+ * next n_extra columns; 0 up to width.  Rows B <= r < rows repeat row B - 1.
+ * x has row stride ldx >= width. */
+int mlp_load_features(const double* sbus, long long sbus_stride, const double* sgen, const float* extra, int n,
+                      int n_extra, const float* mean, const float* inv_std, void* x, long long ldx, int B, int rows,
+                      int width, void* stream);
 /* Mean-squared error on the first n_out of ld columns: grad (bf16 [B][ld]) and
  * *loss += mean squared difference (fp32, may be NULL). */
 int mlp_mse_grad(const float* pred, int ld, const float* target, int n_out, int B, void* grad, float* loss,

@@ -169,12 +169,41 @@ def test_warm_entry_point_exact_prediction_and_failed_row(torch):
     cfg8 = cupf.NRConfig(tolerance=1e-5, max_iter=10)
     Vw, fmw, itw = s.solve_batch_warm_device(S, v0, pred, config=cfg8)
     assert itw == 1 and bool((fmw <= 1e-5).all())
+    # the same prediction given standardized, with its scale and shift
+    mean, std = pred.mean(0), pred.std(0).clamp_min(1e-6)
+    z = ((pred - mean) / std).contiguous()
+    Vz, fmz, itz = s.solve_batch_warm_device(S, v0, z, config=cfg8, pred_scale=std.contiguous(),
+                                            pred_shift=mean.contiguous())
+    assert itz == 1 and bool((fmz <= 1e-5).all()) and s.last_all_converged
     pred[3, 5] = float("nan")
     Vw, fmw, itw = s.solve_batch_warm_device(S, v0, pred, config=cfg8)
     assert np.isinf(fmw[3].item())
+    assert not s.last_all_converged  # a failed scenario is never reported as converged
     ok = torch.ones(B, dtype=torch.bool, device="cuda")
     ok[3] = False
     assert bool((fmw[ok] <= 1e-5).all())
+
+
+def test_load_features_match_the_torch_features(torch):
+    """mlp_load_features builds, from Sbus, exactly the standardized bf16
+    inputs that the torch feature path plus mlp_standardize produce."""
+    from cupf import grids as G
+    from cupf.warm_start import WarmStart
+
+    g = G.grid_118()
+    ws = WarmStart(g, hidden=128, layers=1, seed=0)
+    B = 100  # padded to 128 inside; the padding rows repeat the last scenario
+    S = torch.tensor(g.scenarios(B, seed=7), device="cuda")
+    raw = ws.features(S)
+    ws.x_mean = raw.mean(0)
+    ws.x_istd = 1.0 / raw.std(0).clamp_min(1e-6)
+    h = ws.mlp.buffers(128)
+    ref = torch.cat([raw, raw[-1:].expand(28, -1)]).contiguous()
+    ws.mlp.standardize(h, ref, ws.x_mean, ws.x_istd)
+    a = h["x"].clone()
+    h["x"].zero_()
+    ws.mlp.load_features(h, S, ws.sgen, ws.vm_pv, ws.x_mean, ws.x_istd)
+    assert torch.equal(h["x"], a)
 
 
 def test_device_entry_points_follow_the_callers_stream(torch):
