@@ -296,3 +296,42 @@ def test_jacobian_kinds_match_oracle(oracle, kind):
     for b in (0, 39):
         ref = oracle.solve(g, S[b], g.v0, tol=1e-12, max_iter=30)["V"]
         assert np.abs(r.V_numpy[b] - ref).max() <= 1e-8
+
+
+def test_graph_loop_capped_and_failed_scenarios_match_stream_mode():
+    """The device-side Newton loop (one graph per solve, conditional WHILE
+    node) keeps the host loop's semantics: with the iteration cap reached it
+    reports the cap, the last evaluated norms and the state after the last
+    update; a warm-started scenario whose state goes non-finite fails alone
+    (final mismatch inf) and the solve reports not all converged."""
+    import torch
+
+    g = G.grid_2000()
+    S, V0 = g.scenarios(40, seed=45), g.flat_start(40)
+    for mi in (1, 2, 3):
+        a = solve(make_solver(g, cupf.ComputePolicy.Mixed), g, S, V0, cfg(1e-8, mi))
+        b = solve(make_solver(g, cupf.ComputePolicy.Mixed, graph=True), g, S, V0, cfg(1e-8, mi))
+        assert np.array_equal(a.iterations_numpy, b.iterations_numpy) and (b.iterations_numpy == mi).all()
+        assert np.array_equal(a.final_mismatch_numpy, b.final_mismatch_numpy)
+        assert np.array_equal(a.V_numpy, b.V_numpy)
+        assert not b.converged_numpy.any()
+    dS = torch.tensor(S, device="cuda")
+    v0 = torch.tensor(g.v0, device="cuda")
+    pvpq = torch.tensor(np.concatenate([g.pv, g.pq]), device="cuda")
+    pq = torch.tensor(g.pq, device="cuda")
+    ref, _, _ = make_solver(g, cupf.ComputePolicy.FP64).solve_batch_device(
+        dS, torch.tensor(V0, device="cuda"), config=cfg(1e-10, 20))
+    pred = torch.cat([torch.angle(ref)[:, pvpq], torch.abs(ref)[:, pq]], 1).float().contiguous()
+    pred[7, 3] = float("nan")
+    out = {}
+    for graph in (False, True):
+        s = make_solver(g, cupf.ComputePolicy.Mixed, graph=graph)
+        V, fm, it = s.solve_batch_warm_device(dS, v0, pred, config=cfg(1e-8, 10))
+        out[graph] = (V, fm, it, s.last_all_converged)
+    for graph in (False, True):
+        V, fm, it, allc = out[graph]
+        assert np.isinf(fm[7].item()) and not allc
+        ok = torch.ones(40, dtype=torch.bool, device="cuda")
+        ok[7] = False
+        assert bool((fm[ok] <= 1e-8).all())
+    assert torch.equal(out[False][1], out[True][1]) and out[False][2] == out[True][2]
