@@ -204,7 +204,9 @@ def run_engine(args) -> None:
         warm_info = {"train_scenarios": int(X.shape[0]), "drawn": args.train, "load_range": [0.7, 1.3],
                      "epochs": args.epochs, "generate_s": round(t1 - t0, 2),
                      "train_s": round(time.perf_counter() - t1, 2), "final_train_loss": hist[-1],
-                     "net": "loads+PV setpoints 4400 -> 3 x 1024 GELU -> 3598 (+ input skip into the output layer)"}
+                     "net": "loads+PV setpoints 4400 -> 3 x 1024 GELU -> 3598 (+ input skip into the output layer)",
+                     "output_layer": "least-squares refit on the trained hidden features; inference with split "
+                                     "bf16 hi+lo weights"}
         del X, Y, keep
 
     def step_flat(solver):

@@ -16,6 +16,11 @@
 //                   EPI_BIAS_F32   out = acc + bias                  (fp32)
 //                   EPI_BIAS_GELU  z = acc + bias; aux = z; out = gelu(z)  (bf16)
 //                   EPI_DGELU      out = acc * gelu'(aux)            (bf16)
+//                 With a_kblocks > 0 the A tile of k-block kb is A's k-block
+//                 kb mod a_kblocks: B = [B_hi | B_lo] (2K columns) against A
+//                 (K columns) gives A (B_hi + B_lo)^T in one accumulator,
+//                 the split-weight output layer (bf16 hi + bf16 lo carry
+//                 about 16 mantissa bits of the fp32 weights).
 //                 Every mbarrier wait is bounded; on a timeout the kernel
 //                 raises the error flag, still waits (bounded) for its own
 //                 MMAs and frees its TMEM before returning.
@@ -161,6 +166,7 @@ struct GemmArgs {
   __nv_bfloat16* aux;  // [M][ldaux] pre-activations (written by EPI_BIAS_GELU, read by EPI_DGELU)
   long long ldaux;
   int epi;
+  int a_kblocks;  // > 0: A's k-block index wraps modulo a_kblocks (split-weight B)
   int* error;
 };
 
@@ -203,7 +209,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         break;
       }
       mbar_expect_tx(full + s, 2 * kTileBytes);
-      tma_load_2d(sA + s * kTileBytes, &ta, kb * kBK, m0, full + s);
+      const int ka = g.a_kblocks > 0 ? kb % g.a_kblocks : kb;
+      tma_load_2d(sA + s * kTileBytes, &ta, ka * kBK, m0, full + s);
       tma_load_2d(sB + s * kTileBytes, &tb, kb * kBK, n0, full + s);
     }
   } else if (threadIdx.x == 32) {
@@ -490,7 +497,26 @@ int mlp_gemm_bf16(const void* A, long long lda, const void* B, long long ldb, in
       throw std::invalid_argument("mlp_gemm_bf16: operands must be 16-byte aligned");
     configure_gemm();
     const CUtensorMap ta = make_map(A, M, K, lda), tb = make_map(B, N, K, ldb);
-    GemmArgs g{M, N, K, out, ldo, bias, static_cast<__nv_bfloat16*>(aux), ldaux, epi, error_flag()};
+    GemmArgs g{M, N, K, out, ldo, bias, static_cast<__nv_bfloat16*>(aux), ldaux, epi, 0, error_flag()};
+    k_gemm_bf16<<<dim3(N / kBN, M / kBM), kThreads, kGemmSmem, static_cast<cudaStream_t>(stream)>>>(ta, tb, g);
+  });
+}
+
+int mlp_gemm_bf16_split(const void* A, long long lda, const void* B, long long ldb, int M, int N, int K, int epi,
+                        void* out, long long ldo, const float* bias, void* stream) {
+  return guarded([&] {
+    if (M <= 0 || N <= 0 || K <= 0 || M % kBM || N % kBN || K % kBK)
+      throw std::invalid_argument("mlp_gemm_bf16_split: M and N must be multiples of 128, K of 64");
+    if (epi != EPI_F32 && epi != EPI_BIAS_F32)
+      throw std::invalid_argument("mlp_gemm_bf16_split: only the fp32 epilogues keep the split's precision");
+    if (epi == EPI_BIAS_F32 && !bias) throw std::invalid_argument("mlp_gemm_bf16_split: bias missing");
+    if (lda < K || ldb < 2LL * K || ldo < N || lda % 8 || ldb % 8 || ldo % 8)
+      throw std::invalid_argument("mlp_gemm_bf16_split: need lda >= K, ldb >= 2K, ldo >= N, all multiples of 8");
+    if ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B) | reinterpret_cast<uintptr_t>(out)) & 15)
+      throw std::invalid_argument("mlp_gemm_bf16_split: operands must be 16-byte aligned");
+    configure_gemm();
+    const CUtensorMap ta = make_map(A, M, K, lda), tb = make_map(B, N, 2 * K, ldb);
+    GemmArgs g{M, N, 2 * K, out, ldo, bias, nullptr, 0, epi, K / kBK, error_flag()};
     k_gemm_bf16<<<dim3(N / kBN, M / kBM), kThreads, kGemmSmem, static_cast<cudaStream_t>(stream)>>>(ta, tb, g);
   });
 }

@@ -42,7 +42,13 @@ class MLP:
     Hidden layers: a_{l+1} = gelu(a_l W_l^T + b_l).  With skip=True the output
     layer reads [a_L | x] (the last hidden activation next to the standardized
     input), so the dominant, nearly linear part of the load-to-state map has a
-    direct path and the GELU stack learns the nonlinear remainder."""
+    direct path and the GELU stack learns the nonlinear remainder.
+
+    Inference evaluates the output layer with split weights, W = hi + lo with
+    hi = bf16(W) and lo = bf16(W - hi), in one GEMM (mlp_gemm_bf16_split).
+    Rounding the output weights to bf16 alone adds independent noise to every
+    bus's predicted angle; Newton's mismatch sees that noise across every
+    branch, while the network's smooth, large-scale error costs it little."""
 
     def __init__(self, n_in: int, n_out: int, hidden: int = 1024, layers: int = 3, seed: int = 0,
                  device=None, skip: bool = True):
@@ -85,6 +91,9 @@ class MLP:
         self._refresh_transposes()
         self.step = 0
         self._bufs: dict[int, dict] = {}
+        self.split_out = True        # inference: output layer with hi + lo weights
+        self.Wsplit16 = None         # [no, 2 cat_w] bf16: [hi | lo] of the fp32 output weights
+        self._split_stale = True
 
     # -- low-level wrappers --
     def _stream(self):
@@ -105,6 +114,33 @@ class MLP:
                                            out.stride(0), _ptr(bias) if bias is not None else None,
                                            _ptr(aux) if aux is not None else None,
                                            aux.stride(0) if aux is not None else 0, self._stream()))
+
+    def gemm_split(self, A, Wsplit, out, bias) -> None:
+        """out = A (W_hi + W_lo)^T + bias, fp32; Wsplit [N, 2K] holds [hi | lo]."""
+        M, K = A.shape
+        N = Wsplit.shape[0]
+        if Wsplit.shape[1] != 2 * K or A.stride(1) != 1 or Wsplit.stride(1) != 1 or out.stride(1) != 1:
+            raise ValueError("gemm_split: need A [M, K] and Wsplit [N, 2K] with unit column stride")
+        self._check(self.lib.mlp_gemm_bf16_split(_ptr(A), A.stride(0), _ptr(Wsplit), Wsplit.stride(0), M, N, K,
+                                                 EPI_BIAS_F32, _ptr(out), out.stride(0), _ptr(bias), self._stream()))
+
+    def _build_split(self) -> None:
+        t = self.torch
+        W = self.W[self.layers]
+        hi = W.to(t.bfloat16)
+        lo = (W - hi.float()).to(t.bfloat16)
+        self.Wsplit16 = t.cat([hi, lo], dim=1).contiguous()
+        self._split_stale = False
+
+    def set_output_layer(self, W, b) -> None:
+        """Replace the output layer's first n_out rows (fp32 W [n_out, d_in],
+        b [n_out]); refreshes the bf16 copies and the split weights."""
+        L = self.layers
+        self.W[L][: self.n_out].copy_(W)
+        self.b[L][: self.n_out].copy_(b)
+        self.W16[L].copy_(self.W[L].to(self.torch.bfloat16))
+        self._refresh_transposes()
+        self._build_split()
 
     def transpose(self, a, out) -> None:
         r, c = a.shape
@@ -145,15 +181,27 @@ class MLP:
         return h["a"][i - 1]
 
     # -- passes --
-    def forward(self, h: dict, keep_pre: bool = True):
-        """Forward pass on the standardized features in h['x']; fp32 [B, no]
-        outputs.  keep_pre=False (inference) skips storing the GELU
-        pre-activations that only the backward pass reads."""
+    def hidden_layers(self, h: dict, keep_pre: bool = True) -> None:
+        """The GELU layers on the standardized features in h['x']; the output
+        layer's input is then _layer_input(h, layers)."""
         for i in range(self.layers):
             self.gemm(self._layer_input(h, i), self.W16[i], h["a"][i], EPI_BIAS_GELU, bias=self.b[i],
                       aux=h["z"][i] if keep_pre else None)
-        self.gemm(self._layer_input(h, self.layers), self.W16[self.layers], h["p"], EPI_BIAS_F32,
-                  bias=self.b[self.layers])
+
+    def forward(self, h: dict, keep_pre: bool = True):
+        """Forward pass on the standardized features in h['x']; fp32 [B, no]
+        outputs.  keep_pre=True (training) stores the GELU pre-activations
+        the backward pass reads and uses the bf16 output weights the
+        gradients are taken for; keep_pre=False (inference) stores none and
+        evaluates the output layer with split weights when split_out is set."""
+        self.hidden_layers(h, keep_pre)
+        L = self.layers
+        if not keep_pre and self.split_out:
+            if self._split_stale:
+                self._build_split()
+            self.gemm_split(self._layer_input(h, L), self.Wsplit16, h["p"], self.b[L])
+        else:
+            self.gemm(self._layer_input(h, L), self.W16[L], h["p"], EPI_BIAS_F32, bias=self.b[L])
         return h["p"]
 
     def backward(self, h: dict, target) -> None:
@@ -311,7 +359,11 @@ class WarmStart:
 
     # -- training --
     def fit(self, X, Y, epochs: int = 10, batch: int = 1024, lr: float = 1e-3, lr_min: float = 1e-5,
-            seed: int = 0, log=None):
+            seed: int = 0, log=None, refit: bool = True):
+        """Adam on the mean-squared error of the standardized targets (cosine
+        learning rate from lr to lr_min), then, with refit, the output layer
+        solved in closed form on the trained hidden features
+        (refit_output)."""
         t = self.torch
         self.x_mean = X.mean(0)
         self.x_istd = 1.0 / X.std(0).clamp_min(1e-6)
@@ -341,7 +393,50 @@ class WarmStart:
                 log(f"epoch {ep}: loss {loss:.3e} ({time.perf_counter() - t0:.1f} s)")
         if self.mlp.error_flag():
             raise RuntimeError("warm-start GEMM reported a wait timeout")
+        if refit:
+            self.refit_output(X, Y)
         return self.history
+
+    def refit_output(self, X, Y, ridge: float = 1e-6, chunk: int = 8192) -> None:
+        """Least-squares output layer on the trained hidden features.
+
+        The hidden layers (the project's kernels, bf16) map every training
+        row to the output layer's input a = [a_L | x]; the output layer is
+        then the ridge solution of min ||[a 1] [W^T; b] - Y_std||^2, with the
+        normal equations accumulated and solved in FP64 by torch (a plain
+        library GEMM and solve, ridge = ridge x the mean diagonal).  Adam's
+        stochastic steps leave independent per-output noise in W that the
+        exact minimiser does not have; set_output_layer installs the result
+        as split weights for inference."""
+        t = self.torch
+        mlp = self.mlp
+        if self.y_mean is None:
+            raise RuntimeError("refit_output: fit the network first")
+        L = mlp.layers
+        h = mlp.buffers(chunk)
+        n = X.shape[0]
+        D = mlp.dims_in[L] + 1
+        f64 = t.float64
+        AtA = t.zeros(D, D, dtype=f64, device=self.dev)
+        AtY = t.zeros(D, self.n_out, dtype=f64, device=self.dev)
+        for c0 in range(0, n, chunk):
+            m = min(chunk, n - c0)
+            xb = X[c0:c0 + m]
+            if m < chunk:
+                xb = t.cat([xb, xb[-1:].expand(chunk - m, -1)])
+            mlp.standardize(h, xb.contiguous(), self.x_mean, self.x_istd)
+            mlp.hidden_layers(h, keep_pre=False)
+            A = t.cat([mlp._layer_input(h, L)[:m].to(f64), t.ones(m, 1, dtype=f64, device=self.dev)], dim=1)
+            AtA.addmm_(A.T, A)
+            AtY.addmm_(A.T, ((Y[c0:c0 + m] - self.y_mean) / self.y_std).to(f64))
+        if mlp.error_flag():
+            raise RuntimeError("warm-start GEMM reported a wait timeout")
+        d = AtA.diagonal()
+        AtA.diagonal().add_(ridge * float(d[d > 0].mean()))
+        sol = t.linalg.solve(AtA, AtY)
+        if not bool(t.isfinite(sol).all()):
+            raise RuntimeError("refit_output: the least-squares solve is not finite")
+        mlp.set_output_layer(sol[:-1].T.float(), sol[-1].float())
 
     # -- inference --
     def predict_standardized(self, sbus):

@@ -29,6 +29,13 @@ const char* mlp_last_error(void);
  * (bf16).  aux has row stride ldaux. */
 int mlp_gemm_bf16(const void* A, long long lda, const void* B, long long ldb, int M, int N, int K, int epi,
                   void* out, long long ldo, const float* bias, void* aux, long long ldaux, void* stream);
+/* Split-weight GEMM: out = A (B_hi + B_lo)^T (+ bias), fp32 out [M][ldo].
+ * A is [M][lda] bf16 with K columns; B is [N][ldb] bf16 holding B_hi in
+ * columns [0, K) and B_lo in [K, 2K) (B_lo = bf16(W - B_hi) of fp32 weights
+ * W), so the product carries about 16 mantissa bits of W at the cost of a
+ * GEMM with 2K.  epi: 0 (out = C) or 1 (out = C + bias). */
+int mlp_gemm_bf16_split(const void* A, long long lda, const void* B, long long ldb, int M, int N, int K, int epi,
+                        void* out, long long ldo, const float* bias, void* stream);
 /* Device error flag of the GEMM (1 or 2 after a bounded wait gave up); copied
  * to *out_host with a synchronising copy, optionally reset. */
 int mlp_error_flag(int* out_host, int reset);

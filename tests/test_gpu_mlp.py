@@ -235,3 +235,75 @@ def test_device_entry_points_follow_the_callers_stream(torch):
     pred.copy_(exact)              # queued behind the sleep
     Vw, fmw, itw = s.solve_batch_warm_device(S, v0, pred, config=cupf.NRConfig(tolerance=1e-6, max_iter=10))
     assert bool((fmw <= 1e-6).all()) and itw <= 2
+
+
+@pytest.mark.parametrize("M,N,K", [(128, 128, 64), (256, 384, 5504)])
+def test_split_gemm_carries_the_fp32_weights(torch, M, N, K):
+    """mlp_gemm_bf16_split: A (W_hi + W_lo)^T + bias within fp32 accumulation
+    of the fp64 product with the fp32 weights, where the bf16 weights alone
+    are off by their rounding."""
+    import ctypes as C
+    from cupf.warm_start import MLP, EPI_BIAS_F32, EPI_BIAS_GELU, _ptr
+
+    g = torch.Generator(device="cuda").manual_seed(M + K)
+    A = torch.randn(M, K, device="cuda", generator=g).to(torch.bfloat16)
+    W = torch.randn(N, K, device="cuda", generator=g) / K ** 0.5
+    bias = torch.randn(N, device="cuda", generator=g)
+    hi = W.to(torch.bfloat16)
+    Ws = torch.cat([hi, (W - hi.float()).to(torch.bfloat16)], 1).contiguous()
+    net = MLP(64, 64, hidden=128, layers=1)
+    out = torch.empty(M, N, device="cuda")
+    net.gemm_split(A, Ws, out, bias)
+    ref = (A.double() @ W.double().T + bias.double()).cpu().numpy()
+    err_split = _rel(out.cpu().numpy(), ref)
+    net.gemm(A, hi, out, EPI_BIAS_F32, bias=bias)
+    err_bf16 = _rel(out.cpu().numpy(), ref)
+    # hi + lo carries W to within 2^-16 relative per weight (about 5e-6 rms)
+    assert err_split < 3e-5 and err_bf16 > 30 * err_split, (err_split, err_bf16)
+    assert net.error_flag() == 0
+    rc = net.lib.mlp_gemm_bf16_split(_ptr(A), K, _ptr(Ws), 2 * K, M, N, K, EPI_BIAS_GELU, _ptr(out), N, _ptr(bias),
+                                     C.c_void_p(0))
+    assert rc != 0 and b"fp32 epilogues" in net.lib.mlp_last_error()
+
+
+def test_refit_output_solves_the_least_squares_problem(torch):
+    """refit_output: the output layer equals the FP64 ridge solution on the
+    hidden features the network's own kernels compute, lowers the training
+    error, and inference evaluates it through the split weights."""
+    import cupf
+    from cupf import grids as G
+    from cupf.warm_start import WarmStart
+
+    g = G.grid_118()
+    o = cupf.NewtonOptions()
+    o.backend = cupf.BackendKind.CUDA
+    o.compute = cupf.ComputePolicy.Mixed
+    o.custom.serial_nd = True
+    s = cupf.NewtonSolver(o)
+    s.initialize(g.indptr, g.indices, g.data, g.n_bus, g.n_bus, g.pv, g.pq)
+    ws = WarmStart(g, hidden=128, layers=2, seed=0)
+    X, Y, _ = ws.generate(s, 3000, seed=5)
+    ws.fit(X, Y, epochs=5, batch=512, lr=2e-3, refit=False)
+    net, L = ws.mlp, ws.mlp.layers
+    n = X.shape[0]
+    Bp = (n + 127) // 128 * 128
+    h = net.buffers(Bp)
+    net.standardize(h, torch.cat([X, X[-1:].expand(Bp - n, -1)]).contiguous(), ws.x_mean, ws.x_istd)
+    net.hidden_layers(h, keep_pre=False)
+    A = np.hstack([net._layer_input(h, L)[:n].double().cpu().numpy(), np.ones((n, 1))])
+    T = ((Y - ws.y_mean) / ws.y_std).double().cpu().numpy()
+    AtA = A.T @ A
+    d = np.diag(AtA)
+    AtA[np.diag_indices_from(AtA)] += 1e-6 * d[d > 0].mean()
+    sol = np.linalg.solve(AtA, A.T @ T)
+    before = float(((net.forward(h)[:n, : ws.n_out].double().cpu().numpy() - T) ** 2).mean())
+    ws.refit_output(X, Y)
+    Wr = net.W[L][: ws.n_out].double().cpu().numpy()
+    assert np.abs(Wr - sol[:-1].T).max() <= 1e-5 * np.abs(sol).max()
+    assert np.abs(net.b[L][: ws.n_out].double().cpu().numpy() - sol[-1]).max() <= 1e-5 * np.abs(sol).max()
+    p = net.forward(h, keep_pre=False)[:n, : ws.n_out].double().cpu().numpy()
+    exact = A @ sol
+    # split weights: within 2^-16 |w| per weight; a 4x margin for fp32 rounding
+    assert (np.abs(p - exact) <= 2.0 ** -14 * (np.abs(A) @ np.abs(sol)) + 1e-6).all()
+    assert float(((p - T) ** 2).mean()) < before
+
