@@ -6,12 +6,17 @@
 //
 //   k_gemm_bf16   C[M,N] = A[M,K] * B[N,K]^T, A and B bf16 and K-contiguous,
 //                 fp32 accumulation in tensor memory.  One CTA computes a
-//                 128 x 128 tile: a producer thread streams 128 x 64 tiles of
-//                 A and B into shared memory with TMA (128-byte swizzle,
-//                 4-stage mbarrier ring), an MMA thread issues tcgen05.mma
-//                 (M = 128, N = 128, K = 16 per instruction) into a 128-column
-//                 TMEM accumulator, and the four warps read the accumulator
-//                 back (tcgen05.ld 32x32b) for a fused epilogue:
+//                 128 x BN tile: a producer thread streams 128 x 64 tiles of
+//                 A and BN x 64 tiles of B into shared memory with TMA
+//                 (128-byte swizzle, mbarrier ring), an MMA thread issues
+//                 tcgen05.mma (M = 128, N = BN, K = 16 per instruction) into
+//                 a BN-column TMEM accumulator, and the four warps read the
+//                 accumulator back (tcgen05.ld 32x32b) for a fused epilogue.
+//                 Two shapes: BN = 128 with a 3-stage ring and two CTAs per
+//                 SM when the 128 x 128 tiles fill the 148 SMs (the second
+//                 CTA's loads overlap the first one's MMAs), else BN = 64
+//                 tiles, twice as many CTAs for the narrow 1024-wide
+//                 hidden layers.  Epilogues:
 //                   EPI_F32        out = acc                         (fp32)
 //                   EPI_BIAS_F32   out = acc + bias                  (fp32)
 //                   EPI_BIAS_GELU  z = acc + bias; aux = z; out = gelu(z)  (bf16)
@@ -47,10 +52,15 @@
 namespace cupf_b200 {
 namespace {
 
-constexpr int kBM = 128, kBN = 128, kBK = 64, kStages = 4, kThreads = 128;
-constexpr uint32_t kTileBytes = kBM * kBK * 2;  // 16 KB per operand tile (kBN == kBM)
+constexpr int kBM = 128, kBK = 64, kThreads = 128;
+constexpr uint32_t kTileA = kBM * kBK * 2;     // 16 KB A tile per stage
 constexpr long long kSpinLimit = 1ll << 22;    // mbarrier polls before a wait gives up
-constexpr size_t kGemmSmem = 1024 + 2 * kStages * kTileBytes + 256;
+
+// shared memory of one CTA: 1 KB alignment slack, the ring, the barriers
+template <int BN, int STAGES>
+constexpr size_t gemm_smem() {
+  return 1024 + (size_t)STAGES * (kTileA + (uint32_t)BN * kBK * 2) + 256;
+}
 
 enum { EPI_F32 = 0, EPI_BIAS_F32 = 1, EPI_BIAS_GELU = 2, EPI_DGELU = 3 };
 
@@ -170,60 +180,62 @@ struct GemmArgs {
   int* error;
 };
 
-__global__ void __launch_bounds__(kThreads, 1)
+template <int BN, int STAGES, int MINB>
+__global__ void __launch_bounds__(kThreads, MINB)
     k_gemm_bf16(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, GemmArgs g) {
+  constexpr uint32_t kTileB = (uint32_t)BN * kBK * 2;
   extern __shared__ unsigned char smem_raw[];
   unsigned char* base =
       reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   unsigned char* sA = base;
-  unsigned char* sB = base + kStages * kTileBytes;
-  uint64_t* full = reinterpret_cast<uint64_t*>(base + 2 * kStages * kTileBytes);
-  uint64_t* empty = full + kStages;
-  uint64_t* done = empty + kStages;
+  unsigned char* sB = base + STAGES * kTileA;
+  uint64_t* full = reinterpret_cast<uint64_t*>(base + STAGES * (kTileA + kTileB));
+  uint64_t* empty = full + STAGES;
+  uint64_t* done = empty + STAGES;
   uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int m0 = blockIdx.y * kBM, n0 = blockIdx.x * kBN;
+  const int m0 = blockIdx.y * kBM, n0 = blockIdx.x * BN;
   const int nk = g.K / kBK;
 
   if (threadIdx.x == 0) {
-    for (int s = 0; s < kStages; ++s) {
+    for (int s = 0; s < STAGES; ++s) {
       mbar_init(full + s, 1);
       mbar_init(empty + s, 1);
     }
     mbar_init(done, 1);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
-  if (warp == 0) tmem_alloc(tslot, kBN);
+  if (warp == 0) tmem_alloc(tslot, BN);
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tslot;
   bool ok = true;
 
   if (threadIdx.x == 0) {
-    // producer: stage s holds k-block kb; refill it once the MMAs of kb - kStages are done
+    // producer: stage s holds k-block kb; refill it once the MMAs of kb - STAGES are done
     for (int kb = 0; kb < nk; ++kb) {
-      const int s = kb % kStages;
-      if (kb >= kStages && !mbar_wait(empty + s, ((kb / kStages) - 1) & 1)) {
+      const int s = kb % STAGES;
+      if (kb >= STAGES && !mbar_wait(empty + s, ((kb / STAGES) - 1) & 1)) {
         ok = false;
         break;
       }
-      mbar_expect_tx(full + s, 2 * kTileBytes);
+      mbar_expect_tx(full + s, kTileA + kTileB);
       const int ka = g.a_kblocks > 0 ? kb % g.a_kblocks : kb;
-      tma_load_2d(sA + s * kTileBytes, &ta, ka * kBK, m0, full + s);
-      tma_load_2d(sB + s * kTileBytes, &tb, kb * kBK, n0, full + s);
+      tma_load_2d(sA + s * kTileA, &ta, ka * kBK, m0, full + s);
+      tma_load_2d(sB + s * kTileB, &tb, kb * kBK, n0, full + s);
     }
   } else if (threadIdx.x == 32) {
     // MMA issuer
-    constexpr uint32_t idesc = idesc_bf16(kBM, kBN);
+    constexpr uint32_t idesc = idesc_bf16(kBM, BN);
     for (int kb = 0; kb < nk; ++kb) {
-      const int s = kb % kStages;
-      if (!mbar_wait(full + s, (kb / kStages) & 1)) {
+      const int s = kb % STAGES;
+      if (!mbar_wait(full + s, (kb / STAGES) & 1)) {
         ok = false;
         break;
       }
       tc_fence_after();
-      const uint64_t da = smem_desc_sw128(sA + s * kTileBytes), db = smem_desc_sw128(sB + s * kTileBytes);
+      const uint64_t da = smem_desc_sw128(sA + s * kTileA), db = smem_desc_sw128(sB + s * kTileB);
 #pragma unroll
       for (int k = 0; k < kBK / 16; ++k)  // K = 16 per instruction: advance 32 bytes inside the swizzled row
         tc_mma(tmem, da + (uint64_t)(2 * k), db + (uint64_t)(2 * k), idesc, (kb > 0 || k > 0) ? 1u : 0u);
@@ -242,7 +254,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   } else {
     const int row = m0 + warp * 32 + lane;
     const uint32_t tl = tmem + ((uint32_t)(warp * 32) << 16);
-    for (int c0 = 0; c0 < kBN; c0 += 32) {
+    for (int c0 = 0; c0 < BN; c0 += 32) {
       float v[32];
       tmem_ld32(tl + (uint32_t)c0, v);
       const int col = n0 + c0;
@@ -282,7 +294,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 0) tmem_dealloc(tmem, kBN);
+  if (warp == 0) tmem_dealloc(tmem, BN);
 }
 
 // ---- element-wise / reduction kernels ----
@@ -415,12 +427,12 @@ EncodeTiled encoder() {
   return fn;
 }
 
-// [rows][k] bf16 with row stride ld, K contiguous, boxes of 128 rows x 64 elements, 128-byte swizzle
-CUtensorMap make_map(const void* ptr, int rows, int k, long long ld) {
+// [rows][k] bf16 with row stride ld, K contiguous, boxes of box_rows rows x 64 elements, 128-byte swizzle
+CUtensorMap make_map(const void* ptr, int rows, int k, long long ld, int box_rows) {
   CUtensorMap m;
   const cuuint64_t dims[2] = {(cuuint64_t)k, (cuuint64_t)rows};
   const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
-  const cuuint32_t box[2] = {(cuuint32_t)kBK, (cuuint32_t)kBM};
+  const cuuint32_t box[2] = {(cuuint32_t)kBK, (cuuint32_t)box_rows};
   const cuuint32_t estr[2] = {1, 1};
   const CUresult r = encoder()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(ptr), dims, strides, box,
                                estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
@@ -443,6 +455,18 @@ int* error_flag() {
   return f;
 }
 
+// the two tile shapes: wide grids, and grids with fewer 128 x 128 tiles than SMs
+constexpr int kWideBN = 128, kWideStages = 3, kWideMinBlocks = 2;
+constexpr int kNarrowBN = 64, kNarrowStages = 4, kNarrowMinBlocks = 2;
+constexpr int kSMs = 148;
+
+template <int BN, int STAGES, int MINB>
+void set_smem_attribute() {
+  const cudaError_t e = cudaFuncSetAttribute(k_gemm_bf16<BN, STAGES, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)gemm_smem<BN, STAGES>());
+  if (e != cudaSuccess) throw std::runtime_error(std::string("gemm smem attribute: ") + cudaGetErrorString(e));
+}
+
 void configure_gemm() {
   static std::mutex mu;
   static std::map<int, bool> done;
@@ -450,9 +474,26 @@ void configure_gemm() {
   cudaGetDevice(&dev);
   std::lock_guard<std::mutex> lock(mu);
   if (done[dev]) return;
-  const cudaError_t e = cudaFuncSetAttribute(k_gemm_bf16, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem);
-  if (e != cudaSuccess) throw std::runtime_error(std::string("gemm smem attribute: ") + cudaGetErrorString(e));
+  set_smem_attribute<kWideBN, kWideStages, kWideMinBlocks>();
+  set_smem_attribute<kNarrowBN, kNarrowStages, kNarrowMinBlocks>();
   done[dev] = true;
+}
+
+template <int BN, int STAGES, int MINB>
+void launch_shape(const void* A, long long lda, int ka_cols, const void* B, long long ldb, GemmArgs g,
+                  cudaStream_t stream) {
+  const CUtensorMap ta = make_map(A, g.M, ka_cols, lda, kBM), tb = make_map(B, g.N, g.K, ldb, BN);
+  k_gemm_bf16<BN, STAGES, MINB><<<dim3(g.N / BN, g.M / kBM), kThreads, gemm_smem<BN, STAGES>(), stream>>>(ta, tb, g);
+}
+
+// A has ka_cols columns (== g.K unless A's k-blocks wrap); M, N multiples of 128
+void launch_gemm(const void* A, long long lda, int ka_cols, const void* B, long long ldb, const GemmArgs& g,
+                 cudaStream_t stream) {
+  configure_gemm();
+  if ((long long)(g.M / kBM) * (g.N / 128) >= kSMs)
+    launch_shape<kWideBN, kWideStages, kWideMinBlocks>(A, lda, ka_cols, B, ldb, g, stream);
+  else
+    launch_shape<kNarrowBN, kNarrowStages, kNarrowMinBlocks>(A, lda, ka_cols, B, ldb, g, stream);
 }
 
 unsigned grid1d(long long n) { return (unsigned)std::min<long long>((n + 255) / 256, 148LL * 16); }
@@ -485,7 +526,7 @@ const char* mlp_last_error() { return g_err.c_str(); }
 int mlp_gemm_bf16(const void* A, long long lda, const void* B, long long ldb, int M, int N, int K, int epi,
                   void* out, long long ldo, const float* bias, void* aux, long long ldaux, void* stream) {
   return guarded([&] {
-    if (M <= 0 || N <= 0 || K <= 0 || M % kBM || N % kBN || K % kBK)
+    if (M <= 0 || N <= 0 || K <= 0 || M % kBM || N % 128 || K % kBK)
       throw std::invalid_argument("mlp_gemm_bf16: M and N must be multiples of 128, K of 64");
     if (epi < EPI_F32 || epi > EPI_DGELU) throw std::invalid_argument("mlp_gemm_bf16: unknown epilogue");
     if ((epi == EPI_BIAS_F32 || epi == EPI_BIAS_GELU) && !bias) throw std::invalid_argument("mlp_gemm_bf16: bias missing");
@@ -495,17 +536,15 @@ int mlp_gemm_bf16(const void* A, long long lda, const void* B, long long ldb, in
       throw std::invalid_argument("mlp_gemm_bf16: leading dimensions must be >= the row length and multiples of 8");
     if ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B) | reinterpret_cast<uintptr_t>(out)) & 15)
       throw std::invalid_argument("mlp_gemm_bf16: operands must be 16-byte aligned");
-    configure_gemm();
-    const CUtensorMap ta = make_map(A, M, K, lda), tb = make_map(B, N, K, ldb);
     GemmArgs g{M, N, K, out, ldo, bias, static_cast<__nv_bfloat16*>(aux), ldaux, epi, 0, error_flag()};
-    k_gemm_bf16<<<dim3(N / kBN, M / kBM), kThreads, kGemmSmem, static_cast<cudaStream_t>(stream)>>>(ta, tb, g);
+    launch_gemm(A, lda, K, B, ldb, g, static_cast<cudaStream_t>(stream));
   });
 }
 
 int mlp_gemm_bf16_split(const void* A, long long lda, const void* B, long long ldb, int M, int N, int K, int epi,
                         void* out, long long ldo, const float* bias, void* stream) {
   return guarded([&] {
-    if (M <= 0 || N <= 0 || K <= 0 || M % kBM || N % kBN || K % kBK)
+    if (M <= 0 || N <= 0 || K <= 0 || M % kBM || N % 128 || K % kBK)
       throw std::invalid_argument("mlp_gemm_bf16_split: M and N must be multiples of 128, K of 64");
     if (epi != EPI_F32 && epi != EPI_BIAS_F32)
       throw std::invalid_argument("mlp_gemm_bf16_split: only the fp32 epilogues keep the split's precision");
@@ -514,10 +553,8 @@ int mlp_gemm_bf16_split(const void* A, long long lda, const void* B, long long l
       throw std::invalid_argument("mlp_gemm_bf16_split: need lda >= K, ldb >= 2K, ldo >= N, all multiples of 8");
     if ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B) | reinterpret_cast<uintptr_t>(out)) & 15)
       throw std::invalid_argument("mlp_gemm_bf16_split: operands must be 16-byte aligned");
-    configure_gemm();
-    const CUtensorMap ta = make_map(A, M, K, lda), tb = make_map(B, N, 2 * K, ldb);
     GemmArgs g{M, N, 2 * K, out, ldo, bias, nullptr, 0, epi, K / kBK, error_flag()};
-    k_gemm_bf16<<<dim3(N / kBN, M / kBM), kThreads, kGemmSmem, static_cast<cudaStream_t>(stream)>>>(ta, tb, g);
+    launch_gemm(A, lda, K, B, ldb, g, static_cast<cudaStream_t>(stream));
   });
 }
 

@@ -20,7 +20,8 @@ def _rel(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
 
 
-@pytest.mark.parametrize("M,N,K", [(128, 128, 64), (256, 384, 1024), (384, 128, 4480)])
+# 128 x 64 tiles below 148 tiles of 128 x 128, else 128 x 128 tiles two per SM
+@pytest.mark.parametrize("M,N,K", [(128, 128, 64), (256, 384, 1024), (384, 128, 4480), (1280, 2048, 320)])
 def test_gemm_f32_matches_torch(torch, M, N, K):
     from cupf.warm_start import MLP, EPI_F32, EPI_BIAS_F32
 
@@ -237,7 +238,7 @@ def test_device_entry_points_follow_the_callers_stream(torch):
     assert bool((fmw <= 1e-6).all()) and itw <= 2
 
 
-@pytest.mark.parametrize("M,N,K", [(128, 128, 64), (256, 384, 5504)])
+@pytest.mark.parametrize("M,N,K", [(128, 128, 64), (256, 384, 5504), (1024, 3712, 1024)])
 def test_split_gemm_carries_the_fp32_weights(torch, M, N, K):
     """mlp_gemm_bf16_split: A (W_hi + W_lo)^T + bias within fp32 accumulation
     of the fp64 product with the fp32 weights, where the bf16 weights alone
