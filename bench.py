@@ -468,9 +468,17 @@ def cpu_baseline(g, sample: int) -> dict:
     r = solver.solve_many(g, S, V0, TOL, MAX_ITER, threads)
     dt = time.perf_counter() - t0
     conv = int((r["final_mismatch"] <= TOL).sum())
+    # the same path on one core, on a smaller slice of the same scenarios
+    n1 = max(8, sample // 16)
+    t1 = time.perf_counter()
+    r1 = solver.solve_many(g, S[:n1], V0[:n1], TOL, MAX_ITER, 1)
+    dt1 = time.perf_counter() - t1
+    conv1 = int((r1["final_mismatch"] <= TOL).sum())
     return {"value": round(conv / dt, 2), "unit": UNIT, "cores": threads, "kind": kind,
             "sample": f"{sample} scenarios of the 2,000-bus workload, one solver per thread, "
-                      f"{'reference cpu-klu NewtonSolver (KLU replaced by the oracle LU)' if kind == 'reference' else 'oracle C port'}"}
+                      f"{'reference cpu-klu NewtonSolver (KLU replaced by the oracle LU)' if kind == 'reference' else 'oracle C port'}",
+            "single_core": {"value": round(conv1 / dt1, 2), "unit": UNIT, "cores": 1,
+                            "sample": f"the first {n1} of those scenarios on one thread"}}
 
 
 def run_reference(args) -> None:
