@@ -48,6 +48,7 @@ EngineConfig engine_config(const cls_config& c, int32_t compute, int32_t use_gra
   e.use_matching = c.matching;
   e.static_pivot = c.pivot_strategy == CLS_PIVOT_STATIC_DIAGONAL_SHIFT ? 1 : 0;
   e.shift_epsilon = c.shift_retry_epsilon;
+  e.autotune = c.autotune;
   e.use_cuda_graph = use_graph;
   return e;
 }
@@ -110,6 +111,15 @@ bool copy_plan_array(const Engine& e, const char* name, int32_t* out, int64_t ca
   CUPF_ARR("diag12", ja.diag12)
   CUPF_ARR("diag22", ja.diag22)
 #undef CUPF_ARR
+  if (n == "factor_level_warps") {  // the autotuner's choice per factor level (0: built-in rule)
+    const std::vector<int32_t> w = e.factor_level_warps();
+    if (len) *len = (int64_t)w.size();
+    if (out) {
+      if (cap < (int64_t)w.size()) return false;
+      std::copy(w.begin(), w.end(), out);
+    }
+    return true;
+  }
   if (!v) return false;
   if (len) *len = (int64_t)v->size();
   if (out) {
@@ -153,7 +163,8 @@ cls_status cls_create(const cls_config* config, cls_handle* out) {
   *out = nullptr;
   cls_config c{CLS_PRECISION_FP64, 0, CLS_PIVOT_STATIC_DIAGONAL_SHIFT, 1, 8, 1e-8};
   if (config) c = *config;
-  if ((c.matching != 0 && c.matching != 1) || c.max_panel_width < 1 || c.max_panel_width > 8)
+  if ((c.matching != 0 && c.matching != 1) || c.max_panel_width < 1 || c.max_panel_width > 8 ||
+      (c.autotune != 0 && c.autotune != 1))
     return CLS_INVALID_VALUE;
   auto* h = new (std::nothrow) cls_solver_s();
   if (!h) return CLS_ALLOCATION_FAILED;
@@ -344,6 +355,8 @@ pf_status pf_create(const pf_options* options, pf_handle* out) {
       throw std::invalid_argument("NewtonSolver: unsupported compute policy");
     if (o.custom.matching != 0 && o.custom.matching != 1)
       throw std::invalid_argument("NewtonSolver: matching must be None or Structural");
+    if (o.custom.autotune != 0 && o.custom.autotune != 1)
+      throw std::invalid_argument("NewtonSolver: autotune must be 0 or 1");
     if (o.cuda_jacobian < PF_JACOBIAN_EDGE || o.cuda_jacobian > PF_JACOBIAN_VERTEX_WARP)
       throw std::invalid_argument("NewtonSolver: cuda_jacobian must be Edge, EdgeAtomic or VertexWarp");
     cls_config c = o.custom;

@@ -143,6 +143,14 @@ struct Engine::Impl {
   int64_t graph_body_launches = 0;
   DBuf ctl, fin_dev;           // LoopCtl, final norms [Bp]
   LoopCtl* h_ctl = nullptr;    // pinned
+  // batch size and precision the factor launches were tuned for
+  int tuned_Bp = -1;
+  bool tuned_double = false;
+  void invalidate_graph() {
+    if (exec) cudaGraphExecDestroy(exec);
+    exec = nullptr;
+    graph_Bp = -1;
+  }
 
   ~Impl() {
     for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
@@ -599,8 +607,8 @@ void Engine::stage_times_ms(double* out5, int64_t* launches5) const {
 }
 
 template <typename T>
-void Engine::factor_all(cudaStream_t s, int store_l, const void* J) {
-  auto& d = *d_;
+FactorArgs<T, T> Engine::factor_args(int store_l, const void* J) const {
+  const auto& d = *d_;
   FactorArgs<T, T> a;
   a.plan = d.pl;
   a.groups = d.Bp / kWarp;
@@ -617,6 +625,76 @@ void Engine::factor_all(cudaStream_t s, int store_l, const void* J) {
   a.sing = d.sing.as<int>();
   a.front_scratch = d.front_scratch_elems ? d.front_scratch.as<T>() : nullptr;
   a.front_scratch_elems = d.front_scratch_elems;
+  return a;
+}
+
+// The autotuner of the factor launches.  Candidates: 1, 2, 4 and 8 warps per
+// block (each block factors one front for 32 scenarios; its warps split the
+// staging, the assembly and the non-pivot rows, so every element sees the
+// same operations in the same order whatever the split).  Each candidate, and
+// the built-in rule, factors the batch twice with an event after every level;
+// a level keeps the candidate with the shortest time if it beats the rule by
+// 3 %, else the rule.  Runs on the caller's stream outside any capture.
+template <typename T>
+void Engine::autotune_factor(cudaStream_t s, const void* J) {
+  auto& d = *d_;
+  const bool dbl = std::is_same<T, double>::value;
+  if (d.tuned_Bp == d.Bp && d.tuned_double == dbl) return;
+  const size_t nl = d.levels.size();
+  const FactorArgs<T, T> a = factor_args<T>(1, J);
+  constexpr int kCand[4] = {1, 2, 4, 8};
+  std::vector<double> t((size_t)5 * nl, 1e30);  // [candidate 0..3, rule = 4][level]
+  std::vector<cudaEvent_t> ev(nl + 1);
+  for (auto& e : ev) CUPF_CUDA(cudaEventCreate(&e));
+  try {
+    for (int rep = 0; rep < 2; ++rep) {
+      for (int c = 0; c < 5; ++c) {
+        for (auto& lv : d.levels) lv.warps = c < 4 ? kCand[c] : 0;
+        CUPF_CUDA(cudaEventRecord(ev[0], s));
+        for (size_t l = 0; l < nl; ++l) {
+          launch_factor_level<T, T>(d.levels[l], a, s);
+          CUPF_CUDA(cudaEventRecord(ev[l + 1], s));
+        }
+        CUPF_CUDA(cudaEventSynchronize(ev[nl]));
+        for (size_t l = 0; l < nl; ++l) {
+          float ms = 0.f;
+          CUPF_CUDA(cudaEventElapsedTime(&ms, ev[l], ev[l + 1]));
+          double& cell = t[(size_t)c * nl + l];
+          cell = std::min(cell, (double)ms);
+        }
+      }
+    }
+  } catch (...) {
+    for (auto& lv : d.levels) lv.warps = 0;
+    for (auto& e : ev) cudaEventDestroy(e);
+    throw;
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  for (size_t l = 0; l < nl; ++l) {
+    int best = -1;
+    double bt = t[(size_t)4 * nl + l] * 0.97;
+    for (int c = 0; c < 4; ++c)
+      if (t[(size_t)c * nl + l] < bt) {
+        bt = t[(size_t)c * nl + l];
+        best = c;
+      }
+    d.levels[l].warps = best >= 0 ? kCand[best] : 0;
+  }
+  d.tuned_Bp = d.Bp;
+  d.tuned_double = dbl;
+  d.invalidate_graph();  // a captured solve holds the old launch shapes
+}
+
+std::vector<int32_t> Engine::factor_level_warps() const {
+  std::vector<int32_t> w;
+  for (const auto& lv : d_->levels) w.push_back(lv.warps);
+  return w;
+}
+
+template <typename T>
+void Engine::factor_all(cudaStream_t s, int store_l, const void* J) {
+  auto& d = *d_;
+  const FactorArgs<T, T> a = factor_args<T>(store_l, J);
   stage_begin(2, s);
   for (const auto& lv : d.levels) {
     launch_factor_level<T, T>(lv, a, s);
@@ -765,6 +843,13 @@ SolveStats Engine::run_loop(double tol, int32_t max_iter, int32_t prepare_adjoin
   SolveStats stats;
   launches_ = 0;
   adjoint_ready_ = false;
+  if (cfg_.autotune && max_iter > 0 &&
+      (d.tuned_Bp != d.Bp || d.tuned_double != std::is_same<T, double>::value)) {
+    // tune on the Jacobian of the starting state (the loop recomputes it)
+    launch_ibus_mismatch(d.g, st, s);
+    launch_jacobian<T>(d.g, st, d.J.as<T>(), s);
+    autotune_factor<T>(s, d.J.p);
+  }
   CUPF_CUDA(cudaMemsetAsync(d.norm.p, 0, d.Bp * sizeof(unsigned long long), s));
   CUPF_CUDA(cudaMemsetAsync(d.sing.p, 0, d.Bp * sizeof(int), s));
   for (int b = 0; b < d.B; ++b) d.h_final[b] = 0.0;
@@ -1072,6 +1157,10 @@ void Engine::factorize_values(const void* d_values, int32_t values_is_double, in
   }
   CUPF_CUDA(cudaMemsetAsync(d.F.p, 0, (size_t)ja_.dim * d.Bp * 8, s));
   CUPF_CUDA(cudaMemsetAsync(d.Fp.p, 0, (size_t)ja_.dim * d.Bp * (dbl ? 8 : 4), s));
+  if (cfg_.autotune) {
+    if (dbl) autotune_factor<double>(s, d.J.p);
+    else autotune_factor<float>(s, d.J.p);
+  }
   CUPF_CUDA(cudaMemsetAsync(d.sing.p, 0, d.Bp * sizeof(int), s));
   if (dbl) factor_all<double>(s, 1, d.J.p);
   else factor_all<float>(s, 1, d.J.p);

@@ -34,6 +34,7 @@ struct EngineConfig {
   double shift_epsilon = 1e-8;    // threshold and replacement magnitude
   int32_t use_cuda_graph = 0;     // run each solve as one graph (device-side convergence test)
   int32_t adjoint_refine_steps = 2;
+  int32_t autotune = 0;           // tune the factor levels' warps per block per batch size
 };
 
 struct SolveStats {
@@ -111,6 +112,8 @@ class Engine {
 
   const JacobianAnalysis& jacobian() const { return ja_; }
   const SymbolicPlan& symbolic() const { return sp_; }
+  // warps per block of each factor level launch (0: the built-in rule)
+  std::vector<int32_t> factor_level_warps() const;
   const FactorProgram& program() const { return fp_; }
   const EngineConfig& config() const { return cfg_; }
   int32_t n_bus() const { return ja_.n_bus; }
@@ -159,6 +162,12 @@ class Engine {
   void iteration_tail(cudaStream_t s, int store_l);
   template <typename T>
   void factor_all(cudaStream_t s, int store_l, const void* J);
+  template <typename T>
+  FactorArgs<T, T> factor_args(int store_l, const void* J) const;
+  // times every factor level with each candidate block shape on the values J
+  // and keeps the fastest per level (once per batch size and precision)
+  template <typename T>
+  void autotune_factor(cudaStream_t s, const void* J);
   template <typename T>
   void backward_all(cudaStream_t s);
   template <typename T>

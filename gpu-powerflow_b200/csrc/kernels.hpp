@@ -20,6 +20,7 @@ struct LevelLaunch {
   // the launch starts at fe_base + (q - begin) * max_src), so a block finds
   // its list without reading the launch record first
   long long fe_base = 0;
+  int warps = 0;   // warps per block of the factor launch (0: the built-in rule)
 };
 
 template <typename T, typename TJ>

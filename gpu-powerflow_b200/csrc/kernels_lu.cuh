@@ -697,6 +697,7 @@ void launch_factor_t(const LevelLaunch& lv, const FactorArgs<T, TJ>& a, cudaStre
   // for fronts of at most 10 rows; eight warps: 0.891 ms)
   int warps = fmax <= 16 ? 2 : (fmax <= 24 ? 4 : 8);
   if (items < 4L * 148) warps = 8;
+  if (lv.warps > 0) warps = lv.warps;  // chosen by the engine's autotuner
   const size_t smem = sm.total();
   auto run = [&](auto kern) {
     allow_full_smem(reinterpret_cast<const void*>(kern));

@@ -13,7 +13,10 @@ Differences a user can see:
   * ``ComputePolicy.FP32`` runs the Mixed kernels (FP64 state and mismatch,
     FP32 Jacobian and factors); ``CustomPrecision.TF32`` runs the FP32 front
     kernels, whose fronts are too narrow for tensor cores;
-  * ``CustomSolverConfig.max_panel_width`` is limited to 1..8.
+  * ``CustomSolverConfig.max_panel_width`` is limited to 1..8;
+  * ``CustomSolverConfig.autotune`` (not in the reference, on by default)
+    times each factor level's block shape at the first solve of a batch size
+    and keeps the fastest; the results do not depend on it.
 """
 from __future__ import annotations
 
@@ -113,7 +116,7 @@ class CuDSSOptions(_Struct):
 class CustomSolverConfig(_Struct):
     _fields = {"precision": CustomPrecision.FP32, "matching": CustomMatchingMode["None"],
                "pivot_strategy": CustomPivotStrategy.StaticDiagonalShift, "serial_nd": False,
-               "max_panel_width": 8, "shift_retry_epsilon": 1.0e-8}
+               "max_panel_width": 8, "shift_retry_epsilon": 1.0e-8, "autotune": True}
 
 
 class NewtonOptions(_Struct):
@@ -261,7 +264,7 @@ def _check(lib, h, st: int) -> None:
 
 def _cls_config(c: CustomSolverConfig) -> _capi.ClsConfig:
     return _capi.ClsConfig(int(c.precision), int(c.matching), int(c.pivot_strategy), int(bool(c.serial_nd)),
-                           int(c.max_panel_width), float(c.shift_retry_epsilon))
+                           int(c.max_panel_width), float(c.shift_retry_epsilon), int(bool(c.autotune)))
 
 
 def _nr_config(cfg: NRConfig | None) -> _capi.PfNRConfig:

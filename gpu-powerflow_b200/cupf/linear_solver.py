@@ -23,13 +23,15 @@ class SolverConfig:
     """SolverConfig (solver.hpp:35-65); precision uses CustomPrecision values."""
 
     def __init__(self, precision: int = 0, pivot_strategy: int = 1, serial_nd: bool = True,
-                 max_panel_width: int = 8, shift_retry_epsilon: float = 1e-8, matching: int = 0):
+                 max_panel_width: int = 8, shift_retry_epsilon: float = 1e-8, matching: int = 0,
+                 autotune: bool = True):
         self.precision = int(precision)
         self.matching = int(matching)  # MatchingMode: 0 None, 1 Structural
         self.pivot_strategy = int(pivot_strategy)
         self.serial_nd = bool(serial_nd)
         self.max_panel_width = int(max_panel_width)
         self.shift_retry_epsilon = float(shift_retry_epsilon)
+        self.autotune = bool(autotune)  # per-level factor launch shapes timed at the first factorization
 
 
 class CustomSolverError(RuntimeError):
@@ -43,7 +45,7 @@ class LinearSolver:
         self._lib = _capi.load()
         c = config or SolverConfig()
         cfg = _capi.ClsConfig(c.precision, c.matching, c.pivot_strategy, int(c.serial_nd), c.max_panel_width,
-                              c.shift_retry_epsilon)
+                              c.shift_retry_epsilon, int(c.autotune))
         h = C.c_void_p()
         st = self._lib.cls_create(C.byref(cfg), C.byref(h))
         if st:

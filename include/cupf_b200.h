@@ -73,6 +73,11 @@ typedef struct {
   int32_t serial_nd;            /* 1 = one METIS_NodeND call, 0 = separator recursion */
   int32_t max_panel_width;      /* 1..8 (front kernels are built for panels of at most 8 pivots) */
   double shift_retry_epsilon;   /* static-shift threshold and magnitude */
+  int32_t autotune;             /* 1 = at the first factorization of each batch size, time every
+                                   factor level with 1, 2, 4 and 8 warps per block on the actual
+                                   values and keep the fastest per level (results do not change:
+                                   the warps of a block share one front's arithmetic, each
+                                   element's operation order is fixed); 0 = built-in rule */
 } cls_config;
 
 typedef struct cls_solver_s* cls_handle;

@@ -82,6 +82,7 @@ def test_option_defaults_mirror_reference():
     assert c.tolerance == 1e-8 and c.max_iter == 50
     cs = cupf.CustomSolverConfig()
     assert cs.max_panel_width == 8 and cs.shift_retry_epsilon == 1e-8
+    assert cs.autotune is True  # the engine's own option: per-level factor launch shapes
     assert cs.pivot_strategy == cupf.CustomPivotStrategy.StaticDiagonalShift
     so = cupf.SolveOptions()
     assert so.prepare_adjoint_cache is False

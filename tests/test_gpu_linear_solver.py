@@ -209,3 +209,27 @@ def test_pivot_strategy_none_keeps_small_pivots():
     assert not f0 and np.abs(x0 - exact).max() <= 1e-9 * np.abs(exact).max()
     x1, f1 = out[1]
     assert f1 and np.abs(x1 - exact).max() > 1e-6 * np.abs(exact).max()
+
+
+def test_autotuned_factorization_is_bit_identical():
+    """SolverConfig(autotune=True): the first factorization of a batch size
+    times the factor levels' block shapes on the given values and keeps the
+    fastest per level; the factors, and so the solutions, do not change."""
+    import torch
+
+    d, A = load("case1354pegase")
+    rng = np.random.default_rng(3)
+    B = 64
+    vals = batch_values(d, B, rng)
+    rhs = np.repeat(d["F"][None, :], B, axis=0) + 0.1 * rng.standard_normal((B, A.shape[0]))
+    out = []
+    for tune in (False, True):
+        ls = cupf.LinearSolver(cupf.SolverConfig(precision=int(cupf.CustomPrecision.FP32), serial_nd=True,
+                                                 autotune=tune))
+        ls.set_data(d["row_ptr"], d["col_idx"])
+        ls.analyze()
+        ls.setup(B)
+        for _ in range(2):
+            ls.factorize(torch.tensor(vals, dtype=torch.float32, device="cuda"))
+        out.append(ls.solve(torch.tensor(rhs, dtype=torch.float64, device="cuda")).cpu().numpy())
+    assert np.array_equal(out[0], out[1])

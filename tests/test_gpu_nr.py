@@ -19,12 +19,13 @@ GOLD = Path(__file__).resolve().parent / "golden"
 POLICIES = {"FP64": cupf.ComputePolicy.FP64, "FP32": cupf.ComputePolicy.FP32, "Mixed": cupf.ComputePolicy.Mixed}
 
 
-def make_solver(g, compute, graph=False, serial_nd=True):
+def make_solver(g, compute, graph=False, serial_nd=True, autotune=False):
     o = cupf.NewtonOptions()
     o.backend = cupf.BackendKind.CUDA
     o.compute = compute
     o.use_cuda_graph = graph
     o.custom.serial_nd = serial_nd
+    o.custom.autotune = autotune
     s = cupf.NewtonSolver(o)
     s.initialize(g.indptr, g.indices, g.data, g.n_bus, g.n_bus, g.pv, g.pq)
     return s
@@ -335,3 +336,24 @@ def test_graph_loop_capped_and_failed_scenarios_match_stream_mode():
         ok[7] = False
         assert bool((fm[ok] <= 1e-8).all())
     assert torch.equal(out[False][1], out[True][1]) and out[False][2] == out[True][2]
+
+
+@pytest.mark.parametrize("policy", ["FP64", "Mixed"])
+@pytest.mark.parametrize("graph", [False, True])
+def test_autotuned_factor_launches_give_identical_solves(policy, graph):
+    """CustomSolverConfig.autotune: the warps per block of every factor level
+    are timed and chosen at the first solve of each batch size; the solves
+    stay bit for bit those of the built-in rule."""
+    g = G.grid_2000()
+    S, V0 = g.scenarios(256, seed=77), g.flat_start(256)
+    base = make_solver(g, POLICIES[policy], graph)
+    tuned = make_solver(g, POLICIES[policy], graph, autotune=True)
+    assert not tuned.plan_array("factor_level_warps").any()  # nothing tuned before a solve
+    for B in (256, 96, 256):  # a new batch size tunes again
+        a = solve(base, g, S[:B], V0[:B], cfg())
+        b = solve(tuned, g, S[:B], V0[:B], cfg())
+        assert np.array_equal(a.V_numpy, b.V_numpy)
+        assert np.array_equal(a.final_mismatch_numpy, b.final_mismatch_numpy)
+        w = tuned.plan_array("factor_level_warps")
+        assert w.size > 0 and set(w.tolist()) <= {0, 1, 2, 4, 8}
+    assert not base.plan_array("factor_level_warps").any()
