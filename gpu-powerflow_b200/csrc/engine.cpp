@@ -632,9 +632,13 @@ FactorArgs<T, T> Engine::factor_args(int store_l, const void* J) const {
 // block (each block factors one front for 32 scenarios; its warps split the
 // staging, the assembly and the non-pivot rows, so every element sees the
 // same operations in the same order whatever the split).  Each candidate, and
-// the built-in rule, factors the batch twice with an event after every level;
-// a level keeps the candidate with the shortest time if it beats the rule by
-// 3 %, else the rule.  Runs on the caller's stream outside any capture.
+// the built-in rule, factors the batch three times with an event after every
+// level; a level keeps the candidate with the shortest time if it beats the
+// rule by 3 % and 0.5 us, else the rule.  Then the whole factorization is
+// timed as it runs in a solve (chained launches, no events between levels),
+// three times with the choice and three times with the rule; the choice is
+// kept only if it is at least 1 % faster.  Runs on the caller's stream
+// outside any capture.
 template <typename T>
 void Engine::autotune_factor(cudaStream_t s, const void* J) {
   auto& d = *d_;
@@ -647,7 +651,7 @@ void Engine::autotune_factor(cudaStream_t s, const void* J) {
   std::vector<cudaEvent_t> ev(nl + 1);
   for (auto& e : ev) CUPF_CUDA(cudaEventCreate(&e));
   try {
-    for (int rep = 0; rep < 2; ++rep) {
+    for (int rep = 0; rep < 3; ++rep) {
       for (int c = 0; c < 5; ++c) {
         for (auto& lv : d.levels) lv.warps = c < 4 ? kCand[c] : 0;
         CUPF_CUDA(cudaEventRecord(ev[0], s));
@@ -669,17 +673,43 @@ void Engine::autotune_factor(cudaStream_t s, const void* J) {
     for (auto& e : ev) cudaEventDestroy(e);
     throw;
   }
-  for (auto& e : ev) cudaEventDestroy(e);
+  std::vector<int> choice(nl, 0);
   for (size_t l = 0; l < nl; ++l) {
+    const double rule = t[(size_t)4 * nl + l];
     int best = -1;
-    double bt = t[(size_t)4 * nl + l] * 0.97;
+    double bt = std::min(rule * 0.97, rule - 0.5e-3);
     for (int c = 0; c < 4; ++c)
       if (t[(size_t)c * nl + l] < bt) {
         bt = t[(size_t)c * nl + l];
         best = c;
       }
-    d.levels[l].warps = best >= 0 ? kCand[best] : 0;
+    choice[l] = best >= 0 ? kCand[best] : 0;
   }
+  // the whole factorization as a solve runs it: the choice against the rule
+  double whole[2] = {1e30, 1e30};  // [rule, choice]
+  try {
+    for (int rep = 0; rep < 3; ++rep)
+      for (int v = 0; v < 2; ++v) {
+        for (size_t l = 0; l < nl; ++l) d.levels[l].warps = v ? choice[l] : 0;
+        CUPF_CUDA(cudaEventRecord(ev[0], s));
+        for (const auto& lv : d.levels) launch_factor_level<T, T>(lv, a, s);
+        CUPF_CUDA(cudaEventRecord(ev[1], s));
+        CUPF_CUDA(cudaEventSynchronize(ev[1]));
+        float ms = 0.f;
+        CUPF_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+        whole[v] = std::min(whole[v], (double)ms);
+      }
+  } catch (...) {
+    for (auto& lv : d.levels) lv.warps = 0;
+    for (auto& e : ev) cudaEventDestroy(e);
+    throw;
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  const bool keep = whole[1] < 0.99 * whole[0];
+  for (size_t l = 0; l < nl; ++l) d.levels[l].warps = keep ? choice[l] : 0;
+  if (debug_sync())
+    std::fprintf(stderr, "[cupf] factor autotune: rule %.3f ms, choice %.3f ms, %s\n", whole[0], whole[1],
+                 keep ? "kept" : "rule kept");
   d.tuned_Bp = d.Bp;
   d.tuned_double = dbl;
   d.invalidate_graph();  // a captured solve holds the old launch shapes
