@@ -308,3 +308,42 @@ def test_refit_output_solves_the_least_squares_problem(torch):
     assert (np.abs(p - exact) <= 2.0 ** -14 * (np.abs(A) @ np.abs(sol)) + 1e-6).all()
     assert float(((p - T) ** 2).mean()) < before
 
+
+
+def test_host_pipeline_matches_serial_solves(torch):
+    """cupf.streaming.HostPipeline: batches of different sizes from pinned
+    host memory, uploads and downloads overlapped with the solves, give the
+    results of solving each batch alone, bit for bit; a shared output buffer
+    ends with the last batch's results."""
+    import cupf
+    from cupf import grids as G
+    from cupf.streaming import HostPipeline
+
+    g = G.grid_118()
+    o = cupf.NewtonOptions()
+    o.backend = cupf.BackendKind.CUDA
+    o.compute = cupf.ComputePolicy.Mixed
+    o.use_cuda_graph = True
+    o.custom.serial_nd = True
+    s = cupf.NewtonSolver(o)
+    s.initialize(g.indptr, g.indices, g.data, g.n_bus, g.n_bus, g.pv, g.pq)
+    cfg = cupf.NRConfig(tolerance=1e-8, max_iter=10)
+    v0 = torch.tensor(g.v0, device="cuda")
+    sizes = [64, 33, 64, 7, 100]
+    ins = [torch.tensor(g.scenarios(b, seed=40 + i)).pin_memory() for i, b in enumerate(sizes)]
+
+    def solve(s_dev):
+        v, fm, _ = s.solve_batch_device(s_dev, v0[None, :].expand(s_dev.shape[0], -1).contiguous(), config=cfg)
+        return v, fm
+
+    V_out = [torch.empty(b, g.n_bus, dtype=torch.complex128).pin_memory() for b in sizes]
+    fm_out = [torch.empty(b, dtype=torch.float64).pin_memory() for b in sizes]
+    HostPipeline(solve).run(ins, V_out, fm_out)
+    for i, b in enumerate(sizes):
+        v, fm = solve(ins[i].cuda())
+        assert torch.equal(V_out[i], v.cpu()) and torch.equal(fm_out[i], fm.cpu())
+        assert bool((fm_out[i] <= 1e-8).all())
+    shared = torch.empty(64, g.n_bus, dtype=torch.complex128).pin_memory()
+    fms = [torch.empty(64, dtype=torch.float64).pin_memory() for _ in range(3)]
+    HostPipeline(solve).run([ins[0], ins[2], ins[0]], [shared] * 3, fms)
+    assert torch.equal(shared, V_out[0])
