@@ -111,8 +111,8 @@ bool copy_plan_array(const Engine& e, const char* name, int32_t* out, int64_t ca
   CUPF_ARR("diag12", ja.diag12)
   CUPF_ARR("diag22", ja.diag22)
 #undef CUPF_ARR
-  if (n == "factor_level_warps") {  // the autotuner's choice per factor level (0: built-in rule)
-    const std::vector<int32_t> w = e.factor_level_warps();
+  if (n == "factor_level_warps" || n == "backward_launch_warps") {  // the autotuner's choices (0: built-in rule)
+    const std::vector<int32_t> w = n == "factor_level_warps" ? e.factor_level_warps() : e.backward_launch_warps();
     if (len) *len = (int64_t)w.size();
     if (out) {
       if (cap < (int64_t)w.size()) return false;

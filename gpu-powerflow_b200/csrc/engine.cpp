@@ -143,9 +143,9 @@ struct Engine::Impl {
   int64_t graph_body_launches = 0;
   DBuf ctl, fin_dev;           // LoopCtl, final norms [Bp]
   LoopCtl* h_ctl = nullptr;    // pinned
-  // batch size and precision the factor launches were tuned for
-  int tuned_Bp = -1;
-  bool tuned_double = false;
+  // batch size and precision the factor and backward launches were tuned for
+  int tuned_Bp = -1, tuned_bw_Bp = -1;
+  bool tuned_double = false, tuned_bw_double = false;
   void invalidate_graph() {
     if (exec) cudaGraphExecDestroy(exec);
     exec = nullptr;
@@ -628,71 +628,62 @@ FactorArgs<T, T> Engine::factor_args(int store_l, const void* J) const {
   return a;
 }
 
-// The autotuner of the factor launches.  Candidates: 1, 2, 4 and 8 warps per
-// block (each block factors one front for 32 scenarios; its warps split the
-// staging, the assembly and the non-pivot rows, so every element sees the
-// same operations in the same order whatever the split).  Each candidate, and
-// the built-in rule, factors the batch three times with an event after every
-// level; a level keeps the candidate with the shortest time if it beats the
-// rule by 3 % and 0.5 us, else the rule.  Then the whole factorization is
-// timed as it runs in a solve (chained launches, no events between levels),
-// three times with the choice and three times with the rule; the choice is
-// kept only if it is at least 1 % faster.  Runs on the caller's stream
-// outside any capture.
-template <typename T>
-void Engine::autotune_factor(cudaStream_t s, const void* J) {
-  auto& d = *d_;
-  const bool dbl = std::is_same<T, double>::value;
-  if (d.tuned_Bp == d.Bp && d.tuned_double == dbl) return;
-  const size_t nl = d.levels.size();
-  const FactorArgs<T, T> a = factor_args<T>(1, J);
+namespace {
+
+// Chooses a block shape (warps per block) for each of n launches that run in
+// sequence on stream s.  set(i, w) gives launch i the shape w (0: its
+// built-in rule); launch(i) issues it.  Candidates 1, 2, 4 and 8 warps and
+// the rule each run the whole sequence three times with an event after every
+// launch; a launch keeps the fastest candidate if it beats the rule by 3 %
+// and by 0.5 us, else the rule.  Then the whole sequence is timed as a solve
+// runs it (chained launches, no events in between), three times with the
+// choice and three with the rule; the choice stays only if it is at least
+// 1 % faster.  Leaves the chosen shapes set; returns whether they were kept.
+template <typename Set, typename Launch>
+bool choose_block_shapes(size_t n, Set set, Launch launch, cudaStream_t s, const char* what) {
   constexpr int kCand[4] = {1, 2, 4, 8};
-  std::vector<double> t((size_t)5 * nl, 1e30);  // [candidate 0..3, rule = 4][level]
-  std::vector<cudaEvent_t> ev(nl + 1);
-  for (auto& e : ev) CUPF_CUDA(cudaEventCreate(&e));
+  std::vector<double> t((size_t)5 * n, 1e30);  // [candidate 0..3, rule = 4][launch]
+  std::vector<cudaEvent_t> ev(n + 1, nullptr);
+  auto cleanup = [&] {
+    for (auto& e : ev)
+      if (e) cudaEventDestroy(e);
+  };
+  std::vector<int> choice(n, 0);
+  double whole[2] = {1e30, 1e30};  // [rule, choice]
   try {
-    for (int rep = 0; rep < 3; ++rep) {
+    for (auto& e : ev) CUPF_CUDA(cudaEventCreate(&e));
+    for (int rep = 0; rep < 3; ++rep)
       for (int c = 0; c < 5; ++c) {
-        for (auto& lv : d.levels) lv.warps = c < 4 ? kCand[c] : 0;
+        for (size_t i = 0; i < n; ++i) set(i, c < 4 ? kCand[c] : 0);
         CUPF_CUDA(cudaEventRecord(ev[0], s));
-        for (size_t l = 0; l < nl; ++l) {
-          launch_factor_level<T, T>(d.levels[l], a, s);
-          CUPF_CUDA(cudaEventRecord(ev[l + 1], s));
+        for (size_t i = 0; i < n; ++i) {
+          launch(i);
+          CUPF_CUDA(cudaEventRecord(ev[i + 1], s));
         }
-        CUPF_CUDA(cudaEventSynchronize(ev[nl]));
-        for (size_t l = 0; l < nl; ++l) {
+        CUPF_CUDA(cudaEventSynchronize(ev[n]));
+        for (size_t i = 0; i < n; ++i) {
           float ms = 0.f;
-          CUPF_CUDA(cudaEventElapsedTime(&ms, ev[l], ev[l + 1]));
-          double& cell = t[(size_t)c * nl + l];
+          CUPF_CUDA(cudaEventElapsedTime(&ms, ev[i], ev[i + 1]));
+          double& cell = t[(size_t)c * n + i];
           cell = std::min(cell, (double)ms);
         }
       }
+    for (size_t i = 0; i < n; ++i) {
+      const double rule = t[(size_t)4 * n + i];
+      int best = -1;
+      double bt = std::min(rule * 0.97, rule - 0.5e-3);
+      for (int c = 0; c < 4; ++c)
+        if (t[(size_t)c * n + i] < bt) {
+          bt = t[(size_t)c * n + i];
+          best = c;
+        }
+      choice[i] = best >= 0 ? kCand[best] : 0;
     }
-  } catch (...) {
-    for (auto& lv : d.levels) lv.warps = 0;
-    for (auto& e : ev) cudaEventDestroy(e);
-    throw;
-  }
-  std::vector<int> choice(nl, 0);
-  for (size_t l = 0; l < nl; ++l) {
-    const double rule = t[(size_t)4 * nl + l];
-    int best = -1;
-    double bt = std::min(rule * 0.97, rule - 0.5e-3);
-    for (int c = 0; c < 4; ++c)
-      if (t[(size_t)c * nl + l] < bt) {
-        bt = t[(size_t)c * nl + l];
-        best = c;
-      }
-    choice[l] = best >= 0 ? kCand[best] : 0;
-  }
-  // the whole factorization as a solve runs it: the choice against the rule
-  double whole[2] = {1e30, 1e30};  // [rule, choice]
-  try {
     for (int rep = 0; rep < 3; ++rep)
       for (int v = 0; v < 2; ++v) {
-        for (size_t l = 0; l < nl; ++l) d.levels[l].warps = v ? choice[l] : 0;
+        for (size_t i = 0; i < n; ++i) set(i, v ? choice[i] : 0);
         CUPF_CUDA(cudaEventRecord(ev[0], s));
-        for (const auto& lv : d.levels) launch_factor_level<T, T>(lv, a, s);
+        for (size_t i = 0; i < n; ++i) launch(i);
         CUPF_CUDA(cudaEventRecord(ev[1], s));
         CUPF_CUDA(cudaEventSynchronize(ev[1]));
         float ms = 0.f;
@@ -700,24 +691,90 @@ void Engine::autotune_factor(cudaStream_t s, const void* J) {
         whole[v] = std::min(whole[v], (double)ms);
       }
   } catch (...) {
-    for (auto& lv : d.levels) lv.warps = 0;
-    for (auto& e : ev) cudaEventDestroy(e);
+    for (size_t i = 0; i < n; ++i) set(i, 0);
+    cleanup();
     throw;
   }
-  for (auto& e : ev) cudaEventDestroy(e);
+  cleanup();
   const bool keep = whole[1] < 0.99 * whole[0];
-  for (size_t l = 0; l < nl; ++l) d.levels[l].warps = keep ? choice[l] : 0;
+  for (size_t i = 0; i < n; ++i) set(i, keep ? choice[i] : 0);
   if (debug_sync())
-    std::fprintf(stderr, "[cupf] factor autotune: rule %.3f ms, choice %.3f ms, %s\n", whole[0], whole[1],
+    std::fprintf(stderr, "[cupf] %s autotune: rule %.3f ms, choice %.3f ms, %s\n", what, whole[0], whole[1],
                  keep ? "kept" : "rule kept");
+  return keep;
+}
+
+}  // namespace
+
+// The autotuner of the factor launches: each block factors one front for 32
+// scenarios and its warps split the staging, the assembly and the non-pivot
+// rows, so every element sees the same operations in the same order whatever
+// the split.  Tunes once per batch size and precision, on the values J.
+template <typename T>
+void Engine::autotune_factor(cudaStream_t s, const void* J) {
+  auto& d = *d_;
+  const bool dbl = std::is_same<T, double>::value;
+  if (d.tuned_Bp == d.Bp && d.tuned_double == dbl) return;
+  const FactorArgs<T, T> a = factor_args<T>(1, J);
+  choose_block_shapes(
+      d.levels.size(), [&](size_t i, int w) { d.levels[i].warps = w; },
+      [&](size_t i) { launch_factor_level<T, T>(d.levels[i], a, s); }, s, "factor");
   d.tuned_Bp = d.Bp;
   d.tuned_double = dbl;
   d.invalidate_graph();  // a captured solve holds the old launch shapes
 }
 
+// The same for the backward sweep (the tree-top launch, then the levels):
+// each warp back-substitutes one front for 32 scenarios on its own, so the
+// block shape only groups independent warps.  Reads the factors the last
+// factorization left (U, Y) and rewrites X, as every sweep does.
+template <typename T>
+void Engine::autotune_backward(cudaStream_t s) {
+  auto& d = *d_;
+  const bool dbl = std::is_same<T, double>::value;
+  if (d.tuned_bw_Bp == d.Bp && d.tuned_bw_double == dbl) return;
+  const SweepArgs<T> a = sweep_args<T>();
+  std::vector<LevelLaunch*> seq;
+  if (d.bw_nlev > 0) seq.push_back(&d.bw_top);
+  for (int l = d.bw_first - 1; l >= 0; --l) seq.push_back(&d.levels[l]);
+  const bool has_top = d.bw_nlev > 0;
+  choose_block_shapes(
+      seq.size(), [&](size_t i, int w) { seq[i]->bw_wpb = w; },
+      [&](size_t i) {
+        if (i == 0 && has_top)
+          launch_backward_top<T>(d.bw_top, d.bw_bounds.as<int>(), d.bw_nlev, a, s);
+        else
+          launch_backward_level<T>(*seq[i], a, s);
+      },
+      s, "backward");
+  d.tuned_bw_Bp = d.Bp;
+  d.tuned_bw_double = dbl;
+  d.invalidate_graph();
+}
+
+template <typename T>
+SweepArgs<T> Engine::sweep_args() const {
+  const auto& d = *d_;
+  SweepArgs<T> a;
+  a.plan = d.pl;
+  a.groups = d.Bp / kWarp;
+  a.Bp = d.Bp;
+  a.U = d.U.as<T>();
+  a.Y = d.Y.as<T>();
+  a.X = d.X.as<T>();
+  return a;
+}
+
 std::vector<int32_t> Engine::factor_level_warps() const {
   std::vector<int32_t> w;
   for (const auto& lv : d_->levels) w.push_back(lv.warps);
+  return w;
+}
+
+std::vector<int32_t> Engine::backward_launch_warps() const {
+  std::vector<int32_t> w;
+  if (d_->bw_nlev > 0) w.push_back(d_->bw_top.bw_wpb);
+  for (int l = d_->bw_first - 1; l >= 0; --l) w.push_back(d_->levels[l].bw_wpb);
   return w;
 }
 
@@ -738,13 +795,7 @@ void Engine::factor_all(cudaStream_t s, int store_l, const void* J) {
 template <typename T>
 void Engine::backward_all(cudaStream_t s) {
   auto& d = *d_;
-  SweepArgs<T> a;
-  a.plan = d.pl;
-  a.groups = d.Bp / kWarp;
-  a.Bp = d.Bp;
-  a.U = d.U.as<T>();
-  a.Y = d.Y.as<T>();
-  a.X = d.X.as<T>();
+  const SweepArgs<T> a = sweep_args<T>();
   stage_begin(3, s);
   const int64_t n = backward_levels<T>(a, s);
   launches_ += n;
@@ -874,11 +925,13 @@ SolveStats Engine::run_loop(double tol, int32_t max_iter, int32_t prepare_adjoin
   launches_ = 0;
   adjoint_ready_ = false;
   if (cfg_.autotune && max_iter > 0 &&
-      (d.tuned_Bp != d.Bp || d.tuned_double != std::is_same<T, double>::value)) {
+      (d.tuned_Bp != d.Bp || d.tuned_double != std::is_same<T, double>::value || d.tuned_bw_Bp != d.Bp ||
+       d.tuned_bw_double != std::is_same<T, double>::value)) {
     // tune on the Jacobian of the starting state (the loop recomputes it)
     launch_ibus_mismatch(d.g, st, s);
     launch_jacobian<T>(d.g, st, d.J.as<T>(), s);
     autotune_factor<T>(s, d.J.p);
+    autotune_backward<T>(s);  // on the factors the factor tuning left
   }
   CUPF_CUDA(cudaMemsetAsync(d.norm.p, 0, d.Bp * sizeof(unsigned long long), s));
   CUPF_CUDA(cudaMemsetAsync(d.sing.p, 0, d.Bp * sizeof(int), s));

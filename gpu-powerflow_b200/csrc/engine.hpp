@@ -114,6 +114,8 @@ class Engine {
   const SymbolicPlan& symbolic() const { return sp_; }
   // warps per block of each factor level launch (0: the built-in rule)
   std::vector<int32_t> factor_level_warps() const;
+  // the same for the backward sweep's launches, tree top first
+  std::vector<int32_t> backward_launch_warps() const;
   const FactorProgram& program() const { return fp_; }
   const EngineConfig& config() const { return cfg_; }
   int32_t n_bus() const { return ja_.n_bus; }
@@ -168,6 +170,10 @@ class Engine {
   // and keeps the fastest per level (once per batch size and precision)
   template <typename T>
   void autotune_factor(cudaStream_t s, const void* J);
+  template <typename T>
+  void autotune_backward(cudaStream_t s);
+  template <typename T>
+  SweepArgs<T> sweep_args() const;
   template <typename T>
   void backward_all(cudaStream_t s);
   template <typename T>

@@ -21,6 +21,7 @@ struct LevelLaunch {
   // its list without reading the launch record first
   long long fe_base = 0;
   int warps = 0;   // warps per block of the factor launch (0: the built-in rule)
+  int bw_wpb = 0;  // warps per block of the backward-sweep launch (0: the built-in rule)
 };
 
 template <typename T, typename TJ>

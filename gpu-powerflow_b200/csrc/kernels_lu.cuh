@@ -747,9 +747,11 @@ void launch_backward_level(const LevelLaunch& lv, const SweepArgs<T>& a, cudaStr
   const size_t per_warp = (size_t)warp_elems * kWarp * sizeof(T);
   int wpb = (int)std::min<size_t>(8, kSmemLimit / per_warp);
   if (wpb < 1) throw std::runtime_error("backward level: front exceeds shared memory");
+  const int cap = wpb;
   const long items = (long)lv.count * a.groups;
   wpb = (int)std::min<long>(wpb, std::max<long>(1, items / 148));
   wpb = std::max(1, std::min(wpb, 4));
+  if (lv.bw_wpb > 0) wpb = std::min(lv.bw_wpb, cap);  // chosen by the engine's autotuner
   const size_t smem = per_warp * wpb;
   auto kern = k_backward_level<T>;
   allow_full_smem(reinterpret_cast<const void*>(kern));
@@ -766,8 +768,9 @@ void launch_backward_top(const LevelLaunch& top, const int* lv_bounds, int nlev,
   if (top.count == 0 || nlev == 0) return;
   const int warp_elems = top.max_nc * top.max_fsz + top.max_fsz;
   const size_t per_warp = (size_t)warp_elems * kWarp * sizeof(T);
-  const int wpb = (int)std::min<size_t>(4, kSmemLimit / per_warp);
-  if (wpb < 1) throw std::runtime_error("backward sweep: front exceeds shared memory");
+  const int cap = (int)std::min<size_t>(8, kSmemLimit / per_warp);
+  if (cap < 1) throw std::runtime_error("backward sweep: front exceeds shared memory");
+  const int wpb = top.bw_wpb > 0 ? std::min(top.bw_wpb, cap) : std::min(4, cap);
   auto kern = k_backward_top<T>;
   allow_full_smem(reinterpret_cast<const void*>(kern));
   launch_chained(kern, dim3((unsigned)a.groups), dim3(wpb * kWarp), per_warp * wpb, s, "backward sweep (tree top)",

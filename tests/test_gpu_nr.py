@@ -342,8 +342,8 @@ def test_graph_loop_capped_and_failed_scenarios_match_stream_mode():
 @pytest.mark.parametrize("graph", [False, True])
 def test_autotuned_factor_launches_give_identical_solves(policy, graph):
     """CustomSolverConfig.autotune: the warps per block of every factor level
-    are timed and chosen at the first solve of each batch size; the solves
-    stay bit for bit those of the built-in rule."""
+    and backward-sweep launch are timed and chosen at the first solve of each
+    batch size; the solves stay bit for bit those of the built-in rule."""
     g = G.grid_2000()
     S, V0 = g.scenarios(256, seed=77), g.flat_start(256)
     base = make_solver(g, POLICIES[policy], graph)
@@ -356,4 +356,7 @@ def test_autotuned_factor_launches_give_identical_solves(policy, graph):
         assert np.array_equal(a.final_mismatch_numpy, b.final_mismatch_numpy)
         w = tuned.plan_array("factor_level_warps")
         assert w.size > 0 and set(w.tolist()) <= {0, 1, 2, 4, 8}
+        wb = tuned.plan_array("backward_launch_warps")
+        assert wb.size > 0 and set(wb.tolist()) <= {0, 1, 2, 4, 8}
     assert not base.plan_array("factor_level_warps").any()
+    assert not base.plan_array("backward_launch_warps").any()
