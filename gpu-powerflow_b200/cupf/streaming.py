@@ -14,9 +14,12 @@ three batches at once on three streams:
 
 so a steady stream of batches costs about max(solve, upload, download) per
 batch instead of their sum (PCIe is full duplex; the copies use the copy
-engines, not the SMs).  Events order everything: a solve waits for its
-upload, a download waits for its solve, and a slot is overwritten only after
-the solve that read it.
+engines, not the SMs).  An optional prepare stage (the warm start's network
+inference) runs batch k+1 on a fourth stream while batch k solves: the
+solve's narrow levels leave SMs idle that the GEMMs can use.  Events order
+everything: a prepare and a solve wait for their upload, a solve for its
+prepare, a download for its solve, and a slot (input buffer, prepared state)
+is overwritten only after the solve that read it.
 """
 from __future__ import annotations
 
@@ -24,16 +27,24 @@ from __future__ import annotations
 class HostPipeline:
     """solve(sbus_device) -> (V_device, final_mismatch_device) runs one batch
     on the current stream (e.g. ``lambda s: warm.solve(solver, s, cfg)[:2]``
-    or ``lambda s: solver.solve_batch_device(s, v0, config=cfg)[:2]``)."""
+    or ``lambda s: solver.solve_batch_device(s, v0, config=cfg)[:2]``).
 
-    def __init__(self, solve, device=None):
+    With prepare(sbus_device, slot) -> state, the pipeline calls
+    solve(sbus_device, state) instead; prepare runs on its own stream, one
+    batch ahead, and must keep its state in storage of its slot (0 or 1)
+    (e.g. ``prepare=lambda s, j: warm.predict_standardized(s, slot=j)`` with
+    ``solve=lambda s, p: warm.solve(solver, s, cfg, pred=p)[:2]``)."""
+
+    def __init__(self, solve, device=None, prepare=None):
         import torch
 
         self.torch = torch
         self.solve = solve
+        self.prepare = prepare
         self.dev = torch.device(device or "cuda")
         self.up = torch.cuda.Stream(self.dev)
         self.down = torch.cuda.Stream(self.dev)
+        self.prep = torch.cuda.Stream(self.dev) if prepare is not None else None
         self._slots = None
 
     def _slot_buffers(self, rows: int, n: int):
@@ -63,8 +74,10 @@ class HostPipeline:
         slots = self._slot_buffers(max(int(s.shape[0]) for s in sbus), n)
         comp = t.cuda.current_stream(self.dev)
         uploaded = [t.cuda.Event(), t.cuda.Event()]
+        prepared = [t.cuda.Event(), t.cuda.Event()]
         solved = [None, None]   # the event after the last solve that read each slot
         inputs = [None, None]
+        states = [None, None]
 
         def upload(k: int) -> None:
             j = k % 2
@@ -75,6 +88,11 @@ class HostPipeline:
                 dst.copy_(sbus[k], non_blocking=True)
                 uploaded[j].record(self.up)
             inputs[j] = dst
+            if self.prepare is not None:
+                with t.cuda.stream(self.prep):
+                    self.prep.wait_event(uploaded[j])  # (after the slot's last solve, through the upload)
+                    states[j] = self.prepare(dst, j)
+                    prepared[j].record(self.prep)
 
         upload(0)
         for k in range(K):
@@ -82,7 +100,11 @@ class HostPipeline:
             if k + 1 < K:
                 upload(k + 1)
             comp.wait_event(uploaded[j])
-            V, fm = self.solve(inputs[j])
+            if self.prepare is not None:
+                comp.wait_event(prepared[j])
+                V, fm = self.solve(inputs[j], states[j])
+            else:
+                V, fm = self.solve(inputs[j])
             done = t.cuda.Event()
             done.record(comp)
             solved[j] = done

@@ -90,7 +90,7 @@ class MLP:
             self.vb.append(torch.zeros(d_out, device=self.dev))
         self._refresh_transposes()
         self.step = 0
-        self._bufs: dict[int, dict] = {}
+        self._bufs: dict[tuple, dict] = {}
         self.split_out = True        # inference: output layer with hi + lo weights
         self.Wsplit16 = None         # [no, 2 cat_w] bf16: [hi | lo] of the fp32 output weights
         self._split_stale = True
@@ -150,10 +150,13 @@ class MLP:
         for i in range(1, self.layers + 1):
             self.transpose(self.W16[i], self.WT16[i])
 
-    def buffers(self, B: int) -> dict:
+    def buffers(self, B: int, slot: int = 0) -> dict:
+        """Activation and gradient buffers for batch B; independent sets per
+        slot let two inferences be in flight at once (HostPipeline)."""
         if B % 128:
             raise ValueError("batch must be a multiple of 128")
-        if B not in self._bufs:
+        key = (B, slot)
+        if key not in self._bufs:
             t, d = self.torch, self.dev
             bf = t.bfloat16
             H, L = self.hidden, self.layers
@@ -170,8 +173,8 @@ class MLP:
                  "gW": [t.empty(self.dims_out[i], self.dims_in[i], device=d) for i in range(L + 1)],
                  "gb": [t.empty(self.dims_out[i], device=d) for i in range(L + 1)],
                  "loss": t.zeros(1, device=d)}
-            self._bufs[B] = h
-        return self._bufs[B]
+            self._bufs[key] = h
+        return self._bufs[key]
 
     def _layer_input(self, h: dict, i: int):
         if i == 0:
@@ -439,13 +442,14 @@ class WarmStart:
         mlp.set_output_layer(sol[:-1].T.float(), sol[-1].float())
 
     # -- inference --
-    def predict_standardized(self, sbus):
+    def predict_standardized(self, sbus, slot: int = 0):
         """Network output fp32 [B rounded up to 128, no], still standardized
         (state = out * y_std + y_mean on the first n_out columns): the
         features are built from Sbus by one kernel and no pre-activations
-        are kept."""
+        are kept.  The output lives in the buffers of `slot` until the next
+        prediction into that slot."""
         Bp = _round_up(sbus.shape[0], 128)
-        h = self.mlp.buffers(Bp)
+        h = self.mlp.buffers(Bp, slot)
         self.mlp.load_features(h, sbus, self.sgen, self.vm_pv, self.x_mean, self.x_istd)
         return self.mlp.forward(h, keep_pre=False)
 
@@ -455,13 +459,16 @@ class WarmStart:
         out = self.predict_standardized(sbus)
         return (out[:B, : self.n_out] * self.y_std + self.y_mean).contiguous()
 
-    def solve(self, solver, sbus, config=None):
+    def solve(self, solver, sbus, config=None, pred=None):
         """Warm-started batched solve with flat-start fallback.  Returns
-        (V, final_mismatch, iterations_warm, n_fallback)."""
+        (V, final_mismatch, iterations_warm, n_fallback).  pred: this batch's
+        predict_standardized output when it was computed beforehand (on
+        another stream, ordered before this call's stream)."""
         import cupf
 
         cfg = config or cupf.NRConfig()
-        pred = self.predict_standardized(sbus)
+        if pred is None:
+            pred = self.predict_standardized(sbus)
         V, fm, it = solver.solve_batch_warm_device(sbus, self.v0, pred, config=cfg, pred_scale=self.y_std,
                                                    pred_shift=self.y_mean)
         if solver.last_all_converged:  # known from the solve itself: no extra synchronisation

@@ -347,3 +347,38 @@ def test_host_pipeline_matches_serial_solves(torch):
     fms = [torch.empty(64, dtype=torch.float64).pin_memory() for _ in range(3)]
     HostPipeline(solve).run([ins[0], ins[2], ins[0]], [shared] * 3, fms)
     assert torch.equal(shared, V_out[0])
+
+
+def test_host_pipeline_overlaps_the_warm_start_network(torch):
+    """HostPipeline with a prepare stage: the next batch's network inference
+    runs on its own stream into its own slot's buffers while the current
+    batch solves; every batch equals its serial warm-started solve, bit for
+    bit."""
+    import cupf
+    from cupf import grids as G
+    from cupf.streaming import HostPipeline
+    from cupf.warm_start import WarmStart
+
+    g = G.grid_118()
+    o = cupf.NewtonOptions()
+    o.backend = cupf.BackendKind.CUDA
+    o.compute = cupf.ComputePolicy.Mixed
+    o.use_cuda_graph = True
+    o.custom.serial_nd = True
+    s = cupf.NewtonSolver(o)
+    s.initialize(g.indptr, g.indices, g.data, g.n_bus, g.n_bus, g.pv, g.pq)
+    ws = WarmStart(g, hidden=256, layers=2, seed=0)
+    X, Y, _ = ws.generate(s, 4096, seed=2)
+    ws.fit(X, Y, epochs=5, batch=512, lr=2e-3)
+    cfg = cupf.NRConfig(tolerance=1e-8, max_iter=10)
+    sizes = [128, 100, 128, 128, 60]
+    ins = [torch.tensor(g.scenarios(b, seed=70 + i)).pin_memory() for i, b in enumerate(sizes)]
+    V_out = [torch.empty(b, g.n_bus, dtype=torch.complex128).pin_memory() for b in sizes]
+    fm_out = [torch.empty(b, dtype=torch.float64).pin_memory() for b in sizes]
+    pipe = HostPipeline(lambda sd, p: ws.solve(s, sd, cfg, pred=p)[:2],
+                        prepare=lambda sd, j: ws.predict_standardized(sd, slot=j))
+    pipe.run(ins, V_out, fm_out)
+    for i in range(len(sizes)):
+        v, fm, _, _ = ws.solve(s, ins[i].cuda(), cfg)
+        assert torch.equal(V_out[i], v.cpu()) and torch.equal(fm_out[i], fm.cpu())
+        assert bool((fm_out[i] <= 1e-8).all())
