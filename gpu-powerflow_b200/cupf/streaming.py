@@ -42,6 +42,8 @@ class HostPipeline:
         self.solve = solve
         self.prepare = prepare
         self.dev = torch.device(device or "cuda")
+        if self.dev.index is None:  # the worker thread selects the device by index
+            self.dev = torch.device("cuda", torch.cuda.current_device())
         self.up = torch.cuda.Stream(self.dev)
         self.down = torch.cuda.Stream(self.dev)
         self.prep = torch.cuda.Stream(self.dev) if prepare is not None else None
@@ -58,7 +60,15 @@ class HostPipeline:
         copies to overlap); V_out[k] (complex128 [B_k, n]) and fm_out[k]
         (float64 [B_k]) receive batch k's voltages and final mismatch norms.
         Output tensors may repeat in the lists: downloads run in batch order
-        on one stream.  Returns when every download has landed."""
+        on one stream.  Returns when every download has landed.
+
+        The solves run in a worker thread, one after another on the caller's
+        stream (the engine's solve blocks its thread until the batch is done
+        and releases the GIL meanwhile); this thread issues the uploads and
+        the prepare stage of the next batch during the current solve."""
+        import queue
+        import threading
+
         t = self.torch
         K = len(sbus)
         if len(V_out) != K or len(fm_out) != K:
@@ -73,46 +83,71 @@ class HostPipeline:
                 raise ValueError("HostPipeline.run: output shapes must match their input batch")
         slots = self._slot_buffers(max(int(s.shape[0]) for s in sbus), n)
         comp = t.cuda.current_stream(self.dev)
-        uploaded = [t.cuda.Event(), t.cuda.Event()]
-        prepared = [t.cuda.Event(), t.cuda.Event()]
-        solved = [None, None]   # the event after the last solve that read each slot
-        inputs = [None, None]
-        states = [None, None]
+        solved = [None, None]                                # event after the last solve that read each slot
+        free = [threading.Semaphore(1), threading.Semaphore(1)]  # the slot's last solve has been issued
+        ready: queue.Queue = queue.Queue()
+        failure = []
 
-        def upload(k: int) -> None:
-            j = k % 2
-            with t.cuda.stream(self.up):
-                if solved[j] is not None:
-                    self.up.wait_event(solved[j])  # the slot's previous reader is done
-                dst = slots[j][: sbus[k].shape[0]]
-                dst.copy_(sbus[k], non_blocking=True)
-                uploaded[j].record(self.up)
-            inputs[j] = dst
-            if self.prepare is not None:
-                with t.cuda.stream(self.prep):
-                    self.prep.wait_event(uploaded[j])  # (after the slot's last solve, through the upload)
-                    states[j] = self.prepare(dst, j)
-                    prepared[j].record(self.prep)
+        def worker() -> None:
+            try:
+                t.cuda.set_device(self.dev)
+                with t.cuda.stream(comp):
+                    for k in range(K):
+                        item = ready.get()
+                        if item is None:
+                            return
+                        j, dst, state, up_ev, prep_ev = item
+                        comp.wait_event(up_ev)
+                        if prep_ev is not None:
+                            comp.wait_event(prep_ev)
+                            V, fm = self.solve(dst, state)
+                        else:
+                            V, fm = self.solve(dst)
+                        done = t.cuda.Event()
+                        done.record(comp)
+                        solved[j] = done
+                        self.down.wait_event(done)
+                        with t.cuda.stream(self.down):
+                            V_out[k].copy_(V, non_blocking=True)
+                            fm_out[k].copy_(fm, non_blocking=True)
+                        # keep the device results alive until their download ran
+                        V.record_stream(self.down)
+                        fm.record_stream(self.down)
+                        free[j].release()
+            except BaseException as e:  # handed to the caller's thread
+                failure.append(e)
+                for f in free:
+                    f.release()
 
-        upload(0)
-        for k in range(K):
-            j = k % 2
-            if k + 1 < K:
-                upload(k + 1)
-            comp.wait_event(uploaded[j])
-            if self.prepare is not None:
-                comp.wait_event(prepared[j])
-                V, fm = self.solve(inputs[j], states[j])
-            else:
-                V, fm = self.solve(inputs[j])
-            done = t.cuda.Event()
-            done.record(comp)
-            solved[j] = done
-            self.down.wait_event(done)
-            with t.cuda.stream(self.down):
-                V_out[k].copy_(V, non_blocking=True)
-                fm_out[k].copy_(fm, non_blocking=True)
-            # keep the device results alive until their download ran
-            V.record_stream(self.down)
-            fm.record_stream(self.down)
-        self.down.synchronize()
+        th = threading.Thread(target=worker, daemon=True)
+        th.start()
+        issued = 0
+        try:
+            for k in range(K):
+                j = k % 2
+                free[j].acquire()           # batch k-2's solve was issued (and its event recorded)
+                if failure:
+                    break
+                up_ev = t.cuda.Event()
+                with t.cuda.stream(self.up):
+                    if solved[j] is not None:
+                        self.up.wait_event(solved[j])  # its reads of the slot come first
+                    dst = slots[j][: sbus[k].shape[0]]
+                    dst.copy_(sbus[k], non_blocking=True)
+                    up_ev.record(self.up)
+                state, prep_ev = None, None
+                if self.prepare is not None:
+                    prep_ev = t.cuda.Event()
+                    with t.cuda.stream(self.prep):
+                        self.prep.wait_event(up_ev)
+                        state = self.prepare(dst, j)
+                        prep_ev.record(self.prep)
+                ready.put((j, dst, state, up_ev, prep_ev))
+                issued += 1
+        finally:
+            if issued < K:
+                ready.put(None)  # the worker stops after the batches it was given
+            th.join()
+        self.down.synchronize()  # no copy into the caller's buffers is left running
+        if failure:
+            raise failure[0]

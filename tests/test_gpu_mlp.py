@@ -382,3 +382,36 @@ def test_host_pipeline_overlaps_the_warm_start_network(torch):
         v, fm, _, _ = ws.solve(s, ins[i].cuda(), cfg)
         assert torch.equal(V_out[i], v.cpu()) and torch.equal(fm_out[i], fm.cpu())
         assert bool((fm_out[i] <= 1e-8).all())
+
+
+def test_host_pipeline_hands_failures_to_the_caller(torch):
+    """A solve that raises in the pipeline's worker thread, or a prepare that
+    raises in the caller's thread, ends run() with that exception; nothing
+    is left waiting."""
+    from cupf.streaming import HostPipeline
+
+    ins = [torch.ones(32, 8, dtype=torch.complex128).pin_memory() * (i + 1) for i in range(5)]
+    V_out = [torch.empty(32, 8, dtype=torch.complex128).pin_memory() for _ in range(5)]
+    fm_out = [torch.empty(32, dtype=torch.float64).pin_memory() for _ in range(5)]
+    calls = []
+
+    def solve(sd):
+        calls.append(1)
+        if len(calls) == 2:
+            raise RuntimeError("solve failed")
+        return sd * 2, sd.real[:, 0].clone()
+
+    with pytest.raises(RuntimeError, match="solve failed"):
+        HostPipeline(solve).run(ins, V_out, fm_out)
+    assert torch.equal(V_out[0], ins[0] * 2)
+
+    def prepare(sd, slot):
+        if float(sd.real[0, 0]) == 2.0:
+            raise ValueError("prepare failed")
+        return slot
+
+    with pytest.raises(ValueError, match="prepare failed"):
+        HostPipeline(lambda sd, st: (sd * 3, sd.real[:, 0].clone()), prepare=prepare).run(ins, V_out, fm_out)
+    # and a clean run after both
+    HostPipeline(lambda sd: (sd * 4, sd.real[:, 0].clone())).run(ins, V_out, fm_out)
+    assert all(torch.equal(V_out[i], ins[i] * 4) for i in range(5))
