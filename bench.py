@@ -63,40 +63,109 @@ def _peaks() -> dict:
 
 
 class ClockSampler:
-    """SM clocks and throttle reasons sampled by NVML from a background thread
-    during the timed region (10 ms period: the timed legs last a few hundred
-    milliseconds; NVML reads only, no settings)."""
+    """SM clocks and throttle reasons during the timed region (reads only, no
+    settings).  Sampled every 20 ms by an nvidia-smi child process, so that
+    this process's threads and interpreter lock do not thin the samples;
+    NVML from a background thread when nvidia-smi is absent."""
 
+    # clocks_event_reasons.active bits (nvml.h nvmlClocksEventReason*)
+    BITS = ((0x8, "hw_slowdown"), (0x40, "hw_thermal_slowdown"), (0x20, "sw_thermal_slowdown"),
+            (0x4, "sw_power_cap"), (0x80, "hw_power_brake"))
     REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
                ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
                ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
                ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"),
                ("hw_power_brake", "nvmlClocksEventReasonHwPowerBrakeSlowdown"))
 
-    def __init__(self, index: int, period: float = 0.01):
-        self.index, self.period = index, period
+    def __init__(self, index: int, uuid: str | None = None, period: float = 0.01):
+        self.index, self.uuid, self.period = index, uuid, period
         self.sm, self.reasons, self.max_mhz = [], set(), None
         self._stop = None
+        self._proc = None
+        self._path = None
+
+    def parse(self, text: str) -> None:
+        """Lines of 'clocks.sm, clocks.max.sm, clocks_event_reasons.active'."""
+        for line in text.splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) != 3:
+                continue
+            try:
+                sm, mx, bits = float(parts[0]), float(parts[1]), int(parts[2], 16)
+            except ValueError:
+                continue
+            self.sm.append(sm)
+            self.max_mhz = mx
+            for bit, name in self.BITS:
+                if bits & bit:
+                    self.reasons.add(name)
+
+    def _start_smi(self) -> bool:
+        import shutil
+        import subprocess
+        import tempfile
+
+        exe = shutil.which("nvidia-smi")
+        if not exe:
+            return False
+        fd, self._path = tempfile.mkstemp(suffix=".csv")
+        target = f"GPU-{self.uuid}" if self.uuid else str(self.index)
+        with os.fdopen(fd, "w") as out:
+            self._proc = subprocess.Popen(
+                [exe, "-i", target, "--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.active",
+                 "--format=csv,noheader,nounits", "-lms", "20"], stdout=out, stderr=subprocess.DEVNULL)
+        t0 = time.time()
+        while time.time() - t0 < 5.0 and os.path.getsize(self._path) == 0 and self._proc.poll() is None:
+            time.sleep(0.02)
+        if os.path.getsize(self._path) > 0:
+            with open(self._path) as f:  # samples from before the timed region do not count
+                self._skip = len(f.read().splitlines())
+            return True
+        self._end_smi()
+        return False
+
+    def _end_smi(self) -> str:
+        text = ""
+        if self._proc is not None:
+            self._proc.terminate()
+            try:
+                self._proc.wait(timeout=5)
+            except Exception:
+                self._proc.kill()
+            self._proc = None
+        if self._path:
+            with open(self._path) as f:
+                text = f.read()
+            os.unlink(self._path)
+            self._path = None
+        return text
 
     def __enter__(self):
+        # both samplers run; nvidia-smi's samples are used when it produced any
+        self._skip = 0
+        self.source = None
+        self._nvml = ([], set(), None)
+        self._start_smi()
         import threading
         try:
             import pynvml as nv
             nv.nvmlInit()
             h = nv.nvmlDeviceGetHandleByIndex(self.index)
-            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            nv_max = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
         except Exception:
             return self
         self._stop = threading.Event()
+        sm, reasons = [], set()
+        self._nvml = (sm, reasons, nv_max)
 
         def run():
             while True:
                 try:
-                    self.sm.append(float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)))
+                    sm.append(float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)))
                     bits = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
                     for name, attr in self.REASONS:
                         if bits & getattr(nv, attr, 0):
-                            self.reasons.add(name)
+                            reasons.add(name)
                 except Exception:
                     pass
                 if self._stop.wait(self.period):
@@ -109,10 +178,18 @@ class ClockSampler:
         if self._stop is not None:
             self._stop.set()
             self._thread.join(timeout=5)
+        if self._proc is not None:
+            lines = self._end_smi().splitlines()
+            self.parse("\n".join(lines[self._skip:]))
+        if self.sm:
+            self.source = "nvidia-smi, every 20 ms"
+        elif self._nvml[0]:
+            self.sm, self.reasons, self.max_mhz = list(self._nvml[0]), set(self._nvml[1]), self._nvml[2]
+            self.source = "NVML from a thread, every 10 ms"
 
     def summary(self) -> dict:
         return {"sm_mhz": statistics.median(self.sm) if self.sm else None, "sm_max_mhz": self.max_mhz,
-                "reasons": sorted(self.reasons), "samples": len(self.sm)}
+                "reasons": sorted(self.reasons), "samples": len(self.sm), "source": self.source}
 
 
 def _dist():
@@ -254,7 +331,12 @@ def run_engine(args) -> None:
     torch.cuda.synchronize(dev)
     # the timed legs sit between cudaProfilerStart/Stop, so a profiler started
     # with profiling off (ncu --profile-from-start off) sees exactly them
-    with ClockSampler(local) as clk:
+    uuid = None
+    try:
+        uuid = str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:
+        pass
+    with ClockSampler(local, uuid) as clk:
         torch.cuda.profiler.start()
         r_mix = timed(lambda: step_flat(mixed), args.steps, args.warmup)
         r_64 = timed(lambda: step_flat(fp64), args.steps, args.warmup)

@@ -955,10 +955,11 @@ SolveStats Engine::run_loop(double tol, int32_t max_iter, int32_t prepare_adjoin
     hc->max_iter = max_iter;
     hc->B = d.B;
     hc->tolerate = tolerate_nonfinite_ ? 1 : 0;
-    CUPF_CUDA(cudaMemcpyAsync(d.ctl.p, hc, sizeof(LoopCtl), cudaMemcpyHostToDevice, s));
+    // control in and results out by kernels on pinned memory (no copy-engine
+    // transfers that could queue behind a caller's batch copies)
+    launch_ctl_load(hc, d.ctl.as<LoopCtl>(), s);
     CUPF_CUDA(cudaGraphLaunch(d.exec, s));
-    CUPF_CUDA(cudaMemcpyAsync(hc, d.ctl.p, sizeof(LoopCtl), cudaMemcpyDeviceToHost, s));
-    CUPF_CUDA(cudaMemcpyAsync(d.h_final, d.fin_dev.p, d.B * sizeof(double), cudaMemcpyDeviceToHost, s));
+    launch_ctl_store(d.ctl.as<LoopCtl>(), hc, d.fin_dev.as<double>(), d.h_final, d_final, d.B, s);
     CUPF_CUDA(cudaStreamSynchronize(s));
     completed = hc->completed;
     gmax = hc->gmax;
@@ -1023,7 +1024,9 @@ SolveStats Engine::run_loop(double tol, int32_t max_iter, int32_t prepare_adjoin
     B_ = d.B;
     adjoint_ready_ = true;
   }
-  if (d_final) CUPF_CUDA(cudaMemcpyAsync(d_final, d.h_final, d.B * sizeof(double), cudaMemcpyHostToDevice, s));
+  // (graph mode: the store kernel already wrote d_final)
+  if (d_final && !use_graph)
+    CUPF_CUDA(cudaMemcpyAsync(d_final, d.h_final, d.B * sizeof(double), cudaMemcpyHostToDevice, s));
   CUPF_CUDA(cudaStreamSynchronize(s));
   CUPF_CUDA(cudaGetLastError());
   if (profiling_) collect_stage_times();

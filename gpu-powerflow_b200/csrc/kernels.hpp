@@ -178,6 +178,15 @@ struct LoopCtl {
 // Reads the per-scenario norms of the last mismatch, records them as the
 // final mismatches, counts the evaluation and sets the loop's condition to
 // 1 (iterate again) or 0 (converged, iteration cap, or non-finite).
+// The graph-mode solve's control block and results travel through pinned
+// host memory that the kernels read and write directly (unified addressing),
+// not through copies: small copies would queue on the copy engines behind a
+// stream of batch uploads and downloads.  load: host control -> device;
+// store: device control -> host, final norms -> host and (if given) to the
+// caller's device buffer.
+void launch_ctl_load(const LoopCtl* host_ctl, LoopCtl* ctl, cudaStream_t s);
+void launch_ctl_store(const LoopCtl* ctl, LoopCtl* host_ctl, const double* final_norm, double* host_final,
+                      double* d_final, int B, cudaStream_t s);
 void launch_loop_check(cudaGraphConditionalHandle h, LoopCtl* ctl, const unsigned long long* norm_bits,
                        double* final_norm, cudaStream_t s);
 void launch_sumsq2(const double* R, const double* G, int dim, int B, int Bp, double* scratch, cudaStream_t s);

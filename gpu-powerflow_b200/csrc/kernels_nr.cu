@@ -830,4 +830,31 @@ void launch_loop_check(cudaGraphConditionalHandle h, LoopCtl* ctl, const unsigne
   k_loop_check<<<1, kCheckThreads, 0, s>>>(h, ctl, norm_bits, final_norm);
 }
 
+namespace {
+__global__ void k_ctl_load(const LoopCtl* __restrict__ host_ctl, LoopCtl* __restrict__ ctl) {
+  if (threadIdx.x == 0) *ctl = *host_ctl;
+}
+__global__ void k_ctl_store(const LoopCtl* __restrict__ ctl, LoopCtl* __restrict__ host_ctl,
+                            const double* __restrict__ final_norm, double* __restrict__ host_final,
+                            double* __restrict__ d_final, int B) {
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < B; b += gridDim.x * blockDim.x) {
+    const double v = final_norm[b];
+    host_final[b] = v;
+    if (d_final) d_final[b] = v;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) *host_ctl = *ctl;
+  __threadfence_system();
+}
+}  // namespace
+
+void launch_ctl_load(const LoopCtl* host_ctl, LoopCtl* ctl, cudaStream_t s) {
+  k_ctl_load<<<1, 32, 0, s>>>(host_ctl, ctl);
+}
+
+void launch_ctl_store(const LoopCtl* ctl, LoopCtl* host_ctl, const double* final_norm, double* host_final,
+                      double* d_final, int B, cudaStream_t s) {
+  const int blocks = std::max(1, std::min((B + 255) / 256, 64));
+  k_ctl_store<<<blocks, 256, 0, s>>>(ctl, host_ctl, final_norm, host_final, d_final, B);
+}
+
 }  // namespace cupf_b200
