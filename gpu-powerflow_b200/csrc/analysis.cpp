@@ -6,6 +6,7 @@
 #include "analysis.hpp"
 
 #include <algorithm>
+#include <cstdio>
 #include <cstring>
 #include <mutex>
 #include <numeric>
@@ -332,6 +333,25 @@ bool structural_matching(int32_t n, const int32_t* row_ptr, const int32_t* col_i
 // ===========================================================================
 // Symbolic plan
 // ===========================================================================
+
+std::string fronts_csv(const SymbolicPlan& sp) {
+  std::string out = "q,p,fsz,nc,uc,level,parent,asm_len,extend_elems\n";
+  char line[160];
+  for (int32_t L = 0; L + 1 < (int32_t)sp.level_ptr.size(); ++L)
+    for (int32_t q = sp.level_ptr[L]; q < sp.level_ptr[L + 1]; ++q) {
+      const int32_t p = sp.plcols_level[q];
+      const int32_t fsz = sp.front_ptr[p + 1] - sp.front_ptr[p];
+      const int32_t nc = sp.panel_ncols[p];
+      const int32_t uc = fsz - nc;
+      const int32_t parent = sp.panel_parent.empty() ? -1 : sp.panel_parent[p];
+      const int32_t asm_len = sp.asm_ptr.empty() ? 0 : sp.asm_ptr[p + 1] - sp.asm_ptr[p];
+      const long long extend = parent >= 0 ? (long long)uc * uc : 0;
+      std::snprintf(line, sizeof line, "%d,%d,%d,%d,%d,%d,%d,%d,%lld\n", q, p, fsz, nc, uc, L, parent, asm_len,
+                    extend);
+      out += line;
+    }
+  return out;
+}
 
 SymbolicPlan analyze_symbolic(int32_t n, const int32_t* row_ptr, const int32_t* col_idx, const SymbolicOptions& opt) {
   if (n <= 0) throw std::invalid_argument("analyze_symbolic: empty matrix");

@@ -73,6 +73,12 @@ struct SymbolicPlan {
   std::vector<int32_t> a_row, a_col;  // per Jacobian CSR entry: position inside the front
 };
 
+// Per-front structure as CSV text (the columns of the reference's
+// MaybeDumpFronts, custom_linear_solver/src/analyze/pipeline.cpp:162-193):
+// q,p,fsz,nc,uc,level,parent,asm_len,extend_elems, one row per panel, levels
+// leaves first and each level's panels in ascending order (plcols_level).
+std::string fronts_csv(const SymbolicPlan& sp);
+
 SymbolicPlan analyze_symbolic(int32_t n, const int32_t* row_ptr, const int32_t* col_idx,
                               const SymbolicOptions& opt);
 

@@ -5,6 +5,7 @@
 // the phase's failure status, with the message kept on the handle.
 #include "../../include/cupf_b200.h"
 
+#include <cstdio>
 #include <cstring>
 #include <memory>
 #include <stdexcept>
@@ -127,6 +128,13 @@ bool copy_plan_array(const Engine& e, const char* name, int32_t* out, int64_t ca
     if (!v->empty()) std::memcpy(out, v->data(), v->size() * sizeof(int32_t));
   }
   return true;
+}
+
+bool write_text_file(const char* path, const std::string& text) {
+  FILE* f = std::fopen(path, "w");
+  if (!f) return false;
+  const bool ok = std::fwrite(text.data(), 1, text.size(), f) == text.size();
+  return std::fclose(f) == 0 && ok;
 }
 
 // Stream of a device-pointer entry point: the caller's stream, where NULL is
@@ -314,6 +322,12 @@ cls_status cls_singular_flags(cls_handle h, int32_t* out_host, int32_t batch) {
 cls_status cls_plan_array(cls_handle h, const char* name, int32_t* out, int64_t capacity, int64_t* len) {
   if (!h || !h->eng) return CLS_INVALID_STATE;
   return copy_plan_array(*h->eng, name, out, capacity, len) ? CLS_SUCCESS : CLS_INVALID_VALUE;
+}
+
+cls_status cls_dump_fronts_csv(cls_handle h, const char* path) {
+  if (!h || !h->eng || h->eng->symbolic().level_ptr.empty()) return CLS_INVALID_STATE;
+  if (!path) return CLS_INVALID_VALUE;
+  return write_text_file(path, fronts_csv(h->eng->symbolic())) ? CLS_SUCCESS : CLS_INVALID_VALUE;
 }
 
 // ===========================================================================
@@ -700,6 +714,15 @@ pf_status pf_plan_array(pf_handle h, const char* name, int32_t* out, int64_t cap
   if (!h || !h->eng || h->eng->dim() <= 0) return PF_INVALID_ARGUMENT;
   if (!copy_plan_array(*h->eng, name, out, capacity, len)) {
     h->err = std::string("unknown plan array or capacity too small: ") + (name ? name : "");
+    return PF_INVALID_ARGUMENT;
+  }
+  return PF_OK;
+}
+
+pf_status pf_dump_fronts_csv(pf_handle h, const char* path) {
+  if (!h || !h->eng || h->eng->symbolic().level_ptr.empty()) return PF_INVALID_ARGUMENT;
+  if (!path || !write_text_file(path, fronts_csv(h->eng->symbolic()))) {
+    h->err = std::string("cannot write the front CSV to ") + (path ? path : "(null)");
     return PF_INVALID_ARGUMENT;
   }
   return PF_OK;

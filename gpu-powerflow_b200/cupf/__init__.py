@@ -525,6 +525,12 @@ class NewtonSolver:
         _check(self._lib, self._h, self._lib.pf_info(self._h, C.byref(inf)))
         return {f[0]: getattr(inf, f[0]) for f in _capi.PfInfo._fields_}
 
+    def dump_fronts_csv(self, path) -> None:
+        """Per-front structure of the Jacobian's factor plan as CSV
+        (q,p,fsz,nc,uc,level,parent,asm_len,extend_elems; the reference's
+        front dump, custom_linear_solver/src/analyze/pipeline.cpp:162-193)."""
+        _check(self._lib, self._h, self._lib.pf_dump_fronts_csv(self._h, str(path).encode()))
+
     def plan_array(self, name: str) -> np.ndarray:
         ln = C.c_int64(0)
         _check(self._lib, self._h, self._lib.pf_plan_array(self._h, name.encode(), None, 0, C.byref(ln)))

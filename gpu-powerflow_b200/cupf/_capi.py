@@ -59,11 +59,11 @@ EXPORTS = [
     "cls_create", "cls_destroy", "cls_set_data", "cls_analyze", "cls_analyze_host", "cls_setup", "cls_set_stream", "cls_factorize",
     "cls_factorize_static_scratch",
     "cls_solve", "cls_solve_transpose", "cls_singular_flags", "cls_status_string", "cls_last_error",
-    "cls_plan_array",
+    "cls_plan_array", "cls_dump_fronts_csv",
     "pf_create", "pf_destroy", "pf_last_error", "pf_initialize", "pf_analyze_host", "pf_solve_batch", "pf_solve_batch_device",
     "pf_solve_batch_ybus", "pf_solve_batch_ybus_device",
     "pf_solve_batch_warm_device", "pf_solve_forward_device", "pf_solve_backward_device", "pf_solve_adjoint",
-    "pf_info", "pf_plan_array",
+    "pf_info", "pf_plan_array", "pf_dump_fronts_csv",
     "pf_evaluate", "pf_set_profiling", "pf_stage_times", "pf_plan_array64", "pf_singular_flags",
     "pf_case_load", "pf_case_last_error", "pf_case_dims", "pf_case_name", "pf_case_copy", "pf_case_destroy",
 ]
@@ -96,6 +96,7 @@ def _declare(lib: C.CDLL) -> None:
         "cls_status_string": ([_i32], C.c_char_p),
         "cls_last_error": ([_vp], C.c_char_p),
         "cls_plan_array": ([_vp, C.c_char_p, _vp, _i64, _p(_i64)], _i32),
+        "cls_dump_fronts_csv": ([_vp, C.c_char_p], _i32),
         "pf_create": ([_p(PfOptions), _p(_vp)], _i32),
         "pf_destroy": ([_vp], _i32),
         "pf_last_error": ([_vp], C.c_char_p),
@@ -119,6 +120,7 @@ def _declare(lib: C.CDLL) -> None:
                               _vp, _p(PfAdjointResult)], _i32),
         "pf_info": ([_vp, _p(PfInfo)], _i32),
         "pf_plan_array": ([_vp, C.c_char_p, _vp, _i64, _p(_i64)], _i32),
+        "pf_dump_fronts_csv": ([_vp, C.c_char_p], _i32),
         "pf_evaluate": ([_vp, _vp, _vp, _i32, _vp, _vp], _i32),
         "pf_set_profiling": ([_vp, _i32], _i32),
         "pf_plan_array64": ([_vp, C.c_char_p, _vp, _i64, _p(_i64)], _i32),

@@ -139,6 +139,11 @@ class LinearSolver:
         self._check(self._lib.cls_singular_flags(self._h, out.ctypes.data_as(C.c_void_p), self.batch))
         return out
 
+    def dump_fronts_csv(self, path) -> None:
+        """Per-front structure of the analysed plan as CSV (the columns of
+        SolverConfig::analyze_dump_fronts_path, solver.cpp:120)."""
+        self._check(self._lib.cls_dump_fronts_csv(self._h, str(path).encode()))
+
     def plan_array(self, name: str) -> np.ndarray:
         ln = C.c_int64(0)
         self._check(self._lib.cls_plan_array(self._h, name.encode(), None, 0, C.byref(ln)))

@@ -136,6 +136,16 @@ const char* cls_last_error(cls_handle h);
  * "front_off", "a_pos_csr", "graph_xadj", "graph_adjncy", "sym_col_ptr",
  * "sym_row_idx").  With out == NULL only *len is set. */
 cls_status cls_plan_array(cls_handle h, const char* name, int32_t* out, int64_t capacity, int64_t* len);
+/* Writes the per-front structure of the analysed plan to a CSV file:
+ * q,p,fsz,nc,uc,level,parent,asm_len,extend_elems, the columns of the
+ * reference's front dump (SolverConfig::analyze_dump_fronts_path,
+ * custom_linear_solver/src/solver.cpp:120, written by MaybeDumpFronts,
+ * analyze/pipeline.cpp:162-193).  Rows follow the panel levels, leaves first,
+ * each level's panels ascending: the order of the reference's dump under
+ * analyze_fronts_only; its full analysis lists the same rows in its own
+ * dispatch order inside each level.  Returns CLS_INVALID_VALUE when the file
+ * cannot be written. */
+cls_status cls_dump_fronts_csv(cls_handle h, const char* path);
 
 /* ------------------------------------------------------------------------ */
 /* Newton layer (NewtonSolver)                                               */
@@ -297,6 +307,8 @@ pf_status pf_info(pf_handle h, pf_info_t* out);
  * "map11", "map21", "map12", "map22", "diag11", "diag21", "diag12", "diag22",
  * plus every cls_plan_array name. */
 pf_status pf_plan_array(pf_handle h, const char* name, int32_t* out, int64_t capacity, int64_t* len);
+/* The front CSV of cls_dump_fronts_csv for the Newton handle's Jacobian plan. */
+pf_status pf_dump_fronts_csv(pf_handle h, const char* path);
 /* New (verification): evaluate the mismatch F and the Jacobian values at the
  * given voltages with the engine's own kernels.  Host buffers: V [batch][n_bus]
  * complex, sbus [batch][n_bus] complex; outputs F [batch][dim_f] and J

@@ -180,6 +180,8 @@ class Reference:
         L.ref_symbolic_names.argtypes = [C.c_void_p, C.c_char_p, C.c_int]
         L.ref_symbolic_free.restype = None
         L.ref_symbolic_free.argtypes = [C.c_void_p]
+        L.ref_symbolic_text.restype = C.c_int
+        L.ref_symbolic_text.argtypes = [C.c_void_p, C.c_char_p, C.c_char_p, C.c_int]
         L.ref_load_dump_case.restype = C.c_int
         L.ref_load_dump_case.argtypes = [C.c_char_p] + [C.POINTER(C.c_int32)] * 4 + [C.c_void_p] * 7
 
@@ -259,6 +261,14 @@ class Reference:
                 if ln > 0:
                     self.lib.ref_symbolic_copy(h, nm.encode(), a)
                 out[nm] = a
+            # the reference's own front CSVs (MaybeDumpFronts): the
+            # analyze_fronts_only order and the full analysis's order
+            for nm in ("fronts_csv_level", "fronts_csv_full"):
+                ln = self.lib.ref_symbolic_text(h, nm.encode(), None, 0)
+                if ln >= 0:
+                    tb = C.create_string_buffer(ln + 1)
+                    self.lib.ref_symbolic_text(h, nm.encode(), tb, ln + 1)
+                    out[nm] = tb.value.decode()
             return out
         finally:
             self.lib.ref_symbolic_free(h)

@@ -23,8 +23,12 @@
 // Everything else -- METIS ND, Etree, FillPattern, RelaxedPanels,
 // ComputeMultifrontalSymbolic, panel levels, subtree/tier orders, assembly
 // map, arena layout -- is the reference's code.
+#include <unistd.h>
+
 #include <algorithm>
 #include <cstdint>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <string>
@@ -39,7 +43,27 @@ namespace {
 
 struct RefSymbolic {
   std::map<std::string, std::vector<int>> arrays;
+  std::map<std::string, std::string> texts;
 };
+
+// The reference's MaybeDumpFronts (pipeline.cpp:162-193) writes to a path;
+// its output is read back as text.
+std::string dump_fronts_text(const custom_linear_solver::plan::MultifrontalPlan& plan) {
+  char path[] = "/tmp/ref_fronts_XXXXXX";
+  const int fd = mkstemp(path);
+  if (fd < 0) return std::string();
+  close(fd);
+  custom_linear_solver::plan::MaybeDumpFronts(plan, path);
+  std::string text;
+  if (FILE* f = std::fopen(path, "r")) {
+    char buf[4096];
+    size_t k;
+    while ((k = std::fread(buf, 1, sizeof buf, f)) > 0) text.append(buf, k);
+    std::fclose(f);
+  }
+  std::remove(path);
+  return text;
+}
 
 }  // namespace
 
@@ -204,6 +228,7 @@ void* ref_symbolic_run_m(int n, const int* csr_row_ptr, const int* csr_col_idx, 
     for (int p = 0; p < P; ++p) plcols[next[plevel[p]]++] = p;
   }
   plan.h_plcols = plcols;
+  out->texts["fronts_csv_level"] = dump_fronts_text(plan);  // the analyze_fronts_only dump
   A["plevel"] = plevel;
   A["panel_level_ptr"] = plan.panel_level_ptr;
   A["plcols_level"] = plcols;
@@ -226,6 +251,7 @@ void* ref_symbolic_run_m(int n, const int* csr_row_ptr, const int* csr_col_idx, 
   A["plcols_tier"] = plan.h_plcols_tier;
   A["level_tier_off"] = plan.h_level_tier_off;
   A["asm_local"] = BuildAssemblyMap(plan, sf, P);
+  out->texts["fronts_csv_full"] = dump_fronts_text(plan);  // the full analysis's dump
 
   // a_pos (formula of BuildAPosDevice, lower.cu:35-62), reported in CSR order
   std::vector<int> a_pos_csr(nnz, -1);
@@ -283,6 +309,17 @@ int ref_symbolic_names(void* h, char* buf, int cap) {
   if ((int)all.size() + 1 > cap) return -1;
   std::memcpy(buf, all.c_str(), all.size() + 1);
   return 0;
+}
+
+// Text outputs ("fronts_csv_level", "fronts_csv_full"): returns the length,
+// copying it (with a terminating NUL) when buf has room; -1 if unknown.
+int ref_symbolic_text(void* h, const char* name, char* buf, int cap) {
+  auto* s = static_cast<RefSymbolic*>(h);
+  auto it = s->texts.find(name);
+  if (it == s->texts.end()) return -1;
+  const int len = (int)it->second.size();
+  if (buf && cap > len) std::memcpy(buf, it->second.c_str(), (size_t)len + 1);
+  return len;
 }
 
 void ref_symbolic_free(void* h) { delete static_cast<RefSymbolic*>(h); }

@@ -79,6 +79,16 @@ class _Case:
         self.dim_f = self.pv.size + 2 * self.pq.size
 
 
+def fronts_hashes(sym: dict) -> dict:
+    """The reference's front CSVs (MaybeDumpFronts, pipeline.cpp:162-193):
+    the analyze_fronts_only dump as text, and the full analysis's rows with
+    their dispatch position q dropped, sorted (the same rows, another order)."""
+    level = sym["fronts_csv_level"]
+    rows = sorted(",".join(line.split(",")[1:]) for line in sym["fronts_csv_full"].splitlines()[1:])
+    return {"fronts_csv_level": hashlib.sha256(level.encode()).hexdigest(),
+            "fronts_rows_full": hashlib.sha256("\n".join(rows).encode()).hexdigest()}
+
+
 def read_mtx(path: Path):
     import scipy.io
     import scipy.sparse as sp
@@ -94,8 +104,22 @@ def read_mtx(path: Path):
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref-root", default="/root/reference")
+    ap.add_argument("--fronts-only", action="store_true",
+                    help="only add the front-CSV hashes to the existing hashes.json (other fixtures untouched)")
     args = ap.parse_args()
     ref = orc.Reference()
+    if args.fronts_only:
+        hashes = json.loads((HERE / "hashes.json").read_text())
+        for name, mk in {"118": G.grid_118, "500": G.grid_500, "2000": G.grid_2000, "10000": G.grid_10000}.items():
+            ja = ref.jacobian_analysis(mk())
+            hashes[f"grid{name}"]["fronts"] = fronts_hashes(ref.symbolic(ja["row_ptr"], ja["col_idx"],
+                                                                         parallel_nd=False))
+        for case in DATASETS:
+            d = np.load(HERE / f"linsys_{case}.npz")
+            hashes[case]["fronts"] = fronts_hashes(ref.symbolic(d["row_ptr"], d["col_idx"], parallel_nd=False))
+        (HERE / "hashes.json").write_text(json.dumps(hashes, indent=1, sort_keys=True) + "\n")
+        print("front-CSV hashes added to", HERE / "hashes.json")
+        return
     hashes: dict = {}
 
     c2 = G.two_bus_case()
@@ -112,7 +136,7 @@ def main() -> None:
         hashes[f"grid{name}"] = {"jacobian": {k: digest(ja[k]) for k in JAC_KEYS},
                                  "symbolic": {k: digest(sym[k]) for k in SYMBOLIC_KEYS},
                                  "front_total": int(sym["front_total"][0]), "dim": int(ja["row_ptr"].size - 1),
-                                 "nnz": int(ja["col_idx"].size)}
+                                 "nnz": int(ja["col_idx"].size), "fronts": fronts_hashes(sym)}
         symm = ref.symbolic(ja["row_ptr"], ja["col_idx"], parallel_nd=False, use_matching=True)
         hashes[f"grid{name}"]["symbolic_matching"] = {k: digest(symm[k]) for k in MATCHING_KEYS}
         if name == "118":
@@ -145,7 +169,8 @@ def main() -> None:
                             mismatch_inf_norm=meta["mismatch_inf_norm"])
         sym = ref.symbolic(rp, ci, parallel_nd=False)
         hashes[case] = {"symbolic": {k: digest(sym[k]) for k in SYMBOLIC_KEYS},
-                        "front_total": int(sym["front_total"][0]), "dim": int(rp.size - 1), "nnz": int(ci.size)}
+                        "front_total": int(sym["front_total"][0]), "dim": int(rp.size - 1), "nnz": int(ci.size),
+                        "fronts": fronts_hashes(sym)}
         symm = ref.symbolic(rp, ci, parallel_nd=False, use_matching=True)
         hashes[case]["symbolic_matching"] = {k: digest(symm[k]) for k in MATCHING_KEYS}
 

@@ -228,3 +228,59 @@ def test_matching_fails_without_a_perfect_matching():
     ls.set_data(rp, ci)
     with pytest.raises(Exception):
         ls.analyze_host()
+
+
+def _sha(text: str) -> str:
+    return hashlib.sha256(text.encode()).hexdigest()
+
+
+def _rows_without_q(text: str) -> str:
+    return "\n".join(sorted(",".join(line.split(",")[1:]) for line in text.splitlines()[1:]))
+
+
+@pytest.mark.parametrize("name", list(GRIDS))
+def test_fronts_csv_matches_the_reference_dump(analyzed, name, tmp_path):
+    """pf_dump_fronts_csv writes, byte for byte, the reference's front dump
+    under analyze_fronts_only (MaybeDumpFronts, analyze/pipeline.cpp:162-193);
+    its full analysis lists the same rows in its own order inside each
+    level."""
+    path = tmp_path / "fronts.csv"
+    analyzed(name).dump_fronts_csv(path)
+    text = path.read_text()
+    assert text.startswith("q,p,fsz,nc,uc,level,parent,asm_len,extend_elems\n")
+    gold = HASHES[f"grid{name}"]["fronts"]
+    assert _sha(text) == gold["fronts_csv_level"]
+    assert _sha(_rows_without_q(text)) == gold["fronts_rows_full"]
+
+
+@pytest.mark.parametrize("case", ["case118", "case1354pegase"])
+def test_linear_solver_fronts_csv_on_reference_datasets(case, tmp_path):
+    d = np.load(GOLD / f"linsys_{case}.npz")
+    ls = cupf.LinearSolver(cupf.SolverConfig(serial_nd=True))
+    ls.set_data(d["row_ptr"], d["col_idx"])
+    ls.analyze_host()
+    path = tmp_path / "fronts.csv"
+    ls.dump_fronts_csv(path)
+    text = path.read_text()
+    assert _sha(text) == HASHES[case]["fronts"]["fronts_csv_level"]
+    assert _sha(_rows_without_q(text)) == HASHES[case]["fronts"]["fronts_rows_full"]
+    with pytest.raises(Exception):
+        ls.dump_fronts_csv(tmp_path / "no_such_dir" / "fronts.csv")
+
+
+@pytest.mark.skipif(not __import__("oracle.oracle", fromlist=["LIB_REF"]).LIB_REF.exists(),
+                    reason="oracle/_ref not built (reference sources absent)")
+def test_fronts_csv_against_the_live_reference(analyzed, tmp_path):
+    """The same on the 118-bus grid against the reference run here: the text
+    itself, so a difference shows where it is."""
+    from oracle.oracle import Reference
+
+    g = GRIDS["118"]()
+    s = analyzed("118")
+    ref = Reference()
+    sym = ref.symbolic(s.plan_array("jac_row_ptr"), s.plan_array("jac_col_idx"), parallel_nd=False)
+    path = tmp_path / "fronts.csv"
+    s.dump_fronts_csv(path)
+    assert path.read_text() == sym["fronts_csv_level"]
+    assert _rows_without_q(path.read_text()) == _rows_without_q(sym["fronts_csv_full"])
+    assert g.n_bus == 118
