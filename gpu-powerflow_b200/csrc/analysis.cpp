@@ -224,16 +224,17 @@ std::vector<int32_t> nd_recurse(const Graph& g, int depth, int base_thr, int see
 }
 
 // RunNdOnGraph (metis_nd.cpp:241-278) with the reference's parallel-ND knobs
-// (depth 4, base 4000 below 20000 vertices else 20000; pipeline.hpp defaults).
+// (recursion depth; base-case size base_small below 20,000 vertices, else
+// base_large; defaults 4, 4000, 20000).
 std::vector<int32_t> nd_order(const std::vector<int32_t>& xadj, const std::vector<int32_t>& adjncy, int n,
-                              bool serial, int seed) {
+                              bool serial, int seed, int depth, int base_small, int base_large) {
   std::vector<int32_t> perm(n);
   std::iota(perm.begin(), perm.end(), 0);
   if (n <= 1 || adjncy.empty()) return perm;
   Graph g{std::vector<idx_t>(xadj.begin(), xadj.end()), std::vector<idx_t>(adjncy.begin(), adjncy.end())};
   if (!serial) {
-    const int base_thr = n < 20000 ? 4000 : 20000;
-    return nd_recurse(g, 4, base_thr, seed);
+    const int base_thr = n < 20000 ? base_small : base_large;
+    return nd_recurse(g, depth, base_thr, seed);
   }
   return nodend(g, seed);
 }
@@ -389,7 +390,8 @@ SymbolicPlan analyze_symbolic(int32_t n, const int32_t* row_ptr, const int32_t* 
   // Ordering (pipeline.cpp:236-258).  perm orders the rows; the columns
   // follow the rows, or with a matching the matched column of each row:
   // col_perm[k] = row_to_col[perm[k]], iperm = col_perm^-1.
-  sp.perm = nd_order(sp.graph_xadj, sp.graph_adjncy, n, opt.serial_nd, opt.metis_seed);
+  sp.perm = nd_order(sp.graph_xadj, sp.graph_adjncy, n, opt.serial_nd, opt.metis_seed, opt.par_nd_depth,
+                     opt.par_nd_base_small, opt.par_nd_base_large);
   sp.row_iperm.assign(n, 0);
   for (int32_t k = 0; k < n; ++k) sp.row_iperm[sp.perm[k]] = k;
   if (opt.use_matching) {

@@ -45,6 +45,9 @@ struct SymbolicOptions {
   bool serial_nd = true;     // one METIS_NodeND call; false = separator recursion
   int metis_seed = 42;
   bool use_matching = false;  // structural (Hopcroft-Karp) column matching
+  // separator recursion (serial_nd = false): depth and base-case sizes, the
+  // small one below 20,000 vertices (SolverConfig::parallel_nd_*, solver.hpp:44-46)
+  int par_nd_depth = 4, par_nd_base_small = 4000, par_nd_base_large = 20000;
 };
 
 struct SymbolicPlan {

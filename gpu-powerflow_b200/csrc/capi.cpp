@@ -50,6 +50,9 @@ EngineConfig engine_config(const cls_config& c, int32_t compute, int32_t use_gra
   e.static_pivot = c.pivot_strategy == CLS_PIVOT_STATIC_DIAGONAL_SHIFT ? 1 : 0;
   e.shift_epsilon = c.shift_retry_epsilon;
   e.autotune = c.autotune;
+  e.par_nd_depth = c.parallel_nd_depth > 0 ? c.parallel_nd_depth : 4;
+  e.par_nd_base_small = c.parallel_nd_base_small > 0 ? c.parallel_nd_base_small : 4000;
+  e.par_nd_base_large = c.parallel_nd_base_large > 0 ? c.parallel_nd_base_large : 20000;
   e.use_cuda_graph = use_graph;
   return e;
 }
@@ -172,7 +175,8 @@ cls_status cls_create(const cls_config* config, cls_handle* out) {
   cls_config c{CLS_PRECISION_FP64, 0, CLS_PIVOT_STATIC_DIAGONAL_SHIFT, 1, 8, 1e-8};
   if (config) c = *config;
   if ((c.matching != 0 && c.matching != 1) || c.max_panel_width < 1 || c.max_panel_width > 8 ||
-      (c.autotune != 0 && c.autotune != 1))
+      (c.autotune != 0 && c.autotune != 1) || c.parallel_nd_depth < 0 || c.parallel_nd_base_small < 0 ||
+      c.parallel_nd_base_large < 0)
     return CLS_INVALID_VALUE;
   auto* h = new (std::nothrow) cls_solver_s();
   if (!h) return CLS_ALLOCATION_FAILED;
@@ -371,6 +375,8 @@ pf_status pf_create(const pf_options* options, pf_handle* out) {
       throw std::invalid_argument("NewtonSolver: matching must be None or Structural");
     if (o.custom.autotune != 0 && o.custom.autotune != 1)
       throw std::invalid_argument("NewtonSolver: autotune must be 0 or 1");
+    if (o.custom.parallel_nd_depth < 0 || o.custom.parallel_nd_base_small < 0 || o.custom.parallel_nd_base_large < 0)
+      throw std::invalid_argument("NewtonSolver: the parallel nested-dissection parameters must not be negative");
     if (o.cuda_jacobian < PF_JACOBIAN_EDGE || o.cuda_jacobian > PF_JACOBIAN_VERTEX_WARP)
       throw std::invalid_argument("NewtonSolver: cuda_jacobian must be Edge, EdgeAtomic or VertexWarp");
     cls_config c = o.custom;

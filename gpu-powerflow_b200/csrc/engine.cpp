@@ -468,6 +468,9 @@ void Engine::analyze_host(int32_t n_bus, const int32_t* indptr, const int32_t* i
   so.max_panel_width = cfg_.max_panel_width;
   so.serial_nd = cfg_.serial_nd != 0;
   so.use_matching = cfg_.use_matching != 0;
+  so.par_nd_depth = cfg_.par_nd_depth;
+  so.par_nd_base_small = cfg_.par_nd_base_small;
+  so.par_nd_base_large = cfg_.par_nd_base_large;
   sp_ = analyze_symbolic(ja_.dim, ja_.row_ptr.data(), ja_.col_idx.data(), so);
   fp_ = build_factor_program(sp_);
   if (fp_.max_fsz > 64) throw std::runtime_error("initialize: a front exceeds 64 rows (unsupported)");
@@ -487,6 +490,9 @@ void Engine::analyze_matrix_host(int32_t n, int32_t nnz, const int32_t* row_ptr,
   so.max_panel_width = cfg_.max_panel_width;
   so.serial_nd = cfg_.serial_nd != 0;
   so.use_matching = cfg_.use_matching != 0;
+  so.par_nd_depth = cfg_.par_nd_depth;
+  so.par_nd_base_small = cfg_.par_nd_base_small;
+  so.par_nd_base_large = cfg_.par_nd_base_large;
   sp_ = analyze_symbolic(n, row_ptr, col_idx, so);
   fp_ = build_factor_program(sp_);
 }
@@ -503,6 +509,9 @@ void Engine::initialize_matrix(int32_t n, int32_t nnz, const int32_t* row_ptr, c
   so.max_panel_width = cfg_.max_panel_width;
   so.serial_nd = cfg_.serial_nd != 0;
   so.use_matching = cfg_.use_matching != 0;
+  so.par_nd_depth = cfg_.par_nd_depth;
+  so.par_nd_base_small = cfg_.par_nd_base_small;
+  so.par_nd_base_large = cfg_.par_nd_base_large;
   sp_ = analyze_symbolic(n, row_ptr, col_idx, so);
   fp_ = build_factor_program(sp_);
   if (fp_.max_fsz > 64) throw std::runtime_error("Analyze: a front exceeds 64 rows (unsupported)");

@@ -35,6 +35,7 @@ struct EngineConfig {
   int32_t use_cuda_graph = 0;     // run each solve as one graph (device-side convergence test)
   int32_t adjoint_refine_steps = 2;
   int32_t autotune = 0;           // tune the factor levels' warps per block per batch size
+  int32_t par_nd_depth = 4, par_nd_base_small = 4000, par_nd_base_large = 20000;
 };
 
 struct SolveStats {

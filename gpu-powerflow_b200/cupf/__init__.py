@@ -116,7 +116,8 @@ class CuDSSOptions(_Struct):
 class CustomSolverConfig(_Struct):
     _fields = {"precision": CustomPrecision.FP32, "matching": CustomMatchingMode["None"],
                "pivot_strategy": CustomPivotStrategy.StaticDiagonalShift, "serial_nd": False,
-               "max_panel_width": 8, "shift_retry_epsilon": 1.0e-8, "autotune": True}
+               "max_panel_width": 8, "shift_retry_epsilon": 1.0e-8, "autotune": True,
+               "parallel_nd_depth": 4, "parallel_nd_base_small": 4000, "parallel_nd_base_large": 20000}
 
 
 class NewtonOptions(_Struct):
@@ -264,7 +265,8 @@ def _check(lib, h, st: int) -> None:
 
 def _cls_config(c: CustomSolverConfig) -> _capi.ClsConfig:
     return _capi.ClsConfig(int(c.precision), int(c.matching), int(c.pivot_strategy), int(bool(c.serial_nd)),
-                           int(c.max_panel_width), float(c.shift_retry_epsilon), int(bool(c.autotune)))
+                           int(c.max_panel_width), float(c.shift_retry_epsilon), int(bool(c.autotune)),
+                           int(c.parallel_nd_depth), int(c.parallel_nd_base_small), int(c.parallel_nd_base_large))
 
 
 def _nr_config(cfg: NRConfig | None) -> _capi.PfNRConfig:

@@ -24,7 +24,8 @@ class SolverConfig:
 
     def __init__(self, precision: int = 0, pivot_strategy: int = 1, serial_nd: bool = True,
                  max_panel_width: int = 8, shift_retry_epsilon: float = 1e-8, matching: int = 0,
-                 autotune: bool = True):
+                 autotune: bool = True, parallel_nd_depth: int = 4, parallel_nd_base_small: int = 4000,
+                 parallel_nd_base_large: int = 20000):
         self.precision = int(precision)
         self.matching = int(matching)  # MatchingMode: 0 None, 1 Structural
         self.pivot_strategy = int(pivot_strategy)
@@ -32,6 +33,10 @@ class SolverConfig:
         self.max_panel_width = int(max_panel_width)
         self.shift_retry_epsilon = float(shift_retry_epsilon)
         self.autotune = bool(autotune)  # per-level factor launch shapes timed at the first factorization
+        # separator recursion when serial_nd is False (SolverConfig::parallel_nd_*)
+        self.parallel_nd_depth = int(parallel_nd_depth)
+        self.parallel_nd_base_small = int(parallel_nd_base_small)
+        self.parallel_nd_base_large = int(parallel_nd_base_large)
 
 
 class CustomSolverError(RuntimeError):
@@ -45,7 +50,8 @@ class LinearSolver:
         self._lib = _capi.load()
         c = config or SolverConfig()
         cfg = _capi.ClsConfig(c.precision, c.matching, c.pivot_strategy, int(c.serial_nd), c.max_panel_width,
-                              c.shift_retry_epsilon, int(c.autotune))
+                              c.shift_retry_epsilon, int(c.autotune), c.parallel_nd_depth, c.parallel_nd_base_small,
+                              c.parallel_nd_base_large)
         h = C.c_void_p()
         st = self._lib.cls_create(C.byref(cfg), C.byref(h))
         if st:

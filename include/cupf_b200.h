@@ -78,6 +78,11 @@ typedef struct {
                                    values and keep the fastest per level (results do not change:
                                    the warps of a block share one front's arithmetic, each
                                    element's operation order is fixed); 0 = built-in rule */
+  int32_t parallel_nd_depth;    /* separator recursion when serial_nd = 0 (SolverConfig::
+                                   parallel_nd_depth, parallel_nd_base_small, parallel_nd_base_large,
+                                   solver.hpp:44-46): recursion depth, and the graph size below */
+  int32_t parallel_nd_base_small; /* which a part is ordered by one METIS call, for graphs of fewer */
+  int32_t parallel_nd_base_large; /* than 20,000 vertices / otherwise; 0 = the defaults 4, 4000, 20000 */
 } cls_config;
 
 typedef struct cls_solver_s* cls_handle;

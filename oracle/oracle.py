@@ -172,6 +172,8 @@ class Reference:
         L.ref_symbolic_run.argtypes = [C.c_int, _i32p, _i32p, C.c_int, C.c_int, C.c_int]
         L.ref_symbolic_run_m.restype = C.c_void_p
         L.ref_symbolic_run_m.argtypes = [C.c_int, _i32p, _i32p, C.c_int, C.c_int, C.c_int, C.c_int]
+        L.ref_symbolic_run_p.restype = C.c_void_p
+        L.ref_symbolic_run_p.argtypes = [C.c_int, _i32p, _i32p] + [C.c_int] * 7
         L.ref_symbolic_len.restype = C.c_int
         L.ref_symbolic_len.argtypes = [C.c_void_p, C.c_char_p]
         L.ref_symbolic_copy.restype = C.c_int
@@ -243,11 +245,14 @@ class Reference:
         return out
 
     def symbolic(self, row_ptr, col_idx, max_panel_width: int = 8, parallel_nd: bool = False,
-                 float_front: bool = True, use_matching: bool = False) -> dict:
+                 float_front: bool = True, use_matching: bool = False, nd_depth: int = 4,
+                 nd_base_small: int = 4000, nd_base_large: int = 20000) -> dict:
+        """The reference's symbolic analysis; nd_* are SolverConfig's
+        parallel_nd_depth / parallel_nd_base_small / parallel_nd_base_large."""
         rp, ci = _i32(row_ptr), _i32(col_idx)
         n = rp.size - 1
-        h = self.lib.ref_symbolic_run_m(n, rp, ci, max_panel_width, int(parallel_nd), int(float_front),
-                                        int(use_matching))
+        h = self.lib.ref_symbolic_run_p(n, rp, ci, max_panel_width, int(parallel_nd), int(float_front),
+                                        int(use_matching), nd_depth, nd_base_small, nd_base_large)
         if not h:
             raise RuntimeError("reference symbolic analysis failed")
         try:

@@ -69,8 +69,9 @@ std::string dump_fronts_text(const custom_linear_solver::plan::MultifrontalPlan&
 
 extern "C" {
 
-void* ref_symbolic_run_m(int n, const int* csr_row_ptr, const int* csr_col_idx, int max_panel_width,
-                         int parallel_nd, int float_front, int use_matching) {
+void* ref_symbolic_run_p(int n, const int* csr_row_ptr, const int* csr_col_idx, int max_panel_width,
+                         int parallel_nd, int float_front, int use_matching, int nd_depth, int nd_base_small,
+                         int nd_base_large) {
   using namespace custom_linear_solver;
   using namespace custom_linear_solver::plan;
   namespace sym = custom_linear_solver::symbolic;
@@ -125,7 +126,8 @@ void* ref_symbolic_run_m(int n, const int* csr_row_ptr, const int* csr_col_idx, 
   std::vector<int> perm(n, 0);
   {
     std::vector<int> gx = xadj, ga = adjncy;
-    if (!reordering::MetisNdFromGraph(n, gx, ga, perm, parallel_nd != 0, 42, 4, 4000, 20000)) {
+    if (!reordering::MetisNdFromGraph(n, gx, ga, perm, parallel_nd != 0, 42, nd_depth, nd_base_small,
+                                      nd_base_large)) {
       delete out;
       return nullptr;
     }
@@ -278,6 +280,13 @@ void* ref_symbolic_run_m(int n, const int* csr_row_ptr, const int* csr_col_idx, 
     }
   A["a_pos_csr"] = a_pos_csr;
   return out;
+}
+
+// SolverConfig defaults for the parallel-ND knobs (solver.hpp:44-46)
+void* ref_symbolic_run_m(int n, const int* csr_row_ptr, const int* csr_col_idx, int max_panel_width,
+                         int parallel_nd, int float_front, int use_matching) {
+  return ref_symbolic_run_p(n, csr_row_ptr, csr_col_idx, max_panel_width, parallel_nd, float_front, use_matching, 4,
+                            4000, 20000);
 }
 
 void* ref_symbolic_run(int n, const int* csr_row_ptr, const int* csr_col_idx, int max_panel_width,

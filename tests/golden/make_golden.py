@@ -89,6 +89,22 @@ def fronts_hashes(sym: dict) -> dict:
             "fronts_rows_full": hashlib.sha256("\n".join(rows).encode()).hexdigest()}
 
 
+# separator recursion (SolverConfig::parallel_nd_*) where the Jacobian's graph
+# is split: (grid, depth, base_small); the oracle serialises the reference's
+# METIS calls, so its threaded recursion is deterministic
+PARALLEL_ND_CASES = (("2000", 2, 500), ("2000", 4, 1000), ("10000", 4, 4000))
+
+
+def parallel_nd_hashes(ref) -> dict:
+    grids = {"2000": G.grid_2000, "10000": G.grid_10000}
+    out = {}
+    for name, depth, small in PARALLEL_ND_CASES:
+        ja = ref.jacobian_analysis(grids[name]())
+        sym = ref.symbolic(ja["row_ptr"], ja["col_idx"], parallel_nd=True, nd_depth=depth, nd_base_small=small)
+        out[f"grid{name}_d{depth}_b{small}"] = {k: digest(sym[k]) for k in SYMBOLIC_KEYS}
+    return out
+
+
 def read_mtx(path: Path):
     import scipy.io
     import scipy.sparse as sp
@@ -104,12 +120,14 @@ def read_mtx(path: Path):
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref-root", default="/root/reference")
-    ap.add_argument("--fronts-only", action="store_true",
-                    help="only add the front-CSV hashes to the existing hashes.json (other fixtures untouched)")
+    ap.add_argument("--added-only", action="store_true",
+                    help="only add the front-CSV and parallel-ND hashes to the existing hashes.json "
+                         "(other fixtures untouched)")
     args = ap.parse_args()
     ref = orc.Reference()
-    if args.fronts_only:
+    if args.added_only:
         hashes = json.loads((HERE / "hashes.json").read_text())
+        hashes["parallel_nd"] = parallel_nd_hashes(ref)
         for name, mk in {"118": G.grid_118, "500": G.grid_500, "2000": G.grid_2000, "10000": G.grid_10000}.items():
             ja = ref.jacobian_analysis(mk())
             hashes[f"grid{name}"]["fronts"] = fronts_hashes(ref.symbolic(ja["row_ptr"], ja["col_idx"],
@@ -118,7 +136,7 @@ def main() -> None:
             d = np.load(HERE / f"linsys_{case}.npz")
             hashes[case]["fronts"] = fronts_hashes(ref.symbolic(d["row_ptr"], d["col_idx"], parallel_nd=False))
         (HERE / "hashes.json").write_text(json.dumps(hashes, indent=1, sort_keys=True) + "\n")
-        print("front-CSV hashes added to", HERE / "hashes.json")
+        print("front-CSV and parallel-ND hashes added to", HERE / "hashes.json")
         return
     hashes: dict = {}
 
@@ -182,6 +200,7 @@ def main() -> None:
     hashes["case118_rowperm"] = {"symbolic_matching": {k: digest(symm[k]) for k in MATCHING_KEYS},
                                  "seed": ROWPERM_SEED}
 
+    hashes["parallel_nd"] = parallel_nd_hashes(ref)
     (HERE / "hashes.json").write_text(json.dumps(hashes, indent=1, sort_keys=True) + "\n")
     print("golden fixtures written to", HERE)
 

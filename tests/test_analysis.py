@@ -284,3 +284,60 @@ def test_fronts_csv_against_the_live_reference(analyzed, tmp_path):
     assert path.read_text() == sym["fronts_csv_level"]
     assert _rows_without_q(path.read_text()) == _rows_without_q(sym["fronts_csv_full"])
     assert g.n_bus == 118
+
+
+@pytest.mark.skipif(not __import__("oracle.oracle", fromlist=["LIB_REF"]).LIB_REF.exists(),
+                    reason="oracle/_ref not built (reference sources absent)")
+@pytest.mark.parametrize("name,depth,small", [("2000", 2, 500), ("2000", 4, 1000), ("10000", 4, 4000)])
+def test_parallel_nd_matches_the_reference_recursion(name, depth, small):
+    """Separator recursion (serial_nd = False) with SolverConfig's
+    parallel_nd_depth / parallel_nd_base_small (metis_nd.cpp:241-278), at
+    sizes where the Jacobian's graph is split: every plan array equals the
+    reference's own recursion.  The oracle runs the reference with its METIS
+    calls serialised (oracle/ref_shim/metis_lock_shim.c), which makes its
+    threaded recursion deterministic; the engine runs the halves one after
+    the other."""
+    from oracle.oracle import Reference
+
+    g = GRIDS[name]()
+    o = cupf.NewtonOptions()
+    o.backend = cupf.BackendKind.CUDA
+    o.custom.serial_nd = False
+    o.custom.parallel_nd_depth = depth
+    o.custom.parallel_nd_base_small = small
+    s = cupf.NewtonSolver(o)
+    s.analyze_host(g.indptr, g.indices, g.n_bus, g.pv, g.pq)
+    ref = Reference()
+    rp, ci = s.plan_array("jac_row_ptr"), s.plan_array("jac_col_idx")
+    r1 = ref.symbolic(rp, ci, parallel_nd=True, nd_depth=depth, nd_base_small=small)
+    r2 = ref.symbolic(rp, ci, parallel_nd=True, nd_depth=depth, nd_base_small=small)
+    assert np.array_equal(r1["perm"], r2["perm"])  # the serialised reference is deterministic
+    bad = [ours for ours, r in SYMBOLIC.items() if not np.array_equal(s.plan_array(ours), r1[r])]
+    assert not bad, f"arrays differing from the reference: {bad}"
+    serial = _analyzed(g, True)
+    assert not np.array_equal(s.plan_array("perm"), serial.plan_array("perm"))  # the graph was split
+
+
+def test_parallel_nd_parameters_are_validated():
+    o = cupf.NewtonOptions()
+    o.backend = cupf.BackendKind.CUDA
+    o.custom.parallel_nd_depth = -1
+    with pytest.raises(ValueError):
+        cupf.NewtonSolver(o)
+
+
+@pytest.mark.parametrize("name,depth,small", [("2000", 2, 500), ("2000", 4, 1000), ("10000", 4, 4000)])
+def test_parallel_nd_matches_the_reference_golden(name, depth, small):
+    """The same cases against the committed hashes of the reference's plan
+    (tests/golden/make_golden.py), so the check stands without the reference."""
+    g = GRIDS[name]()
+    o = cupf.NewtonOptions()
+    o.backend = cupf.BackendKind.CUDA
+    o.custom.serial_nd = False
+    o.custom.parallel_nd_depth = depth
+    o.custom.parallel_nd_base_small = small
+    s = cupf.NewtonSolver(o)
+    s.analyze_host(g.indptr, g.indices, g.n_bus, g.pv, g.pq)
+    gold = HASHES["parallel_nd"][f"grid{name}_d{depth}_b{small}"]
+    bad = [ours for ours, ref in SYMBOLIC.items() if digest(s.plan_array(ours)) != gold[ref]]
+    assert not bad, f"arrays differing from the reference: {bad}"
