@@ -105,6 +105,20 @@ def parallel_nd_hashes(ref) -> dict:
     return out
 
 
+# relaxed-panel caps below the default 8 (SolverConfig::max_panel_width)
+PANEL_WIDTH_CASES = (("118", 1), ("118", 2), ("118", 4), ("2000", 1), ("2000", 2), ("2000", 4))
+
+
+def panel_width_hashes(ref) -> dict:
+    grids = {"118": G.grid_118, "2000": G.grid_2000}
+    out = {}
+    for name, w in PANEL_WIDTH_CASES:
+        ja = ref.jacobian_analysis(grids[name]())
+        sym = ref.symbolic(ja["row_ptr"], ja["col_idx"], max_panel_width=w, parallel_nd=False)
+        out[f"grid{name}_w{w}"] = {k: digest(sym[k]) for k in SYMBOLIC_KEYS}
+    return out
+
+
 def read_mtx(path: Path):
     import scipy.io
     import scipy.sparse as sp
@@ -121,13 +135,14 @@ def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref-root", default="/root/reference")
     ap.add_argument("--added-only", action="store_true",
-                    help="only add the front-CSV and parallel-ND hashes to the existing hashes.json "
+                    help="only add the front-CSV, parallel-ND and panel-width hashes to the existing hashes.json "
                          "(other fixtures untouched)")
     args = ap.parse_args()
     ref = orc.Reference()
     if args.added_only:
         hashes = json.loads((HERE / "hashes.json").read_text())
         hashes["parallel_nd"] = parallel_nd_hashes(ref)
+        hashes["panel_width"] = panel_width_hashes(ref)
         for name, mk in {"118": G.grid_118, "500": G.grid_500, "2000": G.grid_2000, "10000": G.grid_10000}.items():
             ja = ref.jacobian_analysis(mk())
             hashes[f"grid{name}"]["fronts"] = fronts_hashes(ref.symbolic(ja["row_ptr"], ja["col_idx"],
@@ -136,7 +151,7 @@ def main() -> None:
             d = np.load(HERE / f"linsys_{case}.npz")
             hashes[case]["fronts"] = fronts_hashes(ref.symbolic(d["row_ptr"], d["col_idx"], parallel_nd=False))
         (HERE / "hashes.json").write_text(json.dumps(hashes, indent=1, sort_keys=True) + "\n")
-        print("front-CSV and parallel-ND hashes added to", HERE / "hashes.json")
+        print("front-CSV, parallel-ND and panel-width hashes added to", HERE / "hashes.json")
         return
     hashes: dict = {}
 
@@ -201,6 +216,7 @@ def main() -> None:
                                  "seed": ROWPERM_SEED}
 
     hashes["parallel_nd"] = parallel_nd_hashes(ref)
+    hashes["panel_width"] = panel_width_hashes(ref)
     (HERE / "hashes.json").write_text(json.dumps(hashes, indent=1, sort_keys=True) + "\n")
     print("golden fixtures written to", HERE)
 

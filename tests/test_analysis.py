@@ -341,3 +341,20 @@ def test_parallel_nd_matches_the_reference_golden(name, depth, small):
     gold = HASHES["parallel_nd"][f"grid{name}_d{depth}_b{small}"]
     bad = [ours for ours, ref in SYMBOLIC.items() if digest(s.plan_array(ours)) != gold[ref]]
     assert not bad, f"arrays differing from the reference: {bad}"
+
+
+@pytest.mark.parametrize("name,width", [("118", 1), ("118", 2), ("118", 4), ("2000", 1), ("2000", 2), ("2000", 4)])
+def test_symbolic_plan_at_other_panel_widths(name, width):
+    """Relaxed panels capped below 8 (SolverConfig::max_panel_width,
+    supernode.cpp:55-92): every plan array equals the reference's."""
+    g = GRIDS[name]()
+    o = cupf.NewtonOptions()
+    o.backend = cupf.BackendKind.CUDA
+    o.custom.serial_nd = True
+    o.custom.max_panel_width = width
+    s = cupf.NewtonSolver(o)
+    s.analyze_host(g.indptr, g.indices, g.n_bus, g.pv, g.pq)
+    gold = HASHES["panel_width"][f"grid{name}_w{width}"]
+    bad = [ours for ours, ref in SYMBOLIC.items() if digest(s.plan_array(ours)) != gold[ref]]
+    assert not bad, f"arrays differing from the reference: {bad}"
+    assert int(s.plan_array("panel_ncols").max()) <= width
