@@ -360,3 +360,27 @@ def test_autotuned_factor_launches_give_identical_solves(policy, graph):
         assert wb.size > 0 and set(wb.tolist()) <= {0, 1, 2, 4, 8}
     assert not base.plan_array("factor_level_warps").any()
     assert not base.plan_array("backward_launch_warps").any()
+
+
+@pytest.mark.parametrize("width,serial", [(1, True), (4, True), (8, False)])
+def test_other_plans_solve_like_the_oracle(oracle, width, serial):
+    """The numeric path on plans other than the default: relaxed panels capped
+    at 1 or 4 columns, and a separator-recursion ordering split down to
+    500-vertex parts.  V within 1e-8 of the FP64 oracle on the 2,000-bus grid."""
+    g = G.grid_2000()
+    o = cupf.NewtonOptions()
+    o.backend = cupf.BackendKind.CUDA
+    o.compute = cupf.ComputePolicy.Mixed
+    o.custom.serial_nd = serial
+    o.custom.max_panel_width = width
+    o.custom.parallel_nd_depth = 4
+    o.custom.parallel_nd_base_small = 500
+    s = cupf.NewtonSolver(o)
+    s.initialize(g.indptr, g.indices, g.data, g.n_bus, g.n_bus, g.pv, g.pq)
+    B = 16
+    S, V0 = g.scenarios(B, seed=61), g.flat_start(B)
+    r = solve(s, g, S, V0, cfg())
+    assert r.converged_numpy.all()
+    for b in (0, 7, 15):
+        ref = oracle.solve(g, S[b], V0[b], tol=1e-12, max_iter=30)
+        assert np.abs(r.V_numpy[b] - ref["V"]).max() <= 1e-8
