@@ -973,10 +973,10 @@ SolveStats Engine::run_loop(double tol, int32_t max_iter, int32_t prepare_adjoin
     completed = hc->completed;
     gmax = hc->gmax;
     nonfinite = hc->nonfinite != 0;
-    // first mismatch + test, then per update: the body, plus the closing
-    // mismatch and test when the cap stopped the loop
+    // control load and store, the first mismatch + test, then per update:
+    // the body, plus the closing mismatch and test when the cap stopped the loop
     const int64_t updates = (gmax <= tol || hc->status) ? completed - 1 : completed;
-    launches_ += 2 + updates * d.graph_body_launches;
+    launches_ += 4 + updates * d.graph_body_launches;
     if (debug_sync()) std::fprintf(stderr, "[cupf] %d norm evaluations, max ||F||inf = %.3e\n", completed, gmax);
     if (hc->status) throw std::runtime_error("NewtonSolver: mismatch norm is not finite");
   } else if (max_iter > 0) {
