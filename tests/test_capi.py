@@ -1,6 +1,7 @@
 """The C ABI (include/cupf_b200.h, libcupf_b200.so) and the Python mirror of
 the reference's cupf API, exercised without a GPU: symbols, option defaults,
 argument checks and error behaviour."""
+import ctypes as C
 import re
 from pathlib import Path
 
@@ -182,3 +183,32 @@ def test_null_handle_calls_are_rejected():
     assert lib.pf_set_profiling(None, 1) != 0
     assert isinstance(lib.cls_last_error(None), bytes)
     assert isinstance(lib.pf_last_error(None), bytes)
+
+
+def test_new_options_and_exports_are_checked(tmp_path):
+    """autotune must be 0 or 1 and the parallel-ND parameters non-negative;
+    the front CSV needs an analysed plan and a writable path."""
+    lib = _capi.load()
+    for bad in ({"autotune": 2}, {"parallel_nd_depth": -1}, {"parallel_nd_base_small": -5},
+                {"parallel_nd_base_large": -1}):
+        c = _capi.ClsConfig(0, 0, 1, 1, 8, 1e-8, 0, 0, 0, 0)
+        for k, v in bad.items():
+            setattr(c, k, v)
+        h = C.c_void_p()
+        assert lib.cls_create(C.byref(c), C.byref(h)) != 0, bad
+    # zero parallel-ND fields are the defaults
+    c = _capi.ClsConfig(0, 0, 1, 1, 8, 1e-8, 0, 0, 0, 0)
+    h = C.c_void_p()
+    assert lib.cls_create(C.byref(c), C.byref(h)) == 0
+    assert lib.cls_dump_fronts_csv(h, str(tmp_path / "f.csv").encode()) != 0  # nothing analysed yet
+    lib.cls_destroy(h)
+    assert lib.cls_dump_fronts_csv(None, b"x") != 0
+    assert lib.pf_dump_fronts_csv(None, b"x") != 0
+    g = G.grid_118()
+    s = _solver()
+    s.analyze_host(g.indptr, g.indices, g.n_bus, g.pv, g.pq)
+    with pytest.raises(ValueError):
+        s.dump_fronts_csv(tmp_path / "missing_dir" / "f.csv")
+    s.dump_fronts_csv(tmp_path / "f.csv")
+    lines = (tmp_path / "f.csv").read_text().splitlines()
+    assert len(lines) == 1 + s.info()["num_panels"]
