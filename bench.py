@@ -432,6 +432,27 @@ def run_engine(args) -> None:
     conv_pipe = sum(int((f <= TOL).sum()) for f in fm_bufs[: args.steps])
     e2e_value = _reduce(conv_pipe / args.steps, "sum", world, dev) / (ms_e2e / 1e3)
 
+    # the warm start on 4,096 held-out scenarios from its training distribution
+    # (per-bus U(0.7, 1.3), a seed the training draws do not use): warm against
+    # flat start, in batches of the timed size, outside the timed region
+    heldout = None
+    if ws:
+        rng = np.random.default_rng(31337)
+        hw = {"scenarios": 0, "load_range": [0.7, 1.3], "warm_norm_evaluations": [], "flat_norm_evaluations": [],
+              "converged_warm": 0, "converged_flat": 0, "fallback_to_flat": 0}
+        for _ in range(max(1, 4096 // B)):
+            f = rng.uniform(0.7, 1.3, size=(B, g.n_bus))
+            s_h = torch.tensor(g.sgen[None, :] - f * g.sload[None, :], device=dev)
+            _, fm_w, it_w, nfb_w = ws.solve(mixed, s_h, cfg)
+            _, fm_f, it_f = mixed.solve_batch_device(s_h, v0, config=cfg)
+            hw["scenarios"] += B
+            hw["warm_norm_evaluations"].append(int(it_w))
+            hw["flat_norm_evaluations"].append(int(it_f))
+            hw["converged_warm"] += int((fm_w <= TOL).sum())
+            hw["converged_flat"] += int((fm_f <= TOL).sum())
+            hw["fallback_to_flat"] += int(nfb_w)
+        heldout = hw
+
     # roofline of the dominant kernel (the front factorization): stage timers
     # (CUDA events around each stage's launches) over one extra Mixed solve
     # launched stage by stage, outside the timed region
@@ -480,6 +501,7 @@ def run_engine(args) -> None:
                            "iterations": int(r_mix["iters"]), "converged_per_step": r_mix["conv"]},
             "speedup_vs_fp64": round(value / value_64, 3) if value_64 else None,
             "accuracy": acc,
+            "warm_start_heldout": heldout,
             "e2e": {"value": round(e2e_value, 1), "unit": UNIT, "h2d_bytes_per_step": B * g.n_bus * 16,
                     "d2h_bytes_per_step": B * g.n_bus * 16 + B * 8, "ms_per_step": round(ms_e2e, 4),
                     "method": "cupf.streaming.HostPipeline over pinned host batches: each step uploads its "
