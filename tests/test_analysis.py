@@ -358,3 +358,31 @@ def test_symbolic_plan_at_other_panel_widths(name, width):
     bad = [ours for ours, ref in SYMBOLIC.items() if digest(s.plan_array(ours)) != gold[ref]]
     assert not bad, f"arrays differing from the reference: {bad}"
     assert int(s.plan_array("panel_ncols").max()) <= width
+
+
+REF_DATASETS = Path("/root/reference/custom_linear_solver/tests/datasets/power")
+
+
+@pytest.mark.skipif(not (REF_DATASETS.exists() and
+                         __import__("oracle.oracle", fromlist=["LIB_REF"]).LIB_REF.exists()),
+                    reason="the reference's datasets and oracle/_ref are needed")
+@pytest.mark.parametrize("case", ["case118", "case1354pegase", "case3120sp", "case6468rte", "case8387pegase"])
+@pytest.mark.parametrize("serial", [True, False])
+def test_symbolic_plan_on_every_reference_dataset(case, serial):
+    """cls_analyze_host on the reference's five linear-system patterns (real
+    Newton Jacobians up to 8,387 unknowns), serial and parallel nested
+    dissection at SolverConfig's defaults, against the reference's own plan
+    computed here (the larger two are split by the parallel ordering)."""
+    import scipy.io
+    import scipy.sparse as sp
+    from oracle.oracle import Reference
+
+    J = sp.csr_matrix(scipy.io.mmread(str(REF_DATASETS / case / "J.mtx")))
+    J.sort_indices()
+    rp, ci = J.indptr.astype(np.int32), J.indices.astype(np.int32)
+    ls = cupf.LinearSolver(cupf.SolverConfig(serial_nd=serial))
+    ls.set_data(rp, ci)
+    ls.analyze_host()
+    ref = Reference().symbolic(rp, ci, parallel_nd=not serial)
+    bad = [ours for ours, r in SYMBOLIC.items() if not np.array_equal(ls.plan_array(ours), ref[r])]
+    assert not bad, f"arrays differing from the reference: {bad}"
