@@ -386,3 +386,26 @@ def test_symbolic_plan_on_every_reference_dataset(case, serial):
     ref = Reference().symbolic(rp, ci, parallel_nd=not serial)
     bad = [ours for ours, r in SYMBOLIC.items() if not np.array_equal(ls.plan_array(ours), ref[r])]
     assert not bad, f"arrays differing from the reference: {bad}"
+
+
+@pytest.mark.skipif(not (REF_DATASETS.exists() and
+                         __import__("oracle.oracle", fromlist=["LIB_REF"]).LIB_REF.exists()),
+                    reason="the reference's datasets and oracle/_ref are needed")
+@pytest.mark.parametrize("case", ["case3120sp", "case6468rte", "case8387pegase"])
+def test_matching_plan_on_the_larger_reference_datasets(case):
+    """Structural matching (MatchingMode::Structural) on the larger reference
+    datasets: the matching, both permutations and every plan array equal the
+    reference's own, computed here."""
+    import scipy.io
+    import scipy.sparse as sp
+    from oracle.oracle import Reference
+
+    J = sp.csr_matrix(scipy.io.mmread(str(REF_DATASETS / case / "J.mtx")))
+    J.sort_indices()
+    rp, ci = J.indptr.astype(np.int32), J.indices.astype(np.int32)
+    ls = cupf.LinearSolver(cupf.SolverConfig(serial_nd=True, matching=1))
+    ls.set_data(rp, ci)
+    ls.analyze_host()
+    ref = Reference().symbolic(rp, ci, parallel_nd=False, use_matching=True)
+    bad = [ours for ours, r in MATCHING.items() if not np.array_equal(ls.plan_array(ours), ref[r])]
+    assert not bad, f"arrays differing from the reference: {bad}"
