@@ -101,3 +101,23 @@ def test_oracle_solve_many_threads_agree(oracle):
     many = oracle.solve_many(g, S, V0, 1e-8, 10, 3)
     assert np.array_equal(one["V"], many["V"])
     assert np.array_equal(one["iterations"], many["iterations"])
+
+
+@pytest.mark.skipif(not __import__("oracle.oracle", fromlist=["LIB_REF"]).LIB_REF.exists(),
+                    reason="oracle/_ref not built (reference sources absent)")
+@pytest.mark.parametrize("name", ["500", "10000"])
+def test_nr_matches_the_reference_live(oracle, name):
+    """The oracle's C port against the reference's own CPU NewtonSolver (built
+    in oracle/_ref) on grids the golden fixtures do not hold: the same
+    iteration counts, final mismatches to rounding, V to 1e-10."""
+    from oracle.oracle import Reference
+
+    g = {"500": G.grid_500, "10000": G.grid_10000}[name]()
+    S, V0 = g.scenarios(2, seed=515), g.flat_start(2)
+    ref = Reference()
+    for b in range(2):
+        r = ref.solve(g, S[b], V0[b], 1e-8, 10)
+        o = oracle.solve(g, S[b], V0[b], tol=1e-8, max_iter=10)
+        assert int(o["iterations"]) == int(r["iterations"])
+        assert o["final_mismatch"] <= 1e-8 and r["final_mismatch"] <= 1e-8
+        assert np.abs(o["V"] - r["V"]).max() <= 1e-10
