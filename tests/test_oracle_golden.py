@@ -121,3 +121,21 @@ def test_nr_matches_the_reference_live(oracle, name):
         assert int(o["iterations"]) == int(r["iterations"])
         assert o["final_mismatch"] <= 1e-8 and r["final_mismatch"] <= 1e-8
         assert np.abs(o["V"] - r["V"]).max() <= 1e-10
+
+
+@pytest.mark.skipif(not __import__("oracle.oracle", fromlist=["LIB_REF"]).LIB_REF.exists(),
+                    reason="oracle/_ref not built (reference sources absent)")
+def test_adjoint_matches_the_reference_live(oracle):
+    """The oracle's adjoint against the reference's own CPU adjoint pipeline
+    (newton_solver_adjoint.cpp:33-153, built in oracle/_ref) on the 500-bus
+    grid: lambda and both load gradients to 1e-9 relative."""
+    from oracle.oracle import Reference
+
+    g = G.grid_500()
+    S, V0 = g.scenarios(1, seed=77)[0], g.flat_start(1)[0]
+    rng = np.random.default_rng(5)
+    ga, gm = rng.standard_normal(g.n_bus), rng.standard_normal(g.n_bus)
+    r = Reference().adjoint(g, S, V0, ga, gm, 1e-12, 30)
+    a = oracle.adjoint(g, r["V"], ga, gm)
+    for k, rk in (("lambda", "lambda"), ("grad_p", "grad_p"), ("grad_q", "grad_q")):
+        assert np.abs(a[k] - r[rk]).max() <= 1e-9 * max(1.0, np.abs(r[rk]).max()), k
