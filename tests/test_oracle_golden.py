@@ -125,13 +125,15 @@ def test_nr_matches_the_reference_live(oracle, name):
 
 @pytest.mark.skipif(not __import__("oracle.oracle", fromlist=["LIB_REF"]).LIB_REF.exists(),
                     reason="oracle/_ref not built (reference sources absent)")
-def test_adjoint_matches_the_reference_live(oracle):
+@pytest.mark.parametrize("name", ["500", "10000"])
+def test_adjoint_matches_the_reference_live(oracle, name):
     """The oracle's adjoint against the reference's own CPU adjoint pipeline
-    (newton_solver_adjoint.cpp:33-153, built in oracle/_ref) on the 500-bus
-    grid: lambda and both load gradients to 1e-9 relative."""
+    (newton_solver_adjoint.cpp:33-153, built in oracle/_ref) on grids the
+    golden fixtures do not hold: lambda and both load gradients to 1e-9
+    relative."""
     from oracle.oracle import Reference
 
-    g = G.grid_500()
+    g = {"500": G.grid_500, "10000": G.grid_10000}[name]()
     S, V0 = g.scenarios(1, seed=77)[0], g.flat_start(1)[0]
     rng = np.random.default_rng(5)
     ga, gm = rng.standard_normal(g.n_bus), rng.standard_normal(g.n_bus)
