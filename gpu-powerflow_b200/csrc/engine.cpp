@@ -9,6 +9,8 @@
 // convergence is final_mismatch <= tol (newton_solver.cpp:321-341).
 #include "engine.hpp"
 
+#include <nvtx3/nvToolsExt.h>
+
 #include <algorithm>
 #include <type_traits>
 #include <cmath>
@@ -576,7 +578,22 @@ void Engine::ensure_workspace(int32_t B) {
   }
 }
 
+namespace {
+// NVTX ranges with the reference's stage labels (newton_solver.cpp:521-553,
+// StageScope :42-50).  The v3 headers are header-only and do nothing unless a
+// profiler is attached.
+const char* const kStageNames[5] = {"NR.iteration.mismatch", "NR.iteration.jacobian", "NR.iteration.factorize",
+                                    "NR.iteration.solve", "NR.iteration.voltage_update"};
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
+}  // namespace
+
 void Engine::stage_begin(int stage, cudaStream_t s) {
+  nvtxRangePushA(kStageNames[stage]);
   if (!profiling_) return;
   auto& d = *d_;
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
@@ -587,6 +604,7 @@ void Engine::stage_begin(int stage, cudaStream_t s) {
 }
 
 void Engine::stage_end(int stage, cudaStream_t s) {
+  nvtxRangePop();
   if (!profiling_) return;
   auto& d = *d_;
   if (!d.ev_open[stage]) return;
@@ -928,6 +946,7 @@ void Engine::ensure_loop_graph(const DevState& st) {
 
 template <typename T>
 SolveStats Engine::run_loop(double tol, int32_t max_iter, int32_t prepare_adjoint, cudaStream_t s, double* d_final) {
+  const NvtxRange range("NR.solve_batch");
   auto& d = *d_;
   const DevState st = d.state();
   SolveStats stats;
