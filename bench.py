@@ -192,7 +192,24 @@ class ClockSampler:
                 "reasons": sorted(self.reasons), "samples": len(self.sm), "source": self.source}
 
 
+def _launch_ranks(n: int) -> int:
+    """``--gpus N`` outside torchrun: run this script as N local ranks (one per
+    GPU) through torch.distributed.run on 127.0.0.1 and return its exit code."""
+    import socket
+    import subprocess
+
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr=127.0.0.1", f"--master-port={port}", str(Path(__file__).resolve()), *sys.argv[1:]]
+    return subprocess.run(cmd).returncode
+
+
 def _dist():
+    """World, rank and local rank from torchrun's environment; the process
+    group is NCCL on GPUs (communicator set-up logged by NCCL_DEBUG=INFO,
+    INIT lines only), gloo where CUDA is absent."""
     import torch
     import torch.distributed as dist
 
@@ -201,7 +218,11 @@ def _dist():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if world > 1 and not dist.is_initialized():
         import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            os.environ.setdefault("NCCL_DEBUG", "INFO")
+            os.environ.setdefault("NCCL_DEBUG_SUBSYS", "INIT")
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
     return world, rank, local
 
 
@@ -212,10 +233,13 @@ def _barrier(world: int) -> None:
 
 
 def _reduce(value: float, op: str, world: int, device) -> float:
+    """Max or sum of a per-rank number over the ranks (every rank gets it)."""
     if world == 1:
         return value
     import torch
     import torch.distributed as dist
+    if dist.get_backend() == "gloo":
+        device = "cpu"
     t = torch.tensor([value], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
     return float(t.item())
@@ -249,6 +273,8 @@ def run_engine(args) -> None:
     from cupf import grids
     from cupf.sharding import scenario_shard
 
+    if torch.cuda.device_count() < int(os.environ.get("WORLD_SIZE", "1")):
+        sys.exit(f"bench.py: the engine needs one CUDA device per rank ({torch.cuda.device_count()} visible)")
     world, rank, local = _dist()
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
@@ -469,9 +495,9 @@ def run_engine(args) -> None:
     fbytes = factor_bytes_per_scenario(prof, 4) * B
     peaks = _peaks()
     achieved = fbytes / (per_fact_ms / 1e3) / 1e9
-    # DRAM bytes (read + write) of the 19 level launches of one Mixed
-    # factorization at 1,024 scenarios, from one ncu capture of this workload
-    # (profiles/k_front_factor_2000x1024_levels.md); scaled by the batch
+    # DRAM bytes (read + write) of the level launches of one Mixed
+    # factorization at 1,024 scenarios, from one ncu capture of this
+    # workload; scaled by the batch
     traffic = int(FACTOR_DRAM_BYTES_B1024 * B / 1024) if g.n_bus == 2000 else None
 
     extras = run_extras(args, dev) if (rank == 0 and world == 1 and not args.no_extra) else None
@@ -677,6 +703,11 @@ def main() -> None:
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    world = int(os.environ.get("WORLD_SIZE", "0"))
+    if world == 0 and args.gpus > 1:
+        sys.exit(_launch_ranks(args.gpus))
+    if max(world, 1) != args.gpus:
+        sys.exit(f"bench.py: --gpus {args.gpus} but the launcher started {max(world, 1)} ranks")
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -26,9 +26,11 @@
 //                 (K columns) gives A (B_hi + B_lo)^T in one accumulator,
 //                 the split-weight output layer (bf16 hi + bf16 lo carry
 //                 about 16 mantissa bits of the fp32 weights).
-//                 Every mbarrier wait is bounded; on a timeout the kernel
-//                 raises the error flag, still waits (bounded) for its own
-//                 MMAs and frees its TMEM before returning.
+//                 Every mbarrier wait is bounded.  On a timeout the kernel
+//                 raises the error flag, stops issuing, waits (bounded) for
+//                 the TMA loads and MMAs it already issued, writes NaN into
+//                 the output tiles it could not finish, and frees its TMEM
+//                 before returning.
 //
 // plus the small element-wise and reduction kernels of a training step
 // (transpose, loss gradient, bias gradient, Adam).  GELU is the exact
@@ -38,6 +40,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -59,7 +62,7 @@ constexpr long long kSpinLimit = 1ll << 22;    // mbarrier polls before a wait g
 // shared memory of one CTA: 1 KB alignment slack, the ring, the barriers
 template <int BN, int STAGES>
 constexpr size_t gemm_smem() {
-  return 1024 + (size_t)STAGES * (kTileA + (uint32_t)BN * kBK * 2) + 256;
+  return 1024 + (size_t)STAGES * (kTileA + (uint32_t)BN * kBK * 2) + 256;  // + barriers, TMEM slot, fail flag
 }
 
 enum { EPI_F32 = 0, EPI_BIAS_F32 = 1, EPI_BIAS_GELU = 2, EPI_DGELU = 3 };
@@ -85,9 +88,9 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
       : "memory");
   return done != 0;
 }
-// bounded wait: false when the phase did not complete within kSpinLimit polls
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  for (long long i = 0; i < kSpinLimit; ++i)
+// bounded wait: false when the phase did not complete within `limit` polls
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long long limit = kSpinLimit) {
+  for (long long i = 0; i < limit; ++i)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }
@@ -178,6 +181,8 @@ struct GemmArgs {
   int epi;
   int a_kblocks;  // > 0: A's k-block index wraps modulo a_kblocks (split-weight B)
   int* error;
+  long long spin_limit;  // mbarrier polls before a wait gives up
+  int stall_loads;       // failure-path test: the producer issues no loads, so the MMA thread's wait runs out
 };
 
 template <int BN, int STAGES, int MINB>
@@ -193,6 +198,7 @@ __global__ void __launch_bounds__(kThreads, MINB)
   uint64_t* empty = full + STAGES;
   uint64_t* done = empty + STAGES;
   uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
+  int* s_fail = reinterpret_cast<int*>(tslot + 1);  // some thread's wait ran out
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int m0 = blockIdx.y * kBM, n0 = blockIdx.x * BN;
@@ -204,6 +210,7 @@ __global__ void __launch_bounds__(kThreads, MINB)
       mbar_init(empty + s, 1);
     }
     mbar_init(done, 1);
+    *s_fail = 0;
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   if (warp == 0) tmem_alloc(tslot, BN);
@@ -214,9 +221,10 @@ __global__ void __launch_bounds__(kThreads, MINB)
 
   if (threadIdx.x == 0) {
     // producer: stage s holds k-block kb; refill it once the MMAs of kb - STAGES are done
-    for (int kb = 0; kb < nk; ++kb) {
+    int issued = 0;
+    for (int kb = 0; kb < (g.stall_loads ? 0 : nk); ++kb) {
       const int s = kb % STAGES;
-      if (kb >= STAGES && !mbar_wait(empty + s, ((kb / STAGES) - 1) & 1)) {
+      if (kb >= STAGES && !mbar_wait(empty + s, ((kb / STAGES) - 1) & 1, g.spin_limit)) {
         ok = false;
         break;
       }
@@ -224,13 +232,21 @@ __global__ void __launch_bounds__(kThreads, MINB)
       const int ka = g.a_kblocks > 0 ? kb % g.a_kblocks : kb;
       tma_load_2d(sA + s * kTileA, &ta, ka * kBK, m0, full + s);
       tma_load_2d(sB + s * kTileB, &tb, kb * kBK, n0, full + s);
+      issued = kb + 1;
+    }
+    if (!ok) {
+      // drain: the last load issued into each stage is the only one that can
+      // still be in flight there (nothing newer was issued into that stage);
+      // wait (bounded) for it before the CTA releases its shared memory
+      for (int kb = issued - 1; kb >= 0 && kb >= issued - STAGES; --kb)
+        mbar_wait(full + kb % STAGES, (kb / STAGES) & 1, g.spin_limit);
     }
   } else if (threadIdx.x == 32) {
     // MMA issuer
     constexpr uint32_t idesc = idesc_bf16(kBM, BN);
     for (int kb = 0; kb < nk; ++kb) {
       const int s = kb % STAGES;
-      if (!mbar_wait(full + s, (kb / STAGES) & 1)) {
+      if (!mbar_wait(full + s, (kb / STAGES) & 1, g.spin_limit)) {
         ok = false;
         break;
       }
@@ -243,14 +259,35 @@ __global__ void __launch_bounds__(kThreads, MINB)
     }
     tc_commit(done);  // arrives once every MMA issued above has completed
   }
-  if (!ok) atomicExch(g.error, 1);
+  if (!ok) {
+    atomicExch(g.error, 1);
+    atomicExch(s_fail, 1);
+  }
 
   // every lane waits, then the warp agrees, so the .sync.aligned loads below
   // run warp-converged
-  const bool have = __all_sync(0xffffffffu, mbar_wait(done, 0));
+  const bool have = __all_sync(0xffffffffu, mbar_wait(done, 0, g.spin_limit));
+  if (!have && lane == 0) {
+    atomicExch(g.error, 2);
+    atomicExch(s_fail, 1);
+  }
+  __syncthreads();
   tc_fence_after();
-  if (!have) {
-    if (threadIdx.x == 0) atomicExch(g.error, 2);
+  if (*s_fail) {
+    // a wait ran out, so the accumulator is not known to be complete: mark
+    // this tile's outputs as not-a-number (the warm start treats a
+    // non-finite prediction as missing and solves that scenario from flat
+    // start); the host reads the raised flag
+    const int row = m0 + warp * 32 + lane;
+    for (int c = 0; c < BN; ++c) {
+      if (g.epi == EPI_F32 || g.epi == EPI_BIAS_F32)
+        static_cast<float*>(g.out)[(size_t)row * g.ldo + n0 + c] = __int_as_float(0x7fc00000);
+      else
+        static_cast<__nv_bfloat16*>(g.out)[(size_t)row * g.ldo + n0 + c] = __ushort_as_bfloat16((unsigned short)0x7fc0);
+    }
+    // MMAs issued before the timeout may still be writing the accumulator:
+    // one more bounded wait before the tensor memory is released
+    if (!have) mbar_wait(done, 0, g.spin_limit);
   } else {
     const int row = m0 + warp * 32 + lane;
     const uint32_t tl = tmem + ((uint32_t)(warp * 32) << 16);
@@ -455,6 +492,11 @@ int* error_flag() {
   return f;
 }
 
+// Wait bound of the GEMM's mbarrier polls and the failure-path test switch
+// (mlp_set_wait_test); read at each launch.
+std::atomic<long long> g_spin_limit{kSpinLimit};
+std::atomic<int> g_stall_loads{0};
+
 // the two tile shapes: wide grids, and grids with fewer 128 x 128 tiles than SMs
 constexpr int kWideBN = 128, kWideStages = 3, kWideMinBlocks = 2;
 constexpr int kNarrowBN = 64, kNarrowStages = 4, kNarrowMinBlocks = 2;
@@ -483,6 +525,8 @@ template <int BN, int STAGES, int MINB>
 void launch_shape(const void* A, long long lda, int ka_cols, const void* B, long long ldb, GemmArgs g,
                   cudaStream_t stream) {
   const CUtensorMap ta = make_map(A, g.M, ka_cols, lda, kBM), tb = make_map(B, g.N, g.K, ldb, BN);
+  g.spin_limit = g_spin_limit.load();
+  g.stall_loads = g_stall_loads.load();
   k_gemm_bf16<BN, STAGES, MINB><<<dim3(g.N / BN, g.M / kBM), kThreads, gemm_smem<BN, STAGES>(), stream>>>(ta, tb, g);
 }
 
@@ -536,7 +580,7 @@ int mlp_gemm_bf16(const void* A, long long lda, const void* B, long long ldb, in
       throw std::invalid_argument("mlp_gemm_bf16: leading dimensions must be >= the row length and multiples of 8");
     if ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B) | reinterpret_cast<uintptr_t>(out)) & 15)
       throw std::invalid_argument("mlp_gemm_bf16: operands must be 16-byte aligned");
-    GemmArgs g{M, N, K, out, ldo, bias, static_cast<__nv_bfloat16*>(aux), ldaux, epi, 0, error_flag()};
+    GemmArgs g{M, N, K, out, ldo, bias, static_cast<__nv_bfloat16*>(aux), ldaux, epi, 0, error_flag(), kSpinLimit, 0};
     launch_gemm(A, lda, K, B, ldb, g, static_cast<cudaStream_t>(stream));
   });
 }
@@ -553,9 +597,19 @@ int mlp_gemm_bf16_split(const void* A, long long lda, const void* B, long long l
       throw std::invalid_argument("mlp_gemm_bf16_split: need lda >= K, ldb >= 2K, ldo >= N, all multiples of 8");
     if ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B) | reinterpret_cast<uintptr_t>(out)) & 15)
       throw std::invalid_argument("mlp_gemm_bf16_split: operands must be 16-byte aligned");
-    GemmArgs g{M, N, 2 * K, out, ldo, bias, nullptr, 0, epi, K / kBK, error_flag()};
+    GemmArgs g{M, N, 2 * K, out, ldo, bias, nullptr, 0, epi, K / kBK, error_flag(), kSpinLimit, 0};
     launch_gemm(A, lda, K, B, ldb, g, static_cast<cudaStream_t>(stream));
   });
+}
+
+int mlp_set_wait_test(long long spin_limit, int stall_loads) {
+  if (spin_limit < 1 || (stall_loads != 0 && stall_loads != 1)) {
+    g_err = "mlp_set_wait_test: spin_limit must be positive and stall_loads 0 or 1";
+    return 1;
+  }
+  g_spin_limit.store(spin_limit);
+  g_stall_loads.store(stall_loads);
+  return 0;
 }
 
 int mlp_error_flag(int* out_host, int reset) {

@@ -10,9 +10,9 @@ Differences a user can see:
   * only ``BackendKind.CUDA`` with ``CudaLinearSolverKind.Custom`` is provided
     (the CPU/KLU and cuDSS backends are other libraries); constructing a
     solver with another backend raises ``ValueError``;
-  * ``ComputePolicy.FP32`` runs the Mixed kernels (FP64 state and mismatch,
-    FP32 Jacobian and factors); ``CustomPrecision.TF32`` runs the FP32 front
-    kernels, whose fronts are too narrow for tensor cores;
+  * ``ComputePolicy.FP32`` (FP32 state, mismatch and voltage update) is not
+    built: constructing a solver with it raises ``ValueError``;
+    ``ComputePolicy.Mixed`` keeps the state in FP64 with FP32 factors;
   * ``CustomSolverConfig.max_panel_width`` is limited to 1..8;
   * ``CustomSolverConfig.autotune`` (not in the reference, on by default)
     times each factor level's block shape at the first solve of a batch size

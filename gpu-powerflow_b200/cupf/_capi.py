@@ -70,7 +70,8 @@ EXPORTS = [
 ]
 # exported symbols of include/cupf_mlp.h (warm-start network kernels)
 MLP_EXPORTS = [
-    "mlp_last_error", "mlp_gemm_bf16", "mlp_error_flag", "mlp_transpose_bf16", "mlp_standardize", "mlp_mse_grad",
+    "mlp_last_error", "mlp_gemm_bf16", "mlp_error_flag", "mlp_set_wait_test", "mlp_transpose_bf16", "mlp_standardize",
+    "mlp_mse_grad",
     "mlp_col_sum_bf16", "mlp_adam", "mlp_load_features", "mlp_gemm_bf16_split",
 ]
 
@@ -137,6 +138,7 @@ def _declare(lib: C.CDLL) -> None:
         "mlp_gemm_bf16": ([_vp, _i64, _vp, _i64, _i32, _i32, _i32, _i32, _vp, _i64, _vp, _vp, _i64, _vp], _i32),
         "mlp_gemm_bf16_split": ([_vp, _i64, _vp, _i64, _i32, _i32, _i32, _i32, _vp, _i64, _vp, _vp], _i32),
         "mlp_error_flag": ([_p(_i32), _i32], _i32),
+        "mlp_set_wait_test": ([C.c_longlong, _i32], _i32),
         "mlp_transpose_bf16": ([_vp, _i64, _vp, _i32, _i32, _vp], _i32),
         "mlp_standardize": ([_vp, _vp, _vp, _vp, _i64, _i32, _i32, _i32, _vp], _i32),
         "mlp_load_features": ([_vp, _i64, _vp, _vp, _i32, _i32, _vp, _vp, _vp, _i64, _i32, _i32, _i32, _vp], _i32),

@@ -39,6 +39,13 @@ int mlp_gemm_bf16_split(const void* A, long long lda, const void* B, long long l
 /* Device error flag of the GEMM (1 or 2 after a bounded wait gave up); copied
  * to *out_host with a synchronising copy, optionally reset. */
 int mlp_error_flag(int* out_host, int reset);
+/* Failure-path test of the GEMM's bounded waits (process-wide, read at each
+ * launch).  spin_limit: mbarrier polls before a wait gives up (default
+ * 4,194,304).  stall_loads = 1 makes the producer issue no tile loads, so the
+ * MMA thread's wait for the first tile runs out: the kernel then raises the
+ * error flag (1), writes NaN into its output tiles, frees its tensor memory
+ * and returns.  Nothing faults or hangs; set (4194304, 0) to restore. */
+int mlp_set_wait_test(long long spin_limit, int stall_loads);
 /* out[cols][rows] = in[rows][cols] (bf16; in has row stride ld). */
 int mlp_transpose_bf16(const void* in, long long ld, void* out, int rows, int cols, void* stream);
 /* x[b][k] = bf16((raw[b][k] - mean[k]) * inv_std[k]) for k < n_in, 0 for

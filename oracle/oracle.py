@@ -21,6 +21,9 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 LIB_ORACLE = HERE / "liboracle.so"
 LIB_REF = HERE / "_ref" / "libcupf_ref.so"
+# The reference checkout the oracle/_ref build and the live comparisons read:
+# $CUPF_REFERENCE_ROOT, else a checkout named `reference` beside this repository.
+REFERENCE_ROOT = Path(os.environ.get("CUPF_REFERENCE_ROOT") or (HERE.parent.parent / "reference"))
 
 _i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
 _f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")

@@ -133,7 +133,7 @@ def read_mtx(path: Path):
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref-root", default="/root/reference")
+    ap.add_argument("--ref-root", default=str(orc.REFERENCE_ROOT))
     ap.add_argument("--added-only", action="store_true",
                     help="only add the front-CSV, parallel-ND and panel-width hashes to the existing hashes.json "
                          "(other fixtures untouched)")

@@ -360,7 +360,7 @@ def test_symbolic_plan_at_other_panel_widths(name, width):
     assert int(s.plan_array("panel_ncols").max()) <= width
 
 
-REF_DATASETS = Path("/root/reference/custom_linear_solver/tests/datasets/power")
+REF_DATASETS = __import__("oracle.oracle", fromlist=["REFERENCE_ROOT"]).REFERENCE_ROOT / "custom_linear_solver/tests/datasets/power"
 
 
 @pytest.mark.skipif(not (REF_DATASETS.exists() and

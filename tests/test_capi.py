@@ -110,6 +110,17 @@ def test_unsupported_backends_raise():
         cupf.NewtonSolver(o)
 
 
+def test_fp32_compute_policy_is_rejected_not_aliased():
+    """ComputePolicy.FP32 (FP32 state, mismatch and voltage update; the
+    reference's CudaFp32CustomPipeline) is not built here: asking for it is an
+    error naming the option, not a silent run of the Mixed kernels."""
+    o = cupf.NewtonOptions()
+    o.backend = cupf.BackendKind.CUDA
+    o.compute = cupf.ComputePolicy.FP32
+    with pytest.raises(ValueError, match="ComputePolicy::FP32"):
+        cupf.NewtonSolver(o)
+
+
 def _solver():
     o = cupf.NewtonOptions()
     o.backend = cupf.BackendKind.CUDA

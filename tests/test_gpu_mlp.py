@@ -39,6 +39,36 @@ def test_gemm_f32_matches_torch(torch, M, N, K):
     assert net.error_flag() == 0
 
 
+@pytest.mark.parametrize("M,N,K", [(128, 128, 256), (1280, 2048, 320)])
+def test_gemm_wait_timeout_reports_and_recovers(torch, M, N, K):
+    """The GEMM's bounded waits, made to run out on the host's request (the
+    producer issues no tile loads, the wait limit is 1,000 polls): the kernel
+    returns, raises the error flag and marks its outputs NaN; the context
+    stays usable, and the next GEMM with the normal limit is exact again."""
+    from cupf.warm_start import MLP, EPI_F32
+
+    g = torch.Generator(device="cuda").manual_seed(7)
+    A = torch.randn(M, K, device="cuda", generator=g).to(torch.bfloat16)
+    B = torch.randn(N, K, device="cuda", generator=g).to(torch.bfloat16)
+    net = MLP(64, 64, hidden=128, layers=1)
+    lib = net.lib
+    out = torch.zeros(M, N, device="cuda")
+    assert net.error_flag() == 0
+    assert lib.mlp_set_wait_test(1000, 1) == 0
+    try:
+        net.gemm(A, B, out, EPI_F32)
+        torch.cuda.synchronize()
+    finally:
+        assert lib.mlp_set_wait_test(1 << 22, 0) == 0
+    assert net.error_flag() == 1  # read and reset
+    assert bool(torch.isnan(out).all())
+    net.gemm(A, B, out, EPI_F32)
+    ref = A.float() @ B.float().T
+    assert _rel(out.cpu().numpy(), ref.cpu().numpy()) < 1e-5
+    assert net.error_flag() == 0
+    assert lib.mlp_set_wait_test(0, 0) == 1  # a limit must be positive
+
+
 def test_gemm_gelu_epilogues(torch):
     from cupf.warm_start import MLP, EPI_BIAS_GELU, EPI_DGELU
     from oracle.mlp_oracle import gelu, gelu_grad

@@ -16,7 +16,7 @@ from conftest import gpu_available
 
 pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not gpu_available(), reason="needs a CUDA device")]
 GOLD = Path(__file__).resolve().parent / "golden"
-POLICIES = {"FP64": cupf.ComputePolicy.FP64, "FP32": cupf.ComputePolicy.FP32, "Mixed": cupf.ComputePolicy.Mixed}
+POLICIES = {"FP64": cupf.ComputePolicy.FP64, "Mixed": cupf.ComputePolicy.Mixed}
 
 
 def make_solver(g, compute, graph=False, serial_nd=True, autotune=False):
