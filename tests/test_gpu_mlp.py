@@ -5,7 +5,7 @@ convergence, and the warm start's iteration savings on a real grid."""
 import numpy as np
 import pytest
 
-from conftest import gpu_available
+from conftest import gpu_available, max_dv_vs_oracle
 
 pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not gpu_available(), reason="needs a CUDA device")]
 
@@ -145,10 +145,11 @@ def test_training_reduces_loss(torch):
     assert np.mean(losses[-20:]) < 0.1 * np.mean(losses[:5])
 
 
-def test_warm_start_saves_newton_iterations(torch):
+def test_warm_start_saves_newton_iterations(torch, oracle):
     """Trained on engine solutions of a 118-bus grid (load scaling 0.7-1.3),
     the network's starting point needs fewer Newton iterations than the flat
-    start on held-out scenarios, and reaches the same solution."""
+    start on held-out scenarios, and every scenario from either start lies
+    within 1e-8 of the FP64 oracle solved to 1e-12."""
     import cupf
     from cupf import grids as G
     from cupf.warm_start import WarmStart
@@ -171,7 +172,46 @@ def test_warm_start_saves_newton_iterations(torch):
     Vw, fmw, itw, nfb = ws.solve(s, S, cfg)
     assert bool((fmw <= 1e-8).all()) and bool((fmf <= 1e-8).all())
     assert itw < itf, (itw, itf)
-    assert float((Vw - Vf).abs().max()) <= 1e-7
+    V0 = np.repeat(g.v0[None, :], 512, axis=0)
+    for V in (Vw, Vf):
+        dv = max_dv_vs_oracle(oracle, g, S.cpu().numpy(), V0, V.cpu().numpy())
+        assert dv.max() <= 1e-8, float(dv.max())
+
+
+def test_warm_start_2000_full_batch_matches_oracle(torch, oracle):
+    """The headline configuration's warm start: the bench's network shape
+    (loads and PV setpoints -> 3 x 1,024 GELU -> 3,598, input skip, output
+    layer refit and evaluated with split weights), trained here on a smaller
+    set (16,384 engine-solved scenarios, 12 epochs), then run on the full
+    1,024-scenario U(0.8, 1.2) batch of the 2,000-bus grid.  Every scenario
+    converges to 1e-8 and lies within 1e-8 of the FP64 oracle, and the warm
+    start needs fewer Newton iterations than the flat start."""
+    import cupf
+    from cupf import grids as G
+    from cupf.warm_start import WarmStart
+
+    g = G.grid_2000()
+    o = cupf.NewtonOptions()
+    o.backend = cupf.BackendKind.CUDA
+    o.compute = cupf.ComputePolicy.Mixed
+    o.custom.serial_nd = True
+    o.use_cuda_graph = True
+    s = cupf.NewtonSolver(o)
+    s.initialize(g.indptr, g.indices, g.data, g.n_bus, g.n_bus, g.pv, g.pq)
+    ws = WarmStart(g, hidden=1024, layers=3, seed=0)
+    X, Y, _ = ws.generate(s, 16384, lo=0.7, hi=1.3, seed=777)
+    ws.fit(X, Y, epochs=12, batch=1024, lr=2e-3)
+    B = 1024
+    S_h = g.scenarios(B, seed=9100)
+    S = torch.tensor(S_h, device="cuda")
+    cfg = cupf.NRConfig(tolerance=1e-8, max_iter=10)
+    Vw, fmw, itw, nfb = ws.solve(s, S, cfg)
+    V0 = g.flat_start(B)
+    Vf, fmf, itf = s.solve_batch_device(S, torch.tensor(V0, device="cuda"), config=cfg)
+    assert bool((fmw <= 1e-8).all()) and bool((fmf <= 1e-8).all())
+    assert itw < itf, (itw, itf)
+    dv = max_dv_vs_oracle(oracle, g, S_h, V0, Vw.cpu().numpy())
+    assert dv.size == B and dv.max() <= 1e-8, (int(dv.argmax()), float(dv.max()))
 
 
 def test_warm_entry_point_exact_prediction_and_failed_row(torch):

@@ -12,7 +12,7 @@ import pytest
 
 import cupf
 from cupf import grids as G
-from conftest import gpu_available
+from conftest import gpu_available, max_dv_vs_oracle
 
 pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not gpu_available(), reason="needs a CUDA device")]
 GOLD = Path(__file__).resolve().parent / "golden"
@@ -98,18 +98,24 @@ def test_118_matches_reference_golden():
 
 @pytest.mark.parametrize("policy", ["FP64", "Mixed"])
 def test_2000_matches_oracle(oracle, policy):
+    """The benchmark's workload at full size (2,000 buses x 1,024 scenarios,
+    flat start): every scenario converges and lies within 1e-8 of the FP64
+    oracle solved to 1e-12; in FP64 the batch's iteration count is the
+    oracle's largest at the same stopping rule."""
+    import os
+
     g = G.grid_2000()
-    B = 96
+    B = 1024
     S = g.scenarios(B, seed=23)
     V0 = g.flat_start(B)
-    s = make_solver(g, POLICIES[policy])
+    s = make_solver(g, POLICIES[policy], graph=True)
     r = solve(s, g, S, V0, cfg())
     assert r.converged_numpy.all()
-    for b in (0, 31, 32, 95):
-        tight = oracle.solve(g, S[b], V0[b], tol=1e-12, max_iter=30)
-        assert np.abs(r.V_numpy[b] - tight["V"]).max() <= 1e-8
-        if policy == "FP64":
-            assert r.iterations_numpy[b] == oracle.solve(g, S[b], V0[b], 1e-8, 10)["iterations"]
+    dv = max_dv_vs_oracle(oracle, g, S, V0, r.V_numpy)
+    assert dv.max() <= 1e-8, (int(dv.argmax()), float(dv.max()))
+    if policy == "FP64":
+        its = oracle.solve_many(g, S, V0, tol=1e-8, max_iter=10, threads=os.cpu_count() or 1)["iterations"]
+        assert r.iterations_numpy[0] == its.max()
 
 
 def test_2000_matches_reference_golden():
@@ -122,6 +128,7 @@ def test_2000_matches_reference_golden():
 
 
 def test_10000_mixed_matches_oracle(oracle):
+    """The 10,000-bus x 64 workload: every scenario within 1e-8 of the oracle."""
     g = G.grid_10000()
     B = 64
     S = g.scenarios(B, seed=29)
@@ -129,9 +136,8 @@ def test_10000_mixed_matches_oracle(oracle):
     s = make_solver(g, cupf.ComputePolicy.Mixed)
     r = solve(s, g, S, V0, cfg())
     assert r.converged_numpy.all()
-    for b in (0, 63):
-        tight = oracle.solve(g, S[b], V0[b], tol=1e-12, max_iter=30)
-        assert np.abs(r.V_numpy[b] - tight["V"]).max() <= 1e-8
+    dv = max_dv_vs_oracle(oracle, g, S, V0, r.V_numpy)
+    assert dv.max() <= 1e-8, (int(dv.argmax()), float(dv.max()))
 
 
 def test_identical_rows_agree():
@@ -212,14 +218,15 @@ def test_stage_profiling_counts_launches():
 
 
 def test_uneven_multi_grid_batch(oracle):
-    """The uneven batch (118/500/2,000/10,000 buses, smaller counts here):
-    solved concurrently, one engine and stream per grid, every instance
-    converges and matches the oracle and the same grid solved alone."""
+    """The uneven batch at its full size (118/500/2,000/10,000 buses x
+    256/128/96/32 instances): solved concurrently, one engine and stream per
+    grid; every one of the 512 instances converges, equals the same grid
+    solved alone, and lies within 1e-8 of the oracle."""
     import torch
     from cupf.batching import UnevenBatch
 
     inst = G.uneven_grids()
-    counts = [64, 32, 16, 8]
+    counts = [c for _, c in inst]
     grids = [g for g, _ in inst]
     ub = UnevenBatch(grids)
     S = [torch.tensor(g.scenarios(c, seed=31 + i), device="cuda") for i, (g, c) in enumerate(zip(grids, counts))]
@@ -230,9 +237,8 @@ def test_uneven_multi_grid_batch(oracle):
         V, fm, it = res[i]
         assert bool((fm <= 1e-8).all())
         assert torch.equal(V, alone[i][0])
-        s0 = S[i][0].cpu().numpy()
-        ref = oracle.solve(g, s0, g.v0, tol=1e-12, max_iter=30)["V"]
-        assert np.abs(V[0].cpu().numpy() - ref).max() <= 1e-8
+        dv = max_dv_vs_oracle(oracle, g, S[i].cpu().numpy(), V0[i].cpu().numpy(), V.cpu().numpy())
+        assert dv.size == c and dv.max() <= 1e-8, (g.n_bus, int(dv.argmax()), float(dv.max()))
 
 
 def test_dump_case_solves_like_the_grid(tmp_path):
