@@ -53,6 +53,8 @@ EngineConfig engine_config(const cls_config& c, int32_t compute, int32_t use_gra
   e.par_nd_depth = c.parallel_nd_depth > 0 ? c.parallel_nd_depth : 4;
   e.par_nd_base_small = c.parallel_nd_base_small > 0 ? c.parallel_nd_base_small : 4000;
   e.par_nd_base_large = c.parallel_nd_base_large > 0 ? c.parallel_nd_base_large : 20000;
+  e.wide_min_front = c.wide_min_front > 0 ? c.wide_min_front : 65;
+  e.tc_min_front = c.tc_min_front;
   e.use_cuda_graph = use_graph;
   return e;
 }
@@ -115,8 +117,12 @@ bool copy_plan_array(const Engine& e, const char* name, int32_t* out, int64_t ca
   CUPF_ARR("diag12", ja.diag12)
   CUPF_ARR("diag22", ja.diag22)
 #undef CUPF_ARR
-  if (n == "factor_level_warps" || n == "backward_launch_warps") {  // the autotuner's choices (0: built-in rule)
-    const std::vector<int32_t> w = n == "factor_level_warps" ? e.factor_level_warps() : e.backward_launch_warps();
+  if (n == "factor_level_warps" || n == "backward_launch_warps" || n == "factor_level_tiers" ||
+      n == "tc_threshold") {  // the autotuner's choices (0: built-in rule), the kernel tier of each launch
+    const std::vector<int32_t> w = n == "factor_level_warps"   ? e.factor_level_warps()
+                                   : n == "factor_level_tiers" ? e.factor_level_tiers()
+                                   : n == "tc_threshold"       ? std::vector<int32_t>{e.tc_threshold()}
+                                                               : e.backward_launch_warps();
     if (len) *len = (int64_t)w.size();
     if (out) {
       if (cap < (int64_t)w.size()) return false;
@@ -176,7 +182,8 @@ cls_status cls_create(const cls_config* config, cls_handle* out) {
   if (config) c = *config;
   if ((c.matching != 0 && c.matching != 1) || c.max_panel_width < 1 || c.max_panel_width > 8 ||
       (c.autotune != 0 && c.autotune != 1) || c.parallel_nd_depth < 0 || c.parallel_nd_base_small < 0 ||
-      c.parallel_nd_base_large < 0)
+      c.parallel_nd_base_large < 0 || c.wide_min_front < 0 || c.wide_min_front > 65 || c.tc_min_front < 0 ||
+      c.precision < CLS_PRECISION_FP64 || c.precision > CLS_PRECISION_TF32)
     return CLS_INVALID_VALUE;
   auto* h = new (std::nothrow) cls_solver_s();
   if (!h) return CLS_ALLOCATION_FAILED;
@@ -381,6 +388,10 @@ pf_status pf_create(const pf_options* options, pf_handle* out) {
       throw std::invalid_argument("NewtonSolver: autotune must be 0 or 1");
     if (o.custom.parallel_nd_depth < 0 || o.custom.parallel_nd_base_small < 0 || o.custom.parallel_nd_base_large < 0)
       throw std::invalid_argument("NewtonSolver: the parallel nested-dissection parameters must not be negative");
+    if (o.custom.wide_min_front < 0 || o.custom.wide_min_front > 65 || o.custom.tc_min_front < 0)
+      throw std::invalid_argument("NewtonSolver: wide_min_front must be in [0, 65] and tc_min_front non-negative");
+    if (o.custom.precision < CLS_PRECISION_FP64 || o.custom.precision > CLS_PRECISION_TF32)
+      throw std::invalid_argument("NewtonSolver: unknown custom solver precision");
     if (o.cuda_jacobian < PF_JACOBIAN_EDGE || o.cuda_jacobian > PF_JACOBIAN_VERTEX_WARP)
       throw std::invalid_argument("NewtonSolver: cuda_jacobian must be Edge, EdgeAtomic or VertexWarp");
     cls_config c = o.custom;

@@ -197,6 +197,23 @@ bool Engine::factor_is_double() const {
   return cfg_.compute == kComputeFP64 || cfg_.factor_precision == kFactorFP64;
 }
 
+bool Engine::tf32_factors() const { return cfg_.factor_precision == kFactorTF32 && !factor_is_double(); }
+
+void Engine::assign_tiers(int tc_min) {
+  const int wide_min = std::min(cfg_.wide_min_front > 0 ? cfg_.wide_min_front : kWideFrontRows, kWideFrontRows);
+  tc_min_ = tf32_factors() ? tc_min : 0;
+  for (auto& lv : d_->levels) {
+    lv.tier = lv.max_fsz >= wide_min ? 1 : 0;
+    if (tc_min_ > 0 && lv.max_fsz >= tc_min_) lv.tier = 2;
+  }
+}
+
+std::vector<int32_t> Engine::factor_level_tiers() const {
+  std::vector<int32_t> t;
+  for (const auto& lv : d_->levels) t.push_back(lv.tier);
+  return t;
+}
+
 void Engine::initialize(int32_t n_bus, const int32_t* indptr, const int32_t* indices, const double* ydata,
                         const int32_t* pv, int32_t n_pv, const int32_t* pq, int32_t n_pq) {
   if (!indptr || !indices || !ydata) throw std::invalid_argument("initialize: Ybus arrays must not be null");
@@ -372,6 +389,7 @@ void Engine::upload_plan() {
       d.levels.push_back(lv);
     }
   }
+  assign_tiers(cfg_.tc_min_front > 0 ? cfg_.tc_min_front : kTcDefaultMinFront);
   // The top of the tree for the backward sweep: the trailing levels of at
   // most kBackwardTopFronts fronts.
   d.bw_first = (int)d.levels.size();
@@ -475,7 +493,6 @@ void Engine::analyze_host(int32_t n_bus, const int32_t* indptr, const int32_t* i
   so.par_nd_base_large = cfg_.par_nd_base_large;
   sp_ = analyze_symbolic(ja_.dim, ja_.row_ptr.data(), ja_.col_idx.data(), so);
   fp_ = build_factor_program(sp_);
-  if (fp_.max_fsz > 64) throw std::runtime_error("initialize: a front exceeds 64 rows (unsupported)");
 }
 
 void Engine::analyze_matrix_host(int32_t n, int32_t nnz, const int32_t* row_ptr, const int32_t* col_idx) {
@@ -516,7 +533,6 @@ void Engine::initialize_matrix(int32_t n, int32_t nnz, const int32_t* row_ptr, c
   so.par_nd_base_large = cfg_.par_nd_base_large;
   sp_ = analyze_symbolic(n, row_ptr, col_idx, so);
   fp_ = build_factor_program(sp_);
-  if (fp_.max_fsz > 64) throw std::runtime_error("Analyze: a front exceeds 64 rows (unsupported)");
   upload_plan();
   initialized_ = true;
   adjoint_ready_ = false;
@@ -548,11 +564,14 @@ void Engine::ensure_workspace(int32_t B) {
     d.CB.reserve((size_t)std::max<int64_t>(fp_.cb_total, 1) * Bp * es);
     d.Y.reserve(dim * Bp * es);
     d.X.reserve(dim * Bp * es);
-    // dense fronts of levels too large for shared memory live in global scratch
+    // dense fronts of levels too large for shared memory (and every wide-tier
+    // front) live in global scratch; one launch at a time uses it
     size_t scratch = 0;
     for (const auto& lv : d.levels) {
-      const size_t elems = (size_t)lv.max_fsz * (lv.max_fsz + 1);
-      if (!front_fits_smem(lv, es)) scratch = std::max(scratch, elems * lv.count * (Bp / kWarp));
+      LevelLaunch widest = lv;  // the tier with the largest scratch this launch may be given
+      if (tf32_factors() && lv.max_fsz >= std::min(tc_min_ > 0 ? tc_min_ : kTcDefaultMinFront, kTcDefaultMinFront))
+        widest.tier = 2;
+      scratch = std::max({scratch, level_scratch_elems(lv, es, Bp / kWarp), level_scratch_elems(widest, es, Bp / kWarp)});
     }
     d.front_scratch_elems = scratch;
     if (scratch) d.front_scratch.reserve(scratch * kWarp * es);
@@ -743,6 +762,44 @@ void Engine::autotune_factor(cudaStream_t s, const void* J) {
   const bool dbl = std::is_same<T, double>::value;
   if (d.tuned_Bp == d.Bp && d.tuned_double == dbl) return;
   const FactorArgs<T, T> a = factor_args<T>(1, J);
+  if (tf32_factors() && cfg_.tc_min_front == 0) {
+    // the small/large-front split of TF32 factors: the tensor-core threshold
+    // whose whole factorization is fastest (three timings each, built-in
+    // block shapes); a larger threshold must win by 1 %
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CUPF_CUDA(cudaEventCreate(&e0));
+    CUPF_CUDA(cudaEventCreate(&e1));
+    int best = kTcDefaultMinFront;
+    double best_ms = 1e30;
+    try {
+      for (int t : {kTcDefaultMinFront, 49, 65}) {
+        assign_tiers(t);
+        double ms_t = 1e30;
+        for (int rep = 0; rep < 3; ++rep) {
+          CUPF_CUDA(cudaEventRecord(e0, s));
+          for (const auto& lv : d.levels) launch_factor_level<T, T>(lv, a, s);
+          CUPF_CUDA(cudaEventRecord(e1, s));
+          CUPF_CUDA(cudaEventSynchronize(e1));
+          float ms = 0.f;
+          CUPF_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+          ms_t = std::min(ms_t, (double)ms);
+        }
+        if (debug_sync()) std::fprintf(stderr, "[cupf] tensor-core threshold %d: %.3f ms\n", t, ms_t);
+        if (ms_t < 0.99 * best_ms) {
+          best = t;
+          best_ms = ms_t;
+        }
+      }
+    } catch (...) {
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      assign_tiers(kTcDefaultMinFront);
+      throw;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    assign_tiers(best);
+  }
   choose_block_shapes(
       d.levels.size(), [&](size_t i, int w) { d.levels[i].warps = w; },
       [&](size_t i) { launch_factor_level<T, T>(d.levels[i], a, s); }, s, "factor");
@@ -1327,8 +1384,7 @@ void Engine::factorize_values_static_scratch(const void* d_values, int32_t value
   const bool dbl = factor_is_double();
   const size_t es = dbl ? sizeof(double) : sizeof(float);
   size_t need = 0;  // elements x 32 lanes
-  for (const auto& lv : d.levels)
-    if (!front_fits_smem(lv, es)) need = std::max(need, (size_t)lv.max_fsz * (lv.max_fsz + 1) * lv.count * (Bp / kWarp));
+  for (const auto& lv : d.levels) need = std::max(need, level_scratch_elems(lv, es, Bp / kWarp));
   if (need * kWarp * es > scratch_bytes)
     throw std::invalid_argument("Factorize (static scratch): this batch needs " + std::to_string(need * kWarp * es) +
                                 " bytes of front scratch, the static area holds " + std::to_string(scratch_bytes));

@@ -36,6 +36,8 @@ struct EngineConfig {
   int32_t adjoint_refine_steps = 2;
   int32_t autotune = 0;           // tune the factor levels' warps per block per batch size
   int32_t par_nd_depth = 4, par_nd_base_small = 4000, par_nd_base_large = 20000;
+  int32_t wide_min_front = 65;  // launches with a front this large run the any-size tier
+  int32_t tc_min_front = 0;     // TF32: launches with a front this large use the tensor cores (0: 33 / autotuned)
 };
 
 struct SolveStats {
@@ -115,6 +117,10 @@ class Engine {
   const SymbolicPlan& symbolic() const { return sp_; }
   // warps per block of each factor level launch (0: the built-in rule)
   std::vector<int32_t> factor_level_warps() const;
+  // factor kernel tier of each launch (0 register rows, 1 any-size, 2 tensor
+  // cores) and the tensor-core threshold in use (0 when not TF32)
+  std::vector<int32_t> factor_level_tiers() const;
+  int32_t tc_threshold() const { return tc_min_; }
   // the same for the backward sweep's launches, tree top first
   std::vector<int32_t> backward_launch_warps() const;
   const FactorProgram& program() const { return fp_; }
@@ -147,6 +153,7 @@ class Engine {
   int64_t launches_ = 0;
   bool profiling_ = false;
   bool tolerate_nonfinite_ = false;  // set during warm-started solves
+  int32_t tc_min_ = 0;               // tensor-core tier threshold in use (TF32 factors)
   template <typename T>
   void factor_all_external(cudaStream_t s, const void* J, T* scratch, size_t scratch_elems);
   void stage_begin(int stage, cudaStream_t s);
@@ -155,6 +162,10 @@ class Engine {
 
   void ensure_workspace(int32_t B);
   void upload_plan();
+  // factor kernel tier of every launch: the any-size tier from wide_min_front
+  // rows, and with TF32 factors the tensor-core tier from tc_min rows
+  void assign_tiers(int tc_min);
+  bool tf32_factors() const;
   // selects per-scenario (d_ybus != null) or shared Ybus values for this batch
   void use_scenario_ybus(const double* d_ybus, int64_t ybus_stride, int32_t B, cudaStream_t s);
   template <typename T>

@@ -22,6 +22,10 @@ struct LevelLaunch {
   long long fe_base = 0;
   int warps = 0;   // warps per block of the factor launch (0: the built-in rule)
   int bw_wpb = 0;  // warps per block of the backward-sweep launch (0: the built-in rule)
+  // factor kernel: 0 register rows (fronts of at most 64 rows), 1 the wide
+  // tier on the FP32/FP64 pipes (any size), 2 the wide tier with the trailing
+  // update on the tensor cores (FP32 factors only)
+  int tier = 0;
 };
 
 template <typename T, typename TJ>
@@ -50,9 +54,10 @@ constexpr size_t kSmemLimit = 227 * 1024;  // opt-in dynamic shared memory per b
 struct FrontSmem {
   int chunk = 0;        // staged source rows per buffer
   int nbuf = 1;         // 1, or 2 when a front's sources need more than one chunk
-  int idx_cap = 0;      // source entries whose (src, dst) are staged
+  int idx_cap = 0;      // source entries whose (src, dst) are staged (0: read from global memory)
   size_t idx_bytes = 0, inv_bytes = 0, stage_bytes = 0, front_bytes = 0;
-  size_t total() const { return idx_bytes + inv_bytes + stage_bytes + front_bytes; }
+  size_t us_bytes = 0;  // wide tier: the pivot rows [nc][fs + 1][32] (0: kept in the global scratch)
+  size_t total() const { return idx_bytes + inv_bytes + stage_bytes + front_bytes + us_bytes; }
 };
 
 // The whole source list staged at once when it fits next to the dense front,
@@ -81,6 +86,53 @@ inline FrontSmem plan_front_smem(const LevelLaunch& lv, size_t elem_bytes, bool 
 // True when a level's dense fronts fit in shared memory next to the staging.
 inline bool front_fits_smem(const LevelLaunch& lv, size_t elem_bytes) {
   return plan_front_smem(lv, elem_bytes, true).total() <= kSmemLimit;
+}
+
+// Launches whose fronts have at least this many rows always run a wide tier
+// (no compile-time bound on the front size); the register kernels are built
+// for fronts of up to 64 rows.
+constexpr int kWideFrontRows = 65;
+// TF32 factors: the tensor cores take the trailing updates of launches with
+// fronts of at least this many rows (the fronts beyond 32 rows, where the
+// rank-nc update is large enough to tile), unless configured or autotuned
+// otherwise; the autotuner tries this, 49 and 65.
+constexpr int kTcDefaultMinFront = 33;
+
+// Shared-memory plan of a wide-tier launch: pivot reciprocals, two chunks of
+// staged source rows (the source list itself is read from global memory, it
+// can be thousands of entries long), and the pivot rows Us when they fit;
+// the dense front is in the global scratch.
+inline FrontSmem plan_wide_smem(const LevelLaunch& lv, size_t elem_bytes) {
+  FrontSmem sm;
+  const size_t row = 32 * elem_bytes;
+  sm.idx_cap = 0;
+  sm.idx_bytes = 0;
+  sm.inv_bytes = 8 * row;
+  sm.front_bytes = 0;
+  const int nsrc = lv.max_src > 0 ? lv.max_src : 1;
+  sm.chunk = nsrc <= 64 ? nsrc : 64;
+  sm.nbuf = nsrc <= 64 ? 1 : 2;
+  sm.stage_bytes = (size_t)sm.nbuf * sm.chunk * row;
+  sm.us_bytes = (size_t)lv.max_nc * (lv.max_fsz + 1) * row;
+  if (sm.total() > kSmemLimit) sm.us_bytes = 0;
+  return sm;
+}
+
+// Elements (x 32 scenario lanes) of global scratch one block of a wide-tier
+// launch uses: its dense front, plus the pivot rows when they are not in
+// shared memory.
+inline size_t wide_block_elems(const LevelLaunch& lv, size_t elem_bytes) {
+  const size_t rw = (size_t)lv.max_fsz + 1;
+  return (size_t)lv.max_fsz * rw + (plan_wide_smem(lv, elem_bytes).us_bytes ? 0 : (size_t)lv.max_nc * rw);
+}
+
+// Global front scratch (elements x 32) a factor launch needs for all its
+// blocks (groups = 32-scenario groups of the batch); 0 when its fronts live
+// in shared memory.
+inline size_t level_scratch_elems(const LevelLaunch& lv, size_t elem_bytes, int groups) {
+  if (lv.tier > 0) return wide_block_elems(lv, elem_bytes) * lv.count * groups;
+  if (front_fits_smem(lv, elem_bytes)) return 0;
+  return (size_t)lv.max_fsz * (lv.max_fsz + 1) * lv.count * groups;
 }
 
 template <typename T>

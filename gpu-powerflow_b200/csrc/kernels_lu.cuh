@@ -31,10 +31,12 @@
 #include <set>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 #include <utility>
 
 #include "device_plan.cuh"
 #include "kernels.hpp"
+#include "tcgen05.cuh"
 
 namespace cupf_b200 {
 namespace {
@@ -151,15 +153,21 @@ __device__ __forceinline__ void cp_async_wait() {
 // Fronts whose dense block does not fit next to the staging buffers live in a
 // caller-provided global scratch area (front_scratch), same code.
 // ---------------------------------------------------------------------------
-template <typename T, typename TJ, int FMAX, bool SMEM_FRONT>
-__global__ void __launch_bounds__(256)
-    k_front_factor(DevPlan pl, int level_begin, long long fe_base, int fe_pad, int groups, int Bp, int front_elems,
-                   FrontSmem sm,
-                   const TJ* __restrict__ J, const T* __restrict__ Fp, T* __restrict__ U, T* __restrict__ L,
-                   T* __restrict__ CB, T* __restrict__ Y, int store_l, double eps, int static_pivot,
-                   int* __restrict__ sing, T* __restrict__ front_scratch) {
+// Phases 1 and 2 of a factor block, shared by the front kernels: stage the
+// front's source list (STAGE_LIST: in shared memory; else it is read from
+// global memory where it is used, for lists too long to stage) and its
+// source rows, zero the dense front Fm (shared memory, or this block's slice
+// of the global scratch, whose per-block stride is front_elems x 32) and
+// assemble it.  Returns the launch record; *Fm_out is the assembled front
+// [fs][fs + 1][32].
+template <typename T, typename TJ, bool SMEM_FRONT, bool STAGE_LIST = true>
+__device__ __forceinline__ FrontMeta stage_and_assemble(const DevPlan& pl, int level_begin, long long fe_base,
+                                                        int fe_pad, int groups, int Bp, int front_elems,
+                                                        const FrontSmem& sm, const TJ* __restrict__ J,
+                                                        const T* __restrict__ Fp, const T* __restrict__ CB,
+                                                        T* __restrict__ front_scratch, unsigned char* smem_raw,
+                                                        T** Fm_out) {
   static_assert(sizeof(TJ) == sizeof(T), "Jacobian and factor rows are staged in the same slots");
-  extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int kRowBytes = kWarp * sizeof(T);
   constexpr int kPieces = kRowBytes / 16;  // 16-byte cp.async pieces per source row
   const int W = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -168,30 +176,34 @@ __global__ void __launch_bounds__(256)
   const int grp = item - (item / groups) * groups;
   const size_t col0 = (size_t)grp * kWarp;
   chain_allow_next();
-  long long* s_src = reinterpret_cast<long long*>(smem_raw);
-  int* s_dst = reinterpret_cast<int*>(smem_raw + (size_t)sm.idx_cap * sizeof(long long));
+  const long long e0 = fe_base + (long long)(q - level_begin) * fe_pad;
+  const long long* s_src = pl.fe_src + e0;
+  const int* s_dst = pl.fe_dst + e0;
   // phase 1a: the source list -> shared memory.  Its place follows from the
   // item alone (padded lists), so it is requested together with the launch
   // record: one memory round trip for both.
-  {
-    const long long e0 = fe_base + (long long)(q - level_begin) * fe_pad;
+  if constexpr (STAGE_LIST) {
+    long long* ss = reinterpret_cast<long long*>(smem_raw);
+    int* sd = reinterpret_cast<int*>(smem_raw + (size_t)sm.idx_cap * sizeof(long long));
     for (int e = threadIdx.x; e < fe_pad; e += blockDim.x) {
-      cp_async8(s_src + e, pl.fe_src + e0 + e);
-      cp_async4(s_dst + e, pl.fe_dst + e0 + e);
+      cp_async8(ss + e, pl.fe_src + e0 + e);
+      cp_async4(sd + e, pl.fe_dst + e0 + e);
     }
     cp_async_commit();
+    s_src = ss;
+    s_dst = sd;
   }
   const FrontMeta m = load_front_meta(pl.front_meta, q);
-  const int fs = m.fs, nc = m.nc, uc = fs - nc, rw = fs + 1;
+  const int fs = m.fs, rw = fs + 1;
   const int nsrc = m.split[8];
 
-  T* s_inv = reinterpret_cast<T*>(smem_raw + sm.idx_bytes);  // [8][32] pivot reciprocals
   unsigned char* stage = smem_raw + sm.idx_bytes + sm.inv_bytes;
   T* Fm;
   if constexpr (SMEM_FRONT)
     Fm = reinterpret_cast<T*>(stage + sm.stage_bytes);
   else
     Fm = front_scratch + (size_t)item * front_elems * kWarp;
+  *Fm_out = Fm;
 
   // (the dense front is zeroed while the list arrives)
   // fs * rw * 32 elements is a multiple of 16 bytes: zero with 16-byte stores
@@ -273,6 +285,24 @@ __global__ void __launch_bounds__(256)
   }
   if (cur >= 0) Fm[cur * kWarp + lane] = acc;
   __syncthreads();
+  return m;
+}
+
+template <typename T, typename TJ, int FMAX, bool SMEM_FRONT>
+__global__ void __launch_bounds__(256)
+    k_front_factor(DevPlan pl, int level_begin, long long fe_base, int fe_pad, int groups, int Bp, int front_elems,
+                   FrontSmem sm,
+                   const TJ* __restrict__ J, const T* __restrict__ Fp, T* __restrict__ U, T* __restrict__ L,
+                   T* __restrict__ CB, T* __restrict__ Y, int store_l, double eps, int static_pivot,
+                   int* __restrict__ sing, T* __restrict__ front_scratch) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int W = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const size_t col0 = (size_t)(blockIdx.x % groups) * kWarp;
+  T* Fm = nullptr;
+  const FrontMeta m = stage_and_assemble<T, TJ, SMEM_FRONT>(pl, level_begin, fe_base, fe_pad, groups, Bp, front_elems,
+                                                            sm, J, Fp, CB, front_scratch, smem_raw, &Fm);
+  const int fs = m.fs, nc = m.nc, uc = fs - nc, rw = fs + 1;
+  T* s_inv = reinterpret_cast<T*>(smem_raw + sm.idx_bytes);  // [8][32] pivot reciprocals
 
   // phase 3a: the nc pivot rows.  A pivot is guarded once and its reciprocal
   // kept in s_inv, so every elimination is a multiply (l = a * (1 / u_kk)).
@@ -390,6 +420,326 @@ __global__ void __launch_bounds__(256)
 }
 
 // ---------------------------------------------------------------------------
+// The wide tier: fronts of any size.  Same block shape (one front x 32
+// scenarios) and phases 1-2 as k_front_factor, with the source list read
+// from global memory, the dense front always in this block's slice of the
+// global scratch, and the nc pivot rows Us [nc][fs + 1][32] in shared memory
+// (or after the front in the scratch when they do not fit).  No row is held
+// in registers, so the front size has no compile-time bound:
+//  3a. pivot rows k = 0 .. nc-1 in order: every warp forms the row's
+//      multipliers l_km (m < k) for its lane, then its share of the row's
+//      columns j >= k (j = fs is the right-hand side); warp 0 guards the
+//      pivot and keeps 1 / u_kk;
+//  3b. U rows and y out;
+//  3c. non-pivot rows, one warp per row: the nc multipliers (L21, stored
+//      when store_l), then CB row = A22 row - L21 row * U12, streamed out.
+// Every element sees the register kernel's operations in the same order, so
+// both tiers produce the same factors.
+// ---------------------------------------------------------------------------
+
+// Multipliers of front row Ri against the first n pivot rows (n <= 8):
+// l_m = (a_m - sum_{m' < m} l_m' u_m'm) / u_mm, in the register kernel's order.
+// Us holds the pivot rows with lane stride LS (32, or 33 where other code
+// reads one scenario's column of it).
+template <typename T, int LS = kWarp>
+__device__ __forceinline__ void row_multipliers(const T* Ri, const T* Us, const T* inv_l, int rw, int n, T (&l)[8]) {
+#pragma unroll
+  for (int mm = 0; mm < 8; ++mm) {
+    l[mm] = T(0);
+    if (mm < n) {
+      T r = Ri[(size_t)mm * kWarp];
+#pragma unroll
+      for (int m2 = 0; m2 < 8; ++m2)
+        if (m2 < mm) r -= l[m2] * Us[(size_t)(m2 * rw + mm) * LS];
+      l[mm] = r * inv_l[mm * kWarp];
+    }
+  }
+}
+
+// Phase 3a/3b of the wide tier: the pivot rows into Us (lane stride LS), then
+// U rows and y out.
+template <typename T, int LS = kWarp>
+__device__ __forceinline__ void wide_pivot_rows(const FrontMeta& m, const T* Fl, T* Us, T* inv_l, int Bp, size_t b,
+                                                T* __restrict__ U, T* __restrict__ Y, double eps, int static_pivot,
+                                                bool& shifted) {
+  const int W = blockDim.x >> 5, warp = threadIdx.x >> 5;
+  const int fs = m.fs, nc = m.nc, rw = fs + 1;
+  for (int k = 0; k < nc; ++k) {
+    const T* Rk = Fl + (size_t)k * rw * kWarp;
+    T l[8];
+    row_multipliers<T, LS>(Rk, Us, inv_l, rw, k, l);
+    T* Uk = Us + (size_t)k * rw * LS;
+    for (int j = warp; j <= fs; j += W) {
+      T r = T(0);
+      if (j < k) {
+#pragma unroll
+        for (int mm = 0; mm < 8; ++mm)
+          if (mm == j) r = l[mm];
+      } else {
+        r = Rk[(size_t)j * kWarp];
+#pragma unroll
+        for (int mm = 0; mm < 8; ++mm)
+          if (mm < k) r -= l[mm] * Us[(size_t)(mm * rw + j) * LS];
+      }
+      Uk[(size_t)j * LS] = r;
+    }
+    __syncthreads();
+    if (warp == 0) {
+      const T p = guarded_pivot(Uk[(size_t)k * LS], static_pivot != 0, eps, shifted);
+      Uk[(size_t)k * LS] = p;
+      inv_l[k * kWarp] = T(1) / p;
+    }
+    __syncthreads();
+  }
+  // U rows: elements uo + k * fs + j (j < fs), then y from the rhs column
+  for (int e = warp; e < nc * fs; e += W) {
+    const int k = e / fs, j = e - k * fs;
+    U[(size_t)(m.uo + e) * Bp + b] = Us[(size_t)(k * rw + j) * LS];
+  }
+  for (int k = warp; k < nc; k += W) Y[(size_t)(m.first + k) * Bp + b] = Us[(size_t)(k * rw + fs) * LS];
+}
+
+template <typename T, typename TJ>
+__global__ void __launch_bounds__(256)
+    k_front_factor_wide(DevPlan pl, int level_begin, long long fe_base, int fe_pad, int groups, int Bp,
+                        int front_elems, FrontSmem sm, const TJ* __restrict__ J, const T* __restrict__ Fp,
+                        T* __restrict__ U, T* __restrict__ L, T* __restrict__ CB, T* __restrict__ Y, int store_l,
+                        double eps, int static_pivot, int* __restrict__ sing, T* __restrict__ front_scratch) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int W = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const size_t col0 = (size_t)(blockIdx.x % groups) * kWarp;
+  const size_t b = col0 + lane;
+  T* Fm = nullptr;
+  const FrontMeta m = stage_and_assemble<T, TJ, false, false>(pl, level_begin, fe_base, fe_pad, groups, Bp,
+                                                              front_elems, sm, J, Fp, CB, front_scratch, smem_raw,
+                                                              &Fm);
+  const int fs = m.fs, nc = m.nc, uc = fs - nc, rw = fs + 1;
+  T* inv_l = reinterpret_cast<T*>(smem_raw + sm.idx_bytes) + lane;
+  T* Us = (sm.us_bytes ? reinterpret_cast<T*>(smem_raw + sm.idx_bytes + sm.inv_bytes + sm.stage_bytes)
+                       : Fm + (size_t)fs * rw * kWarp) + lane;
+  const T* Fl = Fm + lane;
+  bool shifted = false;
+  wide_pivot_rows<T>(m, Fl, Us, inv_l, Bp, b, U, Y, eps, static_pivot, shifted);
+  for (int i = nc + warp; i < fs; i += W) {
+    const int ii = i - nc;
+    const T* Ri = Fl + (size_t)i * rw * kWarp;
+    T l[8];
+    row_multipliers(Ri, Us, inv_l, rw, nc, l);
+    if (store_l) {
+      T* Lb = L + (size_t)(m.lo + (long long)ii * nc) * Bp + b;
+#pragma unroll
+      for (int mm = 0; mm < 8; ++mm)
+        if (mm < nc) Lb[(size_t)mm * Bp] = l[mm];
+    }
+    T* Cb = CB + (size_t)(m.co + (long long)ii * (uc + 1)) * Bp + b;
+#pragma unroll 4
+    for (int j = nc; j <= fs; ++j) {
+      T r = Ri[(size_t)j * kWarp];
+#pragma unroll
+      for (int mm = 0; mm < 8; ++mm)
+        if (mm < nc) r -= l[mm] * Us[(size_t)(mm * rw + j) * kWarp];
+      Cb[(size_t)(j - nc) * Bp] = r;
+    }
+  }
+  if (shifted) sing[b] = 1;
+}
+
+// ---------------------------------------------------------------------------
+// The wide tier with the trailing update on the tensor cores (FP32 factors;
+// CustomPrecision::TF32).  Phases 1-3b as k_front_factor_wide, with the
+// pivot rows in shared memory at lane stride 33 (so that one scenario's
+// column is read across the banks); then
+//  3c. the L21 multipliers of every non-pivot row, for the block's 32
+//      scenarios, into shared memory (Ls [uc][8][33]);
+//  3d. per scenario s: its L21 block (uc x nc, padded to M = 128 rows) and
+//      U12^T ((uc + 1) x nc: the trailing columns and the right-hand side,
+//      padded to N rows) are packed as K-major tf32 tiles, each operand
+//      split as x = hi + lo (both tf32, about 21 bits of the fp32 value);
+//      three tcgen05.mma kind::tf32 with K = 8 -- hi*hi + hi*lo + lo*hi, the
+//      Ozaki-style split -- accumulate D = L21 U12 in tensor memory (fp32).
+//      The epilogue reads D back (tcgen05.ld: TMEM lane = front row) and
+//      subtracts it from the trailing block of the front in the scratch;
+//  3e. the trailing block, now A22 - L21 U12 with the updated right-hand
+//      side, is copied to CB, 32 scenarios per coalesced row.
+// One thread issues the MMAs; the wait for their commit is bounded.  When it
+// runs out, the block flags its systems (singular flag 2) and writes NaN to
+// their y and CB rows, so a solve on these factors is visibly non-finite.
+// Limits (checked by the launcher, which uses the FP32 wide tier otherwise):
+// uc <= 128 (one M tile), uc + 1 <= 256 (one N tile), shared memory.
+// ---------------------------------------------------------------------------
+constexpr int kTcLS = kWarp + 1;  // lane stride of Us and Ls in the tensor-core tier
+
+// Shared-memory layout of a tensor-core launch (byte offsets from the base).
+struct TcLayout {
+  int n_pad = 0;      // N of the MMA: the trailing columns + rhs, rounded up to 16
+  int tmem_cols = 0;  // tensor-memory columns allocated (power of 2 >= 32)
+  unsigned us_off = 0, ls_off = 0, a_off = 0, b_off = 0, bar_off = 0, total = 0;
+};
+
+inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+inline TcLayout plan_tc_layout(const LevelLaunch& lv, const FrontSmem& sm) {
+  TcLayout t;
+  const int rw = lv.max_fsz + 1;
+  const int max_uc = lv.max_fsz - 1;  // nc >= 1
+  t.n_pad = (int)align_up((size_t)std::max(max_uc + 1, 16), 16);
+  t.tmem_cols = 32;
+  while (t.tmem_cols < t.n_pad) t.tmem_cols *= 2;
+  size_t off = sm.idx_bytes + sm.inv_bytes + sm.stage_bytes;
+  off = align_up(off, 16);
+  t.us_off = (unsigned)off;
+  off += (size_t)lv.max_nc * rw * kTcLS * sizeof(float);
+  off = align_up(off, 16);
+  t.ls_off = (unsigned)off;
+  off += (size_t)std::max(max_uc, 1) * 8 * kTcLS * sizeof(float);
+  off = align_up(off, 128);
+  t.a_off = (unsigned)off;
+  off += 2 * 128 * 32;  // A hi, A lo: 128 rows x 8 tf32
+  t.b_off = (unsigned)off;
+  off += 2 * (size_t)t.n_pad * 32;  // B hi, B lo: n_pad rows x 8 tf32
+  off = align_up(off, 8);
+  t.bar_off = (unsigned)off;
+  off += 8 + 4 + 4;  // mbarrier, TMEM address slot, failure flag
+  t.total = (unsigned)align_up(off, 16);
+  return t;
+}
+
+inline bool tc_tier_fits(const LevelLaunch& lv, const TcLayout& t) {
+  return lv.max_fsz - 1 <= 128 && t.n_pad <= 256 && t.total <= kSmemLimit;
+}
+
+// byte offset of element (r, k) in a K-major tile of 8-row x 16-byte core
+// matrices, K = 8 tf32: core matrices 128 B apart along K, 8-row groups 256 B
+__device__ __forceinline__ unsigned tc_tile_off(int r, int k) {
+  return (unsigned)((r >> 3) * 256 + (k >> 2) * 128 + (r & 7) * 16 + (k & 3) * 4);
+}
+
+__global__ void __launch_bounds__(256)
+    k_front_factor_tc(DevPlan pl, int level_begin, long long fe_base, int fe_pad, int groups, int Bp,
+                      int front_elems, FrontSmem sm, TcLayout tl, const float* __restrict__ J,
+                      const float* __restrict__ Fp, float* __restrict__ U, float* __restrict__ L,
+                      float* __restrict__ CB, float* __restrict__ Y, int store_l, double eps, int static_pivot,
+                      int* __restrict__ sing, float* __restrict__ front_scratch, long long spin_limit) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  const int W = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const size_t col0 = (size_t)(blockIdx.x % groups) * kWarp;
+  const size_t b = col0 + lane;
+  float* Fm = nullptr;
+  const FrontMeta m = stage_and_assemble<float, float, false, false>(pl, level_begin, fe_base, fe_pad, groups, Bp,
+                                                                      front_elems, sm, J, Fp, CB, front_scratch,
+                                                                      smem_raw, &Fm);
+  const int fs = m.fs, nc = m.nc, uc = fs - nc, rw = fs + 1, nb = uc + 1;
+  float* inv_l = reinterpret_cast<float*>(smem_raw + sm.idx_bytes) + lane;
+  float* Us = reinterpret_cast<float*>(smem_raw + tl.us_off);  // [nc][rw][33]
+  float* Ls = reinterpret_cast<float*>(smem_raw + tl.ls_off);  // [uc][8][33]
+  unsigned char* tA = smem_raw + tl.a_off;
+  unsigned char* tB = smem_raw + tl.b_off;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + tl.bar_off);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(smem_raw + tl.bar_off + 8);
+  int* s_fail = reinterpret_cast<int*>(smem_raw + tl.bar_off + 12);
+  const float* Fl = Fm + lane;
+  if (threadIdx.x == 0) {
+    tc::mbar_init(bar, 1);
+    *s_fail = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  bool shifted = false;
+  wide_pivot_rows<float, kTcLS>(m, Fl, Us + lane, inv_l, Bp, b, U, Y, eps, static_pivot, shifted);
+  // 3c: multipliers of the non-pivot rows (L21), 32 scenarios at a time
+  for (int i = nc + warp; i < fs; i += W) {
+    const int ii = i - nc;
+    float l[8];
+    row_multipliers<float, kTcLS>(Fl + (size_t)i * rw * kWarp, Us + lane, inv_l, rw, nc, l);
+    float* Lr = Ls + (size_t)ii * 8 * kTcLS + lane;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) Lr[k * kTcLS] = l[k];
+    if (store_l) {
+      float* Lb = L + (size_t)(m.lo + (long long)ii * nc) * Bp + b;
+#pragma unroll
+      for (int k = 0; k < 8; ++k)
+        if (k < nc) Lb[(size_t)k * Bp] = l[k];
+    }
+  }
+  if (warp == 0) tc::tmem_alloc(tslot, (uint32_t)tl.tmem_cols);
+  __syncthreads();
+  tc::tc_fence_after();
+  const uint32_t tmem = *tslot;
+  const uint32_t idesc = tc::idesc_tf32(128, tl.n_pad);
+  const int qtr = warp & 3, nsplit = W >> 2, part = warp >> 2;
+  const int row = qtr * 32 + lane;  // this thread's TMEM lane = front row of the trailing block
+  int failed_at = -1;
+  for (int sc = 0; sc < (uc > 0 ? kWarp : 0); ++sc) {  // (a root front has no trailing block)
+    // 3d: scenario sc's operands as hi + lo tf32 tiles
+    for (int e = threadIdx.x; e < 128 * 8; e += blockDim.x) {
+      const int r = e >> 3, k = e & 7;
+      const float x = r < uc ? Ls[((size_t)r * 8 + k) * kTcLS + sc] : 0.0f;
+      const float hi = tc::to_tf32(x);
+      const unsigned o = tc_tile_off(r, k);
+      *reinterpret_cast<float*>(tA + o) = hi;
+      *reinterpret_cast<float*>(tA + 4096 + o) = tc::to_tf32(x - hi);
+    }
+    for (int e = threadIdx.x; e < tl.n_pad * 8; e += blockDim.x) {
+      const int j = e >> 3, k = e & 7;
+      const float x = (j < nb && k < nc) ? Us[((size_t)k * rw + nc + j) * kTcLS + sc] : 0.0f;
+      const float hi = tc::to_tf32(x);
+      const unsigned o = tc_tile_off(j, k);
+      *reinterpret_cast<float*>(tB + o) = hi;
+      *reinterpret_cast<float*>(tB + (size_t)tl.n_pad * 32 + o) = tc::to_tf32(x - hi);
+    }
+    tc::fence_smem_to_async();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      tc::tc_fence_after();
+      const uint64_t ah = tc::smem_desc_plain(tA, 128, 256), al = tc::smem_desc_plain(tA + 4096, 128, 256);
+      const uint64_t bh = tc::smem_desc_plain(tB, 128, 256);
+      const uint64_t bl = tc::smem_desc_plain(tB + (size_t)tl.n_pad * 32, 128, 256);
+      tc::tc_mma_tf32(tmem, ah, bh, idesc, 0u);
+      tc::tc_mma_tf32(tmem, ah, bl, idesc, 1u);
+      tc::tc_mma_tf32(tmem, al, bh, idesc, 1u);
+      tc::tc_commit(bar);
+    }
+    const bool have = __all_sync(0xffffffffu, tc::mbar_wait(bar, (uint32_t)(sc & 1), spin_limit));
+    if (!have && lane == 0) atomicExch(s_fail, 1);
+    __syncthreads();
+    tc::tc_fence_after();
+    if (*s_fail) {
+      failed_at = sc;
+      break;
+    }
+    // epilogue: the W / 4 warps of a TMEM lane quarter split the 16-column chunks
+    float* Fr = Fm + ((size_t)(nc + row) * rw + nc) * kWarp + sc;
+    for (int c = part; c < tl.n_pad / 16; c += nsplit) {
+      float v[16];
+      tc::tmem_ld16(tmem + ((uint32_t)(qtr * 32) << 16) + (uint32_t)(c * 16), v);
+      if (row < uc) {
+#pragma unroll
+        for (int t = 0; t < 16; ++t)
+          if (c * 16 + t < nb) Fr[(size_t)(c * 16 + t) * kWarp] -= v[t];
+      }
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+  }
+  if (failed_at >= 0) tc::mbar_wait(bar, (uint32_t)(failed_at & 1), spin_limit);  // the MMAs still in flight
+  tc::tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(tmem, (uint32_t)tl.tmem_cols);
+  // 3e: the updated trailing block -> CB (NaN when the products did not complete)
+  const float nan = __int_as_float(0x7fc00000);
+  for (int ii = warp; ii < uc; ii += W) {
+    const float* Fr = Fl + ((size_t)(nc + ii) * rw + nc) * kWarp;
+    float* Cb = CB + (size_t)(m.co + (long long)ii * nb) * Bp + b;
+    for (int j = 0; j < nb; ++j) Cb[(size_t)j * Bp] = failed_at < 0 ? Fr[(size_t)j * kWarp] : nan;
+  }
+  if (failed_at >= 0) {
+    for (int k = warp; k < nc; k += W) Y[(size_t)(m.first + k) * Bp + b] = nan;
+    if (warp == 0) sing[b] = 2;
+  } else if (shifted) {
+    sing[b] = 1;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Backward substitution U x = y of one level (root first).  X is in permuted
 // order; a front reads the x of its CB rows, which belong to ancestors.
 // One warp = one front x 32 scenarios.  The warp stages its front's U rows
@@ -398,7 +748,9 @@ __global__ void __launch_bounds__(256)
 // ---------------------------------------------------------------------------
 // One front x 32 scenarios (starting at col0), by one warp, with its
 // staging area Us.
-template <typename T>
+// STAGED = false (fronts whose U rows do not fit in shared memory): the same
+// substitution reading U and x straight from global memory.
+template <typename T, bool STAGED = true>
 __device__ __forceinline__ void backward_front(const DevPlan& pl, int q, size_t col0, int Bp, T* Us,
                                                const T* __restrict__ U, const T* __restrict__ Y,
                                                T* __restrict__ X) {
@@ -409,6 +761,17 @@ __device__ __forceinline__ void backward_front(const DevPlan& pl, int q, size_t 
   const int fs = m.fs, nc = m.nc, uc = fs - nc;
   const int fr0 = m.fr0, first = m.first;
   const long long uo = m.uo;
+  if constexpr (!STAGED) {
+    // x_k = (y_k - sum_{j > k} u_kj x(row j)) / u_kk, k from the last pivot
+    // down; the pivots' x rows are first + k, written by this thread
+    for (int k = nc - 1; k >= 0; --k) {
+      const T* urow = U + (size_t)(uo + (long long)k * fs) * Bp + b;
+      T s = Y[(size_t)(first + k) * Bp + b];
+      for (int j = k + 1; j < fs; ++j) s -= urow[(size_t)j * Bp] * X[(size_t)pl.front_rows[fr0 + j] * Bp + b];
+      X[(size_t)(first + k) * Bp + b] = s / urow[(size_t)k * Bp];
+    }
+    return;
+  }
   T* Xs = Us + (size_t)nc * fs * kWarp;  // [fs][32]
   // U rows: contiguous elements uo .. uo + nc * fs
   for (int t = lane; t < nc * fs * kPieces; t += kWarp) {
@@ -444,7 +807,7 @@ __device__ __forceinline__ void backward_front(const DevPlan& pl, int q, size_t 
   __syncwarp();  // the staging area is reused by the warp's next front
 }
 
-template <typename T>
+template <typename T, bool STAGED = true>
 __global__ void __launch_bounds__(256)
     k_backward_level(DevPlan pl, int level_begin, int level_count, int groups, int Bp, int warp_elems,
                      const T* __restrict__ U, const T* __restrict__ Y, T* __restrict__ X) {
@@ -457,7 +820,7 @@ __global__ void __launch_bounds__(256)
   chain_allow_next();
   chain_wait_previous();  // U, Y and the x of ancestors come from earlier kernels
   T* Us = reinterpret_cast<T*>(smem_raw) + (size_t)warp * warp_elems * kWarp;  // [nc * fs][32]
-  backward_front<T>(pl, q, col0, Bp, Us, U, Y, X);
+  backward_front<T, STAGED>(pl, q, col0, Bp, Us, U, Y, X);
 }
 
 // The narrow top of the tree in one launch: block = one group of 32
@@ -466,7 +829,7 @@ __global__ void __launch_bounds__(256)
 // (the x a front reads come from its ancestors, written by this block).
 // lv_lo[t] .. lv_lo[t + 1]: level-order fronts of the t-th level from the
 // root (descending boundaries, nlev + 1 entries).
-template <typename T>
+template <typename T, bool STAGED = true>
 __global__ void __launch_bounds__(256)
     k_backward_top(DevPlan pl, const int* __restrict__ lv_bounds, int nlev, int Bp, int warp_elems,
                    const T* __restrict__ U, const T* __restrict__ Y, T* __restrict__ X) {
@@ -478,7 +841,7 @@ __global__ void __launch_bounds__(256)
   T* Us = reinterpret_cast<T*>(smem_raw) + (size_t)warp * warp_elems * kWarp;
   for (int t = 0; t < nlev; ++t) {
     const int hi = lv_bounds[t], lo = lv_bounds[t + 1];
-    for (int q = lo + warp; q < hi; q += W) backward_front<T>(pl, q, col0, Bp, Us, U, Y, X);
+    for (int q = lo + warp; q < hi; q += W) backward_front<T, STAGED>(pl, q, col0, Bp, Us, U, Y, X);
     __syncthreads();
   }
 }
@@ -721,12 +1084,69 @@ void configure_front_kernels() {
   CUPF_ALLOW(8) CUPF_ALLOW(12) CUPF_ALLOW(16) CUPF_ALLOW(20) CUPF_ALLOW(24) CUPF_ALLOW(32) CUPF_ALLOW(48)
   CUPF_ALLOW(64)
 #undef CUPF_ALLOW
+  allow_full_smem(reinterpret_cast<const void*>(k_front_factor_wide<T, TJ>));
+  if constexpr (std::is_same<T, float>::value) allow_full_smem(reinterpret_cast<const void*>(k_front_factor_tc));
+}
+
+// A wide-tier launch: one block per front x 32 scenarios, 8 warps unless
+// the autotuner chose otherwise, dense fronts in the global scratch.
+template <typename T, typename TJ>
+void launch_factor_wide(const LevelLaunch& lv, const FactorArgs<T, TJ>& a, cudaStream_t s) {
+  const FrontSmem sm = plan_wide_smem(lv, sizeof(T));
+  if (sm.total() > kSmemLimit) throw std::runtime_error("wide front tier: staging exceeds shared memory");
+  const size_t per_block = wide_block_elems(lv, sizeof(T));
+  const long items = (long)lv.count * a.groups;
+  if (!a.front_scratch || a.front_scratch_elems < per_block * (size_t)items)
+    throw std::runtime_error("wide front tier: the front scratch area is missing or too small");
+  if (per_block > (size_t)INT32_MAX) throw std::runtime_error("wide front tier: front too large");
+  const int warps = lv.warps > 0 ? lv.warps : 8;
+  auto kern = k_front_factor_wide<T, TJ>;
+  allow_full_smem(reinterpret_cast<const void*>(kern));
+  launch_chained(kern, dim3((unsigned)items), dim3(warps * kWarp), sm.total(), s, "front factor (wide tier)", a.plan,
+                 lv.begin, lv.fe_base, lv.max_src, a.groups, a.Bp, (int)per_block, sm, a.J, a.Fp, a.U, a.L, a.CB, a.Y,
+                 a.store_l, a.eps, a.static_pivot, a.sing, a.front_scratch);
+}
+
+// A tensor-core launch (FP32 factors): 4 or 8 warps (every TMEM lane
+// quarter needs its warp); falls back to the FP32 wide tier where the fronts
+// exceed its limits.
+template <typename T, typename TJ>
+void launch_factor_tc(const LevelLaunch& lv, const FactorArgs<T, TJ>& a, cudaStream_t s) {
+  if constexpr (!std::is_same<T, float>::value || !std::is_same<TJ, float>::value) {
+    launch_factor_wide<T, TJ>(lv, a, s);  // the tensor-core tier is built for FP32 factors
+  } else {
+    FrontSmem sm = plan_wide_smem(lv, sizeof(float));
+    sm.us_bytes = 0;  // the pivot rows have their own padded place
+    const TcLayout tl = plan_tc_layout(lv, sm);
+    if (!tc_tier_fits(lv, tl)) {
+      launch_factor_wide<T, TJ>(lv, a, s);
+      return;
+    }
+    const int front_elems = lv.max_fsz * (lv.max_fsz + 1);
+    const long items = (long)lv.count * a.groups;
+    if (!a.front_scratch || a.front_scratch_elems < (size_t)front_elems * (size_t)items)
+      throw std::runtime_error("tensor-core front tier: the front scratch area is missing or too small");
+    const int warps = lv.warps >= 8 || lv.warps == 0 ? 8 : 4;
+    allow_full_smem(reinterpret_cast<const void*>(k_front_factor_tc));
+    launch_chained(k_front_factor_tc, dim3((unsigned)items), dim3(warps * kWarp), (size_t)tl.total, s,
+                   "front factor (tensor-core tier)", a.plan, lv.begin, lv.fe_base, lv.max_src, a.groups, a.Bp,
+                   front_elems, sm, tl, a.J, a.Fp, a.U, a.L, a.CB, a.Y, a.store_l, a.eps, a.static_pivot, a.sing,
+                   a.front_scratch, tc::kSpinLimit);
+  }
 }
 
 template <typename T, typename TJ>
 void launch_factor_level(const LevelLaunch& lv, const FactorArgs<T, TJ>& a, cudaStream_t s) {
   if (lv.count == 0) return;
   if (lv.max_nc > 8) throw std::runtime_error("panels wider than 8 columns are not supported (max_panel_width <= 8)");
+  if (lv.tier == 2) {
+    launch_factor_tc<T, TJ>(lv, a, s);
+    return;
+  }
+  if (lv.tier == 1 || lv.max_fsz >= kWideFrontRows) {
+    launch_factor_wide<T, TJ>(lv, a, s);
+    return;
+  }
   const int f = lv.max_fsz;
   if (f <= 8) launch_factor_t<T, TJ, 8>(lv, a, s);
   else if (f <= 12) launch_factor_t<T, TJ, 12>(lv, a, s);
@@ -735,8 +1155,7 @@ void launch_factor_level(const LevelLaunch& lv, const FactorArgs<T, TJ>& a, cuda
   else if (f <= 24) launch_factor_t<T, TJ, 24>(lv, a, s);
   else if (f <= 32) launch_factor_t<T, TJ, 32>(lv, a, s);
   else if (f <= 48) launch_factor_t<T, TJ, 48>(lv, a, s);
-  else if (f <= 64) launch_factor_t<T, TJ, 64>(lv, a, s);
-  else throw std::runtime_error("front larger than 64 rows is not supported");
+  else launch_factor_t<T, TJ, 64>(lv, a, s);
 }
 
 template <typename T>
@@ -745,10 +1164,15 @@ void launch_backward_level(const LevelLaunch& lv, const SweepArgs<T>& a, cudaStr
   if (lv.max_nc > 8) throw std::runtime_error("panels wider than 8 columns are not supported (max_panel_width <= 8)");
   const int warp_elems = lv.max_nc * lv.max_fsz + lv.max_fsz;
   const size_t per_warp = (size_t)warp_elems * kWarp * sizeof(T);
-  int wpb = (int)std::min<size_t>(8, kSmemLimit / per_warp);
-  if (wpb < 1) throw std::runtime_error("backward level: front exceeds shared memory");
-  const int cap = wpb;
   const long items = (long)lv.count * a.groups;
+  if (per_warp > kSmemLimit) {  // U rows too large to stage: read them from global memory
+    const int w = lv.bw_wpb > 0 ? lv.bw_wpb : 4;
+    launch_chained(k_backward_level<T, false>, dim3((unsigned)((items + w - 1) / w)), dim3(w * kWarp), 0, s,
+                   "backward sweep", a.plan, lv.begin, lv.count, a.groups, a.Bp, warp_elems, a.U, a.Y, a.X);
+    return;
+  }
+  int wpb = (int)std::min<size_t>(8, kSmemLimit / per_warp);
+  const int cap = wpb;
   wpb = (int)std::min<long>(wpb, std::max<long>(1, items / 148));
   wpb = std::max(1, std::min(wpb, 4));
   if (lv.bw_wpb > 0) wpb = std::min(lv.bw_wpb, cap);  // chosen by the engine's autotuner
@@ -768,8 +1192,13 @@ void launch_backward_top(const LevelLaunch& top, const int* lv_bounds, int nlev,
   if (top.count == 0 || nlev == 0) return;
   const int warp_elems = top.max_nc * top.max_fsz + top.max_fsz;
   const size_t per_warp = (size_t)warp_elems * kWarp * sizeof(T);
+  if (per_warp > kSmemLimit) {  // U rows too large to stage: read them from global memory
+    const int w = top.bw_wpb > 0 ? top.bw_wpb : 4;
+    launch_chained(k_backward_top<T, false>, dim3((unsigned)a.groups), dim3(w * kWarp), 0, s,
+                   "backward sweep (tree top)", a.plan, lv_bounds, nlev, a.Bp, warp_elems, a.U, a.Y, a.X);
+    return;
+  }
   const int cap = (int)std::min<size_t>(8, kSmemLimit / per_warp);
-  if (cap < 1) throw std::runtime_error("backward sweep: front exceeds shared memory");
   const int wpb = top.bw_wpb > 0 ? std::min(top.bw_wpb, cap) : std::min(4, cap);
   auto kern = k_backward_top<T>;
   allow_full_smem(reinterpret_cast<const void*>(kern));

@@ -16,7 +16,10 @@ Differences a user can see:
   * ``CustomSolverConfig.max_panel_width`` is limited to 1..8;
   * ``CustomSolverConfig.autotune`` (not in the reference, on by default)
     times each factor level's block shape at the first solve of a batch size
-    and keeps the fastest; the results do not depend on it.
+    and keeps the fastest; the results do not depend on it;
+  * ``CustomSolverConfig.wide_min_front`` and ``tc_min_front`` (not in the
+    reference) set where the any-size front tier and, with
+    ``CustomPrecision.TF32``, the tensor-core trailing update take over.
 """
 from __future__ import annotations
 
@@ -117,7 +120,8 @@ class CustomSolverConfig(_Struct):
     _fields = {"precision": CustomPrecision.FP32, "matching": CustomMatchingMode["None"],
                "pivot_strategy": CustomPivotStrategy.StaticDiagonalShift, "serial_nd": False,
                "max_panel_width": 8, "shift_retry_epsilon": 1.0e-8, "autotune": True,
-               "parallel_nd_depth": 4, "parallel_nd_base_small": 4000, "parallel_nd_base_large": 20000}
+               "parallel_nd_depth": 4, "parallel_nd_base_small": 4000, "parallel_nd_base_large": 20000,
+               "wide_min_front": 0, "tc_min_front": 0}
 
 
 class NewtonOptions(_Struct):
@@ -266,7 +270,8 @@ def _check(lib, h, st: int) -> None:
 def _cls_config(c: CustomSolverConfig) -> _capi.ClsConfig:
     return _capi.ClsConfig(int(c.precision), int(c.matching), int(c.pivot_strategy), int(bool(c.serial_nd)),
                            int(c.max_panel_width), float(c.shift_retry_epsilon), int(bool(c.autotune)),
-                           int(c.parallel_nd_depth), int(c.parallel_nd_base_small), int(c.parallel_nd_base_large))
+                           int(c.parallel_nd_depth), int(c.parallel_nd_base_small), int(c.parallel_nd_base_large),
+                           int(c.wide_min_front), int(c.tc_min_front))
 
 
 def _nr_config(cfg: NRConfig | None) -> _capi.PfNRConfig:

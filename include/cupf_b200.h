@@ -67,7 +67,7 @@ enum { CLS_PIVOT_NONE = 0, CLS_PIVOT_STATIC_DIAGONAL_SHIFT = 1 };
  * (analyze/pipeline.cpp:77-160, 222-272); plan arrays "row_iperm",
  * "col_perm" and "row_to_col" expose it. */
 typedef struct {
-  int32_t precision;            /* CLS_PRECISION_*; TF32 runs the FP32 kernels */
+  int32_t precision;            /* CLS_PRECISION_*; TF32 = FP32 factors with tensor-core trailing updates */
   int32_t matching;             /* 0 = None, 1 = Structural */
   int32_t pivot_strategy;       /* CLS_PIVOT_* */
   int32_t serial_nd;            /* 1 = one METIS_NodeND call, 0 = separator recursion */
@@ -83,6 +83,13 @@ typedef struct {
                                    solver.hpp:44-46): recursion depth, and the graph size below */
   int32_t parallel_nd_base_small; /* which a part is ordered by one METIS call, for graphs of fewer */
   int32_t parallel_nd_base_large; /* than 20,000 vertices / otherwise; 0 = the defaults 4, 4000, 20000 */
+  int32_t wide_min_front;       /* factor launches whose largest front has at least this many rows run the
+                                   wide tier, which takes fronts of any size (the register kernels stop at
+                                   64 rows); 1..65, 0 = 65.  Both give the same factors. */
+  int32_t tc_min_front;         /* precision TF32: launches whose largest front has at least this many rows
+                                   run their trailing update CB = A22 - L21 U12 on the tensor cores
+                                   (tcgen05 kind::tf32, operands split hi + lo, fp32 accumulation); 0 = 33,
+                                   or the fastest of 16, 24, 32, 48 and 64 when autotune is on */
 } cls_config;
 
 typedef struct cls_solver_s* cls_handle;
@@ -139,7 +146,12 @@ const char* cls_last_error(cls_handle h);
  * "panel_width", "panel_of", "front_ptr", "front_rows", "panel_parent",
  * "asm_ptr", "asm_idx", "asm_local", "plevel", "level_ptr", "plcols_level",
  * "front_off", "a_pos_csr", "graph_xadj", "graph_adjncy", "sym_col_ptr",
- * "sym_row_idx").  With out == NULL only *len is set. */
+ * "sym_row_idx"), or of the engine's launch plan: "factor_level_warps" and
+ * "backward_launch_warps" (the autotuner's block shapes, 0 = built-in rule),
+ * "factor_level_tiers" (per factor launch: 0 register-row kernel, 1 any-size
+ * tier, 2 any-size tier with the tensor-core trailing update) and
+ * "tc_threshold" (one value: the front size from which TF32 factors use the
+ * tensor cores, 0 for other precisions).  With out == NULL only *len is set. */
 cls_status cls_plan_array(cls_handle h, const char* name, int32_t* out, int64_t capacity, int64_t* len);
 /* Writes the per-front structure of the analysed plan to a CSV file:
  * q,p,fsz,nc,uc,level,parent,asm_len,extend_elems, the columns of the

@@ -131,13 +131,33 @@ def read_mtx(path: Path):
     return np.asarray(m).reshape(-1)
 
 
+def write_linsys(droot: Path, case: str) -> tuple[np.ndarray, np.ndarray]:
+    """linsys_<case>.npz: a reference dataset's Newton Jacobian (CSR, FP64
+    values) and mismatch vector, as its J.mtx / F.mtx hold them."""
+    J = read_mtx(droot / case / "J.mtx")
+    F = read_mtx(droot / case / "F.mtx")
+    meta = json.loads((droot / case / "metadata.json").read_text())
+    rp, ci = J.indptr.astype(np.int32), J.indices.astype(np.int32)
+    np.savez_compressed(HERE / f"linsys_{case}.npz", row_ptr=rp, col_idx=ci, values=J.data, F=F,
+                        mismatch_inf_norm=meta["mismatch_inf_norm"])
+    return rp, ci
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref-root", default=str(orc.REFERENCE_ROOT))
     ap.add_argument("--added-only", action="store_true",
                     help="only add the front-CSV, parallel-ND and panel-width hashes to the existing hashes.json "
                          "(other fixtures untouched)")
+    ap.add_argument("--linsys", nargs="*", default=None, metavar="CASE",
+                    help="only write linsys_<case>.npz for these reference datasets (other fixtures untouched)")
     args = ap.parse_args()
+    if args.linsys is not None:
+        droot = Path(args.ref_root) / "custom_linear_solver/tests/datasets/power"
+        for case in args.linsys:
+            write_linsys(droot, case)
+        print("linear-system fixtures written:", ", ".join(args.linsys))
+        return
     ref = orc.Reference()
     if args.added_only:
         hashes = json.loads((HERE / "hashes.json").read_text())
@@ -194,12 +214,7 @@ def main() -> None:
 
     droot = Path(args.ref_root) / "custom_linear_solver/tests/datasets/power"
     for case in DATASETS:
-        J = read_mtx(droot / case / "J.mtx")
-        F = read_mtx(droot / case / "F.mtx")
-        meta = json.loads((droot / case / "metadata.json").read_text())
-        rp, ci = J.indptr.astype(np.int32), J.indices.astype(np.int32)
-        np.savez_compressed(HERE / f"linsys_{case}.npz", row_ptr=rp, col_idx=ci, values=J.data, F=F,
-                            mismatch_inf_norm=meta["mismatch_inf_norm"])
+        rp, ci = write_linsys(droot, case)
         sym = ref.symbolic(rp, ci, parallel_nd=False)
         hashes[case] = {"symbolic": {k: digest(sym[k]) for k in SYMBOLIC_KEYS},
                         "front_total": int(sym["front_total"][0]), "dim": int(rp.size - 1), "nnz": int(ci.size),

@@ -233,3 +233,109 @@ def test_autotuned_factorization_is_bit_identical():
             ls.factorize(torch.tensor(vals, dtype=torch.float32, device="cuda"))
         out.append(ls.solve(torch.tensor(rhs, dtype=torch.float64, device="cuda")).cpu().numpy())
     assert np.array_equal(out[0], out[1])
+
+
+# The reference's three larger Newton Jacobians (5,890 / 12,293 / 14,908
+# unknowns).  case8387pegase has fronts of 66, 69 and 77 rows, past the
+# register kernels' 64: the any-size tier factors them.  Residual bars: an
+# unpivoted LU in the engine's ordering computed by SuperLU leaves relative
+# residuals of at most 3.3e-13 (FP64) and 1.6e-4 (FP32) on these systems.
+LARGER = ["case3120sp", "case6468rte", "case8387pegase"]
+PRECISIONS = {"FP64": (cupf.CustomPrecision.FP64, 1e-11), "FP32": (cupf.CustomPrecision.FP32, 1e-3),
+              "TF32": (cupf.CustomPrecision.TF32, 1e-3)}
+
+
+def _factor_solve(d, B, precision, rng, **cfg):
+    import torch
+
+    vals = batch_values(d, B, rng)
+    n = d["row_ptr"].size - 1
+    rhs = np.repeat(d["F"][None, :], B, axis=0) + 0.1 * rng.standard_normal((B, n))
+    ls = cupf.LinearSolver(cupf.SolverConfig(precision=int(precision), serial_nd=True, **cfg))
+    ls.set_data(d["row_ptr"], d["col_idx"])
+    ls.analyze()
+    ls.setup(B)
+    dt = torch.float64 if precision == cupf.CustomPrecision.FP64 else torch.float32
+    ls.factorize(torch.tensor(vals, dtype=dt, device="cuda"))
+    r = torch.tensor(rhs, dtype=torch.float64, device="cuda")
+    return ls, vals, rhs, ls.solve(r).cpu().numpy(), ls.solve_transpose(r).cpu().numpy()
+
+
+def _residuals(d, vals, rhs, x, xt):
+    n = d["row_ptr"].size - 1
+    out = []
+    for b in range(vals.shape[0]):
+        Ab = sp.csr_matrix((vals[b], d["col_idx"], d["row_ptr"]), shape=(n, n))
+        nb = np.linalg.norm(rhs[b])
+        out.append((np.linalg.norm(Ab @ x[b] - rhs[b]) / nb, np.linalg.norm(Ab.T @ xt[b] - rhs[b]) / nb))
+    return np.array(out)
+
+
+@pytest.mark.parametrize("case", LARGER)
+@pytest.mark.parametrize("prec", list(PRECISIONS))
+def test_larger_reference_datasets_factor_and_solve(case, prec):
+    """Factor, solve and transpose solve of the larger reference datasets in
+    every precision, 8 value sets each (+-2 % perturbations), within the
+    residual bars; the launch plan shows which kernel tier factored what
+    (any-size tier on case8387pegase; with TF32 the tensor-core tier on the
+    launches whose fronts reach 33 rows)."""
+    precision, tol = PRECISIONS[prec]
+    d, _ = load(case)
+    ls, vals, rhs, x, xt = _factor_solve(d, 8, precision, np.random.default_rng(2), autotune=False)
+    assert not ls.singular_flags().any()
+    res = _residuals(d, vals, rhs, x, xt)
+    assert res.max() <= tol, res.max(axis=0)
+    tiers = ls.plan_array("factor_level_tiers")
+    fsz = ls.plan_array("fp_fsz")
+    if prec == "TF32":
+        assert int(ls.plan_array("tc_threshold")[0]) == 33
+        assert (2 in tiers) == (fsz.max() >= 33)
+    else:
+        assert 2 not in tiers and (1 in tiers) == (fsz.max() > 64)
+
+
+@pytest.mark.parametrize("precision", [cupf.CustomPrecision.FP64, cupf.CustomPrecision.FP32])
+@pytest.mark.parametrize("case", ["case1354pegase", "case8387pegase"])
+def test_any_size_tier_gives_the_register_kernels_factors(case, precision):
+    """wide_min_front = 1 runs every launch on the any-size tier: the same
+    operations in the same order per element as the register kernels, so the
+    solutions are bit for bit those of the default plan."""
+    d, _ = load(case)
+    out = []
+    for wide in (0, 1):
+        ls, vals, rhs, x, xt = _factor_solve(d, 33, precision, np.random.default_rng(4), autotune=False,
+                                             wide_min_front=wide)
+        tiers = ls.plan_array("factor_level_tiers")
+        assert (tiers == 1).all() if wide else (0 in tiers)
+        out.append((x, xt))
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+
+
+def test_tensor_core_tier_on_every_front_size():
+    """TF32 with tc_min_front = 1: every launch of case1354pegase (fronts of
+    3 to 35 rows, 1 to 8 pivots) runs its trailing update on the tensor cores
+    (split tf32 products, fp32 accumulation); the residuals stay within the
+    FP32 bar and the solutions within 1e-4 of the FP32 factors'."""
+    d, _ = load("case1354pegase")
+    ls, vals, rhs, x, xt = _factor_solve(d, 40, cupf.CustomPrecision.TF32, np.random.default_rng(6), autotune=False,
+                                         tc_min_front=1)
+    assert (ls.plan_array("factor_level_tiers") == 2).all()
+    assert not ls.singular_flags().any()
+    res = _residuals(d, vals, rhs, x, xt)
+    assert res.max() <= 2e-4, res.max(axis=0)
+    _, _, _, x32, _ = _factor_solve(d, 40, cupf.CustomPrecision.FP32, np.random.default_rng(6), autotune=False)
+    assert np.abs(x - x32).max() <= 1e-4 * np.abs(x32).max()
+
+
+def test_tensor_core_threshold_is_autotuned():
+    """TF32 with autotune: the first factorization times the tensor-core
+    threshold (33, 49 or 65 rows) on the actual values and keeps the fastest;
+    any choice factors within the bars."""
+    d, _ = load("case8387pegase")
+    ls, vals, rhs, x, xt = _factor_solve(d, 64, cupf.CustomPrecision.TF32, np.random.default_rng(8), autotune=True)
+    t = int(ls.plan_array("tc_threshold")[0])
+    assert t in (33, 49, 65)
+    tiers, fsz = ls.plan_array("factor_level_tiers"), ls.plan_array("fp_fsz")
+    assert 2 in tiers  # case8387pegase has fronts beyond every candidate
+    res = _residuals(d, vals[:8], rhs[:8], x[:8], xt[:8])
+    assert res.max() <= 1e-3

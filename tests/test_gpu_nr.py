@@ -390,3 +390,29 @@ def test_other_plans_solve_like_the_oracle(oracle, width, serial):
     for b in (0, 7, 15):
         ref = oracle.solve(g, S[b], V0[b], tol=1e-12, max_iter=30)
         assert np.abs(r.V_numpy[b] - ref["V"]).max() <= 1e-8
+
+
+def test_tf32_factors_on_the_10000_bus_grid(oracle):
+    """CustomPrecision.TF32 in the Newton loop (Mixed state): the launches
+    whose fronts reach 33 rows (the top of the 10,000-bus grid's tree, fronts
+    up to 38 rows) run their trailing updates on the tensor cores; every
+    scenario still converges to 1e-8 and lies within 1e-8 of the oracle, the
+    Newton iteration being the refinement back to FP64 accuracy."""
+    g = G.grid_10000()
+    B = 64
+    S = g.scenarios(B, seed=29)
+    V0 = g.flat_start(B)
+    o = cupf.NewtonOptions()
+    o.backend = cupf.BackendKind.CUDA
+    o.compute = cupf.ComputePolicy.Mixed
+    o.custom.precision = cupf.CustomPrecision.TF32
+    o.custom.serial_nd = True
+    o.custom.autotune = False
+    o.use_cuda_graph = True
+    s = cupf.NewtonSolver(o)
+    s.initialize(g.indptr, g.indices, g.data, g.n_bus, g.n_bus, g.pv, g.pq)
+    assert 2 in s.plan_array("factor_level_tiers")
+    r = solve(s, g, S, V0, cfg())
+    assert r.converged_numpy.all()
+    dv = max_dv_vs_oracle(oracle, g, S, V0, r.V_numpy)
+    assert dv.max() <= 1e-8, float(dv.max())
