@@ -237,12 +237,32 @@ def test_autotuned_factorization_is_bit_identical():
 
 # The reference's three larger Newton Jacobians (5,890 / 12,293 / 14,908
 # unknowns).  case8387pegase has fronts of 66, 69 and 77 rows, past the
-# register kernels' 64: the any-size tier factors them.  Residual bars: an
-# unpivoted LU in the engine's ordering computed by SuperLU leaves relative
-# residuals of at most 3.3e-13 (FP64) and 1.6e-4 (FP32) on these systems.
+# register kernels' 64: the any-size tier factors them.  Residual bars: FP64
+# 1e-11 (an unpivoted LU in the engine's ordering, computed by SuperLU, leaves
+# at most 3.3e-13 on these systems); FP32 and TF32 factors: at most 4x the
+# residual of SuperLU's FP32 unpivoted LU of the same system in the same
+# ordering (floor 1e-5).  The +-2 % perturbed value sets reach 3.2e-3 there:
+# that is what FP32 factors without pivoting can do on them, whatever the
+# kernel.
 LARGER = ["case3120sp", "case6468rte", "case8387pegase"]
-PRECISIONS = {"FP64": (cupf.CustomPrecision.FP64, 1e-11), "FP32": (cupf.CustomPrecision.FP32, 1e-3),
-              "TF32": (cupf.CustomPrecision.TF32, 1e-3)}
+PRECISIONS = {"FP64": (cupf.CustomPrecision.FP64, 1e-11), "FP32": (cupf.CustomPrecision.FP32, None),
+              "TF32": (cupf.CustomPrecision.TF32, None)}
+
+
+def _fp32_lu_residuals(d, perm, vals, rhs):
+    """Relative residual of SuperLU's FP32 LU without pivoting, in the
+    engine's ordering, per value set: the accuracy FP32 factors can reach."""
+    n = d["row_ptr"].size - 1
+    out = []
+    for b in range(vals.shape[0]):
+        A = sp.csr_matrix((vals[b], d["col_idx"], d["row_ptr"]), shape=(n, n))
+        Ap = sp.csc_matrix(A[perm][:, perm])
+        lu = spla.splu(Ap.astype(np.float32), permc_spec="NATURAL", diag_pivot_thresh=0.0,
+                       options={"SymmetricMode": True})
+        x = np.empty(n)
+        x[perm] = lu.solve(rhs[b][perm].astype(np.float32)).astype(np.float64)
+        out.append(np.linalg.norm(A @ x - rhs[b]) / np.linalg.norm(rhs[b]))
+    return np.array(out)
 
 
 def _factor_solve(d, B, precision, rng, **cfg):
@@ -284,7 +304,11 @@ def test_larger_reference_datasets_factor_and_solve(case, prec):
     ls, vals, rhs, x, xt = _factor_solve(d, 8, precision, np.random.default_rng(2), autotune=False)
     assert not ls.singular_flags().any()
     res = _residuals(d, vals, rhs, x, xt)
-    assert res.max() <= tol, res.max(axis=0)
+    if tol is None:
+        bar = np.maximum(4.0 * _fp32_lu_residuals(d, ls.plan_array("perm"), vals, rhs), 1e-5)
+        assert (res[:, 0] <= bar).all() and (res[:, 1] <= 4 * bar).all(), (res, bar)
+    else:
+        assert res.max() <= tol, res.max(axis=0)
     tiers = ls.plan_array("factor_level_tiers")
     fsz = ls.plan_array("fp_fsz")
     if prec == "TF32":
@@ -315,14 +339,16 @@ def test_tensor_core_tier_on_every_front_size():
     """TF32 with tc_min_front = 1: every launch of case1354pegase (fronts of
     3 to 35 rows, 1 to 8 pivots) runs its trailing update on the tensor cores
     (split tf32 products, fp32 accumulation); the residuals stay within the
-    FP32 bar and the solutions within 1e-4 of the FP32 factors'."""
+    FP32 bar (4x SuperLU's unpivoted FP32 LU) and the solutions within 1e-4
+    of the FP32 factors'."""
     d, _ = load("case1354pegase")
     ls, vals, rhs, x, xt = _factor_solve(d, 40, cupf.CustomPrecision.TF32, np.random.default_rng(6), autotune=False,
                                          tc_min_front=1)
     assert (ls.plan_array("factor_level_tiers") == 2).all()
     assert not ls.singular_flags().any()
     res = _residuals(d, vals, rhs, x, xt)
-    assert res.max() <= 2e-4, res.max(axis=0)
+    bar = np.maximum(4.0 * _fp32_lu_residuals(d, ls.plan_array("perm"), vals, rhs), 1e-5)
+    assert (res[:, 0] <= bar).all() and (res[:, 1] <= 4 * bar).all(), (res, bar)
     _, _, _, x32, _ = _factor_solve(d, 40, cupf.CustomPrecision.FP32, np.random.default_rng(6), autotune=False)
     assert np.abs(x - x32).max() <= 1e-4 * np.abs(x32).max()
 
@@ -338,4 +364,5 @@ def test_tensor_core_threshold_is_autotuned():
     tiers, fsz = ls.plan_array("factor_level_tiers"), ls.plan_array("fp_fsz")
     assert 2 in tiers  # case8387pegase has fronts beyond every candidate
     res = _residuals(d, vals[:8], rhs[:8], x[:8], xt[:8])
-    assert res.max() <= 1e-3
+    bar = np.maximum(4.0 * _fp32_lu_residuals(d, ls.plan_array("perm"), vals[:8], rhs[:8]), 1e-5)
+    assert (res[:, 0] <= bar).all() and (res[:, 1] <= 4 * bar).all(), (res, bar)
