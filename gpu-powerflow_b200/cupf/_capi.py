@@ -73,6 +73,7 @@ MLP_EXPORTS = [
     "mlp_last_error", "mlp_gemm_bf16", "mlp_error_flag", "mlp_set_wait_test", "mlp_transpose_bf16", "mlp_standardize",
     "mlp_mse_grad",
     "mlp_col_sum_bf16", "mlp_adam", "mlp_load_features", "mlp_gemm_bf16_split",
+    "mlp_gram_f64", "mlp_cholesky_solve_f64", "mlp_refit_last_error",
 ]
 
 _vp = C.c_void_p
@@ -139,6 +140,9 @@ def _declare(lib: C.CDLL) -> None:
         "mlp_gemm_bf16_split": ([_vp, _i64, _vp, _i64, _i32, _i32, _i32, _i32, _vp, _i64, _vp, _vp], _i32),
         "mlp_error_flag": ([_p(_i32), _i32], _i32),
         "mlp_set_wait_test": ([C.c_longlong, _i32], _i32),
+        "mlp_gram_f64": ([_vp, _i64, _i32, _vp, _i64, _i32, _i32, _i32, _i32, _vp, _i64, _vp, _i64, _vp], _i32),
+        "mlp_cholesky_solve_f64": ([_vp, _i64, _i32, _vp, _i64, _i32, C.c_double, _vp, _vp], _i32),
+        "mlp_refit_last_error": ([], C.c_char_p),
         "mlp_transpose_bf16": ([_vp, _i64, _vp, _i32, _i32, _vp], _i32),
         "mlp_standardize": ([_vp, _vp, _vp, _vp, _i64, _i32, _i32, _i32, _vp], _i32),
         "mlp_load_features": ([_vp, _i64, _vp, _vp, _i32, _i32, _vp, _vp, _vp, _i64, _i32, _i32, _i32, _vp], _i32),

@@ -405,12 +405,13 @@ class WarmStart:
 
         The hidden layers (the project's kernels, bf16) map every training
         row to the output layer's input a = [a_L | x]; the output layer is
-        then the ridge solution of min ||[a 1] [W^T; b] - Y_std||^2, with the
-        normal equations accumulated and solved in FP64 by torch (a plain
-        library GEMM and solve, ridge = ridge x the mean diagonal).  Adam's
-        stochastic steps leave independent per-output noise in W that the
-        exact minimiser does not have; set_output_layer installs the result
-        as split weights for inference."""
+        then the ridge solution of min ||[a 1] [W^T; b] - Y_std||^2.  The
+        normal equations are accumulated in FP64 by the project's Gram
+        kernel chunk by chunk (mlp_gram_f64) and solved by its blocked
+        Cholesky (mlp_cholesky_solve_f64), ridge = ridge x the mean diagonal.
+        Adam's stochastic steps leave independent per-output noise in W that
+        the exact minimiser does not have; set_output_layer installs the
+        result as split weights for inference."""
         t = self.torch
         mlp = self.mlp
         if self.y_mean is None:
@@ -418,10 +419,13 @@ class WarmStart:
         L = mlp.layers
         h = mlp.buffers(chunk)
         n = X.shape[0]
-        D = mlp.dims_in[L] + 1
-        f64 = t.float64
-        AtA = t.zeros(D, D, dtype=f64, device=self.dev)
-        AtY = t.zeros(D, self.n_out, dtype=f64, device=self.dev)
+        p = mlp.dims_in[L]
+        D = p + 1
+        q = self.n_out
+        AtA = t.zeros(D, D, dtype=t.float64, device=self.dev)
+        AtY = t.zeros(D, q, dtype=t.float64, device=self.dev)
+        stream = mlp._stream()
+        lib = mlp.lib
         for c0 in range(0, n, chunk):
             m = min(chunk, n - c0)
             xb = X[c0:c0 + m]
@@ -429,14 +433,23 @@ class WarmStart:
                 xb = t.cat([xb, xb[-1:].expand(chunk - m, -1)])
             mlp.standardize(h, xb.contiguous(), self.x_mean, self.x_istd)
             mlp.hidden_layers(h, keep_pre=False)
-            A = t.cat([mlp._layer_input(h, L)[:m].to(f64), t.ones(m, 1, dtype=f64, device=self.dev)], dim=1)
-            AtA.addmm_(A.T, A)
-            AtY.addmm_(A.T, ((Y[c0:c0 + m] - self.y_mean) / self.y_std).to(f64))
+            A = mlp._layer_input(h, L)
+            Ys = ((Y[c0:c0 + m] - self.y_mean) / self.y_std).float().contiguous()
+            rc = lib.mlp_gram_f64(_ptr(A), A.stride(0), 0, _ptr(Ys), Ys.stride(0), 0, m, p, q, _ptr(AtA),
+                                  AtA.stride(0), _ptr(AtY), AtY.stride(0), stream)
+            if rc:
+                raise RuntimeError("refit_output: " + lib.mlp_refit_last_error().decode())
         if mlp.error_flag():
             raise RuntimeError("warm-start GEMM reported a wait timeout")
-        d = AtA.diagonal()
-        AtA.diagonal().add_(ridge * float(d[d > 0].mean()))
-        sol = t.linalg.solve(AtA, AtY)
+        info = t.zeros(1, dtype=t.int32, device=self.dev)
+        rc = lib.mlp_cholesky_solve_f64(_ptr(AtA), AtA.stride(0), D, _ptr(AtY), AtY.stride(0), q, ridge, _ptr(info),
+                                        stream)
+        if rc:
+            raise RuntimeError("refit_output: " + lib.mlp_refit_last_error().decode())
+        if int(info.item()) != 0:
+            raise RuntimeError(f"refit_output: the normal equations are not positive definite "
+                               f"(pivot {int(info.item()) - 1})")
+        sol = AtY
         if not bool(t.isfinite(sol).all()):
             raise RuntimeError("refit_output: the least-squares solve is not finite")
         mlp.set_output_layer(sol[:-1].T.float(), sol[-1].float())

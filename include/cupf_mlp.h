@@ -46,6 +46,27 @@ int mlp_error_flag(int* out_host, int reset);
  * error flag (1), writes NaN into its output tiles, frees its tensor memory
  * and returns.  Nothing faults or hangs; set (4194304, 0) to restore. */
 int mlp_set_wait_test(long long spin_limit, int stall_loads);
+/* Least-squares output layer of the warm start, in FP64 on the CUDA cores
+ * (refit_kernels.cu).  These report their own errors through
+ * mlp_refit_last_error (same return codes).
+ *
+ * Normal equations of [A | 1] (n rows; the ones column is the bias), added
+ * to what AtA and AtY hold:  AtA[(p+1)][(p+1)] += [A|1]^T [A|1] (upper
+ * triangle only, i <= j), AtY[(p+1)][q] += [A|1]^T Y (AtY may be NULL).
+ * A [n][lda] is bf16 (a_type 0) or fp32 (1); Y [n][ldy] fp32 (y_type 0) or
+ * fp64 (1).  Asynchronous on `stream`. */
+int mlp_gram_f64(const void* A, long long lda, int a_type, const void* Y, long long ldy, int y_type, int n, int p,
+                 int q, double* AtA, long long ld_ata, double* AtY, long long ld_aty, void* stream);
+/* Solves (M + ridge) X = R in place for symmetric positive definite M
+ * [D][ldm] given by its upper triangle: ridge = ridge_rel x the mean of the
+ * positive diagonal entries, added to the diagonal; blocked Cholesky
+ * M = U^T U (U overwrites the upper triangle, 64-column panels), then
+ * U^T Y = R and U X = Y with R [D][ldr] (q columns) overwritten by X.
+ * d_info (device int) is set to the first non-positive pivot's index + 1
+ * (0: none).  Asynchronous on `stream`. */
+int mlp_cholesky_solve_f64(double* M, long long ldm, int D, double* R, long long ldr, int q, double ridge_rel,
+                           int* d_info, void* stream);
+const char* mlp_refit_last_error(void);
 /* out[cols][rows] = in[rows][cols] (bf16; in has row stride ld). */
 int mlp_transpose_bf16(const void* in, long long ld, void* out, int rows, int cols, void* stream);
 /* x[b][k] = bf16((raw[b][k] - mean[k]) * inv_std[k]) for k < n_in, 0 for

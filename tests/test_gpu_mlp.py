@@ -337,10 +337,69 @@ def test_split_gemm_carries_the_fp32_weights(torch, M, N, K):
     assert rc != 0 and b"fp32 epilogues" in net.lib.mlp_last_error()
 
 
+@pytest.mark.parametrize("a_type", [0, 1])
+def test_gram_kernel_matches_numpy(torch, a_type):
+    """mlp_gram_f64: [A|1]^T [A|1] (upper triangle) and [A|1]^T Y accumulated
+    in FP64 from bf16 (or fp32) A and fp32 Y, sizes off the 128 tiles, added
+    to what the outputs hold; against numpy in FP64 on the same values."""
+    from cupf import _capi
+
+    lib = _capi.load()
+    rng = np.random.default_rng(21)
+    n, p, q = 1000, 300, 77
+    dt = torch.bfloat16 if a_type == 0 else torch.float32
+    A = torch.tensor(rng.standard_normal((n, p + 5)), dtype=torch.float32, device="cuda").to(dt)
+    Y = torch.tensor(rng.standard_normal((n, q)), dtype=torch.float32, device="cuda")
+    AtA = torch.full((p + 1, p + 1), 2.0, dtype=torch.float64, device="cuda")
+    AtY = torch.full((p + 1, q), -1.0, dtype=torch.float64, device="cuda")
+    ptr = lambda t: t.data_ptr()  # noqa: E731
+    assert lib.mlp_gram_f64(ptr(A), A.stride(0), a_type, ptr(Y), Y.stride(0), 0, n, p, q, ptr(AtA), AtA.stride(0),
+                            ptr(AtY), AtY.stride(0), None) == 0
+    Ah = np.hstack([A[:, :p].double().cpu().numpy(), np.ones((n, 1))])
+    ref = Ah.T @ Ah + 2.0
+    got = AtA.cpu().numpy()
+    iu = np.triu_indices(p + 1)
+    assert np.abs(got[iu] - ref[iu]).max() <= 1e-12 * np.abs(ref).max()
+    assert (got[np.tril_indices(p + 1, -1)] == 2.0).all()  # the lower triangle is left alone
+    refy = Ah.T @ Y.double().cpu().numpy() - 1.0
+    assert np.abs(AtY.cpu().numpy() - refy).max() <= 1e-12 * np.abs(refy).max()
+
+
+@pytest.mark.parametrize("D,q", [(300, 77), (64, 1), (129, 200)])
+def test_cholesky_solve_matches_numpy(torch, D, q):
+    """mlp_cholesky_solve_f64: (M + ridge) X = R for an SPD M given by its
+    upper triangle (64-column panels, a ragged last panel), against numpy;
+    a matrix that is not positive definite reports its pivot."""
+    from cupf import _capi
+
+    lib = _capi.load()
+    rng = np.random.default_rng(D + q)
+    G = rng.standard_normal((D + 20, D))
+    M = G.T @ G
+    R = rng.standard_normal((D, q))
+    Md = torch.tensor(np.triu(M) + np.tril(np.full((D, D), 7.0), -1), dtype=torch.float64, device="cuda")
+    Rd = torch.tensor(R, dtype=torch.float64, device="cuda")
+    info = torch.zeros(1, dtype=torch.int32, device="cuda")
+    ridge = 1e-6
+    assert lib.mlp_cholesky_solve_f64(Md.data_ptr(), Md.stride(0), D, Rd.data_ptr(), Rd.stride(0), q, ridge,
+                                      info.data_ptr(), None) == 0
+    assert int(info.item()) == 0
+    d = np.diag(M)
+    Mr = M + np.eye(D) * ridge * d[d > 0].mean()
+    X = np.linalg.solve(Mr, R)
+    assert np.abs(Rd.cpu().numpy() - X).max() <= 1e-9 * np.abs(X).max()
+    bad = torch.tensor(np.triu(M) - np.eye(D) * (2 * np.abs(M).sum()), dtype=torch.float64, device="cuda")
+    Rd = torch.tensor(R, dtype=torch.float64, device="cuda")
+    assert lib.mlp_cholesky_solve_f64(bad.data_ptr(), bad.stride(0), D, Rd.data_ptr(), Rd.stride(0), q, 0.0,
+                                      info.data_ptr(), None) == 0
+    assert int(info.item()) == 1  # the first pivot is already negative
+
+
 def test_refit_output_solves_the_least_squares_problem(torch):
     """refit_output: the output layer equals the FP64 ridge solution on the
-    hidden features the network's own kernels compute, lowers the training
-    error, and inference evaluates it through the split weights."""
+    hidden features the network's own kernels compute (the project's Gram
+    and Cholesky kernels against numpy), lowers the training error, and
+    inference evaluates it through the split weights."""
     import cupf
     from cupf import grids as G
     from cupf.warm_start import WarmStart
