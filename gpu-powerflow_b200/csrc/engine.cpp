@@ -745,6 +745,11 @@ bool choose_block_shapes(size_t n, Set set, Launch launch, cudaStream_t s, const
   const bool keep = whole[1] < 0.99 * whole[0];
   for (size_t i = 0; i < n; ++i) set(i, keep ? choice[i] : 0);
   if (debug_sync())
+    for (size_t i = 0; i < n; ++i)
+      std::fprintf(stderr, "[cupf] %s launch %zu: rule %.2f us, 1/2/4/8 warps %.2f %.2f %.2f %.2f us, chosen %d\n",
+                   what, i, 1e3 * t[4 * n + i], 1e3 * t[i], 1e3 * t[n + i], 1e3 * t[2 * n + i], 1e3 * t[3 * n + i],
+                   choice[i]);
+  if (debug_sync())
     std::fprintf(stderr, "[cupf] %s autotune: rule %.3f ms, choice %.3f ms, %s\n", what, whole[0], whole[1],
                  keep ? "kept" : "rule kept");
   return keep;

@@ -454,6 +454,45 @@ class WarmStart:
             raise RuntimeError("refit_output: the least-squares solve is not finite")
         mlp.set_output_layer(sol[:-1].T.float(), sol[-1].float())
 
+    # -- checkpoints --
+    def save(self, path) -> None:
+        """Write the trained predictor to an .npz file: the network's FP32
+        weights and biases, the input and output standardization, the
+        unwrapping reference and the grid's shape (checked on load).  The bf16
+        copies, transposes and split output weights are rebuilt on load."""
+        if self.y_mean is None:
+            raise RuntimeError("WarmStart.save: fit the network first")
+        m = self.mlp
+        arrays = {f"W{i}": m.W[i].cpu().numpy() for i in range(m.layers + 1)}
+        arrays.update({f"b{i}": m.b[i].cpu().numpy() for i in range(m.layers + 1)})
+        for k in ("x_mean", "x_istd", "y_mean", "y_std", "va_ref"):
+            arrays[k] = getattr(self, k).cpu().numpy()
+        arrays["vref"] = self.vref.cpu().numpy()
+        arrays["shape"] = np.array([self.g.n_bus, self.g.pv.size, self.g.pq.size, self.n_in, self.n_out, m.hidden,
+                                    m.layers, int(m.skip)], dtype=np.int64)
+        np.savez(path, **arrays)
+
+    def load(self, path) -> None:
+        """Restore a predictor written by save() for this grid and network
+        shape (ValueError when they differ); ready for predict/solve."""
+        t = self.torch
+        d = np.load(path)
+        m = self.mlp
+        want = np.array([self.g.n_bus, self.g.pv.size, self.g.pq.size, self.n_in, self.n_out, m.hidden, m.layers,
+                         int(m.skip)], dtype=np.int64)
+        if not np.array_equal(d["shape"], want):
+            raise ValueError(f"WarmStart.load: checkpoint shape {d['shape'].tolist()} does not match "
+                             f"this grid and network {want.tolist()}")
+        for i in range(m.layers + 1):
+            m.W[i].copy_(t.from_numpy(d[f"W{i}"]))
+            m.b[i].copy_(t.from_numpy(d[f"b{i}"]))
+            m.W16[i].copy_(m.W[i].to(t.bfloat16))
+        m._refresh_transposes()
+        m._build_split()
+        for k in ("x_mean", "x_istd", "y_mean", "y_std", "va_ref"):
+            setattr(self, k, t.from_numpy(d[k]).to(self.dev))
+        self.vref = t.from_numpy(d["vref"]).to(self.dev)
+
     # -- inference --
     def predict_standardized(self, sbus, slot: int = 0):
         """Network output fp32 [B rounded up to 128, no], still standardized

@@ -31,7 +31,7 @@ _f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 
 def build(ref: bool = True) -> None:
     """Compile liboracle.so (and oracle/_ref when the reference sources exist)."""
-    targets = ["oracle"] + (["ref"] if ref else [])
+    targets = ["oracle"] + (["ref", "refgpu"] if ref else [])
     subprocess.run(["make", "-s", "-C", str(HERE), "-j8", *targets], check=True)
 
 

@@ -544,3 +544,36 @@ def test_host_pipeline_hands_failures_to_the_caller(torch):
     # and a clean run after both
     HostPipeline(lambda sd: (sd * 4, sd.real[:, 0].clone())).run(ins, V_out, fm_out)
     assert all(torch.equal(V_out[i], ins[i] * 4) for i in range(5))
+
+
+def test_warm_start_checkpoint_round_trip(torch, tmp_path):
+    """WarmStart.save / load: a predictor restored into a freshly built one
+    (different initial weights) predicts bit for bit what the trained one
+    does; a checkpoint of another network shape is refused."""
+    import cupf
+    from cupf import grids as G
+    from cupf.warm_start import WarmStart
+
+    g = G.grid_118()
+    o = cupf.NewtonOptions()
+    o.backend = cupf.BackendKind.CUDA
+    o.custom.serial_nd = True
+    s = cupf.NewtonSolver(o)
+    s.initialize(g.indptr, g.indices, g.data, g.n_bus, g.n_bus, g.pv, g.pq)
+    ws = WarmStart(g, hidden=128, layers=2, seed=0)
+    X, Y, _ = ws.generate(s, 2048, seed=3)
+    ws.fit(X, Y, epochs=3, batch=512, lr=2e-3)
+    path = tmp_path / "warm118.npz"
+    ws.save(path)
+    S = torch.tensor(g.scenarios(256, seed=12), device="cuda")
+    ref = ws.predict(S).clone()
+    fresh = WarmStart(g, hidden=128, layers=2, seed=5)
+    fresh.load(path)
+    assert torch.equal(fresh.predict(S), ref)
+    cfg = cupf.NRConfig(tolerance=1e-8, max_iter=10)
+    Va, fa, ia, _ = ws.solve(s, S, cfg)
+    Vb, fb, ib, _ = fresh.solve(s, S, cfg)
+    assert ia == ib and torch.equal(Va, Vb)
+    other = WarmStart(g, hidden=256, layers=2, seed=0)
+    with pytest.raises(ValueError):
+        other.load(path)
