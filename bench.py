@@ -426,34 +426,52 @@ def run_engine(args) -> None:
     # the L2 flush runs inside each step, before its solve.
     from cupf.streaming import HostPipeline
 
+    # two solve lanes: a second engine handle, so two batches solve at once
+    # on their own streams (one batch's latency-bound phases overlap the
+    # other's wide ones); primed like the first before any timing
+    mixed2 = make_solver(g, cupf.ComputePolicy.Mixed, graph=not args.no_graph)
+    step_flat(mixed2)
     if ws:
-        # the network of step k+1 runs on its own stream during step k's solve
-        def pipe_prepare(s_dev, slot):
-            return ws.predict_standardized(s_dev, slot=slot)
+        ws.solve(mixed2, sbus, cfg)
+    torch.cuda.synchronize(dev)
 
-        def pipe_solve(s_dev, pred):
-            flush.fill_(1.0)
-            v, fm, _, _ = ws.solve(mixed, s_dev, cfg, pred=pred)
-            return v, fm
-        pipe = HostPipeline(pipe_solve, dev, prepare=pipe_prepare)
-    else:
+    def make_pipe(lanes):
+        if ws:
+            # the network of a step runs on its own stream ahead of the step's solve
+            def pipe_prepare(s_dev, slot):
+                return ws.predict_standardized(s_dev, slot=slot)
+
+            def lane(sv):
+                def pipe_solve(s_dev, pred):
+                    flush.fill_(1.0)
+                    v, fm, _, _ = ws.solve(sv, s_dev, cfg, pred=pred)
+                    return v, fm
+                return pipe_solve
+            return HostPipeline([lane(sv) for sv in lanes], dev, prepare=pipe_prepare)
         v0_dev = v0
 
-        def pipe_solve(s_dev):
-            flush.fill_(1.0)
-            v, fm, _ = mixed.solve_batch_device(s_dev, v0_dev, config=cfg)
-            return v, fm
-        pipe = HostPipeline(pipe_solve, dev)
-    v_bufs = [torch.empty(B, g.n_bus, dtype=torch.complex128).pin_memory() for _ in range(2)]
+        def lane(sv):
+            def pipe_solve(s_dev):
+                flush.fill_(1.0)
+                v, fm, _ = sv.solve_batch_device(s_dev, v0_dev, config=cfg)
+                return v, fm
+            return pipe_solve
+        return HostPipeline([lane(sv) for sv in lanes], dev)
+
+    v_bufs = [torch.empty(B, g.n_bus, dtype=torch.complex128).pin_memory() for _ in range(4)]
     fm_bufs = [torch.empty(B, dtype=torch.float64).pin_memory() for _ in range(max(args.steps, args.warmup))]
-    pipe.run([sbus_p] * args.warmup, [v_bufs[k % 2] for k in range(args.warmup)], fm_bufs[: args.warmup])
-    _barrier(world)
-    torch.cuda.synchronize(dev)
-    t0 = time.perf_counter()
-    pipe.run([sbus_p] * args.steps, [v_bufs[k % 2] for k in range(args.steps)], fm_bufs[: args.steps])
-    ms_e2e = _reduce((time.perf_counter() - t0) * 1e3 / args.steps, "max", world, dev)
-    conv_pipe = sum(int((f <= TOL).sum()) for f in fm_bufs[: args.steps])
-    e2e_value = _reduce(conv_pipe / args.steps, "sum", world, dev) / (ms_e2e / 1e3)
+    e2e_lanes = {}
+    for nl, lanes in ((1, [mixed]), (2, [mixed, mixed2])):
+        pipe = make_pipe(lanes)
+        pipe.run([sbus_p] * args.warmup, [v_bufs[k % 4] for k in range(args.warmup)], fm_bufs[: args.warmup])
+        _barrier(world)
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        pipe.run([sbus_p] * args.steps, [v_bufs[k % 4] for k in range(args.steps)], fm_bufs[: args.steps])
+        ms_l = _reduce((time.perf_counter() - t0) * 1e3 / args.steps, "max", world, dev)
+        conv_l = sum(int((f <= TOL).sum()) for f in fm_bufs[: args.steps])
+        e2e_lanes[nl] = (ms_l, _reduce(conv_l / args.steps, "sum", world, dev) / (ms_l / 1e3))
+    ms_e2e, e2e_value = e2e_lanes[2]
 
     # the warm start on 4,096 held-out scenarios from its training distribution
     # (per-bus U(0.7, 1.3), a seed the training draws do not use): warm against
@@ -537,9 +555,12 @@ def run_engine(args) -> None:
             "warm_start_heldout": heldout,
             "e2e": {"value": round(e2e_value, 1), "unit": UNIT, "h2d_bytes_per_step": B * g.n_bus * 16,
                     "d2h_bytes_per_step": B * g.n_bus * 16 + B * 8, "ms_per_step": round(ms_e2e, 4),
-                    "method": "cupf.streaming.HostPipeline over pinned host batches: each step uploads its "
-                              "Sbus and downloads its V and final norms; step k+1's upload and network "
-                              "inference and step k-1's download overlap step k's solve",
+                    "method": "cupf.streaming.HostPipeline over pinned host batches with two solve lanes (two "
+                              "engine handles, streams and worker threads; batches round-robin): each step "
+                              "uploads its Sbus and downloads its V and final norms; uploads, network "
+                              "inference and downloads overlap the solves, and two solves run at once",
+                    "one_lane": {"value": round(e2e_lanes[1][1], 1), "ms_per_step": round(e2e_lanes[1][0], 4),
+                                 "method": "the same pipeline with one solve lane"},
                     "serial": {"value": round(e2e_serial_value, 1), "ms_per_step": round(ms_e2e_serial, 4),
                                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                                "method": "upload, solve, download one after the other"}},
@@ -576,17 +597,20 @@ def run_extras(args, dev) -> dict:
     # engine and CUDA stream per grid, solved concurrently (mixed, flat start)
     inst = grids.uneven_grids()
     ub = UnevenBatch([g for g, _ in inst])
+    ub_flat = UnevenBatch([g for g, _ in inst], prioritize=False)
     S = [torch.tensor(g.scenarios(c, seed=600 + i), device=dev) for i, (g, c) in enumerate(inst)]
     V0 = [torch.tensor(g.flat_start(c), device=dev) for g, c in inst]
     for _ in range(2):
         ub.solve(S, V0, cfg)
+        ub_flat.solve(S, V0, cfg)
     res = {}
-    for mode, conc in (("concurrent", True), ("sequential", False)):
+    for mode, u, conc in (("concurrent", ub, True), ("concurrent_equal_priority", ub_flat, True),
+                          ("sequential", ub, False)):
         ts, conv = [], 0
         for _ in range(3):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
-            r = ub.solve(S, V0, cfg, concurrent=conc)
+            r = u.solve(S, V0, cfg, concurrent=conc)
             e1.record()
             e1.synchronize()
             ts.append(e0.elapsed_time(e1))
@@ -595,7 +619,8 @@ def run_extras(args, dev) -> dict:
                      "value": round(conv / (statistics.mean(ts) / 1e3), 1)}
     out["uneven_batch"] = {"instances": sum(c for _, c in inst),
                            "grids": [[g.n_bus, c] for g, c in inst], "unit": UNIT,
-                           "method": "one engine + CUDA stream per grid, host thread per grid", **res}
+                           "method": "one engine + CUDA stream per grid, host thread per grid; streams prioritized "
+                                     "by grid size (largest first) unless stated", **res}
     # differentiable large case: 10,000 buses x 64, mixed forward through the
     # torch autograd wrapper, loss = sum (Vm - 1)^2, backward = adjoint J^T solve
     g = grids.grid_10000()

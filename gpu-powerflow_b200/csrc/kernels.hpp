@@ -83,9 +83,26 @@ inline FrontSmem plan_front_smem(const LevelLaunch& lv, size_t elem_bytes, bool 
   return sm;
 }
 
-// True when a level's dense fronts fit in shared memory next to the staging.
-inline bool front_fits_smem(const LevelLaunch& lv, size_t elem_bytes) {
-  return plan_front_smem(lv, elem_bytes, true).total() <= kSmemLimit;
+// Round trips to memory a launch's blocks spend staging their source rows.
+inline int staging_round_trips(const LevelLaunch& lv, const FrontSmem& sm) {
+  const int n = lv.max_src > 0 ? lv.max_src : 1;
+  return (n + sm.chunk - 1) / sm.chunk;
+}
+
+// Where a register-kernel launch keeps its dense fronts.  In shared memory
+// when the front and all its staged source rows fit.  A large front leaves
+// room only for small double-buffered chunks of the source rows, and each
+// chunk is one more dependent memory round trip before the front is
+// assembled; with the front in the global scratch (L2-resident) the whole
+// list is staged in one round trip, at the price of reading the front from
+// L2 during the elimination.  The front moves to the scratch when that
+// saves more than two staging round trips.
+inline bool front_in_shared_memory(const LevelLaunch& lv, size_t elem_bytes) {
+  const FrontSmem a = plan_front_smem(lv, elem_bytes, true);
+  if (a.total() > kSmemLimit) return false;
+  const FrontSmem b = plan_front_smem(lv, elem_bytes, false);
+  if (b.total() > kSmemLimit) return true;
+  return !(staging_round_trips(lv, b) + 2 < staging_round_trips(lv, a));
 }
 
 // Launches whose fronts have at least this many rows always run a wide tier
@@ -98,11 +115,13 @@ constexpr int kWideFrontRows = 65;
 // otherwise; the autotuner tries this, 49 and 65.
 constexpr int kTcDefaultMinFront = 33;
 
-// Shared-memory plan of a wide-tier launch: pivot reciprocals, two chunks of
-// staged source rows (the source list itself is read from global memory, it
-// can be thousands of entries long), and the pivot rows Us when they fit;
-// the dense front is in the global scratch.
-inline FrontSmem plan_wide_smem(const LevelLaunch& lv, size_t elem_bytes) {
+// Shared-memory plan of a wide-tier launch: pivot reciprocals, the staged
+// source rows, and `reserve` bytes after them for the kernel's other arrays
+// (the source list itself is read from global memory: it can be thousands of
+// entries long; the dense front is in the global scratch).  The whole list is
+// staged at once when it fits, else two alternating chunks as large as fit
+// (multiples of 32 rows, at least 32); 0 chunk rows when even that fails.
+inline FrontSmem plan_wide_staging(const LevelLaunch& lv, size_t elem_bytes, size_t reserve) {
   FrontSmem sm;
   const size_t row = 32 * elem_bytes;
   sm.idx_cap = 0;
@@ -110,11 +129,30 @@ inline FrontSmem plan_wide_smem(const LevelLaunch& lv, size_t elem_bytes) {
   sm.inv_bytes = 8 * row;
   sm.front_bytes = 0;
   const int nsrc = lv.max_src > 0 ? lv.max_src : 1;
-  sm.chunk = nsrc <= 64 ? nsrc : 64;
-  sm.nbuf = nsrc <= 64 ? 1 : 2;
+  const size_t avail = kSmemLimit > sm.inv_bytes + reserve ? kSmemLimit - sm.inv_bytes - reserve : 0;
+  if ((size_t)nsrc * row <= avail) {
+    sm.chunk = nsrc;
+    sm.nbuf = 1;
+  } else {
+    sm.chunk = (int)(avail / (2 * row)) / 32 * 32;
+    sm.nbuf = 2;
+  }
   sm.stage_bytes = (size_t)sm.nbuf * sm.chunk * row;
-  sm.us_bytes = (size_t)lv.max_nc * (lv.max_fsz + 1) * row;
-  if (sm.total() > kSmemLimit) sm.us_bytes = 0;
+  return sm;
+}
+
+// The any-size tier's plan: the pivot rows Us [nc][fs + 1][32] in shared
+// memory when at least 32-row staging chunks fit beside them, else in the
+// scratch after the front.
+inline FrontSmem plan_wide_smem(const LevelLaunch& lv, size_t elem_bytes) {
+  const size_t us = (size_t)lv.max_nc * (lv.max_fsz + 1) * 32 * elem_bytes;
+  FrontSmem sm = plan_wide_staging(lv, elem_bytes, us);
+  if (sm.chunk >= 32 || sm.nbuf == 1) {
+    sm.us_bytes = us;
+    return sm;
+  }
+  sm = plan_wide_staging(lv, elem_bytes, 0);
+  sm.us_bytes = 0;
   return sm;
 }
 
@@ -131,7 +169,7 @@ inline size_t wide_block_elems(const LevelLaunch& lv, size_t elem_bytes) {
 // in shared memory.
 inline size_t level_scratch_elems(const LevelLaunch& lv, size_t elem_bytes, int groups) {
   if (lv.tier > 0) return wide_block_elems(lv, elem_bytes) * lv.count * groups;
-  if (front_fits_smem(lv, elem_bytes)) return 0;
+  if (front_in_shared_memory(lv, elem_bytes)) return 0;
   return (size_t)lv.max_fsz * (lv.max_fsz + 1) * lv.count * groups;
 }
 

@@ -578,6 +578,14 @@ struct TcLayout {
 
 inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
+// Bytes the tensor-core tier needs beside the staging (rounding included).
+inline size_t tc_reserve_bytes(const LevelLaunch& lv) {
+  const int rw = lv.max_fsz + 1, max_uc = lv.max_fsz - 1;
+  const size_t n_pad = align_up((size_t)std::max(max_uc + 1, 16), 16);
+  return 16 + (size_t)lv.max_nc * rw * kTcLS * sizeof(float) + 16 + (size_t)std::max(max_uc, 1) * 8 * kTcLS *
+         sizeof(float) + 128 + 2 * 128 * 32 + 2 * n_pad * 32 + 8 + 16 + 16;
+}
+
 inline TcLayout plan_tc_layout(const LevelLaunch& lv, const FrontSmem& sm) {
   TcLayout t;
   const int rw = lv.max_fsz + 1;
@@ -606,6 +614,15 @@ inline TcLayout plan_tc_layout(const LevelLaunch& lv, const FrontSmem& sm) {
 
 inline bool tc_tier_fits(const LevelLaunch& lv, const TcLayout& t) {
   return lv.max_fsz - 1 <= 128 && t.n_pad <= 256 && t.total <= kSmemLimit;
+}
+
+// Staging of a tensor-core launch: as large as fits beside the tier's arrays.
+inline bool plan_tc(const LevelLaunch& lv, FrontSmem* sm, TcLayout* tl) {
+  *sm = plan_wide_staging(lv, sizeof(float), tc_reserve_bytes(lv));
+  sm->us_bytes = 0;  // the pivot rows have their own padded place
+  if (sm->nbuf == 2 && sm->chunk < 32) return false;
+  *tl = plan_tc_layout(lv, *sm);
+  return tc_tier_fits(lv, *tl);
 }
 
 // byte offset of element (r, k) in a K-major tile of 8-row x 16-byte core
@@ -1043,10 +1060,9 @@ template <typename T, typename TJ, int FMAX>
 void launch_factor_t(const LevelLaunch& lv, const FactorArgs<T, TJ>& a, cudaStream_t s) {
   const int fmax = lv.max_fsz;
   const size_t elems = (size_t)fmax * (fmax + 1);
-  FrontSmem sm = plan_front_smem(lv, sizeof(T), true);
-  const bool in_smem = sm.total() <= kSmemLimit;
+  const bool in_smem = front_in_shared_memory(lv, sizeof(T));
+  FrontSmem sm = plan_front_smem(lv, sizeof(T), in_smem);
   if (!in_smem) {
-    sm = plan_front_smem(lv, sizeof(T), false);
     if (sm.total() > kSmemLimit) throw std::runtime_error("factor level: source staging exceeds shared memory");
     if (!a.front_scratch || a.front_scratch_elems < elems * (size_t)lv.count * a.groups)
       throw std::runtime_error("front larger than the shared-memory budget and no scratch area provided");
@@ -1115,10 +1131,9 @@ void launch_factor_tc(const LevelLaunch& lv, const FactorArgs<T, TJ>& a, cudaStr
   if constexpr (!std::is_same<T, float>::value || !std::is_same<TJ, float>::value) {
     launch_factor_wide<T, TJ>(lv, a, s);  // the tensor-core tier is built for FP32 factors
   } else {
-    FrontSmem sm = plan_wide_smem(lv, sizeof(float));
-    sm.us_bytes = 0;  // the pivot rows have their own padded place
-    const TcLayout tl = plan_tc_layout(lv, sm);
-    if (!tc_tier_fits(lv, tl)) {
+    FrontSmem sm;
+    TcLayout tl;
+    if (!plan_tc(lv, &sm, &tl)) {
       launch_factor_wide<T, TJ>(lv, a, s);
       return;
     }

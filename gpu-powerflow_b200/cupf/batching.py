@@ -8,6 +8,12 @@ stream, driven by its own host thread (the ctypes calls into the engine
 release the GIL, and each solve synchronises only its own stream once per
 Newton iteration), so the grids' kernels overlap on the GPU and the small
 grids' latency-bound launches fill the SMs the large grid leaves idle.
+
+The largest grid sets the pace (its Newton loop is the longest chain of
+dependent launches), so with ``prioritize`` the streams get CUDA stream
+priorities by grid size: the largest grid's kernels are scheduled first
+whenever blocks of several grids wait for free SMs, and the smaller grids
+fill in around them.
 """
 from __future__ import annotations
 
@@ -17,7 +23,8 @@ from . import BackendKind, ComputePolicy, NewtonOptions, NewtonSolver, NRConfig
 
 
 class UnevenBatch:
-    def __init__(self, grids, compute=ComputePolicy.Mixed, use_cuda_graph: bool = True, serial_nd: bool = True):
+    def __init__(self, grids, compute=ComputePolicy.Mixed, use_cuda_graph: bool = True, serial_nd: bool = True,
+                 prioritize: bool = True):
         import torch
 
         self.torch = torch
@@ -32,7 +39,19 @@ class UnevenBatch:
             s = NewtonSolver(o)
             s.initialize(g.indptr, g.indices, g.data, g.n_bus, g.n_bus, g.pv, g.pq)
             self.solvers.append(s)
-        self.streams = [torch.cuda.Stream() for _ in self.grids]
+        if prioritize:
+            # (least, greatest) urgency, e.g. (0, -5): a lower number is more
+            # urgent; the largest grid gets the most urgent priority
+            least, greatest = torch.cuda.Stream.priority_range()
+            order = sorted(range(len(self.grids)), key=lambda i: -self.grids[i].n_bus)
+            prio = [0] * len(self.grids)
+            for rank, i in enumerate(order):
+                prio[i] = min(least, greatest + rank)
+            self.priorities = prio
+            self.streams = [torch.cuda.Stream(priority=p) for p in prio]
+        else:
+            self.priorities = [0] * len(self.grids)
+            self.streams = [torch.cuda.Stream() for _ in self.grids]
 
     def solve(self, sbus_list, v0_list, config: NRConfig | None = None, concurrent: bool = True):
         """sbus_list[i], v0_list[i]: complex128 CUDA tensors [B_i, n_i] for grid i.

@@ -478,6 +478,44 @@ def test_host_pipeline_matches_serial_solves(torch):
     assert torch.equal(shared, V_out[0])
 
 
+@pytest.mark.parametrize("lanes", [2, 3])
+def test_host_pipeline_with_concurrent_solve_lanes(torch, lanes):
+    """HostPipeline with several solve lanes (one solver handle, stream and
+    worker thread each; batches round-robin): every batch's results equal the
+    batch solved alone, bit for bit, in batch order, whatever the lane."""
+    import cupf
+    from cupf import grids as G
+    from cupf.streaming import HostPipeline
+
+    g = G.grid_500()
+    cfg = cupf.NRConfig(tolerance=1e-8, max_iter=10)
+    v0 = torch.tensor(g.v0, device="cuda")
+    solvers = []
+    for _ in range(lanes):
+        o = cupf.NewtonOptions()
+        o.backend = cupf.BackendKind.CUDA
+        o.use_cuda_graph = True
+        o.custom.serial_nd = True
+        s = cupf.NewtonSolver(o)
+        s.initialize(g.indptr, g.indices, g.data, g.n_bus, g.n_bus, g.pv, g.pq)
+        solvers.append(s)
+
+    def make(s):
+        def solve(s_dev):
+            v, fm, _ = s.solve_batch_device(s_dev, v0[None, :].expand(s_dev.shape[0], -1).contiguous(), config=cfg)
+            return v, fm
+        return solve
+    sizes = [96, 64, 33, 96, 7, 128, 64]
+    ins = [torch.tensor(g.scenarios(b, seed=70 + i)).pin_memory() for i, b in enumerate(sizes)]
+    V_out = [torch.empty(b, g.n_bus, dtype=torch.complex128).pin_memory() for b in sizes]
+    fm_out = [torch.empty(b, dtype=torch.float64).pin_memory() for b in sizes]
+    HostPipeline([make(s) for s in solvers]).run(ins, V_out, fm_out)
+    ref = make(solvers[0])
+    for i in range(len(sizes)):
+        v, fm = ref(ins[i].cuda())
+        assert torch.equal(V_out[i], v.cpu()) and torch.equal(fm_out[i], fm.cpu()), i
+
+
 def test_host_pipeline_overlaps_the_warm_start_network(torch):
     """HostPipeline with a prepare stage: the next batch's network inference
     runs on its own stream into its own slot's buffers while the current
