@@ -551,14 +551,17 @@ __global__ void __launch_bounds__(256)
 // column is read across the banks); then
 //  3c. the L21 multipliers of every non-pivot row, for the block's 32
 //      scenarios, into shared memory (Ls [uc][8][33]);
-//  3d. per scenario s: its L21 block (uc x nc, padded to M = 128 rows) and
-//      U12^T ((uc + 1) x nc: the trailing columns and the right-hand side,
-//      padded to N rows) are packed as K-major tf32 tiles, each operand
-//      split as x = hi + lo (both tf32, about 21 bits of the fp32 value);
-//      three tcgen05.mma kind::tf32 with K = 8 -- hi*hi + hi*lo + lo*hi, the
-//      Ozaki-style split -- accumulate D = L21 U12 in tensor memory (fp32).
-//      The epilogue reads D back (tcgen05.ld: TMEM lane = front row) and
-//      subtracts it from the trailing block of the front in the scratch;
+//  3d. in rounds of S scenarios (as many as the shared-memory tiles and the
+//      512 tensor-memory columns allow): each scenario's L21 block (uc x nc,
+//      padded to M = 128 rows) and U12^T ((uc + 1) x nc: the trailing
+//      columns and the right-hand side, padded to N rows) are packed as
+//      K-major tf32 tiles, each operand split as x = hi + lo (both tf32,
+//      about 21 bits of the fp32 value); three tcgen05.mma kind::tf32 with
+//      K = 8 -- hi*hi + hi*lo + lo*hi, the Ozaki-style split -- accumulate
+//      D = L21 U12 in the scenario's own tensor-memory columns (fp32), one
+//      commit per round.  The epilogue reads D back (tcgen05.ld: TMEM lane =
+//      front row) and subtracts it from the trailing block of the front in
+//      the scratch;
 //  3e. the trailing block, now A22 - L21 U12 with the updated right-hand
 //      side, is copied to CB, 32 scenarios per coalesced row.
 // One thread issues the MMAs; the wait for their commit is bounded.  When it
@@ -570,29 +573,36 @@ __global__ void __launch_bounds__(256)
 constexpr int kTcLS = kWarp + 1;  // lane stride of Us and Ls in the tensor-core tier
 
 // Shared-memory layout of a tensor-core launch (byte offsets from the base).
+// A round packs the operands of `spr` scenarios and issues their products
+// together (3 MMAs each into its own TMEM columns, one commit).
 struct TcLayout {
   int n_pad = 0;      // N of the MMA: the trailing columns + rhs, rounded up to 16
-  int tmem_cols = 0;  // tensor-memory columns allocated (power of 2 >= 32)
+  int spr = 1;        // scenarios per round (1, 2, 4 or 8)
+  int tmem_cols = 0;  // tensor-memory columns allocated (power of 2 >= 32, >= spr * n_pad)
   unsigned us_off = 0, ls_off = 0, a_off = 0, b_off = 0, bar_off = 0, total = 0;
 };
 
 inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
-// Bytes the tensor-core tier needs beside the staging (rounding included).
-inline size_t tc_reserve_bytes(const LevelLaunch& lv) {
+inline int tc_n_pad(const LevelLaunch& lv) { return (int)align_up((size_t)std::max(lv.max_fsz, 16), 16); }
+
+// Bytes the tensor-core tier needs beside the staging (rounding included)
+// for `spr` scenarios per round.
+inline size_t tc_reserve_bytes(const LevelLaunch& lv, int spr) {
   const int rw = lv.max_fsz + 1, max_uc = lv.max_fsz - 1;
-  const size_t n_pad = align_up((size_t)std::max(max_uc + 1, 16), 16);
-  return 16 + (size_t)lv.max_nc * rw * kTcLS * sizeof(float) + 16 + (size_t)std::max(max_uc, 1) * 8 * kTcLS *
-         sizeof(float) + 128 + 2 * 128 * 32 + 2 * n_pad * 32 + 8 + 16 + 16;
+  return 16 + (size_t)lv.max_nc * rw * kTcLS * sizeof(float) + 16 +
+         (size_t)std::max(max_uc, 1) * 8 * kTcLS * sizeof(float) + 128 + (size_t)spr * 2 * 128 * 32 +
+         (size_t)spr * 2 * tc_n_pad(lv) * 32 + 8 + 16 + 16;
 }
 
-inline TcLayout plan_tc_layout(const LevelLaunch& lv, const FrontSmem& sm) {
+inline TcLayout plan_tc_layout(const LevelLaunch& lv, const FrontSmem& sm, int spr) {
   TcLayout t;
   const int rw = lv.max_fsz + 1;
   const int max_uc = lv.max_fsz - 1;  // nc >= 1
-  t.n_pad = (int)align_up((size_t)std::max(max_uc + 1, 16), 16);
+  t.n_pad = tc_n_pad(lv);
+  t.spr = spr;
   t.tmem_cols = 32;
-  while (t.tmem_cols < t.n_pad) t.tmem_cols *= 2;
+  while (t.tmem_cols < spr * t.n_pad) t.tmem_cols *= 2;
   size_t off = sm.idx_bytes + sm.inv_bytes + sm.stage_bytes;
   off = align_up(off, 16);
   t.us_off = (unsigned)off;
@@ -602,9 +612,9 @@ inline TcLayout plan_tc_layout(const LevelLaunch& lv, const FrontSmem& sm) {
   off += (size_t)std::max(max_uc, 1) * 8 * kTcLS * sizeof(float);
   off = align_up(off, 128);
   t.a_off = (unsigned)off;
-  off += 2 * 128 * 32;  // A hi, A lo: 128 rows x 8 tf32
+  off += (size_t)spr * 2 * 128 * 32;  // per scenario: A hi, A lo (128 rows x 8 tf32)
   t.b_off = (unsigned)off;
-  off += 2 * (size_t)t.n_pad * 32;  // B hi, B lo: n_pad rows x 8 tf32
+  off += (size_t)spr * 2 * t.n_pad * 32;  // per scenario: B hi, B lo (n_pad rows x 8 tf32)
   off = align_up(off, 8);
   t.bar_off = (unsigned)off;
   off += 8 + 4 + 4;  // mbarrier, TMEM address slot, failure flag
@@ -613,16 +623,22 @@ inline TcLayout plan_tc_layout(const LevelLaunch& lv, const FrontSmem& sm) {
 }
 
 inline bool tc_tier_fits(const LevelLaunch& lv, const TcLayout& t) {
-  return lv.max_fsz - 1 <= 128 && t.n_pad <= 256 && t.total <= kSmemLimit;
+  return lv.max_fsz - 1 <= 128 && t.n_pad <= 256 && t.spr * t.n_pad <= 512 && t.total <= kSmemLimit;
 }
 
-// Staging of a tensor-core launch: as large as fits beside the tier's arrays.
+// Staging and layout of a tensor-core launch: the most scenarios per round
+// (8, 4, 2, 1) whose tiles and tensor memory fit, with staging chunks of at
+// least 32 rows beside them.
 inline bool plan_tc(const LevelLaunch& lv, FrontSmem* sm, TcLayout* tl) {
-  *sm = plan_wide_staging(lv, sizeof(float), tc_reserve_bytes(lv));
-  sm->us_bytes = 0;  // the pivot rows have their own padded place
-  if (sm->nbuf == 2 && sm->chunk < 32) return false;
-  *tl = plan_tc_layout(lv, *sm);
-  return tc_tier_fits(lv, *tl);
+  for (int spr : {8, 4, 2, 1}) {
+    if (spr * tc_n_pad(lv) > 512) continue;
+    *sm = plan_wide_staging(lv, sizeof(float), tc_reserve_bytes(lv, spr));
+    sm->us_bytes = 0;  // the pivot rows have their own padded place
+    if (sm->nbuf == 2 && sm->chunk < 32) continue;
+    *tl = plan_tc_layout(lv, *sm, spr);
+    if (tc_tier_fits(lv, *tl)) return true;
+  }
+  return false;
 }
 
 // byte offset of element (r, k) in a K-major tile of 8-row x 16-byte core
@@ -684,51 +700,62 @@ __global__ void __launch_bounds__(256)
   const uint32_t idesc = tc::idesc_tf32(128, tl.n_pad);
   const int qtr = warp & 3, nsplit = W >> 2, part = warp >> 2;
   const int row = qtr * 32 + lane;  // this thread's TMEM lane = front row of the trailing block
-  int failed_at = -1;
-  for (int sc = 0; sc < (uc > 0 ? kWarp : 0); ++sc) {  // (a root front has no trailing block)
-    // 3d: scenario sc's operands as hi + lo tf32 tiles
-    for (int e = threadIdx.x; e < 128 * 8; e += blockDim.x) {
-      const int r = e >> 3, k = e & 7;
-      const float x = r < uc ? Ls[((size_t)r * 8 + k) * kTcLS + sc] : 0.0f;
+  int failed_at = -1;  // the round whose products did not complete
+  const int S = tl.spr;
+  const size_t a_stride = 2 * 128 * 32, b_stride = 2 * (size_t)tl.n_pad * 32;  // bytes per scenario
+  for (int rnd = 0; rnd < (uc > 0 ? kWarp / S : 0); ++rnd) {  // (a root front has no trailing block)
+    const int sc0 = rnd * S;
+    // 3d: the operands of scenarios sc0 .. sc0 + S - 1 as hi + lo tf32 tiles
+    for (int e = threadIdx.x; e < S * 128 * 8; e += blockDim.x) {
+      const int s_ = e / (128 * 8), r = (e >> 3) & 127, k = e & 7;
+      const float x = r < uc ? Ls[((size_t)r * 8 + k) * kTcLS + sc0 + s_] : 0.0f;
       const float hi = tc::to_tf32(x);
-      const unsigned o = tc_tile_off(r, k);
-      *reinterpret_cast<float*>(tA + o) = hi;
-      *reinterpret_cast<float*>(tA + 4096 + o) = tc::to_tf32(x - hi);
+      unsigned char* a = tA + (size_t)s_ * a_stride + tc_tile_off(r, k);
+      *reinterpret_cast<float*>(a) = hi;
+      *reinterpret_cast<float*>(a + 4096) = tc::to_tf32(x - hi);
     }
-    for (int e = threadIdx.x; e < tl.n_pad * 8; e += blockDim.x) {
-      const int j = e >> 3, k = e & 7;
-      const float x = (j < nb && k < nc) ? Us[((size_t)k * rw + nc + j) * kTcLS + sc] : 0.0f;
+    for (int e = threadIdx.x; e < S * tl.n_pad * 8; e += blockDim.x) {
+      const int s_ = e / (tl.n_pad * 8), j = (e >> 3) % tl.n_pad, k = e & 7;
+      const float x = (j < nb && k < nc) ? Us[((size_t)k * rw + nc + j) * kTcLS + sc0 + s_] : 0.0f;
       const float hi = tc::to_tf32(x);
-      const unsigned o = tc_tile_off(j, k);
-      *reinterpret_cast<float*>(tB + o) = hi;
-      *reinterpret_cast<float*>(tB + (size_t)tl.n_pad * 32 + o) = tc::to_tf32(x - hi);
+      unsigned char* bp = tB + (size_t)s_ * b_stride + tc_tile_off(j, k);
+      *reinterpret_cast<float*>(bp) = hi;
+      *reinterpret_cast<float*>(bp + (size_t)tl.n_pad * 32) = tc::to_tf32(x - hi);
     }
     tc::fence_smem_to_async();
     __syncthreads();
     if (threadIdx.x == 0) {
       tc::tc_fence_after();
-      const uint64_t ah = tc::smem_desc_plain(tA, 128, 256), al = tc::smem_desc_plain(tA + 4096, 128, 256);
-      const uint64_t bh = tc::smem_desc_plain(tB, 128, 256);
-      const uint64_t bl = tc::smem_desc_plain(tB + (size_t)tl.n_pad * 32, 128, 256);
-      tc::tc_mma_tf32(tmem, ah, bh, idesc, 0u);
-      tc::tc_mma_tf32(tmem, ah, bl, idesc, 1u);
-      tc::tc_mma_tf32(tmem, al, bh, idesc, 1u);
+      for (int s_ = 0; s_ < S; ++s_) {
+        const unsigned char* a = tA + (size_t)s_ * a_stride;
+        const unsigned char* bp = tB + (size_t)s_ * b_stride;
+        const uint64_t ah = tc::smem_desc_plain(a, 128, 256), al = tc::smem_desc_plain(a + 4096, 128, 256);
+        const uint64_t bh = tc::smem_desc_plain(bp, 128, 256);
+        const uint64_t bl = tc::smem_desc_plain(bp + (size_t)tl.n_pad * 32, 128, 256);
+        const uint32_t d = tmem + (uint32_t)(s_ * tl.n_pad);  // this scenario's accumulator columns
+        tc::tc_mma_tf32(d, ah, bh, idesc, 0u);
+        tc::tc_mma_tf32(d, ah, bl, idesc, 1u);
+        tc::tc_mma_tf32(d, al, bh, idesc, 1u);
+      }
       tc::tc_commit(bar);
     }
-    const bool have = __all_sync(0xffffffffu, tc::mbar_wait(bar, (uint32_t)(sc & 1), spin_limit));
+    const bool have = __all_sync(0xffffffffu, tc::mbar_wait(bar, (uint32_t)(rnd & 1), spin_limit));
     if (!have && lane == 0) atomicExch(s_fail, 1);
     __syncthreads();
     tc::tc_fence_after();
     if (*s_fail) {
-      failed_at = sc;
+      failed_at = rnd;
       break;
     }
-    // epilogue: the W / 4 warps of a TMEM lane quarter split the 16-column chunks
-    float* Fr = Fm + ((size_t)(nc + row) * rw + nc) * kWarp + sc;
-    for (int c = part; c < tl.n_pad / 16; c += nsplit) {
+    // epilogue: the W / 4 warps of a TMEM lane quarter split the (scenario,
+    // 16-column chunk) pairs
+    const int nch = tl.n_pad / 16;
+    for (int w = part; w < S * nch; w += nsplit) {
+      const int s_ = w / nch, c = w - s_ * nch;
       float v[16];
-      tc::tmem_ld16(tmem + ((uint32_t)(qtr * 32) << 16) + (uint32_t)(c * 16), v);
+      tc::tmem_ld16(tmem + ((uint32_t)(qtr * 32) << 16) + (uint32_t)(s_ * tl.n_pad + c * 16), v);
       if (row < uc) {
+        float* Fr = Fm + ((size_t)(nc + row) * rw + nc) * kWarp + sc0 + s_;
 #pragma unroll
         for (int t = 0; t < 16; ++t)
           if (c * 16 + t < nb) Fr[(size_t)(c * 16 + t) * kWarp] -= v[t];
