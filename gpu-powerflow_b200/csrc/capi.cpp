@@ -118,11 +118,12 @@ bool copy_plan_array(const Engine& e, const char* name, int32_t* out, int64_t ca
   CUPF_ARR("diag22", ja.diag22)
 #undef CUPF_ARR
   if (n == "factor_level_warps" || n == "backward_launch_warps" || n == "factor_level_tiers" ||
-      n == "tc_threshold") {  // the autotuner's choices (0: built-in rule), the kernel tier of each launch
-    const std::vector<int32_t> w = n == "factor_level_warps"   ? e.factor_level_warps()
-                                   : n == "factor_level_tiers" ? e.factor_level_tiers()
-                                   : n == "tc_threshold"       ? std::vector<int32_t>{e.tc_threshold()}
-                                                               : e.backward_launch_warps();
+      n == "tc_threshold" || n == "factor_level_placement") {  // the autotuner's choices, each launch's kernel
+    const std::vector<int32_t> w = n == "factor_level_warps"       ? e.factor_level_warps()
+                                   : n == "factor_level_tiers"     ? e.factor_level_tiers()
+                                   : n == "factor_level_placement" ? e.factor_level_placements()
+                                   : n == "tc_threshold"           ? std::vector<int32_t>{e.tc_threshold()}
+                                                                   : e.backward_launch_warps();
     if (len) *len = (int64_t)w.size();
     if (out) {
       if (cap < (int64_t)w.size()) return false;

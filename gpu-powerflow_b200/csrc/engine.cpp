@@ -571,7 +571,8 @@ void Engine::ensure_workspace(int32_t B) {
       LevelLaunch widest = lv;  // the tier with the largest scratch this launch may be given
       if (tf32_factors() && lv.max_fsz >= std::min(tc_min_ > 0 ? tc_min_ : kTcDefaultMinFront, kTcDefaultMinFront))
         widest.tier = 2;
-      scratch = std::max({scratch, level_scratch_elems(lv, es, Bp / kWarp), level_scratch_elems(widest, es, Bp / kWarp)});
+      scratch = std::max({scratch, level_scratch_capacity(lv, es, Bp / kWarp),
+                          level_scratch_capacity(widest, es, Bp / kWarp)});
     }
     d.front_scratch_elems = scratch;
     if (scratch) d.front_scratch.reserve(scratch * kWarp * es);
@@ -676,19 +677,21 @@ FactorArgs<T, T> Engine::factor_args(int store_l, const void* J) const {
 
 namespace {
 
-// Chooses a block shape (warps per block) for each of n launches that run in
-// sequence on stream s.  set(i, w) gives launch i the shape w (0: its
-// built-in rule); launch(i) issues it.  Candidates 1, 2, 4 and 8 warps and
-// the rule each run the whole sequence three times with an event after every
-// launch; a launch keeps the fastest candidate if it beats the rule by 3 %
-// and by 0.5 us, else the rule.  Then the whole sequence is timed as a solve
-// runs it (chained launches, no events in between), three times with the
-// choice and three with the rule; the choice stays only if it is at least
-// 1 % faster.  Leaves the chosen shapes set; returns whether they were kept.
+// Chooses a launch shape for each of n launches that run in sequence on
+// stream s.  Candidate shapes are opaque codes (cand, none of them 0);
+// set(i, code) gives launch i the shape code (0: its built-in rule);
+// launch(i) issues it.  Every candidate and the rule each run the whole
+// sequence three times with an event after every launch; a launch keeps the
+// fastest candidate if it beats the rule by 3 % and by 0.5 us, else the rule.
+// Then the whole sequence is timed as a solve runs it (chained launches, no
+// events in between), three times with the choice and three with the rule;
+// the choice stays only if it is at least 1 % faster.  Leaves the chosen
+// shapes set; returns whether they were kept.
 template <typename Set, typename Launch>
-bool choose_block_shapes(size_t n, Set set, Launch launch, cudaStream_t s, const char* what) {
-  constexpr int kCand[4] = {1, 2, 4, 8};
-  std::vector<double> t((size_t)5 * n, 1e30);  // [candidate 0..3, rule = 4][launch]
+bool choose_block_shapes(size_t n, const std::vector<int>& cand, Set set, Launch launch, cudaStream_t s,
+                         const char* what) {
+  const size_t nc = cand.size();
+  std::vector<double> t((nc + 1) * n, 1e30);  // [candidate 0..nc-1, rule = nc][launch]
   std::vector<cudaEvent_t> ev(n + 1, nullptr);
   auto cleanup = [&] {
     for (auto& e : ev)
@@ -699,8 +702,8 @@ bool choose_block_shapes(size_t n, Set set, Launch launch, cudaStream_t s, const
   try {
     for (auto& e : ev) CUPF_CUDA(cudaEventCreate(&e));
     for (int rep = 0; rep < 3; ++rep)
-      for (int c = 0; c < 5; ++c) {
-        for (size_t i = 0; i < n; ++i) set(i, c < 4 ? kCand[c] : 0);
+      for (size_t c = 0; c <= nc; ++c) {
+        for (size_t i = 0; i < n; ++i) set(i, c < nc ? cand[c] : 0);
         CUPF_CUDA(cudaEventRecord(ev[0], s));
         for (size_t i = 0; i < n; ++i) {
           launch(i);
@@ -710,20 +713,20 @@ bool choose_block_shapes(size_t n, Set set, Launch launch, cudaStream_t s, const
         for (size_t i = 0; i < n; ++i) {
           float ms = 0.f;
           CUPF_CUDA(cudaEventElapsedTime(&ms, ev[i], ev[i + 1]));
-          double& cell = t[(size_t)c * n + i];
+          double& cell = t[c * n + i];
           cell = std::min(cell, (double)ms);
         }
       }
     for (size_t i = 0; i < n; ++i) {
-      const double rule = t[(size_t)4 * n + i];
+      const double rule = t[nc * n + i];
       int best = -1;
       double bt = std::min(rule * 0.97, rule - 0.5e-3);
-      for (int c = 0; c < 4; ++c)
-        if (t[(size_t)c * n + i] < bt) {
-          bt = t[(size_t)c * n + i];
-          best = c;
+      for (size_t c = 0; c < nc; ++c)
+        if (t[c * n + i] < bt) {
+          bt = t[c * n + i];
+          best = (int)c;
         }
-      choice[i] = best >= 0 ? kCand[best] : 0;
+      choice[i] = best >= 0 ? cand[best] : 0;
     }
     for (int rep = 0; rep < 3; ++rep)
       for (int v = 0; v < 2; ++v) {
@@ -744,14 +747,15 @@ bool choose_block_shapes(size_t n, Set set, Launch launch, cudaStream_t s, const
   cleanup();
   const bool keep = whole[1] < 0.99 * whole[0];
   for (size_t i = 0; i < n; ++i) set(i, keep ? choice[i] : 0);
-  if (debug_sync())
-    for (size_t i = 0; i < n; ++i)
-      std::fprintf(stderr, "[cupf] %s launch %zu: rule %.2f us, 1/2/4/8 warps %.2f %.2f %.2f %.2f us, chosen %d\n",
-                   what, i, 1e3 * t[4 * n + i], 1e3 * t[i], 1e3 * t[n + i], 1e3 * t[2 * n + i], 1e3 * t[3 * n + i],
-                   choice[i]);
-  if (debug_sync())
+  if (debug_sync()) {
     std::fprintf(stderr, "[cupf] %s autotune: rule %.3f ms, choice %.3f ms, %s\n", what, whole[0], whole[1],
                  keep ? "kept" : "rule kept");
+    for (size_t i = 0; i < n; ++i) {
+      std::fprintf(stderr, "[cupf] %s launch %zu: rule %.2f us, chosen %d;", what, i, 1e3 * t[nc * n + i], choice[i]);
+      for (size_t c = 0; c < nc; ++c) std::fprintf(stderr, " %d: %.2f", cand[c], 1e3 * t[c * n + i]);
+      std::fprintf(stderr, "\n");
+    }
+  }
   return keep;
 }
 
@@ -805,8 +809,18 @@ void Engine::autotune_factor(cudaStream_t s, const void* J) {
     cudaEventDestroy(e1);
     assign_tiers(best);
   }
+  // shapes: warps per block (1, 2, 4, 8), and for the register tier where
+  // the dense fronts live (code = warps + 256 x placement: shared memory 1,
+  // global scratch 2)
+  std::vector<int> cand;
+  for (int p : {1, 2})
+    for (int w : {1, 2, 4, 8}) cand.push_back(w + 256 * p);
   choose_block_shapes(
-      d.levels.size(), [&](size_t i, int w) { d.levels[i].warps = w; },
+      d.levels.size(), cand,
+      [&](size_t i, int code) {
+        d.levels[i].warps = code & 0xff;
+        d.levels[i].placement = d.levels[i].tier == 0 ? code >> 8 : 0;
+      },
       [&](size_t i) { launch_factor_level<T, T>(d.levels[i], a, s); }, s, "factor");
   d.tuned_Bp = d.Bp;
   d.tuned_double = dbl;
@@ -828,7 +842,7 @@ void Engine::autotune_backward(cudaStream_t s) {
   for (int l = d.bw_first - 1; l >= 0; --l) seq.push_back(&d.levels[l]);
   const bool has_top = d.bw_nlev > 0;
   choose_block_shapes(
-      seq.size(), [&](size_t i, int w) { seq[i]->bw_wpb = w; },
+      seq.size(), std::vector<int>{1, 2, 4, 8}, [&](size_t i, int w) { seq[i]->bw_wpb = w; },
       [&](size_t i) {
         if (i == 0 && has_top)
           launch_backward_top<T>(d.bw_top, d.bw_bounds.as<int>(), d.bw_nlev, a, s);
@@ -858,6 +872,13 @@ std::vector<int32_t> Engine::factor_level_warps() const {
   std::vector<int32_t> w;
   for (const auto& lv : d_->levels) w.push_back(lv.warps);
   return w;
+}
+
+std::vector<int32_t> Engine::factor_level_placements() const {
+  std::vector<int32_t> p;
+  const size_t es = factor_is_double() ? sizeof(double) : sizeof(float);
+  for (const auto& lv : d_->levels) p.push_back(lv.tier > 0 ? 2 : (front_in_shared_memory(lv, es) ? 1 : 2));
+  return p;
 }
 
 std::vector<int32_t> Engine::backward_launch_warps() const {

@@ -120,6 +120,8 @@ class Engine {
   // factor kernel tier of each launch (0 register rows, 1 any-size, 2 tensor
   // cores) and the tensor-core threshold in use (0 when not TF32)
   std::vector<int32_t> factor_level_tiers() const;
+  // where each factor launch keeps its dense fronts: 1 shared memory, 2 the global scratch
+  std::vector<int32_t> factor_level_placements() const;
   int32_t tc_threshold() const { return tc_min_; }
   // the same for the backward sweep's launches, tree top first
   std::vector<int32_t> backward_launch_warps() const;

@@ -26,6 +26,10 @@ struct LevelLaunch {
   // tier on the FP32/FP64 pipes (any size), 2 the wide tier with the trailing
   // update on the tensor cores (FP32 factors only)
   int tier = 0;
+  // register tier: where the dense fronts live -- 0 the built-in rule
+  // (front_in_shared_memory), 1 shared memory, 2 the global scratch (chosen
+  // by the engine's autotuner; a choice that does not fit falls back to the rule)
+  int placement = 0;
 };
 
 template <typename T, typename TJ>
@@ -102,6 +106,8 @@ inline bool front_in_shared_memory(const LevelLaunch& lv, size_t elem_bytes) {
   if (a.total() > kSmemLimit) return false;
   const FrontSmem b = plan_front_smem(lv, elem_bytes, false);
   if (b.total() > kSmemLimit) return true;
+  if (lv.placement == 1) return true;
+  if (lv.placement == 2) return false;
   return !(staging_round_trips(lv, b) + 2 < staging_round_trips(lv, a));
 }
 
@@ -165,11 +171,19 @@ inline size_t wide_block_elems(const LevelLaunch& lv, size_t elem_bytes) {
 }
 
 // Global front scratch (elements x 32) a factor launch needs for all its
-// blocks (groups = 32-scenario groups of the batch); 0 when its fronts live
-// in shared memory.
+// blocks (groups = 32-scenario groups of the batch) with its current tier
+// and placement; 0 when its fronts live in shared memory.
 inline size_t level_scratch_elems(const LevelLaunch& lv, size_t elem_bytes, int groups) {
   if (lv.tier > 0) return wide_block_elems(lv, elem_bytes) * lv.count * groups;
   if (front_in_shared_memory(lv, elem_bytes)) return 0;
+  return (size_t)lv.max_fsz * (lv.max_fsz + 1) * lv.count * groups;
+}
+
+// The most a register-tier launch can need whatever placement the autotuner
+// gives it (the workspace is sized for this).
+inline size_t level_scratch_capacity(const LevelLaunch& lv, size_t elem_bytes, int groups) {
+  if (lv.tier > 0) return level_scratch_elems(lv, elem_bytes, groups);
+  if (plan_front_smem(lv, elem_bytes, false).total() > kSmemLimit) return 0;
   return (size_t)lv.max_fsz * (lv.max_fsz + 1) * lv.count * groups;
 }
 

@@ -149,7 +149,10 @@ const char* cls_last_error(cls_handle h);
  * "sym_row_idx"), or of the engine's launch plan: "factor_level_warps" and
  * "backward_launch_warps" (the autotuner's block shapes, 0 = built-in rule),
  * "factor_level_tiers" (per factor launch: 0 register-row kernel, 1 any-size
- * tier, 2 any-size tier with the tensor-core trailing update) and
+ * tier, 2 any-size tier with the tensor-core trailing update),
+ * "factor_level_placement" (per factor launch: 1 dense fronts in shared
+ * memory, 2 in the global scratch; the autotuner chooses it with the block
+ * shape) and
  * "tc_threshold" (one value: the front size from which TF32 factors use the
  * tensor cores, 0 for other precisions).  With out == NULL only *len is set. */
 cls_status cls_plan_array(cls_handle h, const char* name, int32_t* out, int64_t capacity, int64_t* len);
