@@ -50,9 +50,12 @@ MAX_ITER = 10
 
 
 
-# measured DRAM traffic of one Mixed factorization of the 2,000-bus grid at
-# 1,024 scenarios: 277.9 MB read + 11.9 MB written over its 19 level launches
-FACTOR_DRAM_BYTES_B1024 = 289_800_000
+# DRAM traffic (read + write) of one Mixed factorization of the 2,000-bus
+# grid, per 1,024 scenarios: its 19 level launches captured with ncu at 256
+# scenarios (72.2 MB read; the writes stay in L2 at that size), scaled by 4
+# (the read traffic grows with the batch; a capture at 1,024 scenarios read
+# 278.8 MB and wrote 11.9 MB)
+FACTOR_DRAM_BYTES_B1024 = 288_800_000
 
 def _peaks() -> dict:
     p = ROOT / "MEASURED_PEAKS.json"

@@ -569,7 +569,7 @@ void Engine::ensure_workspace(int32_t B) {
     size_t scratch = 0;
     for (const auto& lv : d.levels) {
       LevelLaunch widest = lv;  // the tier with the largest scratch this launch may be given
-      if (tf32_factors() && lv.max_fsz >= std::min(tc_min_ > 0 ? tc_min_ : kTcDefaultMinFront, kTcDefaultMinFront))
+      if (tf32_factors() && lv.max_fsz >= std::min(tc_min_ > 0 ? tc_min_ : kTcSmallestMinFront, kTcSmallestMinFront))
         widest.tier = 2;
       scratch = std::max({scratch, level_scratch_capacity(lv, es, Bp / kWarp),
                           level_scratch_capacity(widest, es, Bp / kWarp)});
@@ -778,10 +778,10 @@ void Engine::autotune_factor(cudaStream_t s, const void* J) {
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     CUPF_CUDA(cudaEventCreate(&e0));
     CUPF_CUDA(cudaEventCreate(&e1));
-    int best = kTcDefaultMinFront;
+    int best = kTcSmallestMinFront;
     double best_ms = 1e30;
     try {
-      for (int t : {kTcDefaultMinFront, 49, 65}) {
+      for (int t : {kTcSmallestMinFront, 49, 65}) {
         assign_tiers(t);
         double ms_t = 1e30;
         for (int rep = 0; rep < 3; ++rep) {

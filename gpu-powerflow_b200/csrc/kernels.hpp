@@ -116,10 +116,10 @@ inline bool front_in_shared_memory(const LevelLaunch& lv, size_t elem_bytes) {
 // for fronts of up to 64 rows.
 constexpr int kWideFrontRows = 65;
 // TF32 factors: the tensor cores take the trailing updates of launches with
-// fronts of at least this many rows (the fronts beyond 32 rows, where the
-// rank-nc update is large enough to tile), unless configured or autotuned
-// otherwise; the autotuner tries this, 49 and 65.
-constexpr int kTcDefaultMinFront = 33;
+// fronts of at least this many rows (the fronts past the register kernels),
+// unless configured or autotuned otherwise; the autotuner tries 33, 49 and 65.
+constexpr int kTcDefaultMinFront = 65;
+constexpr int kTcSmallestMinFront = 33;  // the smallest threshold the autotuner tries
 
 // Shared-memory plan of a wide-tier launch: pivot reciprocals, the staged
 // source rows, and `reserve` bytes after them for the kernel's other arrays

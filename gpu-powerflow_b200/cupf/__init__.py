@@ -18,8 +18,9 @@ Differences a user can see:
     times each factor level's block shape at the first solve of a batch size
     and keeps the fastest; the results do not depend on it;
   * ``CustomSolverConfig.wide_min_front`` and ``tc_min_front`` (not in the
-    reference) set where the any-size front tier and, with
-    ``CustomPrecision.TF32``, the tensor-core trailing update take over.
+    reference) set where the any-size front tier (default 65 rows) and, with
+    ``CustomPrecision.TF32``, the tensor-core trailing update (default 65
+    rows, autotuned among 33, 49 and 65) take over.
 """
 from __future__ import annotations
 

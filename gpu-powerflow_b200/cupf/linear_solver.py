@@ -38,7 +38,7 @@ class SolverConfig:
         self.parallel_nd_base_small = int(parallel_nd_base_small)
         self.parallel_nd_base_large = int(parallel_nd_base_large)
         # fronts from this size on: the any-size tier (0: 65), and with TF32 the
-        # tensor-core trailing update (0: 33, or autotuned)
+        # tensor-core trailing update (0: 65, or autotuned among 33, 49, 65)
         self.wide_min_front = int(wide_min_front)
         self.tc_min_front = int(tc_min_front)
 

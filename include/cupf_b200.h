@@ -88,8 +88,8 @@ typedef struct {
                                    64 rows); 1..65, 0 = 65.  Both give the same factors. */
   int32_t tc_min_front;         /* precision TF32: launches whose largest front has at least this many rows
                                    run their trailing update CB = A22 - L21 U12 on the tensor cores
-                                   (tcgen05 kind::tf32, operands split hi + lo, fp32 accumulation); 0 = 33,
-                                   or the fastest of 16, 24, 32, 48 and 64 when autotune is on */
+                                   (tcgen05 kind::tf32, operands split hi + lo, fp32 accumulation); 0 = 65,
+                                   or the fastest of 33, 49 and 65 when autotune is on */
 } cls_config;
 
 typedef struct cls_solver_s* cls_handle;

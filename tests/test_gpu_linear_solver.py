@@ -298,7 +298,7 @@ def test_larger_reference_datasets_factor_and_solve(case, prec):
     every precision, 8 value sets each (+-2 % perturbations), within the
     residual bars; the launch plan shows which kernel tier factored what
     (any-size tier on case8387pegase; with TF32 the tensor-core tier on the
-    launches whose fronts reach 33 rows)."""
+    launches whose fronts reach 65 rows, the default threshold)."""
     precision, tol = PRECISIONS[prec]
     d, _ = load(case)
     ls, vals, rhs, x, xt = _factor_solve(d, 8, precision, np.random.default_rng(2), autotune=False)
@@ -312,8 +312,8 @@ def test_larger_reference_datasets_factor_and_solve(case, prec):
     tiers = ls.plan_array("factor_level_tiers")
     fsz = ls.plan_array("fp_fsz")
     if prec == "TF32":
-        assert int(ls.plan_array("tc_threshold")[0]) == 33
-        assert (2 in tiers) == (fsz.max() >= 33)
+        assert int(ls.plan_array("tc_threshold")[0]) == 65
+        assert (2 in tiers) == (fsz.max() >= 65)
     else:
         assert 2 not in tiers and (1 in tiers) == (fsz.max() > 64)
 

@@ -393,8 +393,9 @@ def test_other_plans_solve_like_the_oracle(oracle, width, serial):
 
 
 def test_tf32_factors_on_the_10000_bus_grid(oracle):
-    """CustomPrecision.TF32 in the Newton loop (Mixed state): the launches
-    whose fronts reach 33 rows (the top of the 10,000-bus grid's tree, fronts
+    """CustomPrecision.TF32 in the Newton loop (Mixed state), tensor-core
+    threshold 33: the launches whose fronts reach 33 rows (the top of the
+    10,000-bus grid's tree, fronts
     up to 38 rows) run their trailing updates on the tensor cores; every
     scenario still converges to 1e-8 and lies within 1e-8 of the oracle, the
     Newton iteration being the refinement back to FP64 accuracy."""
@@ -406,6 +407,7 @@ def test_tf32_factors_on_the_10000_bus_grid(oracle):
     o.backend = cupf.BackendKind.CUDA
     o.compute = cupf.ComputePolicy.Mixed
     o.custom.precision = cupf.CustomPrecision.TF32
+    o.custom.tc_min_front = 33
     o.custom.serial_nd = True
     o.custom.autotune = False
     o.use_cuda_graph = True
