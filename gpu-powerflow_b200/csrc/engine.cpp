@@ -1391,7 +1391,8 @@ void Engine::factor_all_external(cudaStream_t s, const void* J, T* scratch, size
   a.sing = d.sing.as<int>();
   a.front_scratch = scratch;
   a.front_scratch_elems = scratch_elems;
-  for (const auto& lv : d.levels) {
+  for (LevelLaunch lv : d.levels) {
+    lv.placement = 0;  // the built-in placement: the static area is sized for it
     launch_factor_level<T, T>(lv, a, s);
     ++launches_;
   }
@@ -1409,8 +1410,11 @@ void Engine::factorize_values_static_scratch(const void* d_values, int32_t value
         "nothing, so run one regular cls_factorize at this batch size (or larger) first");
   const bool dbl = factor_is_double();
   const size_t es = dbl ? sizeof(double) : sizeof(float);
-  size_t need = 0;  // elements x 32 lanes
-  for (const auto& lv : d.levels) need = std::max(need, level_scratch_elems(lv, es, Bp / kWarp));
+  size_t need = 0;  // elements x 32 lanes, with the built-in front placement
+  for (LevelLaunch lv : d.levels) {
+    lv.placement = 0;
+    need = std::max(need, level_scratch_elems(lv, es, Bp / kWarp));
+  }
   if (need * kWarp * es > scratch_bytes)
     throw std::invalid_argument("Factorize (static scratch): this batch needs " + std::to_string(need * kWarp * es) +
                                 " bytes of front scratch, the static area holds " + std::to_string(scratch_bytes));
