@@ -11,7 +11,9 @@ constexpr size_t kStaticFrontScratchBytes = size_t(8) << 20;
 
 // Device address of the area on the current device.  The first call on each
 // device looks the symbol up (cudaGetSymbolAddress, with that device current)
-// and caches it; later calls only read the cache.  Throws on failure.
+// and caches it for the life of the process; later calls only read the
+// cache, which a cudaDeviceReset of that device makes stale.  Throws on
+// failure.
 void* static_front_scratch();
 
 }  // namespace cupf_b200

@@ -128,7 +128,10 @@ cls_status cls_factorize(cls_handle h, const void* values, int32_t value_type);
  * is shared by all handles of the process on a device: calls must not
  * overlap in time.  The first call on each device looks the area's address
  * up (cudaGetSymbolAddress with that device current); make it before any
- * stream capture. */
+ * stream capture.  The address is cached for the life of the process: after
+ * cudaDeviceReset on a device the cache is stale and this entry point must
+ * not be used there again.  The launches use the built-in placement of the
+ * dense fronts (not an autotuned one), which the 8 MiB bound refers to. */
 cls_status cls_factorize_static_scratch(cls_handle h, const void* values, int32_t value_type);
 /* Replaces: Solver::SetRhs / SetSolution / Solve() (solver.hpp:93-94,103);
  * device rhs / solution [batch][n]; pairs f64/f64, f64/f32, f32/f32. */
