@@ -1028,7 +1028,8 @@ void Engine::ensure_loop_graph(const DevState& st) {
 }
 
 template <typename T>
-SolveStats Engine::run_loop(double tol, int32_t max_iter, int32_t prepare_adjoint, cudaStream_t s, double* d_final) {
+SolveStats Engine::run_loop(double tol, int32_t max_iter, int32_t prepare_adjoint, cudaStream_t s, double* d_final,
+                            double* d_v_out) {
   const NvtxRange range("NR.solve_batch");
   auto& d = *d_;
   const DevState st = d.state();
@@ -1071,6 +1072,14 @@ SolveStats Engine::run_loop(double tol, int32_t max_iter, int32_t prepare_adjoin
     launch_ctl_load(hc, d.ctl.as<LoopCtl>(), s);
     CUPF_CUDA(cudaGraphLaunch(d.exec, s));
     launch_ctl_store(d.ctl.as<LoopCtl>(), hc, d.fin_dev.as<double>(), d.h_final, d_final, d.B, s);
+    if (d_v_out && !prepare_adjoint) {
+      // the voltages do not depend on what the host reads back: queue them
+      // before the synchronisation, so the device does not idle through the
+      // host's round trip
+      launch_pack_voltage(d.g, st, d_v_out, s);
+      ++launches_;
+      d_v_out = nullptr;
+    }
     CUPF_CUDA(cudaStreamSynchronize(s));
     completed = hc->completed;
     gmax = hc->gmax;
@@ -1138,6 +1147,10 @@ SolveStats Engine::run_loop(double tol, int32_t max_iter, int32_t prepare_adjoin
   // (graph mode: the store kernel already wrote d_final)
   if (d_final && !use_graph)
     CUPF_CUDA(cudaMemcpyAsync(d_final, d.h_final, d.B * sizeof(double), cudaMemcpyHostToDevice, s));
+  if (d_v_out) {
+    launch_pack_voltage(d.g, st, d_v_out, s);
+    ++launches_;
+  }
   CUPF_CUDA(cudaStreamSynchronize(s));
   CUPF_CUDA(cudaGetLastError());
   if (profiling_) collect_stage_times();
@@ -1203,11 +1216,10 @@ SolveStats Engine::solve_batch_device(const double* d_sbus, int64_t sbus_stride,
   use_scenario_ybus(d_ybus, ybus_stride, B, s);
   const DevState st = d.state();
   launch_seed_state(d.g, st, d_sbus, sbus_stride, d_v0, v0_stride, s);
-  SolveStats out = factor_is_double() ? run_loop<double>(tol, max_iter, prepare_adjoint, s, d_final_mismatch)
-                                      : run_loop<float>(tol, max_iter, prepare_adjoint, s, d_final_mismatch);
-  if (d_v_out) launch_pack_voltage(d.g, st, d_v_out, s);
-  launches_ += 2;
-  CUPF_CUDA(cudaStreamSynchronize(s));
+  SolveStats out = factor_is_double()
+                       ? run_loop<double>(tol, max_iter, prepare_adjoint, s, d_final_mismatch, d_v_out)
+                       : run_loop<float>(tol, max_iter, prepare_adjoint, s, d_final_mismatch, d_v_out);
+  launches_ += 1;
   return out;
 }
 
@@ -1232,11 +1244,10 @@ SolveStats Engine::solve_batch_warm_device(const double* d_sbus, int64_t sbus_st
     explicit Tolerate(bool& x) : f(x) { f = true; }
     ~Tolerate() { f = false; }
   } tolerate(tolerate_nonfinite_);
-  SolveStats out = factor_is_double() ? run_loop<double>(tol, max_iter, prepare_adjoint, s, d_final_mismatch)
-                                      : run_loop<float>(tol, max_iter, prepare_adjoint, s, d_final_mismatch);
-  if (d_v_out) launch_pack_voltage(d.g, st, d_v_out, s);
-  launches_ += 3;
-  CUPF_CUDA(cudaStreamSynchronize(s));
+  SolveStats out = factor_is_double()
+                       ? run_loop<double>(tol, max_iter, prepare_adjoint, s, d_final_mismatch, d_v_out)
+                       : run_loop<float>(tol, max_iter, prepare_adjoint, s, d_final_mismatch, d_v_out);
+  launches_ += 2;
   return out;
 }
 
@@ -1534,7 +1545,7 @@ std::vector<int32_t> Engine::singular_flags() const {
   return out;
 }
 
-template SolveStats Engine::run_loop<float>(double, int32_t, int32_t, cudaStream_t, double*);
-template SolveStats Engine::run_loop<double>(double, int32_t, int32_t, cudaStream_t, double*);
+template SolveStats Engine::run_loop<float>(double, int32_t, int32_t, cudaStream_t, double*, double*);
+template SolveStats Engine::run_loop<double>(double, int32_t, int32_t, cudaStream_t, double*, double*);
 
 }  // namespace cupf_b200

@@ -171,7 +171,10 @@ class Engine {
   // selects per-scenario (d_ybus != null) or shared Ybus values for this batch
   void use_scenario_ybus(const double* d_ybus, int64_t ybus_stride, int32_t B, cudaStream_t s);
   template <typename T>
-  SolveStats run_loop(double tol, int32_t max_iter, int32_t prepare_adjoint, cudaStream_t s, double* d_final);
+  // d_v_out: when given, the final voltages are packed into it (host
+  // layout, complex [B][n]) before the loop's closing synchronisation
+  SolveStats run_loop(double tol, int32_t max_iter, int32_t prepare_adjoint, cudaStream_t s, double* d_final,
+                      double* d_v_out = nullptr);
   template <typename T>
   void ensure_loop_graph(const DevState& st);
   template <typename T>
