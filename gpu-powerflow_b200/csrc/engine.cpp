@@ -22,6 +22,7 @@
 #include <string>
 
 #include "kernels.hpp"
+#include "static_scratch.hpp"
 
 namespace cupf_b200 {
 
@@ -576,6 +577,11 @@ void Engine::ensure_workspace(int32_t B) {
     }
     d.front_scratch_elems = scratch;
     if (scratch) d.front_scratch.reserve(scratch * kWarp * es);
+    // The allocation-free entry point's static area: the runtime loads the
+    // module that holds it (and reserves its memory) at the first lookup of
+    // its address, so that lookup happens here, in a call that allocates,
+    // and never in the first allocation-free factorization.
+    static_front_scratch();
     d.Bp_cap = Bp;
     if (d.exec) {
       cudaGraphExecDestroy(d.exec);
@@ -1235,8 +1241,7 @@ SolveStats Engine::solve_batch_warm_device(const double* d_sbus, int64_t sbus_st
   cudaStream_t s = stream ? stream : d.own;
   use_scenario_ybus(nullptr, 0, B, s);
   const DevState st = d.state();
-  launch_seed_state(d.g, st, d_sbus, sbus_stride, d_v0, v0_stride, s);
-  launch_apply_warm(d.g, st, d_pred, pred_ld, d_scale, d_shift, s);
+  launch_seed_warm(d.g, st, d_sbus, sbus_stride, d_v0, v0_stride, d_pred, pred_ld, d_scale, d_shift, s);
   // a poor prediction may send a scenario to infinity: it is reported as not
   // converged (final mismatch = inf) instead of failing the whole batch
   struct Tolerate {
@@ -1247,7 +1252,7 @@ SolveStats Engine::solve_batch_warm_device(const double* d_sbus, int64_t sbus_st
   SolveStats out = factor_is_double()
                        ? run_loop<double>(tol, max_iter, prepare_adjoint, s, d_final_mismatch, d_v_out)
                        : run_loop<float>(tol, max_iter, prepare_adjoint, s, d_final_mismatch, d_v_out);
-  launches_ += 2;
+  launches_ += 1;
   return out;
 }
 

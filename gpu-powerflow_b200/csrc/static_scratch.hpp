@@ -10,10 +10,11 @@ namespace cupf_b200 {
 constexpr size_t kStaticFrontScratchBytes = size_t(8) << 20;
 
 // Device address of the area on the current device.  The first call on each
-// device looks the symbol up (cudaGetSymbolAddress, with that device current)
-// and caches it for the life of the process; later calls only read the
-// cache, which a cudaDeviceReset of that device makes stale.  Throws on
-// failure.
+// device looks the symbol up (cudaGetSymbolAddress, with that device current),
+// which loads the area's module and so reserves its memory, and caches the
+// address for the life of the process; later calls only read the cache,
+// which a cudaDeviceReset of that device makes stale.  Throws on failure.
+// The engine makes the first call when it allocates a workspace.
 void* static_front_scratch();
 
 }  // namespace cupf_b200

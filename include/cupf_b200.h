@@ -126,9 +126,12 @@ cls_status cls_factorize(cls_handle h, const void* values, int32_t value_type);
  * it rejects a batch whose front scratch exceeds 8 MiB (CLS_INVALID_VALUE,
  * message in cls_last_error).  Nothing has to be zeroed beforehand.  The area
  * is shared by all handles of the process on a device: calls must not
- * overlap in time.  The first call on each device looks the area's address
- * up (cudaGetSymbolAddress with that device current); make it before any
- * stream capture.  The address is cached for the life of the process: after
+ * overlap in time.  The regular call that sizes the handle's workspace
+ * looks the area's address up (cudaGetSymbolAddress with the handle's device
+ * current), which is when the runtime loads the area's module and reserves
+ * its memory, so not even the first call of this entry point does; make
+ * that regular call before any stream capture.  The address is cached for
+ * the life of the process: after
  * cudaDeviceReset on a device the cache is stale and this entry point must
  * not be used there again.  The launches use the built-in placement of the
  * dense fronts (not an autotuned one), which the 8 MiB bound refers to. */
