@@ -238,9 +238,11 @@ void launch_voltage_update(const DevGrid& g, const DevPlan& pl, const DevState& 
 void launch_seed_state(const DevGrid& g, const DevState& st, const double* sbus_c, long long sbus_stride,
                        const double* v0_c, long long v0_stride, cudaStream_t s);
 void launch_pack_voltage(const DevGrid& g, const DevState& st, double* v_c, cudaStream_t s);
-// warm start from a prediction pred[B][ld] in Jacobian-row order (fp32)
-void launch_apply_warm(const DevGrid& g, const DevState& st, const float* pred, long long ld, const float* scale,
-                       const float* shift, cudaStream_t s);
+// launch_seed_state with the state taken from a prediction pred[B][ld] in
+// Jacobian-row order (fp32) where it has rows: the warm start's seed
+void launch_seed_warm(const DevGrid& g, const DevState& st, const double* sbus_c, long long sbus_stride,
+                      const double* v0_c, long long v0_stride, const float* pred, long long ld, const float* scale,
+                      const float* shift, cudaStream_t s);
 // torch-style inputs: base injection [n], loads [B][n], flat start [n]; dtype float or double
 void launch_set_inputs_from_load(const DevGrid& g, const DevState& st, const void* base_re, const void* base_im,
                                  const void* load_p, const void* load_q, const void* va0, const void* vm0,

@@ -310,28 +310,66 @@ __global__ void k_voltage_update(DevGrid g, DevPlan pl, DevState st, const T* __
 // Layout conversions through a 32 x 32 shared tile: host arrays are
 // scenario-major [B][stride], the engine is bus-major [n][Bp].
 // Pad scenarios (B <= b < Bp) replicate scenario B - 1.
-// Warm start: overwrite the seeded angles / magnitudes with a prediction
-// given in Jacobian-row order (pred[b][row]: Va at the angle rows of the PV
-// and PQ buses, Vm at the magnitude rows of the PQ buses) and rebuild V.
-__global__ void k_apply_warm(DevGrid g, DevState st, const float* __restrict__ pred, long long ld,
-                             const float* __restrict__ scale, const float* __restrict__ shift) {
-  const int lane = threadIdx.x, wy = threadIdx.y;
-  const int Bp = st.Bp;
-  const int b = blockIdx.y * kWarp + lane;
-  const long long bb = b < st.B ? b : st.B - 1;
-  for (int i = blockIdx.x * kRows + wy; i < g.n_bus; i += gridDim.x * kRows) {
-    const int fa = g.bus_fa[i], fm = g.bus_fm[i];
-    if (fa < 0 && fm < 0) continue;
-    const size_t o = (size_t)i * Bp + b;
-    double va = st.va[o], vm = st.vm[o];
-    if (fa >= 0) va = (double)(scale ? pred[bb * ld + fa] * scale[fa] + shift[fa] : pred[bb * ld + fa]);
-    if (fm >= 0) vm = (double)(scale ? pred[bb * ld + fm] * scale[fm] + shift[fm] : pred[bb * ld + fm]);
+// ---------------------------------------------------------------------------
+// Seed of a warm-started solve in one pass: Sbus as k_seed_state converts it,
+// and the state from a prediction pred[b][row] in Jacobian-row order (fp32,
+// un-standardized as pred * scale + shift when scale is given): Va at the
+// angle rows of the PV and PQ buses, Vm at the magnitude rows of the PQ
+// buses, V0's angle and magnitude where the prediction has no row, and V
+// rebuilt from them (a bus the prediction does not touch keeps V0's value).
+// The inputs are read along the buses (a warp reads 32 buses of one
+// scenario, so the prediction's rows arrive in runs of consecutive columns)
+// and transposed through shared memory to the bus-major state.
+__global__ void k_seed_warm(DevGrid g, DevState st, const double* __restrict__ sbus_c, long long sbus_stride,
+                            const double* __restrict__ v0_c, long long v0_stride, const float* __restrict__ pred,
+                            long long ld, const float* __restrict__ scale, const float* __restrict__ shift) {
+  __shared__ double t[4][kWarp][kWarp + 1];  // s_re, s_im, va, vm
+  const int tx = threadIdx.x, ty = threadIdx.y;  // (32, 8)
+  const int bus0 = blockIdx.x * kWarp, b0 = blockIdx.y * kWarp;
+  const int bus = bus0 + tx;
+  const int fa = bus < g.n_bus ? g.bus_fa[bus] : -1, fm = bus < g.n_bus ? g.bus_fm[bus] : -1;
+  float sa = 1.f, ha = 0.f, sm = 1.f, hm = 0.f;
+  if (scale) {
+    if (fa >= 0) sa = scale[fa], ha = shift[fa];
+    if (fm >= 0) sm = scale[fm], hm = shift[fm];
+  }
+  for (int r = ty; r < kWarp; r += kRows) {
+    const long long bb = min(b0 + r, st.B - 1);
+    if (bus < g.n_bus) {
+      const size_t so = ((size_t)bb * sbus_stride + bus) * 2, vo = ((size_t)bb * v0_stride + bus) * 2;
+      t[0][r][tx] = sbus_c[so];
+      t[1][r][tx] = sbus_c[so + 1];
+      const double vr = v0_c[vo], vi = v0_c[vo + 1];
+      double va = 0.0, vm = 0.0;
+      if (fa < 0) va = atan2(vi, vr);
+      if (fm < 0) vm = hypot(vr, vi);
+      if (fa >= 0) va = (double)(scale ? pred[bb * ld + fa] * sa + ha : pred[bb * ld + fa]);
+      if (fm >= 0) vm = (double)(scale ? pred[bb * ld + fm] * sm + hm : pred[bb * ld + fm]);
+      t[2][r][tx] = va;
+      t[3][r][tx] = vm;
+    }
+  }
+  __syncthreads();
+  for (int r = ty; r < kWarp; r += kRows) {
+    const int i = bus0 + r;
+    if (i >= g.n_bus) continue;
+    const bool predicted = g.bus_fa[i] >= 0 || g.bus_fm[i] >= 0;
+    const size_t o = (size_t)i * st.Bp + b0 + tx;
+    const double va = t[2][tx][r], vm = t[3][tx][r];
+    st.s_re[o] = t[0][tx][r];
+    st.s_im[o] = t[1][tx][r];
     st.va[o] = va;
     st.vm[o] = vm;
-    double sn, cs;
-    sincos(va, &sn, &cs);
-    st.v_re[o] = vm * cs;
-    st.v_im[o] = vm * sn;
+    if (predicted) {
+      double sn, cs;
+      sincos(va, &sn, &cs);
+      st.v_re[o] = vm * cs;
+      st.v_im[o] = vm * sn;
+    } else {  // a slack bus (no Jacobian row; few per grid): V0 read again
+      const size_t vo = ((size_t)min(b0 + tx, st.B - 1) * v0_stride + i) * 2;
+      st.v_re[o] = v0_c[vo];
+      st.v_im[o] = v0_c[vo + 1];
+    }
   }
 }
 
@@ -719,9 +757,11 @@ void launch_seed_state(const DevGrid& g, const DevState& st, const double* sbus_
   k_seed_state<<<grid, dim3(kWarp, kRows), 0, s>>>(g, st, sbus_c, sbus_stride, v0_c, v0_stride);
 }
 
-void launch_apply_warm(const DevGrid& g, const DevState& st, const float* pred, long long ld, const float* scale,
-                       const float* shift, cudaStream_t s) {
-  k_apply_warm<<<rows_grid(g.n_bus, st.Bp), dim3(kWarp, kRows), 0, s>>>(g, st, pred, ld, scale, shift);
+void launch_seed_warm(const DevGrid& g, const DevState& st, const double* sbus_c, long long sbus_stride,
+                      const double* v0_c, long long v0_stride, const float* pred, long long ld, const float* scale,
+                      const float* shift, cudaStream_t s) {
+  dim3 grid((g.n_bus + kWarp - 1) / kWarp, st.Bp / kWarp);
+  k_seed_warm<<<grid, dim3(kWarp, kRows), 0, s>>>(g, st, sbus_c, sbus_stride, v0_c, v0_stride, pred, ld, scale, shift);
 }
 
 void launch_pack_voltage(const DevGrid& g, const DevState& st, double* v_c, cudaStream_t s) {
