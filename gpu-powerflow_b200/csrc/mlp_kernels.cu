@@ -152,9 +152,15 @@ __global__ void __launch_bounds__(kThreads, MINB)
   tc_fence_after();
   const uint32_t tmem = *tslot;
   bool ok = true;
+  // programmatic dependent launch: the next kernel on the stream may start
+  // its own set-up now; this CTA's first read of memory that an earlier
+  // kernel writes (the producer's first load) waits for that kernel to
+  // finish, and every store here follows that load
+  asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
 
   if (threadIdx.x == 0) {
     // producer: stage s holds k-block kb; refill it once the MMAs of kb - STAGES are done
+    asm volatile("griddepcontrol.wait;\n" ::: "memory");
     int issued = 0;
     for (int kb = 0; kb < (g.stall_loads ? 0 : nk); ++kb) {
       const int s = kb % STAGES;
@@ -307,26 +313,24 @@ __global__ void k_standardize(const float* __restrict__ raw, const float* __rest
 __global__ void k_load_features(const double* __restrict__ sbus, long long sbus_stride, const double* __restrict__ sgen,
                                 const float* __restrict__ extra, int n, int n_extra, const float* __restrict__ mean,
                                 const float* __restrict__ inv_std, __nv_bfloat16* __restrict__ x, long long ldx,
-                                int B, int rows, int width) {
+                                int B, int width) {
+  // block y = one row of x (scenario r; rows past B repeat the last one).  A
+  // thread reads bus k's complex injection once (16 bytes) and writes both
+  // of its features, P at column k and Q at column n + k.
+  const long long r = blockIdx.y;
+  const long long b = r < B ? r : B - 1;
+  const double2* s = reinterpret_cast<const double2*>(sbus) + b * sbus_stride;
+  const double2* sg = reinterpret_cast<const double2*>(sgen);
+  __nv_bfloat16* xr = x + r * ldx;
   const int n_in = 2 * n + n_extra;
-  const long long total = (long long)rows * width;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
-    const int k = (int)(i % width);
-    const long long r = i / width;
-    const long long b = r < B ? r : B - 1;
-    float v = 0.0f;
-    if (k < n_in) {
-      double f;
-      if (k < n)
-        f = sgen[2 * k] - sbus[2 * (b * sbus_stride + k)];
-      else if (k < 2 * n)
-        f = sgen[2 * (k - n) + 1] - sbus[2 * (b * sbus_stride + k - n) + 1];
-      else
-        f = (double)extra[k - 2 * n];
-      v = ((float)f - mean[k]) * inv_std[k];
-    }
-    x[r * ldx + k] = __float2bfloat16(v);
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const double2 v = s[k], g = sg[k];
+    const double fp = g.x - v.x, fq = g.y - v.y;
+    xr[k] = __float2bfloat16(((float)fp - mean[k]) * inv_std[k]);
+    xr[n + k] = __float2bfloat16(((float)fq - mean[n + k]) * inv_std[n + k]);
   }
+  for (int k = 2 * n + blockIdx.x * blockDim.x + threadIdx.x; k < width; k += gridDim.x * blockDim.x)
+    xr[k] = __float2bfloat16(k < n_in ? ((float)(double)extra[k - 2 * n] - mean[k]) * inv_std[k] : 0.0f);
 }
 
 // mean-squared-error gradient on the first n_out columns:
@@ -461,7 +465,18 @@ void launch_shape(const void* A, long long lda, int ka_cols, const void* B, long
   const CUtensorMap ta = make_map(A, g.M, ka_cols, lda, kBM), tb = make_map(B, g.N, g.K, ldb, BN);
   g.spin_limit = g_spin_limit.load();
   g.stall_loads = g_stall_loads.load();
-  k_gemm_bf16<BN, STAGES, MINB><<<dim3(g.N / BN, g.M / kBM), kThreads, gemm_smem<BN, STAGES>(), stream>>>(ta, tb, g);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(g.N / BN, g.M / kBM);
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes = gemm_smem<BN, STAGES>();
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;  // overlap the previous kernel's tail
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  const cudaError_t e = cudaLaunchKernelEx(&cfg, k_gemm_bf16<BN, STAGES, MINB>, ta, tb, g);
+  if (e != cudaSuccess) throw std::runtime_error(std::string("gemm launch: ") + cudaGetErrorString(e));
 }
 
 // A has ka_cols columns (== g.K unless A's k-blocks wrap); M, N multiples of 128
@@ -581,9 +596,13 @@ int mlp_load_features(const double* sbus, long long sbus_stride, const double* s
       throw std::invalid_argument("mlp_load_features: null pointer");
     if (n <= 0 || n_extra < 0 || B <= 0 || rows < B || width < 2 * n + n_extra || ldx < width || sbus_stride < n)
       throw std::invalid_argument("mlp_load_features: inconsistent sizes");
-    k_load_features<<<grid1d((long long)rows * width), 256, 0, static_cast<cudaStream_t>(stream)>>>(
-        sbus, sbus_stride, sgen, extra, n, n_extra, mean, inv_std, static_cast<__nv_bfloat16*>(x), ldx, B, rows,
-        width);
+    if (rows > 65535) throw std::invalid_argument("mlp_load_features: more than 65535 rows");
+    if ((reinterpret_cast<uintptr_t>(sbus) | reinterpret_cast<uintptr_t>(sgen)) & 15)
+      throw std::invalid_argument("mlp_load_features: sbus and sgen must be 16-byte aligned (complex128 elements)");
+    const int per_row = std::max(n, width - 2 * n);
+    const dim3 grid((unsigned)std::min((per_row + 255) / 256, 8), (unsigned)rows);
+    k_load_features<<<grid, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        sbus, sbus_stride, sgen, extra, n, n_extra, mean, inv_std, static_cast<__nv_bfloat16*>(x), ldx, B, width);
   });
 }
 

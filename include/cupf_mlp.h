@@ -78,7 +78,8 @@ int mlp_standardize(const float* raw, const float* mean, const float* inv_std, v
  * x[r][k] = bf16((f_k - mean[k]) * inv_std[k]) with f_k = Re(sgen_k - S_rk)
  * for k < n, Im(sgen - S) at k - n for n <= k < 2n, extra[k - 2n] for the
  * next n_extra columns; 0 up to width.  Rows B <= r < rows repeat row B - 1.
- * x has row stride ldx >= width. */
+ * x has row stride ldx >= width; sbus and sgen start on 16-byte boundaries
+ * (whole complex128 elements); rows <= 65535. */
 int mlp_load_features(const double* sbus, long long sbus_stride, const double* sgen, const float* extra, int n,
                       int n_extra, const float* mean, const float* inv_std, void* x, long long ldx, int B, int rows,
                       int width, void* stream);
