@@ -12,20 +12,26 @@
 //                 tcgen05.mma (M = 128, N = BN, K = 16 per instruction) into
 //                 a BN-column TMEM accumulator, and the four warps read the
 //                 accumulator back (tcgen05.ld 32x32b) for a fused epilogue.
-//                 Two shapes: BN = 128 with a 3-stage ring and two CTAs per
-//                 SM when the 128 x 128 tiles fill the 148 SMs (the second
-//                 CTA's loads overlap the first one's MMAs), else BN = 64
-//                 tiles, twice as many CTAs for the narrow 1024-wide
-//                 hidden layers.  Epilogues:
+//                 Three shapes: BN = 128 with a 3-stage ring and two CTAs
+//                 per SM when the 128 x 128 tiles fill the 148 SMs (the
+//                 second CTA's loads overlap the first one's MMAs); BN = 224
+//                 with a 4-stage ring, one CTA per SM, when those tiles fill
+//                 80-100 % of the SMs in a single wave (the output layer:
+//                 8 x 17 tiles instead of 8 x 29 in 1.6 waves; a partial last
+//                 column tile reads zeros past N and stores nothing there);
+//                 else BN = 64 tiles, twice as many CTAs for the narrow
+//                 1024-wide hidden layers.  Epilogues:
 //                   EPI_F32        out = acc                         (fp32)
 //                   EPI_BIAS_F32   out = acc + bias                  (fp32)
 //                   EPI_BIAS_GELU  z = acc + bias; aux = z; out = gelu(z)  (bf16)
 //                   EPI_DGELU      out = acc * gelu'(aux)            (bf16)
-//                 With a_kblocks > 0 the A tile of k-block kb is A's k-block
-//                 kb mod a_kblocks: B = [B_hi | B_lo] (2K columns) against A
+//                 With a_kblocks > 0, B = [B_hi | B_lo] (2K columns) against A
 //                 (K columns) gives A (B_hi + B_lo)^T in one accumulator,
 //                 the split-weight output layer (bf16 hi + bf16 lo carry
-//                 about 16 mantissa bits of the fp32 weights).
+//                 about 16 mantissa bits of the fp32 weights): on the
+//                 128 x 224 shape each stage holds A's k-block with both of
+//                 its B k-blocks (A read once); on the others the A tile of
+//                 k-block kb is A's k-block kb mod a_kblocks.
 //                 Every mbarrier wait is bounded.  On a timeout the kernel
 //                 raises the error flag, stops issuing, waits (bounded) for
 //                 the TMA loads and MMAs it already issued, writes NaN into
@@ -61,10 +67,11 @@ using namespace tc;
 constexpr int kBM = 128, kBK = 64, kThreads = 128;
 constexpr uint32_t kTileA = kBM * kBK * 2;     // 16 KB A tile per stage
 
-// shared memory of one CTA: 1 KB alignment slack, the ring, the barriers
-template <int BN, int STAGES>
+// shared memory of one CTA: 1 KB alignment slack, the ring (an A tile and NB
+// B tiles per stage), the barriers
+template <int BN, int STAGES, int NB = 1>
 constexpr size_t gemm_smem() {
-  return 1024 + (size_t)STAGES * (kTileA + (uint32_t)BN * kBK * 2) + 256;  // + barriers, TMEM slot, fail flag
+  return 1024 + (size_t)STAGES * (kTileA + (uint32_t)NB * BN * kBK * 2) + 256;  // + barriers, TMEM slot, fail flag
 }
 
 enum { EPI_F32 = 0, EPI_BIAS_F32 = 1, EPI_BIAS_GELU = 2, EPI_DGELU = 3 };
@@ -119,16 +126,28 @@ struct GemmArgs {
   int stall_loads;       // failure-path test: the producer issues no loads, so the MMA thread's wait runs out
 };
 
-template <int BN, int STAGES, int MINB>
+// tensor-memory columns of a BN-column accumulator (a power of two, >= 32)
+template <int BN>
+__host__ __device__ constexpr uint32_t tmem_cols() {
+  return BN <= 32 ? 32u : BN <= 64 ? 64u : BN <= 128 ? 128u : 256u;
+}
+
+// NB = 2 (split weights, a_kblocks > 0): each stage holds A's k-block kb and
+// both B k-blocks that multiply it, kb (hi) and a_kblocks + kb (lo), so A is
+// read once for the two products; NB = 1 with a_kblocks > 0 reads A's
+// k-blocks twice instead (k-block kb of B against A's kb mod a_kblocks).
+template <int BN, int STAGES, int MINB, int NB = 1>
 __global__ void __launch_bounds__(kThreads, MINB)
     k_gemm_bf16(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, GemmArgs g) {
+  static_assert(BN % 32 == 0 && BN >= 32 && BN <= 256, "accumulator width: 32..256 columns in steps of 32");
+  static_assert(NB == 1 || NB == 2, "one B tile per stage, or the hi and lo tiles of split weights");
   constexpr uint32_t kTileB = (uint32_t)BN * kBK * 2;
   extern __shared__ unsigned char smem_raw[];
   unsigned char* base =
       reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   unsigned char* sA = base;
-  unsigned char* sB = base + STAGES * kTileA;
-  uint64_t* full = reinterpret_cast<uint64_t*>(base + STAGES * (kTileA + kTileB));
+  unsigned char* sB = base + STAGES * kTileA;  // [stage][NB] tiles
+  uint64_t* full = reinterpret_cast<uint64_t*>(base + STAGES * (kTileA + NB * kTileB));
   uint64_t* empty = full + STAGES;
   uint64_t* done = empty + STAGES;
   uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
@@ -136,7 +155,7 @@ __global__ void __launch_bounds__(kThreads, MINB)
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int m0 = blockIdx.y * kBM, n0 = blockIdx.x * BN;
-  const int nk = g.K / kBK;
+  const int nk = NB == 2 ? g.a_kblocks : g.K / kBK;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
@@ -147,7 +166,7 @@ __global__ void __launch_bounds__(kThreads, MINB)
     *s_fail = 0;
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
-  if (warp == 0) tmem_alloc(tslot, BN);
+  if (warp == 0) tmem_alloc(tslot, tmem_cols<BN>());
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tslot;
@@ -168,10 +187,12 @@ __global__ void __launch_bounds__(kThreads, MINB)
         ok = false;
         break;
       }
-      mbar_expect_tx(full + s, kTileA + kTileB);
-      const int ka = g.a_kblocks > 0 ? kb % g.a_kblocks : kb;
+      mbar_expect_tx(full + s, kTileA + NB * kTileB);
+      const int ka = NB == 1 && g.a_kblocks > 0 ? kb % g.a_kblocks : kb;
       tma_load_2d(sA + s * kTileA, &ta, ka * kBK, m0, full + s);
-      tma_load_2d(sB + s * kTileB, &tb, kb * kBK, n0, full + s);
+#pragma unroll
+      for (int h = 0; h < NB; ++h)
+        tma_load_2d(sB + (s * NB + h) * kTileB, &tb, (kb + h * g.a_kblocks) * kBK, n0, full + s);
       issued = kb + 1;
     }
     if (!ok) {
@@ -191,10 +212,14 @@ __global__ void __launch_bounds__(kThreads, MINB)
         break;
       }
       tc_fence_after();
-      const uint64_t da = smem_desc_sw128(sA + s * kTileA), db = smem_desc_sw128(sB + s * kTileB);
+      const uint64_t da = smem_desc_sw128(sA + s * kTileA);
 #pragma unroll
-      for (int k = 0; k < kBK / 16; ++k)  // K = 16 per instruction: advance 32 bytes inside the swizzled row
-        tc_mma(tmem, da + (uint64_t)(2 * k), db + (uint64_t)(2 * k), idesc, (kb > 0 || k > 0) ? 1u : 0u);
+      for (int h = 0; h < NB; ++h) {
+        const uint64_t db = smem_desc_sw128(sB + (s * NB + h) * kTileB);
+#pragma unroll
+        for (int k = 0; k < kBK / 16; ++k)  // K = 16 per instruction: advance 32 bytes inside the swizzled row
+          tc_mma(tmem, da + (uint64_t)(2 * k), db + (uint64_t)(2 * k), idesc, (kb > 0 || h > 0 || k > 0) ? 1u : 0u);
+      }
       tc_commit(empty + s);
     }
     tc_commit(done);  // arrives once every MMA issued above has completed
@@ -219,7 +244,7 @@ __global__ void __launch_bounds__(kThreads, MINB)
     // non-finite prediction as missing and solves that scenario from flat
     // start); the host reads the raised flag
     const int row = m0 + warp * 32 + lane;
-    for (int c = 0; c < BN; ++c) {
+    for (int c = 0; c < BN && n0 + c < g.N; ++c) {
       if (g.epi == EPI_F32 || g.epi == EPI_BIAS_F32)
         static_cast<float*>(g.out)[(size_t)row * g.ldo + n0 + c] = __int_as_float(0x7fc00000);
       else
@@ -231,7 +256,7 @@ __global__ void __launch_bounds__(kThreads, MINB)
   } else {
     const int row = m0 + warp * 32 + lane;
     const uint32_t tl = tmem + ((uint32_t)(warp * 32) << 16);
-    for (int c0 = 0; c0 < BN; c0 += 32) {
+    for (int c0 = 0; c0 < BN && n0 + c0 < g.N; c0 += 32) {  // (N - n0 is a multiple of 32)
       float v[32];
       tmem_ld32(tl + (uint32_t)c0, v);
       const int col = n0 + c0;
@@ -271,7 +296,7 @@ __global__ void __launch_bounds__(kThreads, MINB)
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 0) tmem_dealloc(tmem, BN);
+  if (warp == 0) tmem_dealloc(tmem, tmem_cols<BN>());
 }
 
 // ---- element-wise / reduction kernels ----
@@ -435,15 +460,21 @@ int* error_flag() {
 std::atomic<long long> g_spin_limit{kSpinLimit};
 std::atomic<int> g_stall_loads{0};
 
-// the two tile shapes: wide grids, and grids with fewer 128 x 128 tiles than SMs
+// the tile shapes: wide grids; grids with fewer 128 x 128 tiles than SMs;
+// and grids whose 128 x 224 tiles fill 80-100 % of the SMs in one wave (one
+// CTA per SM, a 4-stage ring of 44 KB stages), where 128 x 128 tiles two per
+// SM would leave a partly filled second wave (the network's output layer)
 constexpr int kWideBN = 128, kWideStages = 3, kWideMinBlocks = 2;
 constexpr int kNarrowBN = 64, kNarrowStages = 4, kNarrowMinBlocks = 2;
+constexpr int kTallBN = 224, kTallStages = 4, kTallMinBlocks = 1;
+constexpr int kTallSplitStages = 3;  // stages of A + hi + lo tiles (72 KB each)
 constexpr int kSMs = 148;
 
-template <int BN, int STAGES, int MINB>
+template <int BN, int STAGES, int MINB, int NB = 1>
 void set_smem_attribute() {
-  const cudaError_t e = cudaFuncSetAttribute(k_gemm_bf16<BN, STAGES, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)gemm_smem<BN, STAGES>());
+  const cudaError_t e = cudaFuncSetAttribute(k_gemm_bf16<BN, STAGES, MINB, NB>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)gemm_smem<BN, STAGES, NB>());
   if (e != cudaSuccess) throw std::runtime_error(std::string("gemm smem attribute: ") + cudaGetErrorString(e));
 }
 
@@ -456,26 +487,28 @@ void configure_gemm() {
   if (done[dev]) return;
   set_smem_attribute<kWideBN, kWideStages, kWideMinBlocks>();
   set_smem_attribute<kNarrowBN, kNarrowStages, kNarrowMinBlocks>();
+  set_smem_attribute<kTallBN, kTallStages, kTallMinBlocks>();
+  set_smem_attribute<kTallBN, kTallSplitStages, kTallMinBlocks, 2>();
   done[dev] = true;
 }
 
-template <int BN, int STAGES, int MINB>
+template <int BN, int STAGES, int MINB, int NB = 1>
 void launch_shape(const void* A, long long lda, int ka_cols, const void* B, long long ldb, GemmArgs g,
                   cudaStream_t stream) {
   const CUtensorMap ta = make_map(A, g.M, ka_cols, lda, kBM), tb = make_map(B, g.N, g.K, ldb, BN);
   g.spin_limit = g_spin_limit.load();
   g.stall_loads = g_stall_loads.load();
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(g.N / BN, g.M / kBM);
+  cfg.gridDim = dim3((g.N + BN - 1) / BN, g.M / kBM);  // a partial last column tile reads zeros past N
   cfg.blockDim = dim3(kThreads);
-  cfg.dynamicSmemBytes = gemm_smem<BN, STAGES>();
+  cfg.dynamicSmemBytes = gemm_smem<BN, STAGES, NB>();
   cfg.stream = stream;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;  // overlap the previous kernel's tail
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  const cudaError_t e = cudaLaunchKernelEx(&cfg, k_gemm_bf16<BN, STAGES, MINB>, ta, tb, g);
+  const cudaError_t e = cudaLaunchKernelEx(&cfg, k_gemm_bf16<BN, STAGES, MINB, NB>, ta, tb, g);
   if (e != cudaSuccess) throw std::runtime_error(std::string("gemm launch: ") + cudaGetErrorString(e));
 }
 
@@ -483,7 +516,14 @@ void launch_shape(const void* A, long long lda, int ka_cols, const void* B, long
 void launch_gemm(const void* A, long long lda, int ka_cols, const void* B, long long ldb, const GemmArgs& g,
                  cudaStream_t stream) {
   configure_gemm();
-  if ((long long)(g.M / kBM) * (g.N / 128) >= kSMs)
+  const long long tall = (long long)(g.M / kBM) * ((g.N + kTallBN - 1) / kTallBN);
+  if ((long long)(g.M / kBM) * (g.N / 128) >= kSMs && tall <= kSMs && 5 * tall >= 4 * kSMs) {
+    if (g.a_kblocks > 0)
+      launch_shape<kTallBN, kTallSplitStages, kTallMinBlocks, 2>(A, lda, ka_cols, B, ldb, g, stream);
+    else
+      launch_shape<kTallBN, kTallStages, kTallMinBlocks>(A, lda, ka_cols, B, ldb, g, stream);
+  }
+  else if ((long long)(g.M / kBM) * (g.N / 128) >= kSMs)
     launch_shape<kWideBN, kWideStages, kWideMinBlocks>(A, lda, ka_cols, B, ldb, g, stream);
   else
     launch_shape<kNarrowBN, kNarrowStages, kNarrowMinBlocks>(A, lda, ka_cols, B, ldb, g, stream);

@@ -142,12 +142,13 @@ class HostPipeline:
                     d.set()
 
         def downloader() -> None:
-            # downloads in batch order, each after its batch's solve
+            # downloads in batch order, each after its batch's solve; after a
+            # failure, the batches solved before it still land
             try:
                 t.cuda.set_device(self.dev)
                 for k in range(K):
                     down_ready[k].wait()
-                    if failure or done_ev[k] is None:
+                    if done_ev[k] is None:
                         return
                     ev, V, fm = done_ev[k]
                     self.down.wait_event(ev)
@@ -196,6 +197,16 @@ class HostPipeline:
                 for d in down_ready:
                     d.set()
             dl.join()
+            # after a failure the downloader stops at the first batch without
+            # a result; every batch whose solve did finish still lands
+            for k in range(K):
+                if done_ev[k] is not None:
+                    ev, V, fm = done_ev[k]
+                    self.down.wait_event(ev)
+                    with t.cuda.stream(self.down):
+                        V_out[k].copy_(V, non_blocking=True)
+                        fm_out[k].copy_(fm, non_blocking=True)
+                    done_ev[k] = None
         self.down.synchronize()  # no copy into the caller's buffers is left running
         if failure:
             raise failure[0]

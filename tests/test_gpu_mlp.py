@@ -20,8 +20,11 @@ def _rel(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
 
 
-# 128 x 64 tiles below 148 tiles of 128 x 128, else 128 x 128 tiles two per SM
-@pytest.mark.parametrize("M,N,K", [(128, 128, 64), (256, 384, 1024), (384, 128, 4480), (1280, 2048, 320)])
+# 128 x 64 tiles below 148 tiles of 128 x 128; 128 x 224 tiles when those fill
+# 80-100 % of the SMs in one wave (1024 x 3712: 8 x 17 tiles, the last column
+# tile partial); else 128 x 128 tiles two per SM
+@pytest.mark.parametrize("M,N,K", [(128, 128, 64), (256, 384, 1024), (384, 128, 4480), (1280, 2048, 320),
+                                   (1024, 3712, 1024)])
 def test_gemm_f32_matches_torch(torch, M, N, K):
     from cupf.warm_start import MLP, EPI_F32, EPI_BIAS_F32
 
@@ -39,7 +42,7 @@ def test_gemm_f32_matches_torch(torch, M, N, K):
     assert net.error_flag() == 0
 
 
-@pytest.mark.parametrize("M,N,K", [(128, 128, 256), (1280, 2048, 320)])
+@pytest.mark.parametrize("M,N,K", [(128, 128, 256), (1280, 2048, 320), (1024, 3712, 320)])
 def test_gemm_wait_timeout_reports_and_recovers(torch, M, N, K):
     """The GEMM's bounded waits, made to run out on the host's request (the
     producer issues no tile loads, the wait limit is 1,000 polls): the kernel
@@ -308,7 +311,7 @@ def test_device_entry_points_follow_the_callers_stream(torch):
     assert bool((fmw <= 1e-6).all()) and itw <= 2
 
 
-@pytest.mark.parametrize("M,N,K", [(128, 128, 64), (256, 384, 5504), (1024, 3712, 1024)])
+@pytest.mark.parametrize("M,N,K", [(128, 128, 64), (256, 384, 5504), (1024, 3712, 1024), (1024, 3712, 5504)])
 def test_split_gemm_carries_the_fp32_weights(torch, M, N, K):
     """mlp_gemm_bf16_split: A (W_hi + W_lo)^T + bias within fp32 accumulation
     of the fp64 product with the fp32 weights, where the bf16 weights alone
