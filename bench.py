@@ -670,37 +670,39 @@ def run_extras(args, dev) -> dict:
                                   "final-state factors"}
     # single systems: the 118-bus grid at batch 1 (the reference's CPU-runnable
     # case), FP64 flat start, one graph per solve, device time per solve and
-    # through the host API (Sbus and V0 in, V out)
-    g1 = grids.grid_118()
-    s1 = {}
-    for name, comp in (("fp64", cupf.ComputePolicy.FP64), ("mixed", cupf.ComputePolicy.Mixed)):
-        o = cupf.NewtonOptions()
-        o.backend = cupf.BackendKind.CUDA
-        o.compute = comp
-        o.custom.serial_nd = True
-        o.use_cuda_graph = True
-        sv = cupf.NewtonSolver(o)
-        sv.initialize(g1.indptr, g1.indices, g1.data, g1.n_bus, g1.n_bus, g1.pv, g1.pq)
-        S1 = torch.tensor(g1.scenarios(1, seed=5), device=dev)
-        V1 = torch.tensor(g1.flat_start(1), device=dev)
-        sh, vh = g1.scenarios(1, seed=5), g1.flat_start(1)
-        for _ in range(5):
-            sv.solve_batch_device(S1, V1, config=cfg)
-            sv.solve_batch(g1.indptr, g1.indices, g1.data, g1.n_bus, g1.n_bus, sh, vh, g1.pv, g1.pq, cfg)
-        ts, th = [], []
-        for _ in range(50):
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-            _, fm1, it1 = sv.solve_batch_device(S1, V1, config=cfg)
-            e1.record()
-            e1.synchronize()
-            ts.append(e0.elapsed_time(e1))
-            t0 = time.perf_counter()
-            r1 = sv.solve_batch(g1.indptr, g1.indices, g1.data, g1.n_bus, g1.n_bus, sh, vh, g1.pv, g1.pq, cfg)
-            th.append((time.perf_counter() - t0) * 1e3)
-        s1[name] = {"device_ms": round(statistics.median(ts), 4), "host_api_ms": round(statistics.median(th), 4),
-                    "iterations": int(it1), "converged": bool(r1.converged_numpy.all())}
-    out["c1_118_batch1"] = {**s1, "method": "batch of 1 padded to one 32-scenario lane group; median of 50 solves"}
+    # through the host API (Sbus and V0 in, V out); the 118-bus grid (C1) and,
+    # for the reference's published batch-1 figure, the 2,000-bus grid
+    for key, make in (("c1_118_batch1", grids.grid_118), ("c2_2000_batch1", grids.grid_2000)):
+        g1 = make()
+        s1 = {}
+        for name, comp in (("fp64", cupf.ComputePolicy.FP64), ("mixed", cupf.ComputePolicy.Mixed)):
+            o = cupf.NewtonOptions()
+            o.backend = cupf.BackendKind.CUDA
+            o.compute = comp
+            o.custom.serial_nd = True
+            o.use_cuda_graph = True
+            sv = cupf.NewtonSolver(o)
+            sv.initialize(g1.indptr, g1.indices, g1.data, g1.n_bus, g1.n_bus, g1.pv, g1.pq)
+            S1 = torch.tensor(g1.scenarios(1, seed=5), device=dev)
+            V1 = torch.tensor(g1.flat_start(1), device=dev)
+            sh, vh = g1.scenarios(1, seed=5), g1.flat_start(1)
+            for _ in range(5):
+                sv.solve_batch_device(S1, V1, config=cfg)
+                sv.solve_batch(g1.indptr, g1.indices, g1.data, g1.n_bus, g1.n_bus, sh, vh, g1.pv, g1.pq, cfg)
+            ts, th = [], []
+            for _ in range(50):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                _, fm1, it1 = sv.solve_batch_device(S1, V1, config=cfg)
+                e1.record()
+                e1.synchronize()
+                ts.append(e0.elapsed_time(e1))
+                t0 = time.perf_counter()
+                r1 = sv.solve_batch(g1.indptr, g1.indices, g1.data, g1.n_bus, g1.n_bus, sh, vh, g1.pv, g1.pq, cfg)
+                th.append((time.perf_counter() - t0) * 1e3)
+            s1[name] = {"device_ms": round(statistics.median(ts), 4), "host_api_ms": round(statistics.median(th), 4),
+                        "iterations": int(it1), "converged": bool(r1.converged_numpy.all())}
+        out[key] = {**s1, "method": "batch of 1 padded to one 32-scenario lane group; median of 50 solves"}
     return out
 
 

@@ -55,6 +55,7 @@ EngineConfig engine_config(const cls_config& c, int32_t compute, int32_t use_gra
   e.par_nd_base_large = c.parallel_nd_base_large > 0 ? c.parallel_nd_base_large : 20000;
   e.wide_min_front = c.wide_min_front > 0 ? c.wide_min_front : 65;
   e.tc_min_front = c.tc_min_front;
+  e.batch1_schedule = c.batch1_schedule;
   e.use_cuda_graph = use_graph;
   return e;
 }
@@ -184,7 +185,8 @@ cls_status cls_create(const cls_config* config, cls_handle* out) {
   if ((c.matching != 0 && c.matching != 1) || c.max_panel_width < 1 || c.max_panel_width > 8 ||
       (c.autotune != 0 && c.autotune != 1) || c.parallel_nd_depth < 0 || c.parallel_nd_base_small < 0 ||
       c.parallel_nd_base_large < 0 || c.wide_min_front < 0 || c.wide_min_front > 65 || c.tc_min_front < 0 ||
-      c.precision < CLS_PRECISION_FP64 || c.precision > CLS_PRECISION_TF32)
+      (c.batch1_schedule != 0 && c.batch1_schedule != 1) || c.precision < CLS_PRECISION_FP64 ||
+      c.precision > CLS_PRECISION_TF32)
     return CLS_INVALID_VALUE;
   auto* h = new (std::nothrow) cls_solver_s();
   if (!h) return CLS_ALLOCATION_FAILED;
@@ -391,6 +393,8 @@ pf_status pf_create(const pf_options* options, pf_handle* out) {
       throw std::invalid_argument("NewtonSolver: the parallel nested-dissection parameters must not be negative");
     if (o.custom.wide_min_front < 0 || o.custom.wide_min_front > 65 || o.custom.tc_min_front < 0)
       throw std::invalid_argument("NewtonSolver: wide_min_front must be in [0, 65] and tc_min_front non-negative");
+    if (o.custom.batch1_schedule != 0 && o.custom.batch1_schedule != 1)
+      throw std::invalid_argument("NewtonSolver: batch1_schedule must be 0 (single-system kernel) or 1 (lane kernels)");
     if (o.custom.precision < CLS_PRECISION_FP64 || o.custom.precision > CLS_PRECISION_TF32)
       throw std::invalid_argument("NewtonSolver: unknown custom solver precision");
     if (o.cuda_jacobian < PF_JACOBIAN_EDGE || o.cuda_jacobian > PF_JACOBIAN_VERTEX_WARP)

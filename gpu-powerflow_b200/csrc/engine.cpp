@@ -105,6 +105,9 @@ struct Engine::Impl {
   int bw_first = 0, bw_nlev = 0;
   LevelLaunch bw_top;
   DBuf bw_bounds;
+  // the front tree of the single-system factorization launch (SingleTree)
+  DBuf tree_parent, tree_nchild, tree_e0, tree_leaves, tree_done;
+  int tree_max_fsz = 0, tree_list_cap = 0, tree_leaf_count = 0;
   int64_t tv_total = 0;
   DevGrid g;
   DevPlan pl;
@@ -148,7 +151,8 @@ struct Engine::Impl {
   LoopCtl* h_ctl = nullptr;    // pinned
   // batch size and precision the factor and backward launches were tuned for
   int tuned_Bp = -1, tuned_bw_Bp = -1;
-  bool tuned_double = false, tuned_bw_double = false;
+  bool tuned_double = false, tuned_bw_double = false, tuned_single = false;
+  bool graph_single = false;  // the graph's factor launches use the single-system schedule
   void invalidate_graph() {
     if (exec) cudaGraphExecDestroy(exec);
     exec = nullptr;
@@ -199,6 +203,17 @@ bool Engine::factor_is_double() const {
 }
 
 bool Engine::tf32_factors() const { return cfg_.factor_precision == kFactorTF32 && !factor_is_double(); }
+
+bool Engine::single_system() const { return cfg_.batch1_schedule == 0 && d_->B == 1; }
+
+// The single-system factorization as one tree launch: batch 1, no
+// tensor-core launch among the levels, every front and list in shared memory.
+bool Engine::single_tree(size_t elem_bytes) const {
+  if (!single_system()) return false;
+  for (const auto& lv : d_->levels)
+    if (lv.tier == 2) return false;
+  return single_smem_bytes(d_->tree_max_fsz, d_->tree_list_cap, elem_bytes) <= kSmemLimit;
+}
 
 void Engine::assign_tiers(int tc_min) {
   const int wide_min = std::min(cfg_.wide_min_front > 0 ? cfg_.wide_min_front : kWideFrontRows, kWideFrontRows);
@@ -440,6 +455,39 @@ void Engine::upload_plan() {
     d.fe_src.upload(psrc);
     d.fe_dst.upload(pdst);
   }
+  // the front tree in level order for the single-system launch: each front's
+  // parent and child count (the assembly's children are the tree's), and
+  // where its list starts in the padded lists
+  {
+    const int32_t P = fp_.P;
+    std::vector<int32_t> qof(P, -1), parent(P, -1), nchild(P, 0);
+    std::vector<long long> e0(P, 0);
+    for (int32_t q = 0; q < P; ++q) qof[fp_.level_fronts[q]] = q;
+    for (int32_t q = 0; q < P; ++q) {
+      const int32_t pf = sp_.panel_parent[fp_.level_fronts[q]];
+      if (pf >= 0) {
+        parent[q] = qof[pf];
+        ++nchild[qof[pf]];
+      }
+    }
+    d.tree_max_fsz = 0;
+    d.tree_list_cap = 1;
+    for (const auto& lv : d.levels) {
+      for (int32_t q = lv.begin; q < lv.begin + lv.count; ++q)
+        e0[q] = lv.fe_base + (long long)(q - lv.begin) * lv.max_src;
+      d.tree_max_fsz = std::max(d.tree_max_fsz, lv.max_fsz);
+      d.tree_list_cap = std::max(d.tree_list_cap, lv.max_src);
+    }
+    std::vector<int32_t> leaves;
+    for (int32_t q = 0; q < P; ++q)
+      if (nchild[q] == 0) leaves.push_back(q);
+    d.tree_leaf_count = (int)leaves.size();
+    d.tree_parent.upload(parent);
+    d.tree_nchild.upload(nchild);
+    d.tree_e0.upload(e0);
+    d.tree_leaves.upload(leaves);
+    d.tree_done.reserve(((size_t)P + 1) * sizeof(int));
+  }
 
   DevPlan& pl = d.pl;
   pl.P = fp_.P;
@@ -678,6 +726,7 @@ FactorArgs<T, T> Engine::factor_args(int store_l, const void* J) const {
   a.sing = d.sing.as<int>();
   a.front_scratch = d.front_scratch_elems ? d.front_scratch.as<T>() : nullptr;
   a.front_scratch_elems = d.front_scratch_elems;
+  a.single = single_system() ? 1 : 0;
   return a;
 }
 
@@ -775,7 +824,16 @@ template <typename T>
 void Engine::autotune_factor(cudaStream_t s, const void* J) {
   auto& d = *d_;
   const bool dbl = std::is_same<T, double>::value;
-  if (d.tuned_Bp == d.Bp && d.tuned_double == dbl) return;
+  if (d.tuned_Bp == d.Bp && d.tuned_double == dbl && d.tuned_single == single_system()) return;
+  if (single_system()) {
+    // batch 1: the single-system kernel has no launch shapes to choose (the
+    // tensor-core threshold of TF32 factors stays at its default)
+    d.tuned_Bp = d.Bp;
+    d.tuned_double = dbl;
+    d.tuned_single = true;
+    d.invalidate_graph();
+    return;
+  }
   const FactorArgs<T, T> a = factor_args<T>(1, J);
   if (tf32_factors() && cfg_.tc_min_front == 0) {
     // the small/large-front split of TF32 factors: the tensor-core threshold
@@ -830,6 +888,7 @@ void Engine::autotune_factor(cudaStream_t s, const void* J) {
       [&](size_t i) { launch_factor_level<T, T>(d.levels[i], a, s); }, s, "factor");
   d.tuned_Bp = d.Bp;
   d.tuned_double = dbl;
+  d.tuned_single = false;
   d.invalidate_graph();  // a captured solve holds the old launch shapes
 }
 
@@ -895,15 +954,39 @@ std::vector<int32_t> Engine::backward_launch_warps() const {
 }
 
 template <typename T>
+void Engine::factor_tree(const FactorArgs<T, T>& a, cudaStream_t s) {
+  auto& d = *d_;
+  SingleTree t;
+  t.parent = d.tree_parent.as<int>();
+  t.nchild = d.tree_nchild.as<int>();
+  t.q_e0 = d.tree_e0.as<long long>();
+  t.leaves = d.tree_leaves.as<int>();
+  t.done = d.tree_done.as<int>();
+  t.P = fp_.P;
+  t.n_leaves = d.tree_leaf_count;
+  t.max_fsz = d.tree_max_fsz;
+  t.list_cap = d.tree_list_cap;
+  CUPF_CUDA(cudaMemsetAsync(t.done, 0, ((size_t)t.P + 1) * sizeof(int), s));
+  launch_factor_single_tree<T, T>(a, t, s);
+}
+
+template <typename T>
 void Engine::factor_all(cudaStream_t s, int store_l, const void* J) {
   auto& d = *d_;
   const FactorArgs<T, T> a = factor_args<T>(store_l, J);
   stage_begin(2, s);
-  for (const auto& lv : d.levels) {
-    launch_factor_level<T, T>(lv, a, s);
-    debug_check(s, "factor level");
+  if (single_tree(sizeof(T))) {
+    factor_tree<T>(a, s);
+    debug_check(s, "factor tree");
     ++launches_;
     ++d.stage_launches[2];
+  } else {
+    for (const auto& lv : d.levels) {
+      launch_factor_level<T, T>(lv, a, s);
+      debug_check(s, "factor level");
+      ++launches_;
+      ++d.stage_launches[2];
+    }
   }
   stage_end(2, s);
 }
@@ -967,7 +1050,8 @@ template <typename T>
 void Engine::ensure_loop_graph(const DevState& st) {
   auto& d = *d_;
   const bool dbl = std::is_same<T, double>::value;
-  if (d.exec && d.graph_Bp == d.Bp && d.graph_double == dbl && d.graph_yb == static_cast<const void*>(st.yb_re))
+  if (d.exec && d.graph_Bp == d.Bp && d.graph_double == dbl && d.graph_yb == static_cast<const void*>(st.yb_re) &&
+      d.graph_single == single_system())
     return;
   if (d.exec) cudaGraphExecDestroy(d.exec);
   d.exec = nullptr;
@@ -1029,6 +1113,7 @@ void Engine::ensure_loop_graph(const DevState& st) {
   cudaGraphDestroy(graph);
   d.graph_Bp = d.Bp;
   d.graph_double = dbl;
+  d.graph_single = single_system();
   d.graph_yb = st.yb_re;
   launches_ = before;
 }
@@ -1044,7 +1129,7 @@ SolveStats Engine::run_loop(double tol, int32_t max_iter, int32_t prepare_adjoin
   adjoint_ready_ = false;
   if (cfg_.autotune && max_iter > 0 &&
       (d.tuned_Bp != d.Bp || d.tuned_double != std::is_same<T, double>::value || d.tuned_bw_Bp != d.Bp ||
-       d.tuned_bw_double != std::is_same<T, double>::value)) {
+       d.tuned_bw_double != std::is_same<T, double>::value || d.tuned_single != single_system())) {
     // tune on the Jacobian of the starting state (the loop recomputes it)
     launch_ibus_mismatch(d.g, st, s);
     launch_jacobian<T>(d.g, st, d.J.as<T>(), s);
@@ -1407,6 +1492,12 @@ void Engine::factor_all_external(cudaStream_t s, const void* J, T* scratch, size
   a.sing = d.sing.as<int>();
   a.front_scratch = scratch;
   a.front_scratch_elems = scratch_elems;
+  a.single = single_system() ? 1 : 0;
+  if (single_tree(sizeof(T))) {  // (no scratch: every front is in shared memory)
+    factor_tree<T>(a, s);
+    ++launches_;
+    return;
+  }
   for (LevelLaunch lv : d.levels) {
     lv.placement = 0;  // the built-in placement: the static area is sized for it
     launch_factor_level<T, T>(lv, a, s);

@@ -38,6 +38,7 @@ struct EngineConfig {
   int32_t par_nd_depth = 4, par_nd_base_small = 4000, par_nd_base_large = 20000;
   int32_t wide_min_front = 65;  // launches with a front this large run the any-size tier
   int32_t tc_min_front = 0;     // TF32: launches with a front this large use the tensor cores (0: 33 / autotuned)
+  int32_t batch1_schedule = 0;  // batch 1: 0 the single-system front kernel, 1 the lane kernels
 };
 
 struct SolveStats {
@@ -168,6 +169,12 @@ class Engine {
   // rows, and with TF32 factors the tensor-core tier from tc_min rows
   void assign_tiers(int tc_min);
   bool tf32_factors() const;
+  // batch 1 with the single-system schedule: one block per front, threads over its rows
+  bool single_system() const;
+  // ... and the whole factorization as one launch over the front tree
+  bool single_tree(size_t elem_bytes) const;
+  template <typename T>
+  void factor_tree(const FactorArgs<T, T>& a, cudaStream_t s);
   // selects per-scenario (d_ybus != null) or shared Ybus values for this batch
   void use_scenario_ybus(const double* d_ybus, int64_t ybus_stride, int32_t B, cudaStream_t s);
   template <typename T>

@@ -48,9 +48,36 @@ struct FactorArgs {
   int* sing = nullptr;
   T* front_scratch = nullptr;       // global dense fronts for levels whose front exceeds shared memory
   size_t front_scratch_elems = 0;   // capacity in elements per scenario lane group (x 32)
+  int single = 0;                   // batch 1: the single-system schedule where a front fits shared memory
 };
 
 constexpr size_t kSmemLimit = 227 * 1024;  // opt-in dynamic shared memory per block on sm_100
+
+// Header of the single-system kernels' shared memory: pivot reciprocal (0),
+// shift flag (8), tree item (12).
+constexpr int kSingleHeader = 32;
+
+// The single-system schedule's shared memory: the header, the dense front
+// [fs][fs + 1], and a source list of up to list_cap entries with their values
+// (value, source, destination per entry; +16: the list's 16-byte alignment).
+inline size_t single_smem_bytes(int max_fsz, int list_cap, size_t elem_bytes) {
+  return kSingleHeader + 16 + ((size_t)max_fsz * (max_fsz + 1) + (size_t)list_cap) * elem_bytes +
+         (size_t)list_cap * (sizeof(long long) + sizeof(int));
+}
+
+// The front tree for the single-system factorization launch, in level order
+// (q): parent[q] (-1 at a root), nchild[q], the start of q's source list in
+// the padded lists, the leaves (fronts without children) in level order;
+// done: P + 1 ints zeroed before each launch (per-front child counts, then
+// the leaf counter).
+struct SingleTree {
+  const int* parent = nullptr;
+  const int* nchild = nullptr;
+  const long long* q_e0 = nullptr;
+  const int* leaves = nullptr;
+  int* done = nullptr;
+  int P = 0, n_leaves = 0, max_fsz = 0, list_cap = 0;
+};
 
 // Shared-memory plan of one factor-level launch (same for every block):
 // staged source list (src, dst), pivot reciprocals, staged source rows,
@@ -212,6 +239,8 @@ template <typename T, typename TJ>
 void configure_front_kernels();
 template <typename T, typename TJ>
 void launch_factor_level(const LevelLaunch& lv, const FactorArgs<T, TJ>& a, cudaStream_t s);
+template <typename T, typename TJ>
+void launch_factor_single_tree(const FactorArgs<T, TJ>& a, const SingleTree& t, cudaStream_t s);
 template <typename T>
 void launch_backward_level(const LevelLaunch& lv, const SweepArgs<T>& a, cudaStream_t s);
 // The narrow top levels as one launch (block = 32 scenarios walking the

@@ -430,6 +430,207 @@ __global__ void __launch_bounds__(256)
 }
 
 // ---------------------------------------------------------------------------
+// The single-system schedule (batch 1): one block per front, its threads
+// spread over the front's rows and elements instead of over scenarios (the
+// lane kernels above would keep 31 of every 32 lanes on padding copies).
+//   1. the dense front [fs][fs + 1] in shared memory, zeroed;
+//   2. assembly: each run of list entries with one destination is summed in
+//      list order by one thread (the lane kernels sum the same runs in the
+//      same order);
+//   3. right-looking elimination of the nc pivot columns: per pivot, one
+//      thread guards it and takes its reciprocal, the rows below take their
+//      multiplier l = a_ik * (1 / u_kk), then every trailing element
+//      a_ij -= l_i u_kj.  Each element sees the lane kernels' operations in
+//      the same order, so the factors are the same bits;
+//   4. U rows, y, L21 (store_l) and the contribution block out, each value
+//      written to all 32 lanes of its row: every lane of the batch-innermost
+//      arrays then holds what the lane kernels leave there for a batch of 1
+//      (whose padding lanes copy scenario 0), and the backward sweep and the
+//      adjoint read them unchanged.
+// ---------------------------------------------------------------------------
+// Shared memory of a single-system block: [header | kSingleHeader B]
+// [front fs x (fs + 1)][values x list_cap][sources, destinations x list_cap,
+// from a 16-byte boundary].
+template <typename T>
+struct SingleSmem {
+  T* F;
+  T* vals;
+  long long* srcs;
+  int* dsts;
+  __device__ SingleSmem(unsigned char* raw, int fs, int list_cap) {
+    F = reinterpret_cast<T*>(raw + kSingleHeader);
+    vals = F + fs * (fs + 1);
+    const size_t list_off = (kSingleHeader + ((size_t)fs * (fs + 1) + list_cap) * sizeof(T) + 15) & ~(size_t)15;
+    srcs = reinterpret_cast<long long*>(raw + list_off);
+    dsts = reinterpret_cast<int*>(srcs + list_cap);
+  }
+};
+
+// Phase 1 of front q (whole block): its source list (starting at e0, at most
+// list_cap entries) into shared memory, the front zeroed, and the values
+// that earlier kernels wrote (Jacobian entries, right-hand-side rows); the
+// children's contribution-block values wait for single_finish.
+// wait_previous: wait for the previous kernel before reading those values.
+template <typename T, typename TJ>
+__device__ __forceinline__ FrontMeta single_load(const DevPlan& pl, int q, long long e0, int list_cap, int Bp,
+                                                 const TJ* __restrict__ J, const T* __restrict__ Fp,
+                                                 unsigned char* smem_raw, bool wait_previous) {
+  const int nt = blockDim.x, tid = threadIdx.x;
+  const FrontMeta m = load_front_meta(pl.front_meta, q);
+  const int fs = m.fs, rw = fs + 1, nsrc = m.split[8];
+  const SingleSmem<T> sm(smem_raw, fs, list_cap);
+  for (int e = tid; e < fs * rw; e += nt) sm.F[e] = T(0);
+  if (wait_previous) chain_wait_previous();
+  for (int e = tid; e < nsrc; e += nt) {
+    const unsigned long long sv = (unsigned long long)pl.fe_src[e0 + e];
+    sm.srcs[e] = (long long)sv;
+    sm.dsts[e] = pl.fe_dst[e0 + e];
+    const int kind = (int)(sv >> 62);
+    const size_t off = (size_t)(sv & 0x3FFFFFFFFFFFFFFFull) * Bp;
+    if (kind != 1) sm.vals[e] = kind == 0 ? static_cast<T>(J[off]) : Fp[off];
+  }
+  return m;
+}
+
+// Phase 2 (whole block, after single_load): the contribution-block values
+// (read through L2 only, ld.global.cg: in the tree launch another SM wrote
+// them during this kernel), the assembly, the elimination and the outputs.
+// Returns after the outputs are stored (no barrier at the end).
+template <typename T>
+__device__ __forceinline__ void single_finish(const FrontMeta& m, int list_cap, int Bp, T* __restrict__ U,
+                                              T* __restrict__ L, T* __restrict__ CB, T* __restrict__ Y,
+                                              int store_l, double eps, int static_pivot, int* __restrict__ sing,
+                                              unsigned char* smem_raw) {
+  T& s_inv = *reinterpret_cast<T*>(smem_raw);
+  int& s_shift = *reinterpret_cast<int*>(smem_raw + 8);
+  const int nt = blockDim.x, tid = threadIdx.x, W = nt >> 5, warp = tid >> 5, lane = tid & 31;
+  const int fs = m.fs, nc = m.nc, uc = fs - nc, rw = fs + 1, nsrc = m.split[8];
+  const SingleSmem<T> sm(smem_raw, fs, list_cap);
+  T* F = sm.F;
+  if (tid == 0) s_shift = 0;
+  __syncthreads();
+  for (int e = tid; e < nsrc; e += nt) {
+    const unsigned long long sv = (unsigned long long)sm.srcs[e];
+    if ((int)(sv >> 62) == 1) sm.vals[e] = __ldcg(CB + (size_t)(sv & 0x3FFFFFFFFFFFFFFFull) * Bp);
+  }
+  __syncthreads();
+  // each run of entries with one destination summed in list order by one thread
+  for (int e = tid; e < nsrc; e += nt) {
+    const int d = sm.dsts[e];
+    if (d < 0 || (e > 0 && sm.dsts[e - 1] == d)) continue;  // not the first entry of its run
+    T acc = T(0);
+    for (int f = e; f < nsrc && sm.dsts[f] == d; ++f) acc += sm.vals[f];
+    F[d] = acc;
+  }
+  // right-looking elimination: warp w takes rows k + 1 + w, k + 1 + w + W, ...
+  // (every lane forms the row's multiplier, lane j its columns)
+  for (int k = 0; k < nc; ++k) {
+    __syncthreads();
+    if (tid == 0) {
+      bool sh = false;
+      const T p = guarded_pivot(F[k * rw + k], static_pivot != 0, eps, sh);
+      F[k * rw + k] = p;
+      s_inv = T(1) / p;
+      if (sh) s_shift = 1;
+    }
+    __syncthreads();
+    const T inv = s_inv;
+    for (int i = k + 1 + warp; i < fs; i += W) {
+      const T l = F[i * rw + k] * inv;
+      for (int j = k + 1 + lane; j < rw; j += 32) F[i * rw + j] -= l * F[k * rw + j];
+      __syncwarp();
+      if (lane == 0) F[i * rw + k] = l;
+    }
+  }
+  __syncthreads();
+  // every output value to all 32 lanes of its row (one coalesced store per
+  // warp); warp w takes rows w, w + W, ...
+  for (int k = warp; k < nc; k += W) {
+    T* Uk = U + (size_t)(m.uo + (long long)k * fs) * Bp + lane;
+    for (int j = 0; j < fs; ++j) Uk[(size_t)j * Bp] = F[k * rw + j];
+    Y[(size_t)(m.first + k) * Bp + lane] = F[k * rw + fs];
+  }
+  for (int ii = warp; ii < uc; ii += W) {
+    const T* Fi = F + (nc + ii) * rw;
+    if (store_l) {
+      T* Li = L + (size_t)(m.lo + (long long)ii * nc) * Bp + lane;
+      for (int mm = 0; mm < nc; ++mm) Li[(size_t)mm * Bp] = Fi[mm];
+    }
+    T* Ci = CB + (size_t)(m.co + (long long)ii * (uc + 1)) * Bp + lane;
+    for (int jj = 0; jj <= uc; ++jj) Ci[(size_t)jj * Bp] = Fi[nc + jj];
+  }
+  if (s_shift && warp == 0) sing[lane] = 1;
+}
+
+// One launch per level: block b factors front level_begin + b.
+template <typename T, typename TJ>
+__global__ void __launch_bounds__(256)
+    k_front_factor_single(DevPlan pl, int level_begin, long long fe_base, int fe_pad, int Bp,
+                          const TJ* __restrict__ J, const T* __restrict__ Fp, T* __restrict__ U, T* __restrict__ L,
+                          T* __restrict__ CB, T* __restrict__ Y, int store_l, double eps, int static_pivot,
+                          int* __restrict__ sing) {
+  static_assert(sizeof(TJ) == sizeof(T), "Jacobian and factor rows share one element type");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  chain_allow_next();
+  const int q = level_begin + blockIdx.x;
+  const FrontMeta m = single_load<T, TJ>(pl, q, fe_base + (long long)(q - level_begin) * fe_pad, fe_pad, Bp, J, Fp,
+                                         smem_raw, true);
+  single_finish<T>(m, fe_pad, Bp, U, L, CB, Y, store_l, eps, static_pivot, sing, smem_raw);
+}
+
+// The whole factorization of a single system as one launch over the front
+// tree.  Persistent blocks take the tree's leaves in level order from a
+// counter (next).  A block that has stored a front's outputs counts it done
+// at the parent (done[parent]); the block whose count completes the parent's
+// children goes on with the parent itself, so no block ever waits for
+// another: a front starts as soon as its last child is stored.  While the
+// count is in flight, every block loads the parent's list and its Jacobian
+// and right-hand-side values (kept only by the block that goes on).  done
+// and next start at zero.
+template <typename T, typename TJ>
+__global__ void __launch_bounds__(128)
+    k_factor_single_tree(DevPlan pl, const int* __restrict__ parent, const int* __restrict__ nchild,
+                         const long long* __restrict__ q_e0, const int* __restrict__ leaves, int n_leaves,
+                         int* __restrict__ done, int* __restrict__ next, int list_cap, int Bp,
+                         const TJ* __restrict__ J, const T* __restrict__ Fp, T* __restrict__ U, T* __restrict__ L,
+                         T* __restrict__ CB, T* __restrict__ Y, int store_l, double eps, int static_pivot,
+                         int* __restrict__ sing) {
+  static_assert(sizeof(TJ) == sizeof(T), "Jacobian and factor rows share one element type");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  int& s_item = *reinterpret_cast<int*>(smem_raw + 12);
+  chain_allow_next();
+  chain_wait_previous();  // J and Fp come from earlier kernels
+  int q = -1;             // the front this block goes on with (-1: take the next leaf)
+  FrontMeta m;
+  for (;;) {
+    if (q < 0) {
+      __syncthreads();  // every thread has read s_item
+      if (threadIdx.x == 0) {
+        const int i = atomicAdd(next, 1);
+        s_item = i < n_leaves ? leaves[i] : -1;
+      }
+      __syncthreads();
+      q = s_item;
+      if (q < 0) break;
+      m = single_load<T, TJ>(pl, q, q_e0[q], list_cap, Bp, J, Fp, smem_raw, false);
+    }
+    single_finish<T>(m, list_cap, Bp, U, L, CB, Y, store_l, eps, static_pivot, sing, smem_raw);
+    __threadfence();  // this front's stores before its count at the parent
+    __syncthreads();  // (also: the front's shared memory is free)
+    const int p = parent[q];
+    int last = 0;
+    if (threadIdx.x == 0 && p >= 0) last = atomicAdd(done + p, 1) == nchild[p] - 1;
+    if (p >= 0) m = single_load<T, TJ>(pl, p, q_e0[p], list_cap, Bp, J, Fp, smem_raw, false);
+    if (threadIdx.x == 0) {
+      if (last) __threadfence();  // the other children's stores, counted before ours, before our reads
+      s_item = last ? p : -1;
+    }
+    __syncthreads();
+    q = s_item;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // The wide tier: fronts of any size.  Same block shape (one front x 32
 // scenarios) and phases 1-2 as k_front_factor, with the source list read
 // from global memory, the dense front always in this block's slice of the
@@ -1160,6 +1361,37 @@ void launch_factor_wide(const LevelLaunch& lv, const FactorArgs<T, TJ>& a, cudaS
                  a.store_l, a.eps, a.static_pivot, a.sing, a.front_scratch);
 }
 
+inline size_t single_front_bytes(const LevelLaunch& lv, size_t elem_bytes) {
+  return single_smem_bytes(lv.max_fsz, lv.max_src, elem_bytes);
+}
+
+// One block per front of the launch; 64 threads for fronts of up to 12 rows,
+// 128 up to 24, else 256 (the trailing update has about fs^2 / 2 elements).
+template <typename T, typename TJ>
+void launch_factor_single(const LevelLaunch& lv, const FactorArgs<T, TJ>& a, cudaStream_t s) {
+  const size_t smem = single_front_bytes(lv, sizeof(T));
+  auto kern = k_front_factor_single<T, TJ>;
+  allow_full_smem(reinterpret_cast<const void*>(kern));
+  const int threads = lv.max_fsz <= 12 ? 64 : lv.max_fsz <= 24 ? 128 : 256;
+  launch_chained(kern, dim3((unsigned)lv.count), dim3(threads), smem, s, "front factor (single system)", a.plan,
+                 lv.begin, lv.fe_base, lv.max_src, a.Bp, a.J, a.Fp, a.U, a.L, a.CB, a.Y, a.store_l, a.eps,
+                 a.static_pivot, a.sing);
+}
+
+// The whole single-system factorization as one launch (k_factor_single_tree):
+// persistent blocks of 128 threads, at most 8 per SM's worth.
+template <typename T, typename TJ>
+void launch_factor_single_tree(const FactorArgs<T, TJ>& a, const SingleTree& t, cudaStream_t s) {
+  const size_t smem = single_smem_bytes(t.max_fsz, t.list_cap, sizeof(T));
+  if (smem > kSmemLimit) throw std::runtime_error("single-system tree: a front exceeds shared memory");
+  auto kern = k_factor_single_tree<T, TJ>;
+  allow_full_smem(reinterpret_cast<const void*>(kern));
+  const int blocks = std::max(1, std::min(t.n_leaves, 148 * 8));
+  launch_chained(kern, dim3((unsigned)blocks), dim3(128), smem, s, "front factor (single-system tree)", a.plan,
+                 t.parent, t.nchild, t.q_e0, t.leaves, t.n_leaves, t.done, t.done + t.P, t.list_cap, a.Bp, a.J,
+                 a.Fp, a.U, a.L, a.CB, a.Y, a.store_l, a.eps, a.static_pivot, a.sing);
+}
+
 // A tensor-core launch (FP32 factors): 4 or 8 warps (every TMEM lane
 // quarter needs its warp); falls back to the FP32 wide tier where the fronts
 // exceed its limits.
@@ -1191,6 +1423,10 @@ template <typename T, typename TJ>
 void launch_factor_level(const LevelLaunch& lv, const FactorArgs<T, TJ>& a, cudaStream_t s) {
   if (lv.count == 0) return;
   if (lv.max_nc > 8) throw std::runtime_error("panels wider than 8 columns are not supported (max_panel_width <= 8)");
+  if (a.single && lv.tier != 2 && single_front_bytes(lv, sizeof(T)) <= kSmemLimit) {
+    launch_factor_single<T, TJ>(lv, a, s);  // batch 1 (the tensor-core tier keeps its own kernel)
+    return;
+  }
   if (lv.tier == 2) {
     launch_factor_tc<T, TJ>(lv, a, s);
     return;

@@ -4,6 +4,8 @@
 
 namespace cupf_b200 {
 template void configure_front_kernels<double, double>();
+template void launch_factor_single_tree<double, double>(const FactorArgs<double, double>&,
+                                                       const SingleTree&, cudaStream_t);
 template void launch_factor_level<double, double>(const LevelLaunch&, const FactorArgs<double, double>&,
                                                   cudaStream_t);
 template void launch_backward_top<double>(const LevelLaunch&, const int*, int, const SweepArgs<double>&, cudaStream_t);

@@ -20,7 +20,12 @@ Differences a user can see:
   * ``CustomSolverConfig.wide_min_front`` and ``tc_min_front`` (not in the
     reference) set where the any-size front tier (default 65 rows) and, with
     ``CustomPrecision.TF32``, the tensor-core trailing update (default 65
-    rows, autotuned among 33, 49 and 65) take over.
+    rows, autotuned among 33, 49 and 65) take over;
+  * ``CustomSolverConfig.batch1_schedule`` (not in the reference's config;
+    its solver picks its single-system path by itself at batch 1): 0 (the
+    default) factors a batch of one system with one block per front and its
+    threads over the front's rows, 1 with the batched lane kernels; the
+    factors are the same.
 """
 from __future__ import annotations
 
@@ -122,7 +127,7 @@ class CustomSolverConfig(_Struct):
                "pivot_strategy": CustomPivotStrategy.StaticDiagonalShift, "serial_nd": False,
                "max_panel_width": 8, "shift_retry_epsilon": 1.0e-8, "autotune": True,
                "parallel_nd_depth": 4, "parallel_nd_base_small": 4000, "parallel_nd_base_large": 20000,
-               "wide_min_front": 0, "tc_min_front": 0}
+               "wide_min_front": 0, "tc_min_front": 0, "batch1_schedule": 0}
 
 
 class NewtonOptions(_Struct):
@@ -272,7 +277,7 @@ def _cls_config(c: CustomSolverConfig) -> _capi.ClsConfig:
     return _capi.ClsConfig(int(c.precision), int(c.matching), int(c.pivot_strategy), int(bool(c.serial_nd)),
                            int(c.max_panel_width), float(c.shift_retry_epsilon), int(bool(c.autotune)),
                            int(c.parallel_nd_depth), int(c.parallel_nd_base_small), int(c.parallel_nd_base_large),
-                           int(c.wide_min_front), int(c.tc_min_front))
+                           int(c.wide_min_front), int(c.tc_min_front), int(c.batch1_schedule))
 
 
 def _nr_config(cfg: NRConfig | None) -> _capi.PfNRConfig:

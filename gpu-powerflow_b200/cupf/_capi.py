@@ -16,7 +16,8 @@ class ClsConfig(C.Structure):
     _fields_ = [("precision", C.c_int32), ("matching", C.c_int32), ("pivot_strategy", C.c_int32),
                 ("serial_nd", C.c_int32), ("max_panel_width", C.c_int32), ("shift_retry_epsilon", C.c_double),
                 ("autotune", C.c_int32), ("parallel_nd_depth", C.c_int32), ("parallel_nd_base_small", C.c_int32),
-                ("parallel_nd_base_large", C.c_int32), ("wide_min_front", C.c_int32), ("tc_min_front", C.c_int32)]
+                ("parallel_nd_base_large", C.c_int32), ("wide_min_front", C.c_int32), ("tc_min_front", C.c_int32),
+                ("batch1_schedule", C.c_int32)]
 
 
 class PfOptions(C.Structure):

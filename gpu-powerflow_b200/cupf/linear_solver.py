@@ -25,7 +25,8 @@ class SolverConfig:
     def __init__(self, precision: int = 0, pivot_strategy: int = 1, serial_nd: bool = True,
                  max_panel_width: int = 8, shift_retry_epsilon: float = 1e-8, matching: int = 0,
                  autotune: bool = True, parallel_nd_depth: int = 4, parallel_nd_base_small: int = 4000,
-                 parallel_nd_base_large: int = 20000, wide_min_front: int = 0, tc_min_front: int = 0):
+                 parallel_nd_base_large: int = 20000, wide_min_front: int = 0, tc_min_front: int = 0,
+                 batch1_schedule: int = 0):
         self.precision = int(precision)
         self.matching = int(matching)  # MatchingMode: 0 None, 1 Structural
         self.pivot_strategy = int(pivot_strategy)
@@ -41,6 +42,8 @@ class SolverConfig:
         # tensor-core trailing update (0: 65, or autotuned among 33, 49, 65)
         self.wide_min_front = int(wide_min_front)
         self.tc_min_front = int(tc_min_front)
+        # a batch of one system: 0 one block per front (threads over its rows), 1 the batched lane kernels
+        self.batch1_schedule = int(batch1_schedule)
 
 
 class CustomSolverError(RuntimeError):
@@ -55,7 +58,7 @@ class LinearSolver:
         c = config or SolverConfig()
         cfg = _capi.ClsConfig(c.precision, c.matching, c.pivot_strategy, int(c.serial_nd), c.max_panel_width,
                               c.shift_retry_epsilon, int(c.autotune), c.parallel_nd_depth, c.parallel_nd_base_small,
-                              c.parallel_nd_base_large, c.wide_min_front, c.tc_min_front)
+                              c.parallel_nd_base_large, c.wide_min_front, c.tc_min_front, c.batch1_schedule)
         h = C.c_void_p()
         st = self._lib.cls_create(C.byref(cfg), C.byref(h))
         if st:

@@ -90,6 +90,10 @@ typedef struct {
                                    run their trailing update CB = A22 - L21 U12 on the tensor cores
                                    (tcgen05 kind::tf32, operands split hi + lo, fp32 accumulation); 0 = 65,
                                    or the fastest of 33, 49 and 65 when autotune is on */
+  int32_t batch1_schedule;      /* a batch of one system: 0 = one block per front with its threads over the
+                                   front's rows and elements (the reference's single-system path,
+                                   factorize/single.cuh); 1 = the batched kernels, whose lanes are scenarios
+                                   (31 of 32 then copy the one system).  Both give the same factors. */
 } cls_config;
 
 typedef struct cls_solver_s* cls_handle;

@@ -201,7 +201,7 @@ def test_new_options_and_exports_are_checked(tmp_path):
     the front CSV needs an analysed plan and a writable path."""
     lib = _capi.load()
     for bad in ({"autotune": 2}, {"parallel_nd_depth": -1}, {"parallel_nd_base_small": -5},
-                {"parallel_nd_base_large": -1}):
+                {"parallel_nd_base_large": -1}, {"batch1_schedule": 2}, {"batch1_schedule": -1}):
         c = _capi.ClsConfig(0, 0, 1, 1, 8, 1e-8, 0, 0, 0, 0)
         for k, v in bad.items():
             setattr(c, k, v)
