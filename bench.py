@@ -429,13 +429,18 @@ def run_engine(args) -> None:
     # the L2 flush runs inside each step, before its solve.
     from cupf.streaming import HostPipeline
 
-    # two solve lanes: a second engine handle, so two batches solve at once
-    # on their own streams (one batch's latency-bound phases overlap the
-    # other's wide ones); primed like the first before any timing
-    mixed2 = make_solver(g, cupf.ComputePolicy.Mixed, graph=not args.no_graph)
-    step_flat(mixed2)
-    if ws:
-        ws.solve(mixed2, sbus, cfg)
+    # three solve lanes: more engine handles, so batches solve at once on
+    # their own streams (one batch's latency-bound phases overlap another's
+    # wide ones); primed like the first before any timing.  (A fourth lane
+    # measured within 1-2 % of three.)
+    extra_lanes = []
+    for _ in range(2):
+        sv = make_solver(g, cupf.ComputePolicy.Mixed, graph=not args.no_graph)
+        step_flat(sv)
+        if ws:
+            ws.solve(sv, sbus, cfg)
+        extra_lanes.append(sv)
+    mixed2, mixed3 = extra_lanes
     torch.cuda.synchronize(dev)
 
     def make_pipe(lanes):
@@ -464,7 +469,7 @@ def run_engine(args) -> None:
     v_bufs = [torch.empty(B, g.n_bus, dtype=torch.complex128).pin_memory() for _ in range(4)]
     fm_bufs = [torch.empty(B, dtype=torch.float64).pin_memory() for _ in range(max(args.steps, args.warmup))]
     e2e_lanes = {}
-    for nl, lanes in ((1, [mixed]), (2, [mixed, mixed2])):
+    for nl, lanes in ((1, [mixed]), (2, [mixed, mixed2]), (3, [mixed, mixed2, mixed3])):
         pipe = make_pipe(lanes)
         pipe.run([sbus_p] * args.warmup, [v_bufs[k % 4] for k in range(args.warmup)], fm_bufs[: args.warmup])
         _barrier(world)
@@ -474,7 +479,7 @@ def run_engine(args) -> None:
         ms_l = _reduce((time.perf_counter() - t0) * 1e3 / args.steps, "max", world, dev)
         conv_l = sum(int((f <= TOL).sum()) for f in fm_bufs[: args.steps])
         e2e_lanes[nl] = (ms_l, _reduce(conv_l / args.steps, "sum", world, dev) / (ms_l / 1e3))
-    ms_e2e, e2e_value = e2e_lanes[2]
+    ms_e2e, e2e_value = e2e_lanes[3]
 
     # the warm start on 4,096 held-out scenarios from its training distribution
     # (per-bus U(0.7, 1.3), a seed the training draws do not use): warm against
@@ -558,10 +563,12 @@ def run_engine(args) -> None:
             "warm_start_heldout": heldout,
             "e2e": {"value": round(e2e_value, 1), "unit": UNIT, "h2d_bytes_per_step": B * g.n_bus * 16,
                     "d2h_bytes_per_step": B * g.n_bus * 16 + B * 8, "ms_per_step": round(ms_e2e, 4),
-                    "method": "cupf.streaming.HostPipeline over pinned host batches with two solve lanes (two "
-                              "engine handles, streams and worker threads; batches round-robin): each step "
-                              "uploads its Sbus and downloads its V and final norms; uploads, network "
-                              "inference and downloads overlap the solves, and two solves run at once",
+                    "method": "cupf.streaming.HostPipeline over pinned host batches with three solve lanes "
+                              "(three engine handles, streams and worker threads; batches round-robin): each "
+                              "step uploads its Sbus and downloads its V and final norms; uploads, network "
+                              "inference and downloads overlap the solves, and up to three solves run at once",
+                    "two_lanes": {"value": round(e2e_lanes[2][1], 1), "ms_per_step": round(e2e_lanes[2][0], 4),
+                                  "method": "the same pipeline with two solve lanes"},
                     "one_lane": {"value": round(e2e_lanes[1][1], 1), "ms_per_step": round(e2e_lanes[1][0], 4),
                                  "method": "the same pipeline with one solve lane"},
                     "serial": {"value": round(e2e_serial_value, 1), "ms_per_step": round(ms_e2e_serial, 4),
@@ -702,7 +709,8 @@ def run_extras(args, dev) -> dict:
                 th.append((time.perf_counter() - t0) * 1e3)
             s1[name] = {"device_ms": round(statistics.median(ts), 4), "host_api_ms": round(statistics.median(th), 4),
                         "iterations": int(it1), "converged": bool(r1.converged_numpy.all())}
-        out[key] = {**s1, "method": "batch of 1 padded to one 32-scenario lane group; median of 50 solves"}
+        out[key] = {**s1, "method": "batch of 1 (single-system schedule: the factorization as one launch over "
+                                  "the front tree); median of 50 solves"}
     return out
 
 
