@@ -19,11 +19,11 @@ pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not gpu_available(), reason="n
 GOLD = Path(__file__).resolve().parent / "golden"
 
 
-def _factor_solve(d, precision, schedule, tc_min_front=0):
+def _factor_solve(d, precision, schedule, tc_min_front=0, serial_nd=True, matching=0):
     import torch
 
-    ls = cupf.LinearSolver(cupf.SolverConfig(precision=int(precision), serial_nd=True, batch1_schedule=schedule,
-                                             tc_min_front=tc_min_front))
+    ls = cupf.LinearSolver(cupf.SolverConfig(precision=int(precision), serial_nd=serial_nd, batch1_schedule=schedule,
+                                             tc_min_front=tc_min_front, matching=matching))
     ls.set_data(d["row_ptr"], d["col_idx"])
     ls.analyze()
     ls.setup(1)
@@ -51,6 +51,17 @@ def test_single_system_factors_equal_the_lane_kernels(case, precision):
         A = sp.csr_matrix((d["values"], d["col_idx"], d["row_ptr"]), shape=(n, n))
         r = np.linalg.norm(A @ x1 - d["F"]) / np.linalg.norm(d["F"])
         assert r <= 1e-10, (case, r, fmax)
+
+
+@pytest.mark.parametrize("serial_nd,matching", [(False, 0), (True, 1)])
+def test_single_system_with_other_orderings(serial_nd, matching):
+    """The separator-recursion ordering and the structural matching (other
+    front trees and assembly lists): still the lane kernels' bits."""
+    d = np.load(GOLD / "linsys_case1354pegase.npz")
+    for precision in (cupf.CustomPrecision.FP64, cupf.CustomPrecision.FP32):
+        x1, xt1, _, _ = _factor_solve(d, precision, 0, serial_nd=serial_nd, matching=matching)
+        x0, xt0, _, _ = _factor_solve(d, precision, 1, serial_nd=serial_nd, matching=matching)
+        assert np.array_equal(x1, x0) and np.array_equal(xt1, xt0)
 
 
 def test_single_system_with_tensor_core_launches():

@@ -76,3 +76,24 @@ def test_static_scratch_rejects_a_batch_beyond_its_size():
     with pytest.raises(cupf.linear_solver.CustomSolverError) as e:
         ls.factorize_static_scratch(vals)
     assert "bytes of front scratch" in str(e.value) and e.value.status == 1
+
+
+def test_static_scratch_at_batch_one():
+    """A batch of one factors with the single-system tree launch, which keeps
+    every front in shared memory: the entry point allocates nothing and
+    gives the regular call's solution."""
+    import torch
+
+    d = np.load(GOLD / "linsys_case1354pegase.npz")
+    ls = _solver(d, 1)
+    vals = torch.tensor(d["values"][None, :], device="cuda")
+    rhs = torch.tensor(d["F"][None, :], device="cuda")
+    ls.factorize(vals)
+    x_ref = ls.solve(rhs).cpu().numpy()
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    ls.factorize_static_scratch(vals)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+    assert np.array_equal(ls.solve(rhs).cpu().numpy(), x_ref)
