@@ -397,24 +397,12 @@ __global__ void __launch_bounds__(256)
     for (int k = warp; k < nc; k += W) Y[(size_t)(first + k) * Bp + b] = Pl[(k * rw + fs) * kWarp];
   }
   // ... and the uc non-pivot rows, independent of each other: row i applies
-  // the nc pivot rows in registers and goes straight out as L21 | CB
-  for (int i = nc + warp; i < fs; i += W) {
+  // the nc pivot rows in registers and goes straight out as L21 | CB.  FP32
+  // fronts of up to 16 rows take two rows per pass (two independent chains,
+  // and each pivot-row element read once for both; in FP64 the second row's
+  // registers cost more residency than the pass saves).
+  auto store_row = [&](const T (&r)[FMAX + 1], int i) {
     const int ii = i - nc;
-    const T* Ri = Fl + i * rw * kWarp;
-    T r[FMAX + 1];
-#pragma unroll
-    for (int j = 0; j <= FMAX; ++j) r[j] = j < rw ? Ri[j * kWarp] : T(0);
-#pragma unroll
-    for (int m = 0; m < 8; ++m) {
-      if (m < nc) {
-        const T* Um = Pl + m * rw * kWarp;
-        const T l = r[m] * inv_l[m * kWarp];
-        r[m] = l;
-#pragma unroll
-        for (int j = m + 1; j <= FMAX; ++j)
-          if (j < rw) r[j] -= l * Um[j * kWarp];
-      }
-    }
     if (store_l) {
       T* Lb = L + (size_t)(lo + (long long)ii * nc) * Bp + b;
 #pragma unroll
@@ -425,6 +413,58 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
     for (int j = 0; j <= FMAX; ++j)
       if (j >= nc && j < rw) Cb[(size_t)(j - nc) * Bp] = r[j];
+  };
+  if constexpr (FMAX <= 16 && sizeof(T) == 4) {
+    for (int i = nc + warp; i < fs; i += 2 * W) {
+      const int i2 = i + W;
+      const bool two = i2 < fs;
+      const T* Ri = Fl + i * rw * kWarp;
+      const T* Ri2 = Fl + (two ? i2 : i) * rw * kWarp;
+      T r[FMAX + 1], r2[FMAX + 1];
+#pragma unroll
+      for (int j = 0; j <= FMAX; ++j) {
+        r[j] = j < rw ? Ri[j * kWarp] : T(0);
+        r2[j] = j < rw ? Ri2[j * kWarp] : T(0);
+      }
+#pragma unroll
+      for (int m = 0; m < 8; ++m) {
+        if (m < nc) {
+          const T* Um = Pl + m * rw * kWarp;
+          const T inv = inv_l[m * kWarp];
+          const T l = r[m] * inv, l2 = r2[m] * inv;
+          r[m] = l;
+          r2[m] = l2;
+#pragma unroll
+          for (int j = m + 1; j <= FMAX; ++j)
+            if (j < rw) {
+              const T u = Um[j * kWarp];
+              r[j] -= l * u;
+              r2[j] -= l2 * u;
+            }
+        }
+      }
+      store_row(r, i);
+      if (two) store_row(r2, i2);
+    }
+  } else {
+    for (int i = nc + warp; i < fs; i += W) {
+      const T* Ri = Fl + i * rw * kWarp;
+      T r[FMAX + 1];
+#pragma unroll
+      for (int j = 0; j <= FMAX; ++j) r[j] = j < rw ? Ri[j * kWarp] : T(0);
+#pragma unroll
+      for (int m = 0; m < 8; ++m) {
+        if (m < nc) {
+          const T* Um = Pl + m * rw * kWarp;
+          const T l = r[m] * inv_l[m * kWarp];
+          r[m] = l;
+#pragma unroll
+          for (int j = m + 1; j <= FMAX; ++j)
+            if (j < rw) r[j] -= l * Um[j * kWarp];
+        }
+      }
+      store_row(r, i);
+    }
   }
   if (shifted) sing[b] = 1;
 }
