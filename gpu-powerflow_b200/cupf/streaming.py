@@ -80,7 +80,21 @@ class HostPipeline:
         The solves run in worker threads, one per lane, each lane's batches
         one after another on its stream (the engine's solve blocks its thread
         until the batch is done and releases the GIL meanwhile); this thread
-        issues the uploads and the prepare stage ahead of the solves."""
+        issues the uploads and the prepare stage ahead of the solves.
+        Python's cyclic garbage collector is paused while the batches
+        stream (a collection pass holds every thread for up to tens of
+        milliseconds) and resumed afterwards."""
+        import gc
+
+        resume = gc.isenabled()
+        gc.disable()
+        try:
+            self._run(sbus, V_out, fm_out)
+        finally:
+            if resume:
+                gc.enable()
+
+    def _run(self, sbus, V_out, fm_out) -> None:
         import queue
         import threading
 
