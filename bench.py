@@ -28,6 +28,7 @@ bounded sample of the same workload.
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import os
 import statistics
@@ -331,6 +332,8 @@ def run_engine(args) -> None:
         _barrier(world)
         torch.cuda.synchronize(dev)
         times, conv, iters, fb, launches = [], 0, 0, 0, 0
+        gc.collect()
+        gc.disable()  # (a collection pass inside a step would delay its launches)
         for _ in range(steps):
             flush.fill_(1.0)
             e0 = torch.cuda.Event(enable_timing=True)
@@ -342,6 +345,7 @@ def run_engine(args) -> None:
             times.append(e0.elapsed_time(e1))
             conv += int((fm <= TOL).sum().item())
             iters, fb, launches = it, fb + nfb, launches + nl
+        gc.enable()
         torch.cuda.synchronize(dev)
         _barrier(world)
         return {"ms": statistics.mean(times), "conv": conv / steps, "iters": iters, "fallback": fb / steps,
