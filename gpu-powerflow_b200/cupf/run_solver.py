@@ -57,6 +57,8 @@ def main(argv=None) -> int:
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--wide-min-front", type=int, default=0)
     ap.add_argument("--tc-min-front", type=int, default=0)
+    ap.add_argument("--batch1-schedule", type=int, choices=(0, 1), default=0,
+                    help="batch 1: 0 the single-system tree launch, 1 the batched lane kernels")
     args = ap.parse_args(argv)
 
     import scipy.sparse as sp
@@ -72,7 +74,7 @@ def main(argv=None) -> int:
     cfg = cupf.SolverConfig(precision=PRECISION[args.precision], serial_nd=not args.parallel_nd,
                             max_panel_width=args.max_panel_width, matching=int(args.matching),
                             autotune=not args.no_autotune, wide_min_front=args.wide_min_front,
-                            tc_min_front=args.tc_min_front)
+                            tc_min_front=args.tc_min_front, batch1_schedule=args.batch1_schedule)
     ls = cupf.LinearSolver(cfg)
     ls.set_data(rp, ci)
     ls.analyze()
