@@ -47,6 +47,7 @@ METRIC = "NR solves/sec at ||F||inf<=1e-8 pu: plain FP64 vs mixed+warm-start, 1 
 UNIT = "converged solves/s"
 BATCH = 1024
 TOL = 1e-8
+C5_TOL = 1e-10  # the gradient case: its 1e-6 relative bar on dL/dP wants V well inside 1e-8
 MAX_ITER = 10
 
 
@@ -650,7 +651,12 @@ def run_extras(args, dev) -> dict:
                            "method": "one engine + CUDA stream per grid, host thread per grid; streams prioritized "
                                      "by grid size (largest first) unless stated", **res}
     # differentiable large case: 10,000 buses x 64, mixed forward through the
-    # torch autograd wrapper, loss = sum (Vm - 1)^2, backward = adjoint J^T solve
+    # torch autograd wrapper, loss = sum (Vm - 1)^2, backward = adjoint J^T solve.
+    # Warm start: every scenario starts from the converged nominal-load state
+    # (solved once per grid, outside the timed region); the flat start is
+    # timed beside it.
+    from cupf.warm_start import nominal_state
+
     g = grids.grid_10000()
     o = cupf.NewtonOptions()
     o.backend = cupf.BackendKind.CUDA
@@ -662,37 +668,72 @@ def run_extras(args, dev) -> dict:
     lp, lq = g.load_scenarios(B, seed=808)
     base_re = torch.tensor(g.sgen.real, device=dev, dtype=torch.float32)
     base_im = torch.tensor(g.sgen.imag, device=dev, dtype=torch.float32)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    vnom = nominal_state(s, g, device=dev)
+    torch.cuda.synchronize()
+    setup_ms = (time.perf_counter() - t0) * 1e3
     v0 = torch.tensor(g.v0, device=dev)
-    va0, vm0 = torch.angle(v0).float(), torch.abs(v0).float()
-    c5cfg = cupf.NRConfig(tolerance=TOL, max_iter=20)
-    tf, tb = [], []
-    for rep in range(4):
-        load_p = torch.tensor(lp, device=dev, dtype=torch.float32, requires_grad=True)
-        load_q = torch.tensor(lq, device=dev, dtype=torch.float32, requires_grad=True)
-        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
-        e0.record()
-        va, vm = cupf.solve(load_p, load_q, s, sbus_base_re=base_re, sbus_base_im=base_im, v0_va=va0, v0_vm=vm0,
-                            config=c5cfg)
-        loss = ((vm - 1.0) ** 2).sum()
-        e1.record()
-        loss.backward()
-        e2.record()
-        e2.synchronize()
-        if rep:
-            tf.append(e0.elapsed_time(e1))
-            tb.append(e1.elapsed_time(e2))
+    starts = {"flat": (torch.angle(v0).float(), torch.abs(v0).float()),
+              "warm": (torch.angle(vnom).float(), torch.abs(vnom).float())}
+    c5cfg = cupf.NRConfig(tolerance=C5_TOL, max_iter=20)
+    # the problem the forward solves: Sbus from FP32 base and loads (the Mixed
+    # torch dtype) differenced in FP64, and the PV and slack magnitudes of the
+    # FP32 start (both starts round them alike)
+    f32 = lambda x: x.astype(np.float32).astype(np.float64)
+    sb_h = (f32(g.sgen.real)[None, :] - f32(lp)) + 1j * (f32(g.sgen.imag)[None, :] - f32(lq))
+    S = torch.tensor(sb_h, device=dev)
+    va0, vm0 = starts["flat"]
+    v0_h = np.repeat((vm0.double() * torch.exp(1j * va0.double())).cpu().numpy()[None, :], B, axis=0)
+    c5 = {}
+    for name, (va0, vm0) in starts.items():
+        tf, tb = [], []
+        for rep in range(4):
+            load_p = torch.tensor(lp, device=dev, dtype=torch.float32, requires_grad=True)
+            load_q = torch.tensor(lq, device=dev, dtype=torch.float32, requires_grad=True)
+            e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            e0.record()
+            va, vm = cupf.solve(load_p, load_q, s, sbus_base_re=base_re, sbus_base_im=base_im, v0_va=va0,
+                                v0_vm=vm0, config=c5cfg)
+            loss = ((vm - 1.0) ** 2).sum()
+            e1.record()
+            loss.backward()
+            e2.record()
+            e2.synchronize()
+            if rep:
+                tf.append(e0.elapsed_time(e1))
+                tb.append(e1.elapsed_time(e2))
+        # the same start through the device entry point (FP64 V out): Newton
+        # norms and the oracle check
+        V0 = (vm0.double() * torch.exp(1j * va0.double()))[None, :].expand(B, -1).contiguous()
+        V, fm, it = s.solve_batch_device(S, V0, config=c5cfg)
+        c5[name] = {"forward_ms": round(statistics.mean(tf), 3), "backward_ms": round(statistics.mean(tb), 3),
+                    "newton_norms": int(it), "converged": int((fm <= C5_TOL).sum()), "V": V,
+                    "grad_p": load_p.grad.double().cpu().numpy(), "grad_q": load_q.grad.double().cpu().numpy(),
+                    "loss": float(loss.item())}
     from oracle.oracle import Oracle
 
+    acc = accuracy_vs_oracle(g, sb_h, v0_h, {k: c5[k].pop("V") for k in c5})
     orc = Oracle()
-    S0 = g.sgen - (lp[0] + 1j * lq[0])
-    V = orc.solve(g, S0, g.v0, tol=1e-12, max_iter=30)["V"]
-    a = orc.adjoint(g, V, np.zeros(g.n_bus), 2.0 * (np.abs(V) - 1.0))
-    gp = load_p.grad[0].double().cpu().numpy()
-    relp = float(np.abs(gp - a["grad_p"]).max() / np.abs(a["grad_p"]).max())
-    out["c5_10000x64"] = {"forward_ms": round(statistics.mean(tf), 3), "backward_ms": round(statistics.mean(tb), 3),
-                          "loss": float(loss.item()), "grad_p_rel_err_vs_fp64_oracle_adjoint": relp,
-                          "path": "cupf.solve (CuPFFunction), mixed, flat start; backward = J^T solve on the "
-                                  "final-state factors"}
+    checked = (0, 21, 42, 63)
+    adj = []
+    for b in checked:
+        V = orc.solve(g, sb_h[b], v0_h[b], tol=1e-12, max_iter=30)["V"]
+        adj.append(orc.adjoint(g, V, np.zeros(g.n_bus), 2.0 * (np.abs(V) - 1.0)))
+    for k in c5:
+        gp, gq = c5[k].pop("grad_p"), c5[k].pop("grad_q")
+        c5[k]["grad_rel_err_vs_fp64_oracle_adjoint"] = max(
+            float(np.abs(gx[b] - a[key]).max() / np.abs(a[key]).max())
+            for b, a in zip(checked, adj) for gx, key in ((gp, "grad_p"), (gq, "grad_q")))
+        c5[k]["max_abs_dV_vs_fp64_oracle"] = acc[k]["max_abs_dV_vs_fp64_oracle"]
+        c5[k]["within_1e-8"] = acc[k]["within_1e-8"]
+    out["c5_10000x64"] = {"forward_ms": c5["warm"]["forward_ms"], "backward_ms": c5["warm"]["backward_ms"],
+                          "warm": c5["warm"], "flat": c5["flat"], "warm_setup_ms": round(setup_ms, 1),
+                          "tolerance": C5_TOL, "scenarios_checked": B, "gradient_scenarios_checked": list(checked),
+                          "path": "cupf.solve (CuPFFunction), mixed; warm start = the converged nominal-load "
+                                  "state (nominal_state, once per grid, untimed); backward = J^T solve on the "
+                                  "final-state factors; dV vs the FP64 oracle (1e-12, from the flat start) on the "
+                                  "same problem (FP32 inputs: Sbus, PV and slack magnitudes); gradients vs the oracle's FP64 adjoint at its solution"}
     # single systems: the 118-bus grid at batch 1 (the reference's CPU-runnable
     # case), FP64 flat start, one graph per solve, device time per solve and
     # through the host API (Sbus and V0 in, V out); the 118-bus grid (C1) and,

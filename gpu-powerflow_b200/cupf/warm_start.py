@@ -13,6 +13,9 @@ bias + GELU epilogues for the forward pass, GELU-derivative epilogues and
 transposed GEMMs for the backward pass, and Adam on FP32 master weights.
 torch only allocates the buffers.  Layer widths are padded to multiples of
 128 (the GEMM tile); padded rows and columns stay exactly zero.
+
+nominal_state() is the model-free alternative: every scenario starts from the
+converged nominal-load state, which is what the 10,000-bus gradient case uses.
 """
 from __future__ import annotations
 
@@ -272,6 +275,25 @@ class MLP:
         return v.value
 
 
+def nominal_state(solver, grid, tol: float = 1e-10, max_iter: int = 20, device=None):
+    """The converged state of the grid's nominal-load case (Sbus = grid.sbus,
+    from its flat start), complex128 [n_bus] on the device.  Started from it,
+    a scenario near nominal load needs fewer Newton steps than from the flat
+    start: the model-free warm start for grids too large to train a network
+    for.  Raises if the nominal case does not converge."""
+    import torch
+
+    import cupf
+
+    dev = torch.device(device or "cuda")
+    S = torch.tensor(grid.sbus[None, :], device=dev)
+    V0 = torch.tensor(grid.v0[None, :], device=dev)
+    V, fm, _ = solver.solve_batch_device(S, V0, config=cupf.NRConfig(tolerance=tol, max_iter=max_iter))
+    if not bool((fm <= tol).all()):
+        raise RuntimeError("warm start: the nominal-load case did not converge")
+    return V[0].clone()
+
+
 class WarmStart:
     """Warm-start predictor for one grid (features: P and Q loads at every bus
     and the PV setpoints; outputs: the Newton unknowns in Jacobian-row order)."""
@@ -316,16 +338,8 @@ class WarmStart:
 
     def set_reference(self, solver, tol: float = 1e-10, max_iter: int = 20) -> None:
         """Solve the nominal-load case once; its angles anchor the unwrapping."""
-        import cupf
-
-        t = self.torch
-        S = t.tensor(self.g.sbus[None, :], device=self.dev)
-        V, fm, _ = solver.solve_batch_device(S, self.v0[None, :].contiguous(),
-                                             config=cupf.NRConfig(tolerance=tol, max_iter=max_iter))
-        if not bool((fm <= tol).all()):
-            raise RuntimeError("warm start: the nominal-load case did not converge")
-        self.va_ref = t.angle(V[0])
-        self.vref = V[0].clone()
+        self.vref = nominal_state(solver, self.g, tol, max_iter, self.dev)
+        self.va_ref = self.torch.angle(self.vref)
 
     def generate(self, solver, n: int, lo: float = 0.7, hi: float = 1.3, seed: int = 12345, tol: float = 1e-10,
                  max_iter: int = 20, chunk: int = 8192, keep_all: bool = False):

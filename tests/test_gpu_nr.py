@@ -140,6 +140,26 @@ def test_10000_mixed_matches_oracle(oracle):
     assert dv.max() <= 1e-8, (int(dv.argmax()), float(dv.max()))
 
 
+def test_10000_nominal_state_warm_start(oracle):
+    """The 10,000-bus x 64 workload started from the converged nominal-load
+    state (cupf.warm_start.nominal_state): fewer Newton norms than from the
+    flat start, and every scenario within 1e-8 of the oracle's flat-start
+    solution."""
+    from cupf.warm_start import nominal_state
+
+    g = G.grid_10000()
+    B = 64
+    S = g.scenarios(B, seed=29)
+    s = make_solver(g, cupf.ComputePolicy.Mixed)
+    vnom = nominal_state(s, g).cpu().numpy()
+    flat = solve(s, g, S, g.flat_start(B), cfg(max_iter=20))
+    warm = solve(s, g, S, np.repeat(vnom[None, :], B, axis=0), cfg(max_iter=20))
+    assert warm.converged_numpy.all() and flat.converged_numpy.all()
+    assert warm.iterations_numpy.max() < flat.iterations_numpy.max()
+    dv = max_dv_vs_oracle(oracle, g, S, g.flat_start(B), warm.V_numpy)
+    assert dv.max() <= 1e-8, (int(dv.argmax()), float(dv.max()))
+
+
 def test_identical_rows_agree():
     """test_cpu_solver.cpp:355-359: batch rows of the same case agree."""
     g = G.grid_118()
