@@ -646,6 +646,14 @@ def run_extras(args, dev) -> dict:
             conv = sum(int((fm <= TOL).sum()) for _, fm, _ in r)
         res[mode] = {"ms": round(statistics.mean(ts), 3), "converged": conv,
                      "value": round(conv / (statistics.mean(ts) / 1e3), 1)}
+    # every instance of the last concurrent solve against the FP64 oracle
+    r = ub.solve(S, V0, cfg, concurrent=True)
+    per_grid = {}
+    for i, ((g, c), (v, _, _)) in enumerate(zip(inst, r)):
+        a = accuracy_vs_oracle(g, S[i].cpu().numpy(), V0[i].cpu().numpy(), {"v": v})
+        per_grid[str(g.n_bus)] = {"max_abs_dV_vs_fp64_oracle": a["v"]["max_abs_dV_vs_fp64_oracle"],
+                                  "within_1e-8": a["v"]["within_1e-8"], "scenarios_checked": c}
+    res["accuracy"] = per_grid
     out["uneven_batch"] = {"instances": sum(c for _, c in inst),
                            "grids": [[g.n_bus, c] for g, c in inst], "unit": UNIT,
                            "method": "one engine + CUDA stream per grid, host thread per grid; streams prioritized "

@@ -33,6 +33,8 @@ struct DevPlan {
   const int* crow_ptr = nullptr;
   const int* crow_child = nullptr;
   const int* crow_r = nullptr;
+  const long long* crow_src = nullptr;  // per child entry: its update-vector element, tv_off[child] + row
+  const int* crow_dst = nullptr;        // per child entry: its row in the parent front
   const int* asm_ptr = nullptr;
   const int* asm_local = nullptr;
   const int* perm = nullptr;   // permuted index -> Jacobian row

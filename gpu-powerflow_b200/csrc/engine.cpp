@@ -98,7 +98,7 @@ struct Engine::Impl {
       jt_ptr, jt_row, jt_q;
   // factor program
   DBuf fsz, nc, first, front_ptr, front_rows, u_off, l_off, cb_off, tv_off, arow_ptr, arow_q, arow_col, crow_ptr,
-      crow_child, crow_r, asm_ptr, asm_local, perm, iperm, row_iperm, col_perm, level_fronts, fe_split, fe_dst, fe_src, front_meta;
+      crow_child, crow_r, crow_src, crow_dst, asm_ptr, asm_local, perm, iperm, row_iperm, col_perm, level_fronts, fe_split, fe_dst, fe_src, front_meta;
   std::vector<LevelLaunch> levels;
   // backward sweep: the narrow top levels (launch-list entries from bw_first
   // on) run as one launch over bw_bounds (descending level boundaries)
@@ -356,6 +356,21 @@ void Engine::upload_plan() {
     for (int32_t p = 0; p < fp_.P; ++p) tv[p + 1] = tv[p] + (fp_.fsz[p] - fp_.nc[p]);
     d.tv_total = tv[fp_.P];
     d.tv_off.upload(tv);
+    // the sweeps' gather list: each child entry's update-vector element and
+    // its row in the parent front (entries are grouped by front row)
+    const size_t ne = fp_.crow_child.size();
+    std::vector<long long> src(std::max<size_t>(ne, 1), 0);
+    std::vector<int32_t> dst(std::max<size_t>(ne, 1), 0);
+    for (int32_t p = 0; p < fp_.P; ++p)
+      for (int32_t i = 0; i < fp_.fsz[p]; ++i) {
+        const int32_t fr = fp_.front_ptr[p] + i;
+        for (int32_t e = fp_.crow_ptr[fr]; e < fp_.crow_ptr[fr + 1]; ++e) {
+          src[e] = tv[fp_.crow_child[e]] + fp_.crow_r[e];
+          dst[e] = i;
+        }
+      }
+    d.crow_src.upload(src);
+    d.crow_dst.upload(dst);
   }
   d.arow_ptr.upload(fp_.arow_ptr);
   d.arow_q.upload(fp_.arow_q);
@@ -508,6 +523,8 @@ void Engine::upload_plan() {
   pl.crow_ptr = d.crow_ptr.as<int>();
   pl.crow_child = d.crow_child.as<int>();
   pl.crow_r = d.crow_r.as<int>();
+  pl.crow_src = d.crow_src.as<long long>();
+  pl.crow_dst = d.crow_dst.as<int>();
   pl.asm_ptr = d.asm_ptr.as<int>();
   pl.asm_local = d.asm_local.as<int>();
   pl.perm = d.perm.as<int>();

@@ -1142,56 +1142,125 @@ __global__ void __launch_bounds__(256)
 }
 
 // ---------------------------------------------------------------------------
-// Standalone forward substitution L y = P b (leaves first) for a right-hand
+// Triangular sweeps for right-hand sides given after factorization: the
+// standalone forward substitution and the two adjoint sweeps.  One block per
+// (front, 32 scenarios), one launch per level, chained.  The block's warps
+// split the front's rows: two on wide levels, up to 8 on the narrow top of the
+// tree, so the latency of a large front's loads is spread over more warps.
+//
+// Children's update vectors are gathered into a front's rows (extend-add)
+// from one list per front, sorted by row: each entry holds its absolute
+// update-vector element (crow_src) and its row in the front (crow_dst).  A
+// warp gathers its rows [r0, r1): the lanes fetch 32 list entries in one
+// request, the values of 8 entries are requested together, and each row's
+// entries are summed in list order into ts[row * 32] (ts: this lane's column
+// of the block's [fs][32] area in shared memory; rows without entries get 0).
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ void gather_child_updates(const DevPlan& pl, int fr0, int r0, int r1, size_t b, int Bp,
+                                                     const T* __restrict__ TV, T* __restrict__ ts) {
+  const int lane = threadIdx.x & 31;
+  for (int i = r0; i < r1; ++i) ts[i * kWarp] = T(0);
+  const int e0 = pl.crow_ptr[fr0 + r0], e1 = pl.crow_ptr[fr0 + r1];
+  int cur = -1;
+  T acc = T(0);
+  for (int c = e0; c < e1; c += kWarp) {
+    const int n = min(kWarp, e1 - c);
+    long long src = 0;
+    int dst = -1;
+    if (lane < n) {
+      src = pl.crow_src[c + lane];
+      dst = pl.crow_dst[c + lane];
+    }
+    for (int u0 = 0; u0 < n; u0 += 8) {  // u0 + u <= 31
+      T v[8];
+      int d[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const long long sv = __shfl_sync(0xffffffffu, src, u0 + u);
+        d[u] = __shfl_sync(0xffffffffu, dst, u0 + u);
+        v[u] = d[u] >= 0 ? TV[(size_t)sv * Bp + b] : T(0);
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+        if (d[u] >= 0) {
+          if (d[u] != cur) {
+            if (cur >= 0) ts[cur * kWarp] = acc;
+            cur = d[u];
+            acc = T(0);
+          }
+          acc += v[u];
+        }
+    }
+  }
+  if (cur >= 0) ts[cur * kWarp] = acc;
+}
+
+// A sweep block's item: front p of the level, scenario b of this lane.
+struct SweepItem {
+  int p, fs, nc, fr0, first;
+  size_t b;
+};
+
+__device__ __forceinline__ SweepItem sweep_item(const DevPlan& pl, int level_begin, int groups) {
+  SweepItem it;
+  it.p = pl.level_fronts[level_begin + blockIdx.x / groups];
+  it.b = (size_t)(blockIdx.x % groups) * kWarp + (threadIdx.x & 31);
+  it.fs = pl.fsz[it.p];
+  it.nc = pl.nc[it.p];
+  it.fr0 = pl.front_ptr[it.p];
+  it.first = pl.first[it.p];
+  return it;
+}
+
+// Standalone forward substitution L y = P b (leaves first), for a right-hand
 // side supplied after factorization (linear-solver boundary).  A front gathers
 // its children's update vectors (extend-add of sum_m L21[.][m] y_m), solves its
 // unit-lower pivot block and emits its own update vector.
-// ---------------------------------------------------------------------------
-template <typename T, int FMAX, int NCMAX>
-__global__ void __launch_bounds__(128)
-    k_l_forward_level(DevPlan pl, int level_begin, int level_count, int groups, int Bp, const T* __restrict__ U,
-                      const T* __restrict__ L, const double* __restrict__ G, T* __restrict__ TV, T* __restrict__ Yo) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const long item = (long)blockIdx.x * (blockDim.x >> 5) + warp;
-  if (item >= (long)level_count * groups) return;
-  const int p = pl.level_fronts[level_begin + item / groups];
-  const size_t b = (size_t)(item % groups) * kWarp + lane;
-  const int fs = pl.fsz[p], nc = pl.nc[p];
-  const int fr0 = pl.front_ptr[p], first = pl.first[p];
-  const long long uo = pl.u_off[p], lo = pl.l_off[p];
-  T t[FMAX];
+// Shared memory: [fs_cap][32] gathered rows, [8][32] pivot values.
+template <typename T, int NCMAX>
+__global__ void __launch_bounds__(256)
+    k_l_forward_level(DevPlan pl, int level_begin, int groups, int Bp, int fs_cap, const T* __restrict__ U,
+                      const T* __restrict__ L, const double* __restrict__ G, T* __restrict__ TV,
+                      T* __restrict__ Yo) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  chain_allow_next();
+  const int W = blockDim.x >> 5, warp = threadIdx.x >> 5;
+  const SweepItem it = sweep_item(pl, level_begin, groups);
+  const int fs = it.fs, nc = it.nc;
+  const size_t b = it.b;
+  const long long uo = pl.u_off[it.p], lo = pl.l_off[it.p], to = pl.tv_off[it.p];
+  T* ts = reinterpret_cast<T*>(smem_raw) + (threadIdx.x & 31);
+  T* ys = ts + (size_t)fs_cap * kWarp;
+  chain_wait_previous();
+  gather_child_updates(pl, it.fr0, warp * fs / W, (warp + 1) * fs / W, b, Bp, TV, ts);
+  __syncthreads();
+  if (warp == 0) {
+    T y[NCMAX];
 #pragma unroll
-  for (int j = 0; j < FMAX; ++j) t[j] = T(0);
-  for (int i = 0; i < fs; ++i) {
-    T acc = T(0);
-    for (int e = pl.crow_ptr[fr0 + i]; e < pl.crow_ptr[fr0 + i + 1]; ++e)
-      acc += TV[(size_t)(pl.tv_off[pl.crow_child[e]] + pl.crow_r[e]) * Bp + b];
+    for (int k = 0; k < NCMAX; ++k) {
+      y[k] = T(0);
+      if (k < nc) {
+        T s = static_cast<T>(G[(size_t)pl.perm[it.first + k] * Bp + b]) - ts[k * kWarp];
 #pragma unroll
-    for (int j = 0; j < FMAX; ++j)
-      if (j == i) t[j] = acc;
+        for (int m = 0; m < k; ++m) s -= U[(size_t)(uo + (long long)k * fs + m) * Bp + b] * y[m];
+        y[k] = s;
+        ys[k * kWarp] = s;
+        Yo[(size_t)(it.first + k) * Bp + b] = s;
+      }
+    }
   }
+  __syncthreads();
   T y[NCMAX];
 #pragma unroll
-  for (int k = 0; k < NCMAX; ++k) {
-    y[k] = T(0);
-    if (k < nc) {
-      T s = static_cast<T>(G[(size_t)pl.perm[first + k] * Bp + b]) - t[k];
+  for (int m = 0; m < NCMAX; ++m) y[m] = m < nc ? ys[m * kWarp] : T(0);
+#pragma unroll 4
+  for (int j = nc + warp; j < fs; j += W) {
+    T s = ts[j * kWarp];
 #pragma unroll
-      for (int m = 0; m < k; ++m) s -= U[(size_t)(uo + (long long)k * fs + m) * Bp + b] * y[m];
-      y[k] = s;
-      Yo[(size_t)(first + k) * Bp + b] = s;
-    }
-  }
-  const long long to = pl.tv_off[p];
-#pragma unroll
-  for (int j = 0; j < FMAX; ++j) {
-    if (j >= nc && j < fs) {
-      T s = t[j];
-#pragma unroll
-      for (int m = 0; m < NCMAX; ++m)
-        if (m < nc) s += L[(size_t)(lo + (long long)(j - nc) * nc + m) * Bp + b] * y[m];
-      TV[(size_t)(to + (j - nc)) * Bp + b] = s;
-    }
+    for (int m = 0; m < NCMAX; ++m)
+      if (m < nc) s += L[(size_t)(lo + (long long)(j - nc) * nc + m) * Bp + b] * y[m];
+    TV[(size_t)(to + (j - nc)) * Bp + b] = s;
   }
 }
 
@@ -1200,137 +1269,122 @@ __global__ void __launch_bounds__(128)
 //   U^T w = P g (leaves first) and L^T z = w (root first), lambda = P^T z.
 // U^T forward: a front gathers its children's update vectors t (extend-add of
 // sum_m U12[m][.] w_m), solves its pivots and emits its own t for the parent.
+// Shared memory: [fs_cap][32] gathered rows, [8][32] pivot values.
 // ---------------------------------------------------------------------------
-template <typename T, int FMAX, int NCMAX>
-__global__ void __launch_bounds__(128)
-    k_ut_forward_level(DevPlan pl, int level_begin, int level_count, int groups, int Bp, const T* __restrict__ U,
-                       const double* __restrict__ G, T* __restrict__ TV, T* __restrict__ W) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const long item = (long)blockIdx.x * (blockDim.x >> 5) + warp;
-  if (item >= (long)level_count * groups) return;
-  const int p = pl.level_fronts[level_begin + item / groups];
-  const size_t b = (size_t)(item % groups) * kWarp + lane;
-  const int fs = pl.fsz[p], nc = pl.nc[p];
-  const int fr0 = pl.front_ptr[p], first = pl.first[p];
-  const long long uo = pl.u_off[p];
-  T t[FMAX];
+template <typename T, int NCMAX>
+__global__ void __launch_bounds__(256)
+    k_ut_forward_level(DevPlan pl, int level_begin, int groups, int Bp, int fs_cap, const T* __restrict__ U,
+                       const double* __restrict__ G, T* __restrict__ TV, T* __restrict__ Wv) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  chain_allow_next();
+  const int W = blockDim.x >> 5, warp = threadIdx.x >> 5;
+  const SweepItem it = sweep_item(pl, level_begin, groups);
+  const int fs = it.fs, nc = it.nc;
+  const size_t b = it.b;
+  const long long uo = pl.u_off[it.p], to = pl.tv_off[it.p];
+  T* ts = reinterpret_cast<T*>(smem_raw) + (threadIdx.x & 31);
+  T* wsm = ts + (size_t)fs_cap * kWarp;
+  chain_wait_previous();
+  gather_child_updates(pl, it.fr0, warp * fs / W, (warp + 1) * fs / W, b, Bp, TV, ts);
+  __syncthreads();
+  if (warp == 0) {
+    T w[NCMAX];
 #pragma unroll
-  for (int j = 0; j < FMAX; ++j) t[j] = T(0);
-  // gather children's update vectors into this front's rows
-  for (int i = 0; i < fs; ++i) {
-    T acc = T(0);
-    for (int e = pl.crow_ptr[fr0 + i]; e < pl.crow_ptr[fr0 + i + 1]; ++e)
-      acc += TV[(size_t)(pl.tv_off[pl.crow_child[e]] + pl.crow_r[e]) * Bp + b];
+    for (int k = 0; k < NCMAX; ++k) {
+      w[k] = T(0);
+      if (k < nc) {
+        // J^T's right-hand side is indexed by Jacobian columns
+        T s = static_cast<T>(G[(size_t)pl.col_perm[it.first + k] * Bp + b]) - ts[k * kWarp];
 #pragma unroll
-    for (int j = 0; j < FMAX; ++j)
-      if (j == i) t[j] = acc;
+        for (int m = 0; m < k; ++m) s -= U[(size_t)(uo + (long long)m * fs + k) * Bp + b] * w[m];
+        w[k] = s / U[(size_t)(uo + (long long)k * fs + k) * Bp + b];
+        wsm[k * kWarp] = w[k];
+        Wv[(size_t)(it.first + k) * Bp + b] = w[k];
+      }
+    }
   }
+  __syncthreads();
   T w[NCMAX];
 #pragma unroll
-  for (int k = 0; k < NCMAX; ++k) {
-    w[k] = T(0);
-    if (k < nc) {
-      // J^T's right-hand side is indexed by Jacobian columns
-      T s = static_cast<T>(G[(size_t)pl.col_perm[first + k] * Bp + b]) - t[k];
+  for (int m = 0; m < NCMAX; ++m) w[m] = m < nc ? wsm[m * kWarp] : T(0);
+#pragma unroll 4
+  for (int j = nc + warp; j < fs; j += W) {
+    T s = ts[j * kWarp];
 #pragma unroll
-      for (int m = 0; m < k; ++m) s -= U[(size_t)(uo + (long long)m * fs + k) * Bp + b] * w[m];
-      w[k] = s / U[(size_t)(uo + (long long)k * fs + k) * Bp + b];
-      W[(size_t)(first + k) * Bp + b] = w[k];
-    }
-  }
-  const long long to = pl.tv_off[p];
-#pragma unroll
-  for (int j = 0; j < FMAX; ++j) {
-    if (j >= nc && j < fs) {
-      T s = t[j];
-#pragma unroll
-      for (int m = 0; m < NCMAX; ++m)
-        if (m < nc) s += U[(size_t)(uo + (long long)m * fs + j) * Bp + b] * w[m];
-      TV[(size_t)(to + (j - nc)) * Bp + b] = s;
-    }
+    for (int m = 0; m < NCMAX; ++m)
+      if (m < nc) s += U[(size_t)(uo + (long long)m * fs + j) * Bp + b] * w[m];
+    TV[(size_t)(to + (j - nc)) * Bp + b] = s;
   }
 }
 
-// L^T backward: z_k = w_k - sum_{m>k} L11[m][k] z_m - sum_jj L21[jj][k] z(row jj)
-template <typename T, int FMAX, int NCMAX>
-__global__ void __launch_bounds__(128)
-    k_lt_backward_level(DevPlan pl, int level_begin, int level_count, int groups, int Bp, const T* __restrict__ U,
-                        const T* __restrict__ L, const T* __restrict__ W, T* __restrict__ Z) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const long item = (long)blockIdx.x * (blockDim.x >> 5) + warp;
-  if (item >= (long)level_count * groups) return;
-  const int p = pl.level_fronts[level_begin + item / groups];
-  const size_t b = (size_t)(item % groups) * kWarp + lane;
-  const int fs = pl.fsz[p], nc = pl.nc[p];
-  const int fr0 = pl.front_ptr[p], first = pl.first[p];
-  const long long uo = pl.u_off[p], lo = pl.l_off[p];
-  T zc[FMAX];
+// L^T backward: z_k = w_k - sum_{m>k} L11[m][k] z_m - sum_jj L21[jj][k] z(row jj).
+// The warps split the non-pivot rows jj (ancestors' z, from earlier launches)
+// and each sums its rows' L21 terms for every k; warp 0 then solves the pivot
+// block with those partial sums (shared memory [W][8][32]).
+template <typename T, int NCMAX>
+__global__ void __launch_bounds__(256)
+    k_lt_backward_level(DevPlan pl, int level_begin, int groups, int Bp, const T* __restrict__ U,
+                        const T* __restrict__ L, const T* __restrict__ Wv, T* __restrict__ Z) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  chain_allow_next();
+  const int W = blockDim.x >> 5, warp = threadIdx.x >> 5;
+  const SweepItem it = sweep_item(pl, level_begin, groups);
+  const int fs = it.fs, nc = it.nc;
+  const size_t b = it.b;
+  const long long uo = pl.u_off[it.p], lo = pl.l_off[it.p];
+  T* ps = reinterpret_cast<T*>(smem_raw) + (threadIdx.x & 31);
+  chain_wait_previous();
+  T acc[NCMAX];
 #pragma unroll
-  for (int j = 0; j < FMAX; ++j)
-    zc[j] = (j >= nc && j < fs) ? Z[(size_t)pl.front_rows[fr0 + j] * Bp + b] : T(0);
-  T z[NCMAX];
+  for (int k = 0; k < NCMAX; ++k) acc[k] = T(0);
+#pragma unroll 2
+  for (int j = nc + warp; j < fs; j += W) {
+    const T zj = Z[(size_t)pl.front_rows[it.fr0 + j] * Bp + b];
 #pragma unroll
-  for (int k = NCMAX - 1; k >= 0; --k) {
-    z[k] = T(0);
-    if (k < nc) {
-      T s = W[(size_t)(first + k) * Bp + b];
+    for (int k = 0; k < NCMAX; ++k)
+      if (k < nc) acc[k] += L[(size_t)(lo + (long long)(j - nc) * nc + k) * Bp + b] * zj;
+  }
 #pragma unroll
-      for (int m = k + 1; m < NCMAX; ++m)
-        if (m < nc) s -= U[(size_t)(uo + (long long)m * fs + k) * Bp + b] * z[m];
+  for (int k = 0; k < NCMAX; ++k) ps[(warp * NCMAX + k) * kWarp] = acc[k];
+  __syncthreads();
+  if (warp == 0) {
+    T z[NCMAX];
 #pragma unroll
-      for (int j = 0; j < FMAX; ++j)
-        if (j >= nc && j < fs) s -= L[(size_t)(lo + (long long)(j - nc) * nc + k) * Bp + b] * zc[j];
-      z[k] = s;
-      Z[(size_t)(first + k) * Bp + b] = s;
+    for (int k = NCMAX - 1; k >= 0; --k) {
+      z[k] = T(0);
+      if (k < nc) {
+        T s = Wv[(size_t)(it.first + k) * Bp + b];
+#pragma unroll
+        for (int m = k + 1; m < NCMAX; ++m)
+          if (m < nc) s -= U[(size_t)(uo + (long long)m * fs + k) * Bp + b] * z[m];
+        for (int w = 0; w < W; ++w) s -= ps[(w * NCMAX + k) * kWarp];
+        z[k] = s;
+        Z[(size_t)(it.first + k) * Bp + b] = s;
+      }
     }
   }
 }
 
 // ---------------------------------------------------------------------------
-// Launch helpers: pick the front-size bucket of a level.
+// Sweep launches.
 // ---------------------------------------------------------------------------
-inline int bucket_of(int fmax) {
-  if (fmax <= 8) return 8;
-  if (fmax <= 16) return 16;
-  if (fmax <= 32) return 32;
-  if (fmax <= 64) return 64;
-  if (fmax <= 128) return 128;
-  return -1;
+// Warps per block of a sweep launch: two where the level has many items
+// (fronts x scenario groups; at most 32 blocks are resident on an SM, so one
+// warp per block would leave half of its warp slots empty), up to 8 on the
+// narrow levels.
+inline int sweep_warps(long items) {
+  if (items >= 512) return 2;
+  if (items >= 128) return 4;
+  return 8;
 }
 
-template <typename T, int FMAX, int NCMAX>
-void launch_lf_t(const LevelLaunch& lv, const AdjointSweepArgs<T>& a, cudaStream_t s) {
-  const long items = (long)lv.count * a.groups;
-  const unsigned blocks = (unsigned)((items + 3) / 4);
-  k_l_forward_level<T, FMAX, NCMAX><<<blocks, 128, 0, s>>>(a.plan, lv.begin, lv.count, a.groups, a.Bp, a.U, a.L,
-                                                          a.G, a.TV, a.W);
+template <typename... KArgs, typename... Args>
+void launch_sweep(void (*kern)(KArgs...), long items, int warps, size_t smem, cudaStream_t s, const char* what,
+                  Args&&... args) {
+  if (smem > kSmemLimit) throw std::runtime_error(std::string(what) + ": front too large for shared memory");
+  allow_full_smem(reinterpret_cast<const void*>(kern));
+  launch_chained(kern, dim3((unsigned)items), dim3(warps * kWarp), smem, s, what, std::forward<Args>(args)...);
 }
-
-template <typename T, int FMAX, int NCMAX>
-void launch_ut_t(const LevelLaunch& lv, const AdjointSweepArgs<T>& a, cudaStream_t s) {
-  const long items = (long)lv.count * a.groups;
-  const unsigned blocks = (unsigned)((items + 3) / 4);
-  k_ut_forward_level<T, FMAX, NCMAX><<<blocks, 128, 0, s>>>(a.plan, lv.begin, lv.count, a.groups, a.Bp, a.U, a.G,
-                                                           a.TV, a.W);
-}
-
-template <typename T, int FMAX, int NCMAX>
-void launch_lt_t(const LevelLaunch& lv, const AdjointSweepArgs<T>& a, cudaStream_t s) {
-  const long items = (long)lv.count * a.groups;
-  const unsigned blocks = (unsigned)((items + 3) / 4);
-  k_lt_backward_level<T, FMAX, NCMAX><<<blocks, 128, 0, s>>>(a.plan, lv.begin, lv.count, a.groups, a.Bp, a.U, a.L,
-                                                            a.W, a.Z);
-}
-
-#define CUPF_BUCKET_SWITCH(NCMAX, CALL)                                        \
-  switch (bucket_of(lv.max_fsz)) {                                             \
-    case 8: CALL(8, NCMAX); break;                                             \
-    case 16: CALL(16, NCMAX); break;                                           \
-    case 32: CALL(32, NCMAX); break;                                           \
-    case 64: CALL(64, NCMAX); break;                                           \
-    case 128: CALL(128, NCMAX); break;                                         \
-    default: throw std::runtime_error("front larger than 128 rows is not supported"); \
-  }
 
 }  // namespace
 
@@ -1537,37 +1591,29 @@ void launch_backward_top(const LevelLaunch& top, const int* lv_bounds, int nlev,
 template <typename T>
 void launch_ut_forward_level(const LevelLaunch& lv, const AdjointSweepArgs<T>& a, cudaStream_t s) {
   if (lv.count == 0) return;
-  if (lv.max_nc <= 8) {
-#define CALL(F, N) launch_ut_t<T, (F < 8 ? 8 : F), N>(lv, a, s)
-    CUPF_BUCKET_SWITCH(8, CALL)
-#undef CALL
-  } else {
-    throw std::runtime_error("panels wider than 8 columns are not supported (max_panel_width <= 8)");
-  }
+  if (lv.max_nc > 8) throw std::runtime_error("panels wider than 8 columns are not supported (max_panel_width <= 8)");
+  const long items = (long)lv.count * a.groups;
+  launch_sweep(k_ut_forward_level<T, 8>, items, sweep_warps(items), (size_t)(lv.max_fsz + 8) * kWarp * sizeof(T), s,
+               "adjoint sweep (U^T)", a.plan, lv.begin, a.groups, a.Bp, lv.max_fsz, a.U, a.G, a.TV, a.W);
 }
 
 template <typename T>
 void launch_l_forward_level(const LevelLaunch& lv, const AdjointSweepArgs<T>& a, cudaStream_t s) {
   if (lv.count == 0) return;
-  if (lv.max_nc <= 8) {
-#define CALL(F, N) launch_lf_t<T, (F < 8 ? 8 : F), N>(lv, a, s)
-    CUPF_BUCKET_SWITCH(8, CALL)
-#undef CALL
-  } else {
-    throw std::runtime_error("panels wider than 8 columns are not supported (max_panel_width <= 8)");
-  }
+  if (lv.max_nc > 8) throw std::runtime_error("panels wider than 8 columns are not supported (max_panel_width <= 8)");
+  const long items = (long)lv.count * a.groups;
+  launch_sweep(k_l_forward_level<T, 8>, items, sweep_warps(items), (size_t)(lv.max_fsz + 8) * kWarp * sizeof(T), s,
+               "forward substitution", a.plan, lv.begin, a.groups, a.Bp, lv.max_fsz, a.U, a.L, a.G, a.TV, a.W);
 }
 
 template <typename T>
 void launch_lt_backward_level(const LevelLaunch& lv, const AdjointSweepArgs<T>& a, cudaStream_t s) {
   if (lv.count == 0) return;
-  if (lv.max_nc <= 8) {
-#define CALL(F, N) launch_lt_t<T, (F < 8 ? 8 : F), N>(lv, a, s)
-    CUPF_BUCKET_SWITCH(8, CALL)
-#undef CALL
-  } else {
-    throw std::runtime_error("panels wider than 8 columns are not supported (max_panel_width <= 8)");
-  }
+  if (lv.max_nc > 8) throw std::runtime_error("panels wider than 8 columns are not supported (max_panel_width <= 8)");
+  const long items = (long)lv.count * a.groups;
+  const int warps = sweep_warps(items);
+  launch_sweep(k_lt_backward_level<T, 8>, items, warps, (size_t)warps * 8 * kWarp * sizeof(T), s,
+               "adjoint sweep (L^T)", a.plan, lv.begin, a.groups, a.Bp, a.U, a.L, a.W, a.Z);
 }
 
 }  // namespace cupf_b200
