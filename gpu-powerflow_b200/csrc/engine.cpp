@@ -892,15 +892,22 @@ void Engine::autotune_factor(cudaStream_t s, const void* J) {
   }
   // shapes: warps per block (1, 2, 4, 8), and for the register tier where
   // the dense fronts live (code = warps + 256 x placement: shared memory 1,
-  // global scratch 2)
+  // global scratch 2); and the wide tier with 8, 16 or 32 warps (placement
+  // 3) for the launches of large fronts (the wide tier's own launches take
+  // its 16 and 32 warps as their warp counts; other launches run their
+  // built-in rule under these codes)
   std::vector<int> cand;
   for (int p : {1, 2})
     for (int w : {1, 2, 4, 8}) cand.push_back(w + 256 * p);
+  for (int w : {8, 16, 32}) cand.push_back(w + 256 * 3);
   choose_block_shapes(
       d.levels.size(), cand,
       [&](size_t i, int code) {
-        d.levels[i].warps = code & 0xff;
-        d.levels[i].placement = d.levels[i].tier == 0 ? code >> 8 : 0;
+        LevelLaunch& lv = d.levels[i];
+        int w = code & 0xff, p = code >> 8;
+        if (p == 3 && !(lv.tier == 1 || wide_option(lv))) w = p = 0;
+        lv.warps = w;
+        lv.placement = lv.tier == 0 ? p : 0;
       },
       [&](size_t i) { launch_factor_level<T, T>(d.levels[i], a, s); }, s, "factor");
   d.tuned_Bp = d.Bp;
@@ -959,7 +966,8 @@ std::vector<int32_t> Engine::factor_level_warps() const {
 std::vector<int32_t> Engine::factor_level_placements() const {
   std::vector<int32_t> p;
   const size_t es = factor_is_double() ? sizeof(double) : sizeof(float);
-  for (const auto& lv : d_->levels) p.push_back(lv.tier > 0 ? 2 : (front_in_shared_memory(lv, es) ? 1 : 2));
+  for (const auto& lv : d_->levels)
+    p.push_back(lv.tier > 0 ? 2 : runs_wide(lv, es) ? 3 : (front_in_shared_memory(lv, es) ? 1 : 2));
   return p;
 }
 
@@ -1517,6 +1525,7 @@ void Engine::factor_all_external(cudaStream_t s, const void* J, T* scratch, size
   }
   for (LevelLaunch lv : d.levels) {
     lv.placement = 0;  // the built-in placement: the static area is sized for it
+    if (lv.tier == 0 && lv.warps > 8) lv.warps = 0;  // (a wide-tier shape of the autotuner)
     launch_factor_level<T, T>(lv, a, s);
     ++launches_;
   }

@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 
 #include "device_plan.cuh"
@@ -28,7 +29,9 @@ struct LevelLaunch {
   int tier = 0;
   // register tier: where the dense fronts live -- 0 the built-in rule
   // (front_in_shared_memory), 1 shared memory, 2 the global scratch (chosen
-  // by the engine's autotuner; a choice that does not fit falls back to the rule)
+  // by the engine's autotuner; a choice that does not fit falls back to the
+  // rule); 3 the wide tier instead of register rows (fronts of at least
+  // kWideOptionRows rows; same factors)
   int placement = 0;
 };
 
@@ -147,6 +150,12 @@ constexpr int kWideFrontRows = 65;
 // unless configured or autotuned otherwise; the autotuner tries 33, 49 and 65.
 constexpr int kTcDefaultMinFront = 65;
 constexpr int kTcSmallestMinFront = 33;  // the smallest threshold the autotuner tries
+// Register-tier launches whose fronts reach this many rows may run the wide
+// tier instead (placement 3, an autotuner choice): a few large fronts per
+// launch go faster with up to 32 warps over their columns and rows than with
+// at most 8 warps of register rows.
+constexpr int kWideOptionRows = 33;
+
 
 // Shared-memory plan of a wide-tier launch: pivot reciprocals, the staged
 // source rows, and `reserve` bytes after them for the kernel's other arrays
@@ -189,6 +198,19 @@ inline FrontSmem plan_wide_smem(const LevelLaunch& lv, size_t elem_bytes) {
   return sm;
 }
 
+inline bool wide_option(const LevelLaunch& lv) { return lv.tier == 0 && lv.max_fsz >= kWideOptionRows; }
+
+// Whether a factor launch runs the wide tier: its own tier, fronts past the
+// register kernels, the autotuner's placement 3, or -- the built-in rule --
+// large fronts that would not fit in shared memory (register rows over a
+// front in the L2 scratch are the slowest of the choices there).
+inline bool runs_wide(const LevelLaunch& lv, size_t elem_bytes) {
+  if (lv.tier == 1 || lv.max_fsz >= kWideFrontRows) return true;
+  if (!wide_option(lv)) return false;
+  if (lv.placement == 3) return true;
+  return lv.placement == 0 && !front_in_shared_memory(lv, elem_bytes);
+}
+
 // Elements (x 32 scenario lanes) of global scratch one block of a wide-tier
 // launch uses: its dense front, plus the pivot rows when they are not in
 // shared memory.
@@ -201,7 +223,7 @@ inline size_t wide_block_elems(const LevelLaunch& lv, size_t elem_bytes) {
 // blocks (groups = 32-scenario groups of the batch) with its current tier
 // and placement; 0 when its fronts live in shared memory.
 inline size_t level_scratch_elems(const LevelLaunch& lv, size_t elem_bytes, int groups) {
-  if (lv.tier > 0) return wide_block_elems(lv, elem_bytes) * lv.count * groups;
+  if (lv.tier > 0 || runs_wide(lv, elem_bytes)) return wide_block_elems(lv, elem_bytes) * lv.count * groups;
   if (front_in_shared_memory(lv, elem_bytes)) return 0;
   return (size_t)lv.max_fsz * (lv.max_fsz + 1) * lv.count * groups;
 }
@@ -210,8 +232,11 @@ inline size_t level_scratch_elems(const LevelLaunch& lv, size_t elem_bytes, int 
 // gives it (the workspace is sized for this).
 inline size_t level_scratch_capacity(const LevelLaunch& lv, size_t elem_bytes, int groups) {
   if (lv.tier > 0) return level_scratch_elems(lv, elem_bytes, groups);
-  if (plan_front_smem(lv, elem_bytes, false).total() > kSmemLimit) return 0;
-  return (size_t)lv.max_fsz * (lv.max_fsz + 1) * lv.count * groups;
+  size_t c = plan_front_smem(lv, elem_bytes, false).total() > kSmemLimit
+                 ? 0
+                 : (size_t)lv.max_fsz * (lv.max_fsz + 1) * lv.count * groups;
+  if (wide_option(lv)) c = std::max(c, wide_block_elems(lv, elem_bytes) * lv.count * groups);
+  return c;
 }
 
 template <typename T>

@@ -160,6 +160,20 @@ __device__ __forceinline__ void cp_async_wait() {
 // of the global scratch, whose per-block stride is front_elems x 32) and
 // assemble it.  Returns the launch record; *Fm_out is the assembled front
 // [fs][fs + 1][32].
+// The first entry at or after x of the destination-sorted list d that
+// starts a new destination within the range [A0, Z0) (A0 itself counts as a
+// start; x >= A0), or Z0: a warp-wide scan, 32 entries a step.
+__device__ __forceinline__ int run_start(const int* d, int x, int A0, int Z0) {
+  const int lane = threadIdx.x & 31;
+  for (int base = x; base < Z0; base += kWarp) {
+    const int y = base + lane;
+    const bool cut = y >= Z0 || y <= A0 || d[y] != d[y - 1];
+    const unsigned m = __ballot_sync(0xffffffffu, cut);
+    if (m) return base + __ffs(m) - 1;
+  }
+  return Z0;
+}
+
 template <typename T, typename TJ, bool SMEM_FRONT, bool STAGE_LIST = true>
 __device__ __forceinline__ FrontMeta stage_and_assemble(const DevPlan& pl, int level_begin, long long fe_base,
                                                         int fe_pad, int groups, int Bp, int front_elems,
@@ -244,10 +258,21 @@ __device__ __forceinline__ FrontMeta stage_and_assemble(const DevPlan& pl, int l
 
   // phase 2: assembly.  Warp w owns the destination-disjoint range
   // [split[8w/W], split[8(w+1)/W]); consecutive entries with one destination
-  // are summed in a register (in list order) and stored once.
-  const int wa = warp * 8 / W, wz = (warp + 1) * 8 / W;
-  const int A = wa == 0 ? 0 : pl.front_meta[(size_t)q * kFrontMetaInts + 11 + wa];
-  const int Z = pl.front_meta[(size_t)q * kFrontMetaInts + 11 + wz];
+  // are summed in a register (in list order) and stored once.  With more
+  // than 8 warps (W a multiple of 8) the W/8 warps of a range divide it
+  // evenly, each cut moved forward to the next change of destination.
+  int A, Z;
+  if (W <= 8) {
+    const int wa = warp * 8 / W, wz = (warp + 1) * 8 / W;
+    A = wa == 0 ? 0 : pl.front_meta[(size_t)q * kFrontMetaInts + 11 + wa];
+    Z = pl.front_meta[(size_t)q * kFrontMetaInts + 11 + wz];
+  } else {
+    const int G = W / 8, g = warp / G, sub = warp - g * G;
+    const int A0 = g == 0 ? 0 : pl.front_meta[(size_t)q * kFrontMetaInts + 11 + g];
+    const int Z0 = pl.front_meta[(size_t)q * kFrontMetaInts + 11 + g + 1];
+    A = sub == 0 ? A0 : run_start(s_dst, A0 + (int)((long long)(Z0 - A0) * sub / G), A0, Z0);
+    Z = sub == G - 1 ? Z0 : run_start(s_dst, A0 + (int)((long long)(Z0 - A0) * (sub + 1) / G), A0, Z0);
+  }
   int cur = -1;
   T acc = T(0);
   for (int c = 0; c < nchunks; ++c) {
@@ -750,8 +775,10 @@ __device__ __forceinline__ void wide_pivot_rows(const FrontMeta& m, const T* Fl,
   for (int k = warp; k < nc; k += W) Y[(size_t)(m.first + k) * Bp + b] = Us[(size_t)(k * rw + fs) * LS];
 }
 
-template <typename T, typename TJ>
-__global__ void __launch_bounds__(256)
+// MAXW: the most warps a launch of this instance may have (8, 16 or 32;
+// 32 leaves 64 registers a thread).
+template <typename T, typename TJ, int MAXW = 8>
+__global__ void __launch_bounds__(MAXW * 32)
     k_front_factor_wide(DevPlan pl, int level_begin, long long fe_base, int fe_pad, int groups, int Bp,
                         int front_elems, FrontSmem sm, const TJ* __restrict__ J, const T* __restrict__ Fp,
                         T* __restrict__ U, T* __restrict__ L, T* __restrict__ CB, T* __restrict__ Y, int store_l,
@@ -1408,7 +1435,8 @@ void launch_factor_t(const LevelLaunch& lv, const FactorArgs<T, TJ>& a, cudaStre
   // for fronts of at most 10 rows; eight warps: 0.891 ms)
   int warps = fmax <= 16 ? 2 : (fmax <= 24 ? 4 : 8);
   if (items < 4L * 148) warps = 8;
-  if (lv.warps > 0) warps = lv.warps;  // chosen by the engine's autotuner
+  if (lv.warps > 0) warps = std::min(lv.warps, 8);  // chosen by the engine's autotuner (the wide tier's 16 and 32
+                                                   // warps are not register-kernel shapes)
   const size_t smem = sm.total();
   auto run = [&](auto kern) {
     allow_full_smem(reinterpret_cast<const void*>(kern));
@@ -1432,12 +1460,15 @@ void configure_front_kernels() {
   CUPF_ALLOW(8) CUPF_ALLOW(12) CUPF_ALLOW(16) CUPF_ALLOW(20) CUPF_ALLOW(24) CUPF_ALLOW(32) CUPF_ALLOW(48)
   CUPF_ALLOW(64)
 #undef CUPF_ALLOW
-  allow_full_smem(reinterpret_cast<const void*>(k_front_factor_wide<T, TJ>));
+  allow_full_smem(reinterpret_cast<const void*>(k_front_factor_wide<T, TJ, 8>));
+  allow_full_smem(reinterpret_cast<const void*>(k_front_factor_wide<T, TJ, 16>));
+  allow_full_smem(reinterpret_cast<const void*>(k_front_factor_wide<T, TJ, 32>));
   if constexpr (std::is_same<T, float>::value) allow_full_smem(reinterpret_cast<const void*>(k_front_factor_tc));
 }
 
-// A wide-tier launch: one block per front x 32 scenarios, 8 warps unless
-// the autotuner chose otherwise, dense fronts in the global scratch.
+// A wide-tier launch: one block per front x 32 scenarios, 8 to 32 warps
+// (the rule below unless the autotuner chose), dense fronts in the global
+// scratch.
 template <typename T, typename TJ>
 void launch_factor_wide(const LevelLaunch& lv, const FactorArgs<T, TJ>& a, cudaStream_t s) {
   const FrontSmem sm = plan_wide_smem(lv, sizeof(T));
@@ -1447,12 +1478,22 @@ void launch_factor_wide(const LevelLaunch& lv, const FactorArgs<T, TJ>& a, cudaS
   if (!a.front_scratch || a.front_scratch_elems < per_block * (size_t)items)
     throw std::runtime_error("wide front tier: the front scratch area is missing or too small");
   if (per_block > (size_t)INT32_MAX) throw std::runtime_error("wide front tier: front too large");
-  const int warps = lv.warps > 0 ? lv.warps : 8;
-  auto kern = k_front_factor_wide<T, TJ>;
-  allow_full_smem(reinterpret_cast<const void*>(kern));
-  launch_chained(kern, dim3((unsigned)items), dim3(warps * kWarp), sm.total(), s, "front factor (wide tier)", a.plan,
-                 lv.begin, lv.fe_base, lv.max_src, a.groups, a.Bp, (int)per_block, sm, a.J, a.Fp, a.U, a.L, a.CB, a.Y,
-                 a.store_l, a.eps, a.static_pivot, a.sing, a.front_scratch);
+  // built-in rule: the fewer the blocks, the more warps share a front (a
+  // launch of at most one block per SM gets 32)
+  const int rule = items <= 148 ? 32 : items <= 4 * 148 ? 16 : 8;
+  const int warps = lv.warps > 0 ? std::min(lv.warps, 32) : rule;
+  auto run = [&](auto kern) {
+    allow_full_smem(reinterpret_cast<const void*>(kern));
+    launch_chained(kern, dim3((unsigned)items), dim3(warps * kWarp), sm.total(), s, "front factor (wide tier)",
+                   a.plan, lv.begin, lv.fe_base, lv.max_src, a.groups, a.Bp, (int)per_block, sm, a.J, a.Fp, a.U, a.L,
+                   a.CB, a.Y, a.store_l, a.eps, a.static_pivot, a.sing, a.front_scratch);
+  };
+  // more than 8 warps split each assembly range at destination changes,
+  // which needs a multiple of 8
+  if (warps > 8 && warps % 8) throw std::runtime_error("wide front tier: more than 8 warps must be a multiple of 8");
+  if (warps <= 8) run(k_front_factor_wide<T, TJ, 8>);
+  else if (warps <= 16) run(k_front_factor_wide<T, TJ, 16>);
+  else run(k_front_factor_wide<T, TJ, 32>);
 }
 
 inline size_t single_front_bytes(const LevelLaunch& lv, size_t elem_bytes) {
@@ -1525,7 +1566,7 @@ void launch_factor_level(const LevelLaunch& lv, const FactorArgs<T, TJ>& a, cuda
     launch_factor_tc<T, TJ>(lv, a, s);
     return;
   }
-  if (lv.tier == 1 || lv.max_fsz >= kWideFrontRows) {
+  if (runs_wide(lv, sizeof(T))) {
     launch_factor_wide<T, TJ>(lv, a, s);
     return;
   }

@@ -8,10 +8,13 @@ phases with CUDA events, and report the relative residual of every system.
 
     python -m cupf.run_solver --matrix J.mtx --rhs F.mtx --batch 256 --precision tf32
     python -m cupf.run_solver --npz tests/golden/linsys_case8387pegase.npz --batch 256
+    python -m cupf.run_solver --npz tests/golden/linsys_case8387pegase.npz --batch 64 --transpose
 
 Prints one JSON object: dimensions, the plan's front sizes and per-launch
 kernel tiers, the median factorization and solve times, and the largest
 relative residual ||A_b x_b - r|| / ||r|| over the batch (FP64 on the host).
+With --transpose it also times the transposed solve A^T x = r on the same
+factors (the adjoint's U^T and L^T sweeps) and reports its residual.
 """
 from __future__ import annotations
 
@@ -59,6 +62,8 @@ def main(argv=None) -> int:
     ap.add_argument("--tc-min-front", type=int, default=0)
     ap.add_argument("--batch1-schedule", type=int, choices=(0, 1), default=0,
                     help="batch 1: 0 the single-system tree launch, 1 the batched lane kernels")
+    ap.add_argument("--transpose", action="store_true",
+                    help="also time the transposed solve A^T x = b on the same factors (the adjoint's sweeps)")
     args = ap.parse_args(argv)
 
     import scipy.sparse as sp
@@ -84,31 +89,40 @@ def main(argv=None) -> int:
     dt = torch.float64 if args.precision == "fp64" else torch.float32
     Vd = torch.tensor(V, dtype=dt, device=dev)
     R = torch.tensor(np.repeat(rhs[None, :], B, axis=0), dtype=torch.float64, device=dev)
-    tf, ts = [], []
-    x = None
+    tf, ts, tt = [], [], []
+    x = xt = None
     for k in range(args.warmup + args.repeat):
-        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
         e[0].record()
         ls.factorize(Vd)
         e[1].record()
         x = ls.solve(R)
         e[2].record()
-        e[2].synchronize()
+        if args.transpose:
+            xt = ls.solve_transpose(R)
+        e[3].record()
+        e[3].synchronize()
         if k >= args.warmup:
             tf.append(e[0].elapsed_time(e[1]))
             ts.append(e[1].elapsed_time(e[2]))
+            tt.append(e[2].elapsed_time(e[3]))
     xh = x.cpu().numpy()
-    res = []
+    xth = xt.cpu().numpy() if xt is not None else None
+    res, rest = [], []
     for b in range(B):
         A = sp.csr_matrix((V[b], ci, rp), shape=(n, n))
         res.append(float(np.linalg.norm(A @ xh[b] - rhs) / max(np.linalg.norm(rhs), 1e-300)))
+        if xth is not None:
+            rest.append(float(np.linalg.norm(A.T @ xth[b] - rhs) / max(np.linalg.norm(rhs), 1e-300)))
     fsz = ls.plan_array("fp_fsz")
+    extra = {"solve_transpose_ms": round(statistics.median(tt), 4),
+             "max_relative_residual_transpose": max(rest)} if args.transpose else {}
     print(json.dumps({
         "n": int(n), "nnz": int(ci.size), "batch": B, "precision": args.precision, "fronts": int(fsz.size),
         "max_front": int(fsz.max()), "factor_level_tiers": ls.plan_array("factor_level_tiers").tolist(),
         "tc_threshold": int(ls.plan_array("tc_threshold")[0]),
         "factorize_ms": round(statistics.median(tf), 4), "solve_ms": round(statistics.median(ts), 4),
-        "max_relative_residual": max(res), "singular": int(ls.singular_flags().sum())}))
+        "max_relative_residual": max(res), **extra, "singular": int(ls.singular_flags().sum())}))
     return 0
 
 

@@ -161,8 +161,9 @@ const char* cls_last_error(cls_handle h);
  * "factor_level_tiers" (per factor launch: 0 register-row kernel, 1 any-size
  * tier, 2 any-size tier with the tensor-core trailing update),
  * "factor_level_placement" (per factor launch: 1 dense fronts in shared
- * memory, 2 in the global scratch; the autotuner chooses it with the block
- * shape) and
+ * memory, 2 in the global scratch, 3 a register-tier launch of large fronts
+ * run by the any-size tier instead; the autotuner chooses it with the block
+ * shape, and a launch of the any-size tier may take 16 or 32 warps) and
  * "tc_threshold" (one value: the front size from which TF32 factors use the
  * tensor cores, 0 for other precisions).  With out == NULL only *len is set. */
 cls_status cls_plan_array(cls_handle h, const char* name, int32_t* out, int64_t capacity, int64_t* len);

@@ -211,13 +211,15 @@ def test_pivot_strategy_none_keeps_small_pivots():
     assert f1 and np.abs(x1 - exact).max() > 1e-6 * np.abs(exact).max()
 
 
-def test_autotuned_factorization_is_bit_identical():
+@pytest.mark.parametrize("case", ["case1354pegase", "case8387pegase"])
+def test_autotuned_factorization_is_bit_identical(case):
     """SolverConfig(autotune=True): the first factorization of a batch size
-    times the factor levels' block shapes on the given values and keeps the
+    times the factor levels' block shapes (and, for launches of large fronts,
+    the any-size tier with 8 to 32 warps) on the given values and keeps the
     fastest per level; the factors, and so the solutions, do not change."""
     import torch
 
-    d, A = load("case1354pegase")
+    d, A = load(case)
     rng = np.random.default_rng(3)
     B = 64
     vals = batch_values(d, B, rng)
@@ -323,7 +325,10 @@ def test_larger_reference_datasets_factor_and_solve(case, prec):
 def test_any_size_tier_gives_the_register_kernels_factors(case, precision):
     """wide_min_front = 1 runs every launch on the any-size tier: the same
     operations in the same order per element as the register kernels, so the
-    solutions are bit for bit those of the default plan."""
+    solutions are bit for bit those of the default plan.  At 33 scenarios (two
+    groups) the tier's rule gives the launches 8, 16 and 32 warps (many,
+    some and few blocks); above 8 warps the assembly ranges are split at
+    destination changes."""
     d, _ = load(case)
     out = []
     for wide in (0, 1):

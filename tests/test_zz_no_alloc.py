@@ -38,7 +38,8 @@ def test_static_scratch_factorize_matches_regular_twice_in_a_row():
     ls.factorize(torch.tensor(np.stack([d["values"]] * B), device="cuda"))  # workspace for this batch size
     # the case exercises the static area: some launches keep their fronts in
     # the global scratch under the built-in placement the entry point uses
-    assert 2 in ls.plan_array("factor_level_placement")
+    # (2: register rows over the scratch, 3: the any-size tier)
+    assert set(ls.plan_array("factor_level_placement").tolist()) & {2, 3}
     for call in range(2):
         vals = np.stack([d["values"]] * B) * (1.0 + 0.01 * rng.uniform(-1, 1, (B, d["values"].size)))
         tv = torch.tensor(vals, device="cuda")
