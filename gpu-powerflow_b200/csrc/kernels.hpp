@@ -154,7 +154,7 @@ constexpr int kTcSmallestMinFront = 33;  // the smallest threshold the autotuner
 // tier instead (placement 3, an autotuner choice): a few large fronts per
 // launch go faster with up to 32 warps over their columns and rows than with
 // at most 8 warps of register rows.
-constexpr int kWideOptionRows = 33;
+constexpr int kWideOptionRows = 17;
 
 
 // Shared-memory plan of a wide-tier launch: pivot reciprocals, the staged
