@@ -1073,13 +1073,12 @@ __global__ void __launch_bounds__(256)
 // STAGED = false (fronts whose U rows do not fit in shared memory): the same
 // substitution reading U and x straight from global memory.
 template <typename T, bool STAGED = true>
-__device__ __forceinline__ void backward_front(const DevPlan& pl, int q, size_t col0, int Bp, T* Us,
+__device__ __forceinline__ void backward_front(const DevPlan& pl, const FrontMeta& m, size_t col0, int Bp, T* Us,
                                                const T* __restrict__ U, const T* __restrict__ Y,
                                                T* __restrict__ X) {
   constexpr int kPieces = kWarp * sizeof(T) / 16;
   const int lane = threadIdx.x & 31;
   const size_t b = col0 + lane;
-  const FrontMeta m = load_front_meta(pl.front_meta, q);
   const int fs = m.fs, nc = m.nc, uc = fs - nc;
   const int fr0 = m.fr0, first = m.first;
   const long long uo = m.uo;
@@ -1140,9 +1139,10 @@ __global__ void __launch_bounds__(256)
   const int q = level_begin + (int)(item / groups);
   const size_t col0 = (size_t)(item % groups) * kWarp;
   chain_allow_next();
+  const FrontMeta m = load_front_meta(pl.front_meta, q);  // (plan data: before the wait)
   chain_wait_previous();  // U, Y and the x of ancestors come from earlier kernels
   T* Us = reinterpret_cast<T*>(smem_raw) + (size_t)warp * warp_elems * kWarp;  // [nc * fs][32]
-  backward_front<T, STAGED>(pl, q, col0, Bp, Us, U, Y, X);
+  backward_front<T, STAGED>(pl, m, col0, Bp, Us, U, Y, X);
 }
 
 // The narrow top of the tree in one launch: block = one group of 32
@@ -1163,7 +1163,8 @@ __global__ void __launch_bounds__(256)
   T* Us = reinterpret_cast<T*>(smem_raw) + (size_t)warp * warp_elems * kWarp;
   for (int t = 0; t < nlev; ++t) {
     const int hi = lv_bounds[t], lo = lv_bounds[t + 1];
-    for (int q = lo + warp; q < hi; q += W) backward_front<T, STAGED>(pl, q, col0, Bp, Us, U, Y, X);
+    for (int q = lo + warp; q < hi; q += W)
+      backward_front<T, STAGED>(pl, load_front_meta(pl.front_meta, q), col0, Bp, Us, U, Y, X);
     __syncthreads();
   }
 }
