@@ -284,15 +284,7 @@ __device__ __forceinline__ FrontMeta stage_and_assemble(const DevPlan& pl, int l
     const int cs = c * sm.chunk, ce = min(nsrc, cs + sm.chunk);
     const T* buf = reinterpret_cast<const T*>(stage + (size_t)(c % sm.nbuf) * sm.chunk * kRowBytes) + lane;
     const int a = max(cs, A), z = min(ce, Z);
-    for (int e = a; e < z; e += 8) {
-      T v[8];
-      int d[8];
-#pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        const bool in = e + u < z;
-        d[u] = in ? s_dst[e + u] : -1;
-        v[u] = in ? buf[(e + u - cs) * kWarp] : T(0);
-      }
+    auto add8 = [&](const int (&d)[8], const T (&v)[8]) {
 #pragma unroll
       for (int u = 0; u < 8; ++u) {
         if (d[u] >= 0) {
@@ -303,6 +295,38 @@ __device__ __forceinline__ FrontMeta stage_and_assemble(const DevPlan& pl, int l
           }
           acc += v[u];
         }
+      }
+    };
+    if constexpr (STAGE_LIST) {
+      for (int e = a; e < z; e += 8) {
+        T v[8];
+        int d[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          const bool in = e + u < z;
+          d[u] = in ? s_dst[e + u] : -1;
+          v[u] = in ? buf[(e + u - cs) * kWarp] : T(0);
+        }
+        add8(d, v);
+      }
+    } else {
+      // the list is in global memory: the lanes fetch 32 destinations in one
+      // request (the next 32 already in flight) and pass them round by shuffle
+      int dl = a + lane < z ? s_dst[a + lane] : -1;
+      for (int e0 = a; e0 < z; e0 += kWarp) {
+        const int n = min(kWarp, z - e0);
+        const int dl_next = e0 + kWarp + lane < z ? s_dst[e0 + kWarp + lane] : -1;
+        for (int u0 = 0; u0 < n; u0 += 8) {  // u0 + u <= 31
+          T v[8];
+          int d[8];
+#pragma unroll
+          for (int u = 0; u < 8; ++u) {
+            d[u] = __shfl_sync(0xffffffffu, dl, u0 + u);
+            v[u] = d[u] >= 0 ? buf[(e0 + u0 + u - cs) * kWarp] : T(0);
+          }
+          add8(d, v);
+        }
+        dl = dl_next;
       }
     }
     __syncthreads();
