@@ -379,11 +379,7 @@ pf_status pf_create(const pf_options* options, pf_handle* out) {
       throw std::invalid_argument("NewtonSolver: this engine provides the CUDA backend only");
     if (o.cuda_linear_solver != PF_CUDA_SOLVER_CUSTOM)
       throw std::invalid_argument("NewtonSolver: this engine provides the custom CUDA linear solver only");
-    if (o.compute == PF_COMPUTE_FP32)
-      throw std::invalid_argument(
-          "NewtonSolver: ComputePolicy::FP32 (FP32 state, mismatch and voltage update) is not provided by this "
-          "engine; ComputePolicy::Mixed keeps the state and mismatch in FP64 with FP32 Jacobian and factors");
-    if (o.compute != PF_COMPUTE_FP64 && o.compute != PF_COMPUTE_MIXED)
+    if (o.compute != PF_COMPUTE_FP64 && o.compute != PF_COMPUTE_FP32 && o.compute != PF_COMPUTE_MIXED)
       throw std::invalid_argument("NewtonSolver: unsupported compute policy");
     if (o.custom.matching != 0 && o.custom.matching != 1)
       throw std::invalid_argument("NewtonSolver: matching must be None or Structural");
@@ -401,6 +397,8 @@ pf_status pf_create(const pf_options* options, pf_handle* out) {
       throw std::invalid_argument("NewtonSolver: cuda_jacobian must be Edge, EdgeAtomic or VertexWarp");
     cls_config c = o.custom;
     if (o.compute == PF_COMPUTE_FP64) c.precision = CLS_PRECISION_FP64;
+    // FP32 state factors in FP32 (or TF32), never FP64 (cuda_custom_solver.cpp:71-72)
+    if (o.compute == PF_COMPUTE_FP32 && c.precision == CLS_PRECISION_FP64) c.precision = CLS_PRECISION_FP32;
     EngineConfig ec = engine_config(c, o.compute, o.use_cuda_graph);
     ec.jacobian_kind = o.cuda_jacobian;
     h->eng.reset(new Engine(ec));

@@ -110,9 +110,13 @@ struct DevGrid {
   const int* jt_q = nullptr;
 };
 
-// Per-batch state (all [rows][Bp]).
+// Per-batch state (all [rows][Bp]).  The voltage, injection, current and
+// mismatch arrays are typed double below; under ComputePolicy::FP32
+// (state_f32 = 1) the same buffers hold float, and the stage kernels read
+// them through StateArrays<float>.
 struct DevState {
   int B = 0, Bp = 0;
+  int state_f32 = 0;
   double* v_re = nullptr;
   double* v_im = nullptr;
   double* va = nullptr;

@@ -114,6 +114,7 @@ struct Engine::Impl {
   // workspace
   int Bp_cap = 0, B = 0, Bp = 0;
   DBuf v_re, v_im, va, vm, s_re, s_im, i_re, i_im, F, Fp, norm, sing;
+  bool state_f32 = false;  // ComputePolicy::FP32: the arrays above up to F hold float (reserved at 8 bytes)
   bool fp_double = false;
   DBuf J, U, L, CB, Y, X, front_scratch;
   size_t front_scratch_elems = 0;
@@ -172,6 +173,7 @@ struct Engine::Impl {
     DevState st;
     st.B = B;
     st.Bp = Bp;
+    st.state_f32 = state_f32 ? 1 : 0;
     st.v_re = v_re.as<double>();
     st.v_im = v_im.as<double>();
     st.va = va.as<double>();
@@ -194,12 +196,16 @@ struct Engine::Impl {
 Engine::Engine(const EngineConfig& cfg) : d_(new Impl()), cfg_(cfg) {
   if (cfg_.max_panel_width < 1 || cfg_.max_panel_width > 8)
     throw std::invalid_argument("max_panel_width must be in [1, 8] for this engine");
+  d_->state_f32 = cfg_.compute == kComputeFP32;
 }
 
 Engine::~Engine() = default;
 
+// FP32 state cannot carry FP64 factors: under ComputePolicy::FP32 an FP64
+// factor precision falls back to FP32, as the reference's custom solver does
+// (cuda_custom_solver.cpp:71-72); TF32 stays available.
 bool Engine::factor_is_double() const {
-  return cfg_.compute == kComputeFP64 || cfg_.factor_precision == kFactorFP64;
+  return cfg_.compute == kComputeFP64 || (cfg_.compute != kComputeFP32 && cfg_.factor_precision == kFactorFP64);
 }
 
 bool Engine::tf32_factors() const { return cfg_.factor_precision == kFactorTF32 && !factor_is_double(); }
@@ -1411,6 +1417,10 @@ void Engine::transpose_solve(const double* d_G, double* d_lam, cudaStream_t s) {
 double Engine::solve_adjoint_device(const void* grad_va, const void* grad_vm, void* grad_p, void* grad_q,
                                     double* d_lambda, int32_t B, int32_t is_double, cudaStream_t stream,
                                     bool residual) {
+  if (d_->state_f32)
+    throw std::runtime_error(
+        "NewtonSolver::solve_adjoint(): the adjoint's FP64 residual refinement needs the FP64 state of "
+        "ComputePolicy::FP64 or Mixed; ComputePolicy::FP32 keeps the state in FP32");
   if (!adjoint_ready_)
     throw std::runtime_error("NewtonSolver::solve_adjoint(): missing exact final-state adjoint cache");
   if (B != B_) throw std::invalid_argument("NewtonSolver::solve_adjoint(): batch_size does not match the last forward solve");
@@ -1649,7 +1659,10 @@ void Engine::evaluate_host(const double* V, const double* sbus, int32_t B, doubl
   d.Jd.reserve((size_t)ja_.nnz * d.Bp * 8);
   launch_jacobian<double>(d.g, st, d.Jd.as<double>(), s);
   d.G.reserve(std::max<size_t>(dim, (size_t)ja_.nnz) * B * 8);
-  launch_rows_to_batch<double, double>(d.F.as<double>(), d.G.as<double>(), (int)dim, B, d.Bp, s);
+  if (d.state_f32)
+    launch_rows_to_batch<float, double>(d.F.as<float>(), d.G.as<double>(), (int)dim, B, d.Bp, s);
+  else
+    launch_rows_to_batch<double, double>(d.F.as<double>(), d.G.as<double>(), (int)dim, B, d.Bp, s);
   CUPF_CUDA(cudaMemcpyAsync(F_out, d.G.p, dim * B * 8, cudaMemcpyDeviceToHost, s));
   CUPF_CUDA(cudaStreamSynchronize(s));
   launch_rows_to_batch<double, double>(d.Jd.as<double>(), d.G.as<double>(), ja_.nnz, B, d.Bp, s);

@@ -22,17 +22,38 @@ __device__ __forceinline__ double dmax_nan(double m, double a, bool& bad) {
   return a > m ? a : m;
 }
 
+// The state arrays of a DevState in their element type S: double under the
+// FP64 and Mixed compute policies, float under ComputePolicy::FP32 (the
+// reference's CudaFp32Storage: V, Sbus, Ibus and F all single precision,
+// newton_solver_types.hpp:67-80).
+template <typename S>
+struct StateArrays {
+  S *v_re, *v_im, *va, *vm, *s_re, *s_im, *i_re, *i_im, *F;
+  __device__ __forceinline__ explicit StateArrays(const DevState& st)
+      : v_re(reinterpret_cast<S*>(st.v_re)), v_im(reinterpret_cast<S*>(st.v_im)), va(reinterpret_cast<S*>(st.va)),
+        vm(reinterpret_cast<S*>(st.vm)), s_re(reinterpret_cast<S*>(st.s_re)), s_im(reinterpret_cast<S*>(st.s_im)),
+        i_re(reinterpret_cast<S*>(st.i_re)), i_im(reinterpret_cast<S*>(st.i_im)), F(reinterpret_cast<S*>(st.F)) {}
+};
+
+__device__ __forceinline__ void sin_cos(double a, double* s, double* c) { sincos(a, s, c); }
+__device__ __forceinline__ void sin_cos(float a, float* s, float* c) { sincosf(a, s, c); }
+
 // ---------------------------------------------------------------------------
 // Ibus = Ybus V, F = [Re mis@pv, Re mis@pq, Im mis@pq] with mis = V conj(I) - S,
 // and per-scenario ||F||_inf (cuPF compute_ibus.cu:58-95,
 // compute_mismatch_from_ibus.cu:32-85, reduce_mismatch_norm.cu:49-119 fused).
 // The norm is an atomicMax on the IEEE bits of |F| (order preserving for
-// non-negative doubles); a non-finite entry forces NaN bits.
+// non-negative doubles); a non-finite entry forces NaN bits.  S is the
+// state's type: under ComputePolicy::FP32 the Ybus values are rounded to
+// float and Ibus and F are computed in float (compute_ibus.cu with
+// CudaFp32Storage); the norm of the float entries is exact in double.
 // ---------------------------------------------------------------------------
+template <typename S>
 __global__ void k_ibus_mismatch(DevGrid g, DevState st) {
   const int lane = threadIdx.x, wy = threadIdx.y;
   const int Bp = st.Bp;
   const size_t b = (size_t)blockIdx.y * kWarp + lane;
+  const StateArrays<S> v(st);
   double nmax = 0.0;
   bool bad = false;
   // Ybus value of entry k: shared y[k], or this scenario's yb[k * Bp + b]
@@ -40,28 +61,28 @@ __global__ void k_ibus_mismatch(DevGrid g, DevState st) {
   const double* yim = st.yb_re ? st.yb_im + b : g.y_im;
   const size_t ys = st.yb_re ? (size_t)Bp : 1;
   for (int i = blockIdx.x * kRows + wy; i < g.n_bus; i += gridDim.x * kRows) {
-    double ir = 0.0, ii = 0.0;
+    S ir = S(0), ii = S(0);
     for (int k = g.y_ptr[i]; k < g.y_ptr[i + 1]; ++k) {
       const size_t c = (size_t)g.y_col[k] * Bp + b;
-      const double yr = yre[k * ys], yi = yim[k * ys];
-      const double vr = st.v_re[c], vi = st.v_im[c];
+      const S yr = static_cast<S>(yre[k * ys]), yi = static_cast<S>(yim[k * ys]);
+      const S vr = v.v_re[c], vi = v.v_im[c];
       ir += yr * vr - yi * vi;
       ii += yr * vi + yi * vr;
     }
     const size_t o = (size_t)i * Bp + b;
-    st.i_re[o] = ir;
-    st.i_im[o] = ii;
-    const double vr = st.v_re[o], vi = st.v_im[o];
-    const double mr = (vr * ir + vi * ii) - st.s_re[o];
-    const double mi = (vi * ir - vr * ii) - st.s_im[o];
+    v.i_re[o] = ir;
+    v.i_im[o] = ii;
+    const S vr = v.v_re[o], vi = v.v_im[o];
+    const S mr = (vr * ir + vi * ii) - v.s_re[o];
+    const S mi = (vi * ir - vr * ii) - v.s_im[o];
     const int fa = g.bus_fa[i], fm = g.bus_fm[i];
     if (fa >= 0) {
-      st.F[(size_t)fa * Bp + b] = mr;
-      nmax = dmax_nan(nmax, fabs(mr), bad);
+      v.F[(size_t)fa * Bp + b] = mr;
+      nmax = dmax_nan(nmax, fabs(static_cast<double>(mr)), bad);
     }
     if (fm >= 0) {
-      st.F[(size_t)fm * Bp + b] = mi;
-      nmax = dmax_nan(nmax, fabs(mi), bad);
+      v.F[(size_t)fm * Bp + b] = mi;
+      nmax = dmax_nan(nmax, fabs(static_cast<double>(mi)), bad);
     }
     if (st.Fp) {
       const int pa = g.bus_fa_p[i], pm = g.bus_fm_p[i];
@@ -101,15 +122,16 @@ __global__ void k_ibus_mismatch(DevGrid g, DevState st) {
 // diagonal terms are added by the thread of the Ybus diagonal entry, so every
 // slot is written exactly once (no memset, no atomics).
 // ---------------------------------------------------------------------------
-template <typename TJ>
+template <typename S, typename TJ>
 __global__ void k_jacobian(DevGrid g, DevState st, TJ* __restrict__ J) {
   // arithmetic in the Jacobian's own type, as the reference's fill does
-  // (fill_jacobian_edge_kernel.hpp:58-60: AccumScalar = JScalar); the FP64
-  // state is read and rounded once
+  // (fill_jacobian_edge_kernel.hpp:58-60: AccumScalar = JScalar); the state
+  // is read and rounded once
   using A = TJ;
   const int lane = threadIdx.x, wy = threadIdx.y;
   const int Bp = st.Bp;
   const size_t b = (size_t)blockIdx.y * kWarp + lane;
+  const StateArrays<S> v(st);
   const double* yre = st.yb_re ? st.yb_re + b : g.y_re;
   const double* yim = st.yb_re ? st.yb_im + b : g.y_im;
   const size_t ys = st.yb_re ? (size_t)Bp : 1;
@@ -117,22 +139,22 @@ __global__ void k_jacobian(DevGrid g, DevState st, TJ* __restrict__ J) {
     const int i = g.y_row[k], c = g.y_col[k];
     const A yr = static_cast<A>(yre[k * ys]), yi = static_cast<A>(yim[k * ys]);
     const size_t oi = (size_t)i * Bp + b, oc = (size_t)c * Bp + b;
-    const A vir = static_cast<A>(st.v_re[oi]), vii = static_cast<A>(st.v_im[oi]);
-    const A vcr = static_cast<A>(st.v_re[oc]), vci = static_cast<A>(st.v_im[oc]);
+    const A vir = static_cast<A>(v.v_re[oi]), vii = static_cast<A>(v.v_im[oi]);
+    const A vcr = static_cast<A>(v.v_re[oc]), vci = static_cast<A>(v.v_im[oc]);
     const A yvr = yr * vcr - yi * vci, yvi = yr * vci + yi * vcr;  // y V_c
     // -j V_i conj(y V_c)
     A var = vii * yvr - vir * yvi;
     A vai = -(vii * yvi + vir * yvr);
     // V_i conj(y V_c / |V_c|), with |V_c| the stored magnitude Vm_c (V is
     // built as Vm e^{j Va}, so they agree to rounding); one reciprocal
-    A mc = static_cast<A>(st.vm[oc]);
+    A mc = static_cast<A>(v.vm[oc]);
     mc = mc < A(1e-8) ? A(1e-8) : mc;
     const A inv = A(1) / mc;
     const A ynr = yvr * inv, yni = yvi * inv;
     A vmr = vir * ynr + vii * yni;
     A vmi = vii * ynr - vir * yni;
     if (i == c) {
-      const A ir = static_cast<A>(st.i_re[oi]), ii = static_cast<A>(st.i_im[oi]);
+      const A ir = static_cast<A>(v.i_re[oi]), ii = static_cast<A>(v.i_im[oi]);
       // j V conj(I)
       var += -(vii * ir - vir * ii);
       vai += vir * ir + vii * ii;
@@ -183,23 +205,24 @@ __device__ __forceinline__ EdgeTerms edge_terms(double yr, double yi, double vir
 // Vertex fill: a warp takes one bus row for 32 scenarios and walks its Ybus
 // entries, storing the off-diagonal slots and summing the diagonal in
 // registers (each lane owns its scenario, so no reduction is needed).
-template <typename TJ>
+template <typename S, typename TJ>
 __global__ void k_jacobian_vertex(DevGrid g, DevState st, TJ* __restrict__ J) {
   const int lane = threadIdx.x, wy = threadIdx.y;
   const int Bp = st.Bp;
   const size_t b = (size_t)blockIdx.y * kWarp + lane;
+  const StateArrays<S> v(st);
   const double* yre = st.yb_re ? st.yb_re + b : g.y_re;
   const double* yim = st.yb_re ? st.yb_im + b : g.y_im;
   const size_t ys = st.yb_re ? (size_t)Bp : 1;
   for (int i = blockIdx.x * kRows + wy; i < g.n_bus; i += gridDim.x * kRows) {
     const size_t oi = (size_t)i * Bp + b;
-    const double vir = st.v_re[oi], vii = st.v_im[oi];
+    const double vir = v.v_re[oi], vii = v.v_im[oi];
     double d11 = 0.0, d21 = 0.0, d12 = 0.0, d22 = 0.0;
     int kd = -1;
     for (int k = g.y_ptr[i]; k < g.y_ptr[i + 1]; ++k) {
       const int c = g.y_col[k];
       const size_t oc = (size_t)c * Bp + b;
-      const EdgeTerms t = edge_terms(yre[k * ys], yim[k * ys], vir, vii, st.v_re[oc], st.v_im[oc]);
+      const EdgeTerms t = edge_terms(yre[k * ys], yim[k * ys], vir, vii, v.v_re[oc], v.v_im[oc]);
       d12 += t.dmr;
       d22 += t.dmi;
       if (c == i) {
@@ -246,18 +269,19 @@ __global__ void k_jacobian_zero_diag(DevGrid g, DevState st, TJ* __restrict__ J)
       }
 }
 
-template <typename TJ>
+template <typename S, typename TJ>
 __global__ void k_jacobian_edge_atomic(DevGrid g, DevState st, TJ* __restrict__ J) {
   const int lane = threadIdx.x, wy = threadIdx.y;
   const int Bp = st.Bp;
   const size_t b = (size_t)blockIdx.y * kWarp + lane;
+  const StateArrays<S> v(st);
   const double* yre = st.yb_re ? st.yb_re + b : g.y_re;
   const double* yim = st.yb_re ? st.yb_im + b : g.y_im;
   const size_t ys = st.yb_re ? (size_t)Bp : 1;
   for (int k = blockIdx.x * kRows + wy; k < g.nnz_y; k += gridDim.x * kRows) {
     const int i = g.y_row[k], c = g.y_col[k];
     const size_t oi = (size_t)i * Bp + b, oc = (size_t)c * Bp + b;
-    const EdgeTerms t = edge_terms(yre[k * ys], yim[k * ys], st.v_re[oi], st.v_im[oi], st.v_re[oc], st.v_im[oc]);
+    const EdgeTerms t = edge_terms(yre[k * ys], yim[k * ys], v.v_re[oi], v.v_im[oi], v.v_re[oc], v.v_im[oc]);
     const int kd = g.y_diag[i];
     if (kd < 0) continue;
     const int q11 = g.map11[kd], q21 = g.map21[kd], q12 = g.map12[kd], q22 = g.map22[kd];
@@ -285,23 +309,24 @@ __global__ void k_jacobian_edge_atomic(DevGrid g, DevState st, TJ* __restrict__ 
 // solution X (x_perm[iperm[row]]).  The bus-0 thread clears the scenario's
 // norm for the next mismatch evaluation.
 // ---------------------------------------------------------------------------
-template <typename T>
+template <typename S, typename T>
 __global__ void k_voltage_update(DevGrid g, DevPlan pl, DevState st, const T* __restrict__ X) {
   const int lane = threadIdx.x, wy = threadIdx.y;
   const int Bp = st.Bp;
   const size_t b = (size_t)blockIdx.y * kWarp + lane;
+  const StateArrays<S> v(st);
   for (int i = blockIdx.x * kRows + wy; i < g.n_bus; i += gridDim.x * kRows) {
     const size_t o = (size_t)i * Bp + b;
-    double va = st.va[o], vm = st.vm[o];
+    S va = v.va[o], vm = v.vm[o];
     const int fa = g.bus_fa[i], fm = g.bus_fm[i];
-    if (fa >= 0) va -= static_cast<double>(X[(size_t)pl.iperm[fa] * Bp + b]);
-    if (fm >= 0) vm -= static_cast<double>(X[(size_t)pl.iperm[fm] * Bp + b]);
-    double s, c;
-    sincos(va, &s, &c);
-    st.va[o] = va;
-    st.vm[o] = vm;
-    st.v_re[o] = vm * c;
-    st.v_im[o] = vm * s;
+    if (fa >= 0) va -= static_cast<S>(X[(size_t)pl.iperm[fa] * Bp + b]);
+    if (fm >= 0) vm -= static_cast<S>(X[(size_t)pl.iperm[fm] * Bp + b]);
+    S s, c;
+    sin_cos(va, &s, &c);
+    v.va[o] = va;
+    v.vm[o] = vm;
+    v.v_re[o] = vm * c;
+    v.v_im[o] = vm * s;
     if (i == 0) st.norm_bits[b] = 0ull;
   }
 }
@@ -320,10 +345,12 @@ __global__ void k_voltage_update(DevGrid g, DevPlan pl, DevState st, const T* __
 // The inputs are read along the buses (a warp reads 32 buses of one
 // scenario, so the prediction's rows arrive in runs of consecutive columns)
 // and transposed through shared memory to the bus-major state.
+template <typename S>
 __global__ void k_seed_warm(DevGrid g, DevState st, const double* __restrict__ sbus_c, long long sbus_stride,
                             const double* __restrict__ v0_c, long long v0_stride, const float* __restrict__ pred,
                             long long ld, const float* __restrict__ scale, const float* __restrict__ shift) {
   __shared__ double t[4][kWarp][kWarp + 1];  // s_re, s_im, va, vm
+  const StateArrays<S> v(st);
   const int tx = threadIdx.x, ty = threadIdx.y;  // (32, 8)
   const int bus0 = blockIdx.x * kWarp, b0 = blockIdx.y * kWarp;
   const int bus = bus0 + tx;
@@ -355,28 +382,30 @@ __global__ void k_seed_warm(DevGrid g, DevState st, const double* __restrict__ s
     if (i >= g.n_bus) continue;
     const bool predicted = g.bus_fa[i] >= 0 || g.bus_fm[i] >= 0;
     const size_t o = (size_t)i * st.Bp + b0 + tx;
-    const double va = t[2][tx][r], vm = t[3][tx][r];
-    st.s_re[o] = t[0][tx][r];
-    st.s_im[o] = t[1][tx][r];
-    st.va[o] = va;
-    st.vm[o] = vm;
+    const S va = static_cast<S>(t[2][tx][r]), vm = static_cast<S>(t[3][tx][r]);
+    v.s_re[o] = static_cast<S>(t[0][tx][r]);
+    v.s_im[o] = static_cast<S>(t[1][tx][r]);
+    v.va[o] = va;
+    v.vm[o] = vm;
     if (predicted) {
-      double sn, cs;
-      sincos(va, &sn, &cs);
-      st.v_re[o] = vm * cs;
-      st.v_im[o] = vm * sn;
+      S sn, cs;
+      sin_cos(va, &sn, &cs);
+      v.v_re[o] = vm * cs;
+      v.v_im[o] = vm * sn;
     } else {  // a slack bus (no Jacobian row; few per grid): V0 read again
       const size_t vo = ((size_t)min(b0 + tx, st.B - 1) * v0_stride + i) * 2;
-      st.v_re[o] = v0_c[vo];
-      st.v_im[o] = v0_c[vo + 1];
+      v.v_re[o] = static_cast<S>(v0_c[vo]);
+      v.v_im[o] = static_cast<S>(v0_c[vo + 1]);
     }
   }
 }
 
 // ---------------------------------------------------------------------------
+template <typename S>
 __global__ void k_seed_state(DevGrid g, DevState st, const double* __restrict__ sbus_c, long long sbus_stride,
                              const double* __restrict__ v0_c, long long v0_stride) {
   __shared__ double t[4][kWarp][kWarp + 1];
+  const StateArrays<S> v(st);
   const int tx = threadIdx.x, ty = threadIdx.y;  // (32, 8)
   const int bus0 = blockIdx.x * kWarp, b0 = blockIdx.y * kWarp;
   for (int r = ty; r < kWarp; r += kRows) {
@@ -396,25 +425,27 @@ __global__ void k_seed_state(DevGrid g, DevState st, const double* __restrict__ 
     if (bus >= g.n_bus) continue;
     const size_t o = (size_t)bus * st.Bp + b0 + tx;
     const double vr = t[2][tx][r], vi = t[3][tx][r];
-    st.s_re[o] = t[0][tx][r];
-    st.s_im[o] = t[1][tx][r];
-    st.v_re[o] = vr;
-    st.v_im[o] = vi;
-    st.va[o] = atan2(vi, vr);
-    st.vm[o] = hypot(vr, vi);
+    v.s_re[o] = static_cast<S>(t[0][tx][r]);
+    v.s_im[o] = static_cast<S>(t[1][tx][r]);
+    v.v_re[o] = static_cast<S>(vr);
+    v.v_im[o] = static_cast<S>(vi);
+    v.va[o] = static_cast<S>(atan2(vi, vr));
+    v.vm[o] = static_cast<S>(hypot(vr, vi));
   }
 }
 
+template <typename S>
 __global__ void k_pack_voltage(DevGrid g, DevState st, double* __restrict__ v_c) {
   __shared__ double t[2][kWarp][kWarp + 1];
+  const StateArrays<S> v(st);
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int bus0 = blockIdx.x * kWarp, b0 = blockIdx.y * kWarp;
   for (int r = ty; r < kWarp; r += kRows) {
     const int bus = bus0 + r;
     if (bus < g.n_bus) {
       const size_t o = (size_t)bus * st.Bp + b0 + tx;
-      t[0][r][tx] = st.v_re[o];
-      t[1][r][tx] = st.v_im[o];
+      t[0][r][tx] = static_cast<double>(v.v_re[o]);
+      t[1][r][tx] = static_cast<double>(v.v_im[o]);
     }
   }
   __syncthreads();
@@ -435,10 +466,11 @@ __device__ __forceinline__ double ld_in(const void* p, size_t i) {
 
 // Sbus = base - load, V0 from (va0, vm0); torch_bridge_kernels.cu:116-152.
 // batched_v0 = 1: va0/vm0 are [B][n] (warm starts), else [n] shared.
-template <typename TI>
+template <typename TI, typename S>
 __global__ void k_set_inputs(DevGrid g, DevState st, const void* base_re, const void* base_im, const void* load_p,
                              const void* load_q, const void* va0, const void* vm0, int batched_v0) {
   __shared__ double t[4][kWarp][kWarp + 1];
+  const StateArrays<S> v(st);
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int bus0 = blockIdx.x * kWarp, b0 = blockIdx.y * kWarp;
   const int bus = bus0 + tx;
@@ -457,30 +489,31 @@ __global__ void k_set_inputs(DevGrid g, DevState st, const void* base_re, const 
     const int bs = bus0 + r;
     if (bs >= g.n_bus) continue;
     const size_t o = (size_t)bs * st.Bp + b0 + tx;
-    const double a = batched_v0 ? t[2][tx][r] : ld_in<TI>(va0, bs);
-    const double m = batched_v0 ? t[3][tx][r] : ld_in<TI>(vm0, bs);
-    st.s_re[o] = ld_in<TI>(base_re, bs) - t[0][tx][r];
-    st.s_im[o] = ld_in<TI>(base_im, bs) - t[1][tx][r];
-    double s, c;
-    sincos(a, &s, &c);
-    st.va[o] = a;
-    st.vm[o] = m;
-    st.v_re[o] = m * c;
-    st.v_im[o] = m * s;
+    const S a = static_cast<S>(batched_v0 ? t[2][tx][r] : ld_in<TI>(va0, bs));
+    const S m = static_cast<S>(batched_v0 ? t[3][tx][r] : ld_in<TI>(vm0, bs));
+    v.s_re[o] = static_cast<S>(ld_in<TI>(base_re, bs) - t[0][tx][r]);
+    v.s_im[o] = static_cast<S>(ld_in<TI>(base_im, bs) - t[1][tx][r]);
+    S s, c;
+    sin_cos(a, &s, &c);
+    v.va[o] = a;
+    v.vm[o] = m;
+    v.v_re[o] = m * c;
+    v.v_im[o] = m * s;
   }
 }
 
-template <typename TO>
+template <typename TO, typename S>
 __global__ void k_copy_voltage_outputs(DevGrid g, DevState st, TO* __restrict__ va_out, TO* __restrict__ vm_out) {
   __shared__ double t[2][kWarp][kWarp + 1];
+  const StateArrays<S> v(st);
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int bus0 = blockIdx.x * kWarp, b0 = blockIdx.y * kWarp;
   for (int r = ty; r < kWarp; r += kRows) {
     const int bus = bus0 + r;
     if (bus < g.n_bus) {
       const size_t o = (size_t)bus * st.Bp + b0 + tx;
-      t[0][r][tx] = st.va[o];
-      t[1][r][tx] = st.vm[o];
+      t[0][r][tx] = static_cast<double>(v.va[o]);
+      t[1][r][tx] = static_cast<double>(v.vm[o]);
     }
   }
   __syncthreads();
@@ -723,28 +756,42 @@ dim3 rows_grid(int rows, int Bp) {
 }  // namespace
 
 void launch_ibus_mismatch(const DevGrid& g, const DevState& st, cudaStream_t s) {
-  k_ibus_mismatch<<<rows_grid(g.n_bus, st.Bp), dim3(kWarp, kRows), 0, s>>>(g, st);
+  if (st.state_f32)
+    k_ibus_mismatch<float><<<rows_grid(g.n_bus, st.Bp), dim3(kWarp, kRows), 0, s>>>(g, st);
+  else
+    k_ibus_mismatch<double><<<rows_grid(g.n_bus, st.Bp), dim3(kWarp, kRows), 0, s>>>(g, st);
 }
 
-template <typename TJ>
-void launch_jacobian(const DevGrid& g, const DevState& st, TJ* J, cudaStream_t s) {
+template <typename S, typename TJ>
+void launch_jacobian_s(const DevGrid& g, const DevState& st, TJ* J, cudaStream_t s) {
   if (g.jac_kind == 2) {
-    k_jacobian_vertex<TJ><<<rows_grid(g.n_bus, st.Bp), dim3(kWarp, kRows), 0, s>>>(g, st, J);
+    k_jacobian_vertex<S, TJ><<<rows_grid(g.n_bus, st.Bp), dim3(kWarp, kRows), 0, s>>>(g, st, J);
     return;
   }
   if (g.jac_kind == 1) {
     k_jacobian_zero_diag<TJ><<<rows_grid(g.n_bus, st.Bp), dim3(kWarp, kRows), 0, s>>>(g, st, J);
-    k_jacobian_edge_atomic<TJ><<<rows_grid(g.nnz_y, st.Bp), dim3(kWarp, kRows), 0, s>>>(g, st, J);
+    k_jacobian_edge_atomic<S, TJ><<<rows_grid(g.nnz_y, st.Bp), dim3(kWarp, kRows), 0, s>>>(g, st, J);
     return;
   }
-  k_jacobian<TJ><<<rows_grid(g.nnz_y, st.Bp), dim3(kWarp, kRows), 0, s>>>(g, st, J);
+  k_jacobian<S, TJ><<<rows_grid(g.nnz_y, st.Bp), dim3(kWarp, kRows), 0, s>>>(g, st, J);
+}
+
+template <typename TJ>
+void launch_jacobian(const DevGrid& g, const DevState& st, TJ* J, cudaStream_t s) {
+  if (st.state_f32)
+    launch_jacobian_s<float, TJ>(g, st, J, s);
+  else
+    launch_jacobian_s<double, TJ>(g, st, J, s);
 }
 template void launch_jacobian<float>(const DevGrid&, const DevState&, float*, cudaStream_t);
 template void launch_jacobian<double>(const DevGrid&, const DevState&, double*, cudaStream_t);
 
 template <typename T>
 void launch_voltage_update(const DevGrid& g, const DevPlan& pl, const DevState& st, const T* X, cudaStream_t s) {
-  k_voltage_update<T><<<rows_grid(g.n_bus, st.Bp), dim3(kWarp, kRows), 0, s>>>(g, pl, st, X);
+  if (st.state_f32)
+    k_voltage_update<float, T><<<rows_grid(g.n_bus, st.Bp), dim3(kWarp, kRows), 0, s>>>(g, pl, st, X);
+  else
+    k_voltage_update<double, T><<<rows_grid(g.n_bus, st.Bp), dim3(kWarp, kRows), 0, s>>>(g, pl, st, X);
 }
 template void launch_voltage_update<float>(const DevGrid&, const DevPlan&, const DevState&, const float*,
                                            cudaStream_t);
@@ -754,50 +801,76 @@ template void launch_voltage_update<double>(const DevGrid&, const DevPlan&, cons
 void launch_seed_state(const DevGrid& g, const DevState& st, const double* sbus_c, long long sbus_stride,
                        const double* v0_c, long long v0_stride, cudaStream_t s) {
   dim3 grid((g.n_bus + kWarp - 1) / kWarp, st.Bp / kWarp);
-  k_seed_state<<<grid, dim3(kWarp, kRows), 0, s>>>(g, st, sbus_c, sbus_stride, v0_c, v0_stride);
+  if (st.state_f32)
+    k_seed_state<float><<<grid, dim3(kWarp, kRows), 0, s>>>(g, st, sbus_c, sbus_stride, v0_c, v0_stride);
+  else
+    k_seed_state<double><<<grid, dim3(kWarp, kRows), 0, s>>>(g, st, sbus_c, sbus_stride, v0_c, v0_stride);
 }
 
 void launch_seed_warm(const DevGrid& g, const DevState& st, const double* sbus_c, long long sbus_stride,
                       const double* v0_c, long long v0_stride, const float* pred, long long ld, const float* scale,
                       const float* shift, cudaStream_t s) {
   dim3 grid((g.n_bus + kWarp - 1) / kWarp, st.Bp / kWarp);
-  k_seed_warm<<<grid, dim3(kWarp, kRows), 0, s>>>(g, st, sbus_c, sbus_stride, v0_c, v0_stride, pred, ld, scale, shift);
+  if (st.state_f32)
+    k_seed_warm<float><<<grid, dim3(kWarp, kRows), 0, s>>>(g, st, sbus_c, sbus_stride, v0_c, v0_stride, pred, ld, scale,
+                                                           shift);
+  else
+    k_seed_warm<double><<<grid, dim3(kWarp, kRows), 0, s>>>(g, st, sbus_c, sbus_stride, v0_c, v0_stride, pred, ld,
+                                                            scale, shift);
 }
 
 void launch_pack_voltage(const DevGrid& g, const DevState& st, double* v_c, cudaStream_t s) {
   dim3 grid((g.n_bus + kWarp - 1) / kWarp, st.Bp / kWarp);
-  k_pack_voltage<<<grid, dim3(kWarp, kRows), 0, s>>>(g, st, v_c);
+  if (st.state_f32)
+    k_pack_voltage<float><<<grid, dim3(kWarp, kRows), 0, s>>>(g, st, v_c);
+  else
+    k_pack_voltage<double><<<grid, dim3(kWarp, kRows), 0, s>>>(g, st, v_c);
+}
+
+// (input type) x (state type) of the torch bridge's input kernel
+static void launch_set_inputs(const DevGrid& g, const DevState& st, const void* base_re, const void* base_im,
+                       const void* load_p, const void* load_q, const void* va0, const void* vm0, int is_double,
+                       int batched_v0, cudaStream_t s) {
+  dim3 grid((g.n_bus + kWarp - 1) / kWarp, st.Bp / kWarp);
+  const dim3 blk(kWarp, kRows);
+  if (is_double && !st.state_f32)
+    k_set_inputs<double, double><<<grid, blk, 0, s>>>(g, st, base_re, base_im, load_p, load_q, va0, vm0, batched_v0);
+  else if (is_double)
+    k_set_inputs<double, float><<<grid, blk, 0, s>>>(g, st, base_re, base_im, load_p, load_q, va0, vm0, batched_v0);
+  else if (!st.state_f32)
+    k_set_inputs<float, double><<<grid, blk, 0, s>>>(g, st, base_re, base_im, load_p, load_q, va0, vm0, batched_v0);
+  else
+    k_set_inputs<float, float><<<grid, blk, 0, s>>>(g, st, base_re, base_im, load_p, load_q, va0, vm0, batched_v0);
 }
 
 void launch_set_inputs_from_load(const DevGrid& g, const DevState& st, const void* base_re, const void* base_im,
                                  const void* load_p, const void* load_q, const void* va0, const void* vm0,
                                  int is_double, cudaStream_t s) {
-  dim3 grid((g.n_bus + kWarp - 1) / kWarp, st.Bp / kWarp);
-  if (is_double)
-    k_set_inputs<double><<<grid, dim3(kWarp, kRows), 0, s>>>(g, st, base_re, base_im, load_p, load_q, va0, vm0, 0);
-  else
-    k_set_inputs<float><<<grid, dim3(kWarp, kRows), 0, s>>>(g, st, base_re, base_im, load_p, load_q, va0, vm0, 0);
+  launch_set_inputs(g, st, base_re, base_im, load_p, load_q, va0, vm0, is_double, 0, s);
 }
 
 void launch_set_inputs_batched(const DevGrid& g, const DevState& st, const void* base_re, const void* base_im,
                                const void* load_p, const void* load_q, const void* va0, const void* vm0,
                                int is_double, cudaStream_t s) {
-  dim3 grid((g.n_bus + kWarp - 1) / kWarp, st.Bp / kWarp);
-  if (is_double)
-    k_set_inputs<double><<<grid, dim3(kWarp, kRows), 0, s>>>(g, st, base_re, base_im, load_p, load_q, va0, vm0, 1);
-  else
-    k_set_inputs<float><<<grid, dim3(kWarp, kRows), 0, s>>>(g, st, base_re, base_im, load_p, load_q, va0, vm0, 1);
+  launch_set_inputs(g, st, base_re, base_im, load_p, load_q, va0, vm0, is_double, 1, s);
 }
 
 void launch_copy_voltage_outputs(const DevGrid& g, const DevState& st, void* va_out, void* vm_out, int is_double,
                                  cudaStream_t s) {
   dim3 grid((g.n_bus + kWarp - 1) / kWarp, st.Bp / kWarp);
-  if (is_double)
-    k_copy_voltage_outputs<double><<<grid, dim3(kWarp, kRows), 0, s>>>(g, st, static_cast<double*>(va_out),
-                                                                       static_cast<double*>(vm_out));
+  const dim3 blk(kWarp, kRows);
+  double* dva = static_cast<double*>(va_out);
+  double* dvm = static_cast<double*>(vm_out);
+  float* fva = static_cast<float*>(va_out);
+  float* fvm = static_cast<float*>(vm_out);
+  if (is_double && !st.state_f32)
+    k_copy_voltage_outputs<double, double><<<grid, blk, 0, s>>>(g, st, dva, dvm);
+  else if (is_double)
+    k_copy_voltage_outputs<double, float><<<grid, blk, 0, s>>>(g, st, dva, dvm);
+  else if (!st.state_f32)
+    k_copy_voltage_outputs<float, double><<<grid, blk, 0, s>>>(g, st, fva, fvm);
   else
-    k_copy_voltage_outputs<float><<<grid, dim3(kWarp, kRows), 0, s>>>(g, st, static_cast<float*>(va_out),
-                                                                      static_cast<float*>(vm_out));
+    k_copy_voltage_outputs<float, float><<<grid, blk, 0, s>>>(g, st, fva, fvm);
 }
 
 void launch_gather_adjoint_rhs(const DevGrid& g, const DevState& st, const void* grad_va, const void* grad_vm,

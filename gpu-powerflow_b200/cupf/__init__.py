@@ -10,9 +10,13 @@ Differences a user can see:
   * only ``BackendKind.CUDA`` with ``CudaLinearSolverKind.Custom`` is provided
     (the CPU/KLU and cuDSS backends are other libraries); constructing a
     solver with another backend raises ``ValueError``;
-  * ``ComputePolicy.FP32`` (FP32 state, mismatch and voltage update) is not
-    built: constructing a solver with it raises ``ValueError``;
-    ``ComputePolicy.Mixed`` keeps the state in FP64 with FP32 factors;
+  * ``ComputePolicy.FP32`` keeps V, Sbus, Ibus, the mismatch and the
+    voltage update in FP32 along with the Jacobian and the factors (an FP64
+    factor precision falls back to FP32, as in the reference); its mismatch
+    floor is about 1e-5 pu on 100-2,000-bus grids, so tolerances below that
+    do not converge.  The adjoint raises under it (its FP64 residual
+    refinement needs FP64 state); ``ComputePolicy.Mixed`` keeps the state in
+    FP64 with FP32 factors;
   * ``CustomSolverConfig.max_panel_width`` is limited to 1..8;
   * ``CustomSolverConfig.autotune`` (not in the reference, on by default)
     times each factor level's block shape at the first solve of a batch size

@@ -187,6 +187,8 @@ typedef enum { PF_OK = 0, PF_INVALID_ARGUMENT = 1, PF_RUNTIME_ERROR = 2 } pf_sta
 /* BackendKind, ComputePolicy, CudaLinearSolverKind, CudaJacobianKind
  * (newton_solver_types.hpp:55-101) */
 enum { PF_BACKEND_CPU = 0, PF_BACKEND_CUDA = 1 };
+/* FP64: FP64 everywhere; FP32: FP32 state (V, Sbus, Ibus, F, update), Jacobian and factors
+ * (FP64 factor precision falls back to FP32); Mixed: FP64 state with FP32 Jacobian and factors */
 enum { PF_COMPUTE_FP64 = 0, PF_COMPUTE_FP32 = 1, PF_COMPUTE_MIXED = 2 };
 enum { PF_CUDA_SOLVER_CUDSS = 0, PF_CUDA_SOLVER_CUSTOM = 1 };
 enum { PF_JACOBIAN_EDGE = 0, PF_JACOBIAN_EDGE_ATOMIC = 1, PF_JACOBIAN_VERTEX_WARP = 2 };

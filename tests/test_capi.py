@@ -110,15 +110,18 @@ def test_unsupported_backends_raise():
         cupf.NewtonSolver(o)
 
 
-def test_fp32_compute_policy_is_rejected_not_aliased():
+def test_fp32_compute_policy_constructs():
     """ComputePolicy.FP32 (FP32 state, mismatch and voltage update; the
-    reference's CudaFp32CustomPipeline) is not built here: asking for it is an
-    error naming the option, not a silent run of the Mixed kernels."""
-    o = cupf.NewtonOptions()
-    o.backend = cupf.BackendKind.CUDA
-    o.compute = cupf.ComputePolicy.FP32
-    with pytest.raises(ValueError, match="ComputePolicy::FP32"):
-        cupf.NewtonSolver(o)
+    reference's CudaFp32CustomPipeline) is a solver of its own, with the
+    reference's float32 tensor dtype (torch_bridge.cpp:133-141), whatever
+    factor precision is asked for (FP64 factors fall back to FP32)."""
+    for prec in (cupf.CustomPrecision.FP64, cupf.CustomPrecision.FP32, cupf.CustomPrecision.TF32):
+        o = cupf.NewtonOptions()
+        o.backend = cupf.BackendKind.CUDA
+        o.compute = cupf.ComputePolicy.FP32
+        o.custom.precision = prec
+        s = cupf.NewtonSolver(o)
+        assert s.dtype_name == "float32"
 
 
 def _solver():
