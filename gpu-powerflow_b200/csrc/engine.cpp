@@ -182,7 +182,9 @@ struct Engine::Impl {
     st.s_im = s_im.as<double>();
     st.i_re = i_re.as<double>();
     st.i_im = i_im.as<double>();
-    st.F = F.as<double>();
+    // the mismatch in Jacobian-row order is written only for evaluate_host();
+    // the Newton loop reads F in pivot order (Fp) and its norm
+    st.F = nullptr;
     st.Fp = Fp.p;
     st.fp_double = fp_double ? 1 : 0;
     st.norm_bits = norm.as<unsigned long long>();
@@ -1652,7 +1654,8 @@ void Engine::evaluate_host(const double* V, const double* sbus, int32_t B, doubl
   CUPF_CUDA(cudaMemcpyAsync(ds, sbus, 2 * (size_t)B * n * sizeof(double), cudaMemcpyHostToDevice, s));
   CUPF_CUDA(cudaMemcpyAsync(dv, V, 2 * (size_t)B * n * sizeof(double), cudaMemcpyHostToDevice, s));
   use_scenario_ybus(nullptr, 0, B, s);
-  const DevState st = d.state();
+  DevState st = d.state();
+  st.F = d.F.as<double>();
   launch_seed_state(d.g, st, ds, (long long)n, dv, (long long)n, s);
   CUPF_CUDA(cudaMemsetAsync(d.norm.p, 0, d.Bp * sizeof(unsigned long long), s));
   launch_ibus_mismatch(d.g, st, s);

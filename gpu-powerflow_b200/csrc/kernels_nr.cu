@@ -47,6 +47,9 @@ __device__ __forceinline__ void sin_cos(float a, float* s, float* c) { sincosf(a
 // state's type: under ComputePolicy::FP32 the Ybus values are rounded to
 // float and Ibus and F are computed in float (compute_ibus.cu with
 // CudaFp32Storage); the norm of the float entries is exact in double.
+// F goes out in pivot order and the factor's type (Fp, the LU's right-hand
+// side); the Jacobian-row-order copy st.F is written only when it is set
+// (evaluate), since the Newton loop never reads it.
 // ---------------------------------------------------------------------------
 template <typename S>
 __global__ void k_ibus_mismatch(DevGrid g, DevState st) {
@@ -77,11 +80,11 @@ __global__ void k_ibus_mismatch(DevGrid g, DevState st) {
     const S mi = (vi * ir - vr * ii) - v.s_im[o];
     const int fa = g.bus_fa[i], fm = g.bus_fm[i];
     if (fa >= 0) {
-      v.F[(size_t)fa * Bp + b] = mr;
+      if (v.F) v.F[(size_t)fa * Bp + b] = mr;
       nmax = dmax_nan(nmax, fabs(static_cast<double>(mr)), bad);
     }
     if (fm >= 0) {
-      v.F[(size_t)fm * Bp + b] = mi;
+      if (v.F) v.F[(size_t)fm * Bp + b] = mi;
       nmax = dmax_nan(nmax, fabs(static_cast<double>(mi)), bad);
     }
     if (st.Fp) {
